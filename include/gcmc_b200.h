@@ -1,0 +1,170 @@
+/*
+ * gcmc_b200 -- C ABI of the B200 GCMC engine (fragment-environment LJ+Coulomb
+ * trial-move energies, cavity-bias insertion, on-device accept/update).
+ *
+ * The structs are byte-identical to pyGCMC's (gcmc/cpp/gcmc.h:47-100; numpy
+ * mirror gcmc/python/values.py:18-62), so the caller's numpy structured arrays
+ * are passed as plain pointers, exactly as the reference binding does
+ * (gcmc/cpp/gcmc.cpp:176-182).
+ *
+ * Every entry point except runGCMC_cuda returns a gcmc_status (0 = success).
+ * Pointers are host pointers unless stated otherwise; the library owns all
+ * device memory it allocates and frees it in gcmc_destroy / before returning.
+ */
+#ifndef GCMC_B200_H
+#define GCMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- state structs (gcmc/cpp/gcmc.h:47-100) ---------------- */
+typedef struct { float position[3]; float charge; int32_t type; } Atom;          /* 20 B  */
+typedef struct {
+    char name[4];
+    int32_t startRes;   /* first residue (slot) of this fragment type            */
+    float muex;         /* excess chemical potential (see gcmc_options.muex_kcal) */
+    float conc;         /* bulk concentration, mol/L                             */
+    int32_t confBias;   /* trial poses per insertion / max fragments per move    */
+    float mcTime;
+    int32_t totalNum;   /* occupied slots [startRes, startRes+totalNum)           */
+    int32_t maxNum;     /* slot capacity                                          */
+    int32_t num_atoms;  /* sites per fragment, <= 20                              */
+    Atom atoms[20];     /* template, centred at the origin                        */
+} AtomArray;                                                                      /* 436 B */
+typedef struct {
+    int32_t mcsteps;
+    float cutoff;        /* group-centre cutoff, A                                */
+    float grid_dx;       /* cavity grid spacing and reference translate step, A  */
+    float startxyz[3];   /* box origin                                            */
+    float cryst[3];      /* box edges (orthorhombic, periodic)                    */
+    int32_t showInfo;
+    float cavityFactor;  /* empty voxels / all voxels                             */
+    int32_t fragTypeNum;
+    int32_t totalGridNum;
+    int32_t totalResNum;
+    int32_t totalAtomNum;
+    int32_t ffXNum;      /* fragment atom types (rows of ff)                      */
+    int32_t ffYNum;      /* all atom types (columns of ff)                        */
+    int32_t PME;
+    uint32_t seed;
+} InfoStruct;                                                                     /* 76 B  */
+typedef struct { float position[3]; int32_t atomNum; int32_t atomStart; } residue; /* 20 B */
+
+/* ---------------- status codes ---------------- */
+typedef enum {
+    GCMC_OK = 0,
+    GCMC_ERR_CUDA = 1,      /* a CUDA runtime call failed                          */
+    GCMC_ERR_ARG = 2,       /* inconsistent or out-of-range input                  */
+    GCMC_ERR_LIMIT = 3,     /* a documented size limit is exceeded                 */
+    GCMC_ERR_DEVICE = 4,    /* the device raised an error flag (see gcmc_device_error) */
+    GCMC_ERR_NODEVICE = 5   /* no CUDA device is visible                           */
+} gcmc_status;
+
+/* Engine options.  gcmc_default_options() gives the reference's semantics. */
+typedef struct {
+    int32_t proposal;    /* 0: reference proposals -- insertion axis in the positive
+                            octant, translate by U(0,grid_dx] per axis (gcmc_energy.h:84,
+                            gcmc_move_trn.h:58); 1: symmetric -- uniform SO(3)
+                            insertion, translate in a cube of edge trn_step,
+                            rotate about a uniform axis by up to rot_max             */
+    int32_t muex_kcal;   /* 0: beta*muex with beta in mol/kJ and muex as given
+                            (gcmc_move_add.h:105); 1: muex in kcal/mol (x4.184)     */
+    float trn_step;      /* symmetric translate cube edge, A                        */
+    float rot_max;       /* symmetric rotate max angle, rad                         */
+    uint32_t replica;    /* RNG stream id (the key's second word)                   */
+    int32_t cells_per_cutoff; /* cell-grid resolution R (cells of >= cutoff/R); 0 = 2 */
+    int32_t log_steps;   /* record per-step logs for this many steps (0 = off)      */
+    int32_t log_kmax;    /* per-step pose energies recorded (<= 1024)               */
+} gcmc_options;
+
+/* One per-step record (48 bytes). */
+typedef struct {
+    int32_t step, move, ftype, k;
+    int32_t n_before, n_after, n_clusters, n_accept;
+    int32_t first_accept;  /* pose index of the first accepted cluster, -1 if none */
+    int32_t slot;          /* delete: chosen slot; otherwise -1                     */
+    double e_sum;          /* sum of pose E (insert/delete) or dE (translate/rotate) */
+} gcmc_step_log;
+
+typedef struct gcmc_ctx gcmc_ctx;
+
+/* One replica's input (the reference's seven arrays, gcmc/cpp/gcmc.cu:21). */
+typedef struct {
+    const InfoStruct* info;
+    const AtomArray* fragmentInfo;
+    const residue* residueInfo;
+    const Atom* atomInfo;
+    const float* grid;
+    const float* ff;
+    const int32_t* moveArray;
+} gcmc_replica_in;
+
+/* Drop-in for runGCMC_cuda (gcmc/cpp/gcmc.cu:21, declared gcmc/cpp/gcmc.cpp:159):
+ * runs info->mcsteps steps of moveArray and writes fragmentInfo[].totalNum,
+ * residueInfo[] and atomInfo[] back in place.  Same void signature; the status
+ * of the call is available from gcmc_last_status(). */
+void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo,
+                  Atom* atomInfo, const float* grid, const float* ff, const int* moveArray);
+
+/* Same as runGCMC_cuda with options, returning the status. */
+int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo,
+                  Atom* atomInfo, const float* grid, const float* ff, const int* moveArray,
+                  const gcmc_options* opt);
+
+/* Status of the last runGCMC_cuda call in this thread. */
+int gcmc_last_status(void);
+const char* gcmc_status_string(int status);
+void gcmc_default_options(gcmc_options* opt);
+
+/* ---- device-resident contexts (replaces the per-call allocation of
+ *      gcmc/cpp/gcmc.cu:31-43; one context holds nrep independent replicas) ---- */
+/* stream: a cudaStream_t to launch on (NULL = the library creates one). */
+int gcmc_create(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* opt, void* stream,
+                gcmc_ctx** out);
+/* Advance every replica by nsteps steps of its move schedule (asynchronous). */
+int gcmc_run(gcmc_ctx* ctx, int32_t nsteps);
+/* Same as gcmc_run but launches each step's two kernels individually (no
+ * graph) with CUDA events around them: per step, the pose-energy kernel time,
+ * the accept kernel time (ms) and replica 0's move code.  Synchronous. */
+int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms_accept, int32_t* move);
+/* Wait for the context's stream and report device-side errors. */
+int gcmc_sync(gcmc_ctx* ctx);
+/* Copy replica `rep`'s state back into the caller's arrays (sizes as created). */
+int gcmc_download(gcmc_ctx* ctx, int32_t rep, AtomArray* fragmentInfo, residue* residueInfo,
+                  Atom* atomInfo);
+/* Per-step logs recorded since creation (needs opt.log_steps > 0).  energies
+ * (optional) receives log_kmax doubles per step. */
+int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energies,
+                  int32_t max_steps, int32_t* n_steps);
+/* Counters: steps done, pose energies evaluated, atom-site pairs evaluated. */
+int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, int64_t* pairs);
+/* Device error word (bit 0 cell overflow, bit 1 periodic image > 1 box,
+ * bit 2 slot overflow, bit 3 pose limit). */
+int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);
+/* The cudaStream_t the context launches on. */
+void* gcmc_stream(gcmc_ctx* ctx);
+int gcmc_destroy(gcmc_ctx* ctx);
+
+/* Energies of explicit poses against replica `rep`'s current state
+ * (the calcEnergy of gcmc/cpp/gcmc_energy.h:142-204, batched).
+ * xyz[p*nsites*3], centres[p*3], self[p] (residue to skip, -1 = none);
+ * site charges/types are shared by all poses.  out[p] in kJ/mol;
+ * n_groups (optional) = groups inside the cutoff per pose. */
+int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float* site_q,
+                      const int32_t* site_type, int32_t nsites, const float* centres,
+                      const int32_t* self, int32_t nposes, double* out, int32_t* n_groups);
+
+/* ---- synthetic fixed-atom generators (host) ---- */
+int gcmc_synth_chain_sphere(int n, const float centre[3], float radius, float step, float excl,
+                            uint64_t seed, float* out_xyz, int* n_breaks);
+int gcmc_synth_chain_slab(int n, float lo0, float hi0, float lo1, float hi1, float zc, float half,
+                          float px, float py, float pore, float step, float excl, uint64_t seed,
+                          float* out_xyz, int* n_breaks);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

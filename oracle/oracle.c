@@ -1,0 +1,725 @@
+/*
+ * CPU oracle for the GCMC hot path -- TEST INFRASTRUCTURE ONLY (see oracle.h).
+ *
+ * Compiled with -ffp-contract=off so every float operation written below is
+ * rounded exactly once, as written; the places where the reference's CUDA
+ * build fuses a multiply-add are written as explicit fmaf() calls.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Physical constants of the reference (gcmc/cpp/gcmc.h:28-41). */
+#define OR_TEMPERATURE 300.0
+#define OR_BOLTZMANN 0.0083115
+#define OR_BETA (1.0 / (OR_BOLTZMANN * OR_TEMPERATURE))
+#define OR_MOLES_TO_MOLECULES 0.0006023
+#define OR_KCAL_TO_KJ 4.184
+#define OR_COULOMB 1388.431112 /* gcmc/cpp/gcmc_energy.h:137 */
+#define OR_TWO_PI_F 6.28318530717958647692f
+
+/* RNG purposes (third counter word, high half). */
+enum { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6 };
+
+/* ------------------------------------------------------------------------- */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as    */
+/* easy as 1, 2, 3", SC'11).                                                  */
+/* ------------------------------------------------------------------------- */
+void or_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static void rng(uint32_t seed, uint32_t replica, uint32_t step, uint32_t index, uint32_t purpose,
+                uint32_t draw, uint32_t out[4]) {
+    uint32_t ctr[4] = {step, index, (purpose << 16) | draw, 0u};
+    uint32_t key[2] = {seed, replica};
+    or_philox(ctr, key, out);
+}
+
+/* uniform float in (0,1] and [0,1) from the top 24 bits */
+static inline float u01_oc(uint32_t x) { return (float)((x >> 8) + 1u) * 5.9604644775390625e-08f; }
+static inline float u01_co(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
+/* uniform double in [0,1) from 53 bits of two words */
+static inline double u53(uint32_t a, uint32_t b) {
+    uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+    return (double)m * 1.1102230246251565e-16;
+}
+/* uniform double in (0,1) */
+static inline double u53_open(uint32_t a, uint32_t b) {
+    uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+    return ((double)m + 0.5) * 1.1102230246251565e-16;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Deterministic sin/cos: two-constant reduction by pi/2, then the Taylor     */
+/* polynomials of sin (to r^9) and cos (to r^10) on |r| <= pi/4.  Only         */
+/* correctly rounded operations, so CPU and GPU agree bit for bit.            */
+/* ------------------------------------------------------------------------- */
+void or_det_sincos(float x, float* s_out, float* c_out) {
+    const float two_over_pi = 0.636619772367581343f;
+    const float pio2_hi = 1.57079637050628662109375f;     /* float(pi/2)          */
+    const float pio2_lo = -4.37113900018624283e-8f;       /* pi/2 - float(pi/2)   */
+    float kf = rintf(x * two_over_pi);
+    float r = fmaf(-kf, pio2_hi, x);
+    r = fmaf(-kf, pio2_lo, r);
+    float r2 = r * r;
+    float ps = fmaf(r2, 2.75573192239858925e-6f, -1.98412698412698413e-4f);
+    ps = fmaf(r2, ps, 8.33333333333333333e-3f);
+    ps = fmaf(r2, ps, -1.66666666666666667e-1f);
+    float sr = fmaf(r * r2, ps, r);
+    float pc = fmaf(r2, -2.75573192239858925e-7f, 2.48015873015873016e-5f);
+    pc = fmaf(r2, pc, -1.38888888888888889e-3f);
+    pc = fmaf(r2, pc, 4.16666666666666667e-2f);
+    pc = fmaf(r2, pc, -0.5f);
+    float cr = fmaf(r2, pc, 1.0f);
+    int q = ((int)kf) & 3;
+    float s, c;
+    switch (q) {
+        case 0: s = sr; c = cr; break;
+        case 1: s = cr; c = -sr; break;
+        case 2: s = -sr; c = -cr; break;
+        default: s = -cr; c = sr; break;
+    }
+    *s_out = s;
+    *c_out = c;
+}
+
+/* Rodrigues matrix about axis a (normalised here) by angle with (sin, cos);
+ * formulas of gcmc/cpp/gcmc_energy.h:39-58 with the fused form fixed. */
+static void rodrigues(const float axis[3], float sn, float cs, float R[3][3]) {
+    float a0 = axis[0], a1 = axis[1], a2 = axis[2];
+    float nn = a0 * a0;
+    nn = fmaf(a1, a1, nn);
+    nn = fmaf(a2, a2, nn);
+    float norm = sqrtf(nn);
+    a0 = a0 / norm; a1 = a1 / norm; a2 = a2 / norm;
+    float C = 1.0f - cs;
+    R[0][0] = fmaf(a0 * a0, C, cs);
+    R[0][1] = fmaf(a0 * a1, C, -(a2 * sn));
+    R[0][2] = fmaf(a0 * a2, C, a1 * sn);
+    R[1][0] = fmaf(a1 * a0, C, a2 * sn);
+    R[1][1] = fmaf(a1 * a1, C, cs);
+    R[1][2] = fmaf(a1 * a2, C, -(a0 * sn));
+    R[2][0] = fmaf(a2 * a0, C, -(a1 * sn));
+    R[2][1] = fmaf(a2 * a1, C, a0 * sn);
+    R[2][2] = fmaf(a2 * a2, C, cs);
+}
+
+/* Uniform rotation from three uniforms (Shoemake, "Uniform random rotations",
+ * Graphics Gems III, 1992): unit quaternion -> matrix. */
+static void shoemake(float u1, float u2, float u3, float R[3][3]) {
+    float s2, c2, s3, c3;
+    or_det_sincos(u2 * OR_TWO_PI_F, &s2, &c2);
+    or_det_sincos(u3 * OR_TWO_PI_F, &s3, &c3);
+    float r1 = sqrtf(1.0f - u1), r2 = sqrtf(u1);
+    float x = r1 * s2, y = r1 * c2, z = r2 * s3, w = r2 * c3;
+    float xx = x * x, yy = y * y, zz = z * z;
+    float xy = x * y, xz = x * z, yz = y * z, xw = x * w, yw = y * w, zw = z * w;
+    R[0][0] = 1.0f - 2.0f * (yy + zz);
+    R[0][1] = 2.0f * (xy - zw);
+    R[0][2] = 2.0f * (xz + yw);
+    R[1][0] = 2.0f * (xy + zw);
+    R[1][1] = 1.0f - 2.0f * (xx + zz);
+    R[1][2] = 2.0f * (yz - xw);
+    R[2][0] = 2.0f * (xz - yw);
+    R[2][1] = 2.0f * (yz + xw);
+    R[2][2] = 1.0f - 2.0f * (xx + yy);
+}
+
+/* p' = R p (gcmc/cpp/gcmc_energy.h:62-71 accumulation order, fused) */
+static inline void rotate(const float R[3][3], const float p[3], float out[3]) {
+    for (int j = 0; j < 3; ++j) {
+        float x = p[0] * R[j][0];
+        x = fmaf(p[1], R[j][1], x);
+        x = fmaf(p[2], R[j][2], x);
+        out[j] = x;
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Distances (gcmc/cpp/gcmc_energy.h:110-122).                                */
+/* ------------------------------------------------------------------------- */
+static inline float fast_round_f(float a) {
+    return a >= 0.0f ? (float)(int)(a + 0.5f) : (float)(int)(a - 0.5f);
+}
+static inline double fast_round_d(double a) {
+    return a >= 0.0 ? trunc(a + 0.5) : trunc(a - 0.5);
+}
+
+float or_dist_group(const float a[3], const float b[3], const float L[3]) {
+    float d[3];
+    for (int i = 0; i < 3; ++i) {
+        float x = a[i] - b[i];
+        float r = fast_round_f(x / L[i]);
+        d[i] = fmaf(-r, L[i], x);
+    }
+    float s = d[0] * d[0];
+    s = fmaf(d[1], d[1], s);
+    s = fmaf(d[2], d[2], s);
+    return sqrtf(s);
+}
+
+float or_dist_host(const float a[3], const float b[3], const float L[3]) {
+    float d[3];
+    for (int i = 0; i < 3; ++i) {
+        float x = a[i] - b[i];
+        float r = fast_round_f(x / L[i]);
+        d[i] = x - r * L[i];
+    }
+    float s = d[0] * d[0] + d[1] * d[1];
+    s = s + d[2] * d[2];
+    return sqrtf(s);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Pose energy (gcmc/cpp/gcmc_energy.h:142-204).                              */
+/* ------------------------------------------------------------------------- */
+static double group_pairs64(const or_info* info, const or_atom* atoms, const float* ff, int a0,
+                            int na, const float (*sx)[3], const float* sq, const int32_t* st,
+                            int ns, double* l1) {
+    const double L[3] = {info->cryst[0], info->cryst[1], info->cryst[2]};
+    double e = 0.0;
+    for (int a = a0; a < a0 + na; ++a) {
+        const or_atom* A = &atoms[a];
+        for (int s = 0; s < ns; ++s) {
+            double d2 = 0.0;
+            for (int i = 0; i < 3; ++i) {
+                double d = (double)A->position[i] - (double)sx[s][i];
+                d -= fast_round_d(d / L[i]) * L[i];
+                d2 += d * d;
+            }
+            int tij = st[s] * info->ffYNum + A->type;
+            double sig = ff[2 * tij], eps = ff[2 * tij + 1];
+            double s2 = sig * sig * 100.0 / d2;
+            double s6 = s2 * s2 * s2;
+            double lj = 4.0 * eps * (s6 * s6 - s6);
+            double el = OR_COULOMB * (double)sq[s] * (double)A->charge / sqrt(d2);
+            e += lj + el;
+            *l1 += fabs(lj) + fabs(el);
+        }
+    }
+    return e;
+}
+
+/* FP32 mirror of one reference thread's pair work on one group. */
+static float group_pairs32(const or_info* info, const or_atom* atoms, const float* ff, int a0, int na,
+                           const float (*sx)[3], const float* sq, const int32_t* st, int ns,
+                           float acc) {
+    for (int a = a0; a < a0 + na; ++a) {
+        const or_atom* A = &atoms[a];
+        for (int s = 0; s < ns; ++s) {
+            float dist = or_dist_group(A->position, sx[s], info->cryst);
+            int tij = st[s] * info->ffYNum + A->type;
+            float sigma = ff[2 * tij], epsilon = ff[2 * tij + 1];
+            float sigma_sqrd = sigma * sigma * 100.0f;
+            float sd = sigma_sqrd / (dist * dist);
+            float vdw = 4.0f * epsilon * (powf(sd, 6.0f) - powf(sd, 3.0f));
+            acc = acc + vdw;
+            double el = OR_COULOMB * (double)(sq[s] * A->charge) / (double)dist;
+            acc = (float)((double)acc + el);
+        }
+    }
+    return acc;
+}
+
+double or_pose_energy(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                      const or_atom* atoms, const float* ff, const float (*sx)[3],
+                      const float* sq, const int32_t* st, int32_t ns, const float centre[3],
+                      int32_t self, int32_t mode, int32_t* n_groups, int64_t* pairs) {
+    return or_pose_energy_l1(info, frag, res, atoms, ff, sx, sq, st, ns, centre, self, mode, n_groups, pairs,
+                             NULL);
+}
+
+double or_pose_energy_l1(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                         const or_atom* atoms, const float* ff, const float (*sx)[3],
+                         const float* sq, const int32_t* st, int32_t ns, const float centre[3],
+                         int32_t self, int32_t mode, int32_t* n_groups, int64_t* pairs, double* l1_out) {
+    int ng = 0;
+    int64_t np = 0;
+    double l1 = 0.0;
+    const int nfixed = frag[0].startRes;
+    if (mode == 0) {
+        double e = 0.0;
+        for (int g = 0; g < nfixed; ++g) {
+            if (or_dist_group(centre, res[g].position, info->cryst) <= info->cutoff) {
+                e += group_pairs64(info, atoms, ff, res[g].atomStart, res[g].atomNum, sx, sq, st, ns, &l1);
+                ng++;
+                np += (int64_t)res[g].atomNum * ns;
+            }
+        }
+        for (int t = 0; t < info->fragTypeNum; ++t) {
+            int g0 = frag[t].startRes, g1 = g0 + frag[t].totalNum;
+            for (int g = g0; g < g1; ++g) {
+                if (g == self) continue;
+                if (or_dist_group(centre, res[g].position, info->cryst) <= info->cutoff) {
+                    e += group_pairs64(info, atoms, ff, res[g].atomStart, res[g].atomNum, sx, sq, st, ns, &l1);
+                    ng++;
+                    np += (int64_t)res[g].atomNum * ns;
+                }
+            }
+        }
+        if (n_groups) *n_groups = ng;
+        if (pairs) *pairs = np;
+        if (l1_out) *l1_out = l1;
+        return e;
+    }
+    /* FP32 mirror: 128 virtual threads, strided group loops, tree reduction */
+    float sh[128];
+    for (int tid = 0; tid < 128; ++tid) {
+        float acc = 0.0f;
+        for (int g = tid; g < nfixed; g += 128) {
+            if (or_dist_group(centre, res[g].position, info->cryst) <= info->cutoff) {
+                acc = group_pairs32(info, atoms, ff, res[g].atomStart, res[g].atomNum, sx, sq, st, ns, acc);
+                ng++;
+                np += (int64_t)res[g].atomNum * ns;
+            }
+        }
+        for (int t = 0; t < info->fragTypeNum; ++t) {
+            int g0 = frag[t].startRes, g1 = g0 + frag[t].totalNum;
+            for (int g = tid + g0; g < g1; g += 128) {
+                if (g != self && or_dist_group(centre, res[g].position, info->cryst) <= info->cutoff) {
+                    acc = group_pairs32(info, atoms, ff, res[g].atomStart, res[g].atomNum, sx, sq, st, ns, acc);
+                    ng++;
+                    np += (int64_t)res[g].atomNum * ns;
+                }
+            }
+        }
+        sh[tid] = acc;
+    }
+    for (int s = 64; s > 0; s >>= 1)
+        for (int tid = 0; tid < s; ++tid) sh[tid] += sh[tid + s];
+    if (n_groups) *n_groups = ng;
+    if (pairs) *pairs = np;
+    return (double)sh[0];
+}
+
+/* ------------------------------------------------------------------------- */
+/* Proposals (gcmc/cpp/gcmc_energy.h:75-107, gcmc_move_trn.h:54-75,           */
+/* gcmc_move_rot.h:313-355).                                                  */
+/* ------------------------------------------------------------------------- */
+void or_insert_pose(const or_info* info, const or_atomarray* frag, const float* grid,
+                    const or_options* opt, int32_t ftype, int32_t step, int32_t i,
+                    float (*xyz)[3], float centre[3]) {
+    uint32_t r0[4], r1[4];
+    rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 0, r0);
+    rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 1, r1);
+    int g = (int)(r0[0] % (uint32_t)info->totalGridNum);
+    float t[3];
+    for (int j = 0; j < 3; ++j) {
+        float off = u01_oc(r0[1 + j]) * info->grid_dx;
+        t[j] = off + grid[3 * g + j];
+    }
+    float R[3][3];
+    if (opt->proposal == 0) {
+        float axis[3] = {u01_oc(r1[0]), u01_oc(r1[1]), u01_oc(r1[2])};
+        float phi = u01_oc(r1[3]) * OR_TWO_PI_F;
+        float sn, cs;
+        or_det_sincos(phi, &sn, &cs);
+        rodrigues(axis, sn, cs, R);
+    } else {
+        shoemake(u01_co(r1[0]), u01_co(r1[1]), u01_co(r1[2]), R);
+    }
+    const or_atomarray* F = &frag[ftype];
+    for (int s = 0; s < F->num_atoms; ++s) {
+        float p[3];
+        rotate(R, F->atoms[s].position, p);
+        for (int j = 0; j < 3; ++j) xyz[s][j] = p[j] + t[j];
+    }
+    for (int j = 0; j < 3; ++j) centre[j] = t[j];
+}
+
+void or_move_pose(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                  const or_atom* atoms, const or_options* opt, int32_t ftype, int32_t move,
+                  int32_t step, int32_t i, int32_t slot, float (*xyz)[3], float centre[3]) {
+    const or_atomarray* F = &frag[ftype];
+    const or_residue* Rs = &res[F->startRes + slot];
+    const int ns = F->num_atoms;
+    uint32_t r[4];
+    rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)i, RP_MOVE, 0, r);
+    for (int s = 0; s < ns; ++s)
+        for (int j = 0; j < 3; ++j) xyz[s][j] = atoms[Rs->atomStart + s].position[j];
+    if (move == 2) {
+        for (int j = 0; j < 3; ++j) {
+            float sh = opt->proposal == 0 ? u01_oc(r[j]) * info->grid_dx
+                                          : (u01_co(r[j]) - 0.5f) * opt->trn_step;
+            float c = Rs->position[j];
+            float hi = info->cryst[j] + info->startxyz[j];
+            if (c + sh > hi) sh = sh - info->cryst[j];
+            if (c + sh < info->startxyz[j]) sh = sh + info->cryst[j];
+            centre[j] = c + sh;
+            for (int s = 0; s < ns; ++s) xyz[s][j] = xyz[s][j] + sh;
+        }
+        return;
+    }
+    /* rotate about the unweighted centroid; residue centre unchanged */
+    float R[3][3];
+    if (opt->proposal == 0) {
+        float axis[3] = {u01_oc(r[0]), u01_oc(r[1]), u01_oc(r[2])};
+        float phi = u01_oc(r[3]) * OR_TWO_PI_F;
+        float sn, cs;
+        or_det_sincos(phi, &sn, &cs);
+        rodrigues(axis, sn, cs, R);
+    } else {
+        float z = 2.0f * u01_co(r[0]) - 1.0f;
+        float sp, cp;
+        or_det_sincos(u01_co(r[1]) * OR_TWO_PI_F, &sp, &cp);
+        float rxy = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        float axis[3] = {rxy * cp, rxy * sp, z};
+        float theta = opt->rot_max * (2.0f * u01_co(r[2]) - 1.0f);
+        float sn, cs;
+        or_det_sincos(theta, &sn, &cs);
+        rodrigues(axis, sn, cs, R);
+    }
+    float cen[3] = {0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < 3; ++j)
+        for (int s = 0; s < ns; ++s) cen[j] = cen[j] + xyz[s][j] / (float)ns;
+    for (int s = 0; s < ns; ++s) {
+        float q[3] = {xyz[s][0] - cen[0], xyz[s][1] - cen[1], xyz[s][2] - cen[2]};
+        float p[3];
+        rotate(R, q, p);
+        for (int j = 0; j < 3; ++j) xyz[s][j] = p[j] + cen[j];
+    }
+    for (int j = 0; j < 3; ++j) centre[j] = Rs->position[j];
+}
+
+/* Keyed permutation of [0,n): 4-round Feistel network on the smallest even
+ * bit width covering n, with cycle walking; round function = murmur3 fmix32. */
+static inline uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return h;
+}
+int32_t or_perm_slot(const or_options* opt, uint32_t seed, int32_t step, int32_t i, int32_t n) {
+    uint32_t rk[4];
+    rng(seed, opt->replica, (uint32_t)step, 0u, RP_PERM, 0, rk);
+    int h = 1;
+    while ((1u << (2 * h)) < (uint32_t)n) ++h;
+    uint32_t mask = (1u << h) - 1u;
+    uint32_t x = (uint32_t)i;
+    do {
+        uint32_t Lh = x >> h, Rh = x & mask;
+        for (int r = 0; r < 4; ++r) {
+            uint32_t nl = Rh;
+            Rh = Lh ^ (fmix32(Rh ^ rk[r]) & mask);
+            Lh = nl;
+        }
+        x = (Lh << h) | Rh;
+    } while (x >= (uint32_t)n);
+    return (int32_t)x;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Cluster / Rosenbluth / acceptance pass (gcmc_move_add.h:107-191,           */
+/* gcmc_move_trn.h:160-244).                                                  */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int kind;        /* 0 insert, 1 translate/rotate */
+    double lncav;    /* insert: ln(cavityFactor)     */
+    double B;        /* insert: beta*muex + ln(Nbar) */
+    int* n;          /* insert: running totalNum     */
+    int maxNum;
+} cluster_par;
+
+static int cluster_pass(const or_info* info, const or_options* opt, int step, int k,
+                        const double* E, const float (*c)[3], const cluster_par* P,
+                        int* accepted, int* inserted, int* n_acc, int* first_accept) {
+    const double beta = OR_BETA;
+    unsigned char* U = (unsigned char*)malloc((size_t)k);
+    int* mem = (int*)malloc(sizeof(int) * (size_t)k);
+    memset(U, 1, (size_t)k);
+    int nclus = 0, na = 0;
+    *first_accept = -1;
+    for (int s = 0; s < k; ++s) {
+        if (!U[s]) continue;
+        nclus++;
+        int nm = 0;
+        mem[nm++] = s; /* the seed is always a member */
+        for (int i = s + 1; i < k; ++i)
+            if (U[i] && or_dist_host(c[s], c[i], info->cryst) <= info->cutoff) mem[nm++] = i;
+        double emin = INFINITY;
+        for (int m = 0; m < nm; ++m)
+            if (isfinite(E[mem[m]]) && E[mem[m]] < emin) emin = E[mem[m]];
+        int chosen = s;
+        int acc = 0;
+        if (isfinite(emin)) {
+            double W = 0.0, best = -INFINITY;
+            for (int m = 0; m < nm; ++m) {
+                int i = mem[m];
+                if (!isfinite(E[i])) continue;
+                W += exp(-beta * (E[i] - emin));
+                uint32_t g[4];
+                rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)i, RP_GUMBEL, 0, g);
+                double key = -beta * E[i] - log(-log(u53_open(g[0], g[1])));
+                if (key > best) { best = key; chosen = i; }
+            }
+            double lnp = log(W) - log((double)nm) - beta * emin;
+            if (P->kind == 0) lnp += P->lncav + P->B - log((double)(*P->n) + 1.0);
+            uint32_t ua[4];
+            rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)s, RP_CLUSTER, 0, ua);
+            double u = u53(ua[0], ua[1]);
+            acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+        }
+        for (int m = 0; m < nm; ++m) U[mem[m]] = 0;
+        if (acc) {
+            for (int i = s + 1; i < k; ++i)
+                if (U[i] && or_dist_host(c[chosen], c[i], info->cryst) <= info->cutoff) U[i] = 0;
+            if (*first_accept < 0) *first_accept = chosen;
+            int ins = 1;
+            if (P->kind == 0) {
+                if (*P->n < P->maxNum) (*P->n)++;
+                else ins = 0;
+            }
+            accepted[na] = chosen;
+            inserted[na] = ins;
+            na++;
+        }
+    }
+    free(U);
+    free(mem);
+    *n_acc = na;
+    return nclus;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Moves and the step loop.                                                   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    const or_info* info;
+    or_atomarray* frag;
+    or_residue* res;
+    or_atom* atoms;
+    const float* grid;
+    const float* ff;
+    const or_options* opt;
+} sysref;
+
+static double beta_muex(const or_options* opt, const or_atomarray* F) {
+    double mu = (double)F->muex;
+    if (opt->muex_kcal) mu *= OR_KCAL_TO_KJ;
+    return OR_BETA * mu;
+}
+
+static double ln_nbar(const or_info* info, const or_atomarray* F) {
+    double V = (double)info->cryst[0] * (double)info->cryst[1] * (double)info->cryst[2];
+    return log(V * (double)F->conc * OR_MOLES_TO_MOLECULES);
+}
+
+static void template_sites(const or_atomarray* F, float* q, int32_t* t) {
+    for (int s = 0; s < F->num_atoms; ++s) { q[s] = F->atoms[s].charge; t[s] = F->atoms[s].type; }
+}
+
+static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_log* L, double* Eout,
+                       double* Escale, const double* Ereplay, int kmax, int threads) {
+    const or_info* info = S->info;
+    int mv = moves[step];
+    int f = mv / 4, m = mv % 4;
+    or_atomarray* F = &S->frag[f];
+    const int ns = F->num_atoms;
+    float sq[20];
+    int32_t st[20];
+    template_sites(F, sq, st);
+    int n0 = F->totalNum;
+    if (L) {
+        memset(L, 0, sizeof(*L));
+        L->step = step; L->move = m; L->ftype = f; L->n_before = n0;
+        L->first_accept = -1; L->slot = -1;
+    }
+    int k = 0;
+    if (m == 0) {
+        if (F->totalNum == F->maxNum) goto done;
+        k = F->confBias;
+        if (Eout && k > kmax) return -3;
+        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
+        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        double* E = malloc(sizeof(double) * (size_t)k);
+        double* l1 = malloc(sizeof(double) * (size_t)k);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
+        for (int i = 0; i < k; ++i) {
+            or_insert_pose(info, S->frag, S->grid, S->opt, f, step, i, xyz[i], cen[i]);
+            E[i] = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
+                                     sq, st, ns, cen[i], -1, 0, NULL, NULL, &l1[i]);
+        }
+        double esum = 0.0;
+        for (int i = 0; i < k; ++i) {
+            esum += E[i];
+            if (Eout) Eout[i] = E[i];
+            if (Escale) Escale[i] = l1[i];
+        }
+        free(l1);
+        const double* Ed = Ereplay ? Ereplay : E;
+        int n = F->totalNum;
+        cluster_par P = {0, log((double)info->cavityFactor), beta_muex(S->opt, F) + ln_nbar(info, F), &n,
+                         F->maxNum};
+        int* acc = malloc(sizeof(int) * (size_t)k);
+        int* ins = malloc(sizeof(int) * (size_t)k);
+        int na = 0, fa = -1;
+        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
+        for (int a = 0; a < na; ++a) {
+            if (!ins[a]) continue;
+            int i = acc[a];
+            int slot = F->totalNum++;
+            or_residue* R = &S->res[F->startRes + slot];
+            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
+            for (int s = 0; s < ns; ++s) {
+                or_atom* A = &S->atoms[R->atomStart + s];
+                for (int j = 0; j < 3; ++j) A->position[j] = xyz[i][s][j];
+                A->charge = F->atoms[s].charge;
+                A->type = F->atoms[s].type;
+            }
+        }
+        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
+        free(acc); free(ins); free(xyz); free(cen); free(E);
+    } else if (m == 1) {
+        if (F->totalNum == 0) goto done; /* the reference divides by zero here */
+        k = 1;
+        uint32_t r[4];
+        rng(info->seed, S->opt->replica, (uint32_t)step, 0u, RP_DELETE, 0, r);
+        int slot = (int)(r[0] % (uint32_t)F->totalNum);
+        or_residue* R = &S->res[F->startRes + slot];
+        float xyz[20][3];
+        for (int s = 0; s < ns; ++s)
+            for (int j = 0; j < 3; ++j) xyz[s][j] = S->atoms[R->atomStart + s].position[j];
+        double l1 = 0.0;
+        double E = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz, sq, st,
+                                     ns, R->position, F->startRes + slot, 0, NULL, NULL, &l1);
+        if (Eout) Eout[0] = E;
+        if (Escale) Escale[0] = l1;
+        double Ed = Ereplay ? Ereplay[0] : E;
+        int n = F->totalNum;
+        double lnp = log((double)n) - (beta_muex(S->opt, F) + ln_nbar(info, F)) + OR_BETA * Ed;
+        double u = u53(r[1], r[2]);
+        int acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+        if (acc) {
+            int last = n - 1;
+            or_residue* RL = &S->res[F->startRes + last];
+            for (int j = 0; j < 3; ++j) R->position[j] = RL->position[j];
+            for (int s = 0; s < R->atomNum; ++s)
+                for (int j = 0; j < 3; ++j)
+                    S->atoms[R->atomStart + s].position[j] = S->atoms[RL->atomStart + s].position[j];
+            F->totalNum -= 1;
+        }
+        if (L) {
+            L->n_clusters = 1; L->n_accept = acc; L->first_accept = acc ? 0 : -1;
+            L->slot = slot; L->e_sum = E;
+        }
+    } else {
+        int n = F->totalNum;
+        k = F->confBias < n ? F->confBias : n;
+        if (k == 0) goto done;
+        if (Eout && k > kmax) return -3;
+        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
+        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        int* slots = malloc(sizeof(int) * (size_t)k);
+        double* dE = malloc(sizeof(double) * (size_t)k);
+        double* sc = malloc(sizeof(double) * (size_t)k);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 2)
+        for (int i = 0; i < k; ++i) {
+            int slot = or_perm_slot(S->opt, info->seed, step, i, n);
+            slots[i] = slot;
+            const or_residue* R = &S->res[F->startRes + slot];
+            float old[20][3];
+            for (int s = 0; s < ns; ++s)
+                for (int j = 0; j < 3; ++j) old[s][j] = S->atoms[R->atomStart + s].position[j];
+            double lo = 0.0, ln = 0.0;
+            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
+                                          st, ns, R->position, F->startRes + slot, 0, NULL, NULL, &lo);
+            or_move_pose(info, S->frag, S->res, S->atoms, S->opt, f, m, step, i, slot, xyz[i], cen[i]);
+            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
+                                          sq, st, ns, cen[i], F->startRes + slot, 0, NULL, NULL, &ln);
+            dE[i] = En - Eo;
+            sc[i] = ln + lo;
+        }
+        double esum = 0.0;
+        for (int i = 0; i < k; ++i) {
+            esum += dE[i];
+            if (Eout) Eout[i] = dE[i];
+            if (Escale) Escale[i] = sc[i];
+        }
+        const double* Ed = Ereplay ? Ereplay : dE;
+        cluster_par P = {1, 0.0, 0.0, NULL, 0};
+        int* acc = malloc(sizeof(int) * (size_t)k);
+        int* ins = malloc(sizeof(int) * (size_t)k);
+        int na = 0, fa = -1;
+        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
+        for (int a = 0; a < na; ++a) {
+            int i = acc[a];
+            or_residue* R = &S->res[F->startRes + slots[i]];
+            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
+            for (int s = 0; s < ns; ++s)
+                for (int j = 0; j < 3; ++j) S->atoms[R->atomStart + s].position[j] = xyz[i][s][j];
+        }
+        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
+        free(acc); free(ins); free(xyz); free(cen); free(slots); free(dE); free(sc);
+    }
+done:
+    if (L) { L->k = k; L->n_after = F->totalNum; }
+    return 0;
+}
+
+int32_t or_run(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
+               const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
+               int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
+               const double* replay, int32_t kmax, int32_t threads) {
+    if (threads <= 0) threads = 1;
+    sysref S = {info, frag, res, atoms, grid, ff, opt};
+    for (int s = 0; s < nsteps; ++s) {
+        int step = step0 + s;
+        int rc = do_step(&S, moves, step, log ? &log[s] : NULL, energies ? energies + (size_t)s * kmax : NULL,
+                         escale ? escale + (size_t)s * kmax : NULL, replay ? replay + (size_t)s * kmax : NULL,
+                         kmax, threads);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                        const or_atom* atoms, const float* ff, const float* poses_xyz,
+                        const float* site_q, const int32_t* site_type, int32_t nsites,
+                        const float* centres, const int32_t* self, int32_t nposes, int32_t mode,
+                        double* out, int32_t* n_groups, double* l1, int32_t threads) {
+    if (threads <= 0) threads = 1;
+    int64_t total = 0;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4) reduction(+ : total)
+    for (int p = 0; p < nposes; ++p) {
+        int32_t ng = 0;
+        int64_t np = 0;
+        double m1 = 0.0;
+        out[p] = or_pose_energy_l1(info, frag, res, atoms, ff,
+                                   (const float (*)[3])(poses_xyz + (size_t)p * nsites * 3), site_q,
+                                   site_type, nsites, centres + 3 * p, self ? self[p] : -1, mode, &ng, &np,
+                                   &m1);
+        if (l1) l1[p] = m1;
+        if (n_groups) n_groups[p] = ng;
+        total += np;
+    }
+    return total;
+}
+
+/* Rotation of one point by the Rodrigues matrix of (axis, angle) -- exposes the
+ * pose rotation for the known-answer test of the reference notebook. */
+void or_rotate_point(const float axis[3], float angle, const float p[3], float out[3], float R_out[9]) {
+    float sn, cs, R[3][3];
+    or_det_sincos(angle, &sn, &cs);
+    rodrigues(axis, sn, cs, R);
+    rotate(R, p, out);
+    if (R_out)
+        for (int i = 0; i < 9; ++i) R_out[i] = R[i / 3][i % 3];
+}

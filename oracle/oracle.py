@@ -1,0 +1,138 @@
+"""ctypes wrapper of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, the smoke check and the CPU-baseline leg of the benchmark use
+this module; it checks the engine and is never part of it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+c_void = ctypes.c_void_p
+
+
+class OrOptions(ctypes.Structure):
+    _fields_ = [("proposal", ctypes.c_int32), ("muex_kcal", ctypes.c_int32), ("trn_step", ctypes.c_float),
+                ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("reserved", ctypes.c_int32 * 3)]
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        L.or_run.restype = ctypes.c_int32
+        L.or_run.argtypes = [c_void] * 8 + [ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void,
+                                            ctypes.c_int32, ctypes.c_int32]
+        L.or_energy_batch.restype = ctypes.c_int64
+        L.or_energy_batch.argtypes = [c_void] * 8 + [ctypes.c_int32, c_void, c_void, ctypes.c_int32, ctypes.c_int32,
+                                                     c_void, c_void, c_void, ctypes.c_int32]
+        L.or_philox.argtypes = [c_void, c_void, c_void]
+        L.or_det_sincos.argtypes = [ctypes.c_float, c_void, c_void]
+        L.or_dist_group.restype = ctypes.c_float
+        L.or_dist_group.argtypes = [c_void, c_void, c_void]
+        L.or_dist_host.restype = ctypes.c_float
+        L.or_dist_host.argtypes = [c_void, c_void, c_void]
+        L.or_insert_pose.argtypes = [c_void, c_void, c_void, c_void, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                     c_void, c_void]
+        L.or_move_pose.argtypes = [c_void] * 5 + [ctypes.c_int32] * 5 + [c_void, c_void]
+        L.or_rotate_point.argtypes = [c_void, ctypes.c_float, c_void, c_void, c_void]
+        L.or_perm_slot.restype = ctypes.c_int32
+        L.or_perm_slot.argtypes = [c_void, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(c_void)
+
+
+def options(proposal=0, muex_kcal=0, trn_step=1.0, rot_max=np.radians(15.0), replica=0):
+    return OrOptions(proposal, muex_kcal, trn_step, rot_max, replica)
+
+
+def run(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, want_energies=True,
+        want_scale=False):
+    """Advance a System in place; returns (logs, energies) or, with want_scale,
+    (logs, energies, scale) where scale is the magnitude the relative tolerance
+    of each energy refers to (|E|, or |E_new| + |E_old| for translate/rotate)."""
+    from pygcmc_b200.values import StepLog_dtype
+    opts = opts or options()
+    threads = threads or os.cpu_count() or 1
+    logs = np.zeros(nsteps, dtype=StepLog_dtype)
+    E = np.zeros((nsteps, kmax), dtype=np.float64) if want_energies else None
+    SC = np.zeros((nsteps, kmax), dtype=np.float64) if want_scale else None
+    rp = None if replay is None else np.ascontiguousarray(replay, dtype=np.float64)
+    s = system
+    rc = lib().or_run(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), _p(s.grid), _p(s.ff),
+                      _p(s.moveArray), ctypes.byref(opts), step0, nsteps, _p(logs), _p(E), _p(SC), _p(rp), kmax,
+                      threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed ({rc})")
+    return (logs, E, SC) if want_scale else (logs, E)
+
+
+def energy_batch(system, xyz, q, types, centres, self_res=None, mode=0, threads=None, want_l1=False):
+    """FP64 (mode 0) or FP32-mirror (mode 1) energies of explicit poses:
+    (energies, groups included, pairs) and, with want_l1, the per-pose sum of
+    |pair terms| (FP64 mode)."""
+    threads = threads or os.cpu_count() or 1
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    n, ns = xyz.shape[0], xyz.shape[1]
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    c = np.ascontiguousarray(centres, dtype=np.float32)
+    sr = None if self_res is None else np.ascontiguousarray(self_res, dtype=np.int32)
+    out = np.zeros(n, dtype=np.float64)
+    ng = np.zeros(n, dtype=np.int32)
+    l1 = np.zeros(n, dtype=np.float64)
+    s = system
+    pairs = lib().or_energy_batch(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), _p(s.ff),
+                                  _p(xyz), _p(q), _p(t), ns, _p(c), _p(sr), n, mode, _p(out), _p(ng), _p(l1),
+                                  threads)
+    return (out, ng, int(pairs), l1) if want_l1 else (out, ng, int(pairs))
+
+
+def philox(ctr, key):
+    c = np.asarray(ctr, dtype=np.uint32)
+    k = np.asarray(key, dtype=np.uint32)
+    o = np.zeros(4, dtype=np.uint32)
+    lib().or_philox(_p(c), _p(k), _p(o))
+    return o
+
+
+def det_sincos(x):
+    s, c = np.zeros(1, np.float32), np.zeros(1, np.float32)
+    lib().or_det_sincos(ctypes.c_float(x), _p(s), _p(c))
+    return float(s[0]), float(c[0])
+
+
+def insert_pose(system, ftype, step, i, opts=None):
+    opts = opts or options()
+    ns = int(system.fragmentInfo[ftype]["num_atoms"])
+    xyz = np.zeros((20, 3), np.float32)
+    c = np.zeros(3, np.float32)
+    lib().or_insert_pose(_p(system.SimInfo), _p(system.fragmentInfo), _p(system.grid), ctypes.byref(opts), ftype,
+                         step, i, _p(xyz), _p(c))
+    return xyz[:ns], c
+
+
+def rotate_point(axis, angle, p):
+    a = np.asarray(axis, np.float32)
+    x = np.asarray(p, np.float32)
+    out = np.zeros(3, np.float32)
+    R = np.zeros(9, np.float32)
+    lib().or_rotate_point(_p(a), ctypes.c_float(angle), _p(x), _p(out), _p(R))
+    return out, R.reshape(3, 3)

@@ -1,0 +1,111 @@
+"""ctypes binding of the native library's C ABI (include/gcmc_b200.h).
+
+The library is built in-tree by :mod:`pygcmc_b200.build`; importing this
+module never falls back to anything else -- a missing library raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB_PATH
+
+c_int = ctypes.c_int32
+c_void = ctypes.c_void_p
+
+
+class Options(ctypes.Structure):
+    """gcmc_options (include/gcmc_b200.h)."""
+    _fields_ = [("proposal", c_int), ("muex_kcal", c_int), ("trn_step", ctypes.c_float),
+                ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("cells_per_cutoff", c_int),
+                ("log_steps", c_int), ("log_kmax", c_int)]
+
+
+class ReplicaIn(ctypes.Structure):
+    """gcmc_replica_in: the seven state arrays of one replica."""
+    _fields_ = [("info", c_void), ("fragmentInfo", c_void), ("residueInfo", c_void), ("atomInfo", c_void),
+                ("grid", c_void), ("ff", c_void), ("moveArray", c_void)]
+
+
+STATUS = {0: "ok", 1: "CUDA runtime error", 2: "invalid or inconsistent input",
+          3: "a size limit of the engine is exceeded", 4: "the device raised an error flag",
+          5: "no CUDA device"}
+
+
+class GcmcError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, 'unknown status')} (status {status})")
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"native library missing: {LIB_PATH} (build it with python -m pygcmc_b200.build)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    sig = {
+        "runGCMC_cuda": (None, [c_void] * 7),
+        "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
+        "gcmc_last_status": (c_int, []),
+        "gcmc_status_string": (ctypes.c_char_p, [c_int]),
+        "gcmc_default_options": (None, [P(Options)]),
+        "gcmc_create": (c_int, [c_int, P(ReplicaIn), P(Options), c_void, P(c_void)]),
+        "gcmc_run": (c_int, [c_void, c_int]),
+        "gcmc_sync": (c_int, [c_void]),
+        "gcmc_run_profiled": (c_int, [c_void, c_int, c_void, c_void, c_void]),
+        "gcmc_download": (c_int, [c_void, c_int, c_void, c_void, c_void]),
+        "gcmc_get_logs": (c_int, [c_void, c_int, c_void, c_void, c_int, P(c_int)]),
+        "gcmc_counters": (c_int, [c_void, c_int, P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
+        "gcmc_device_error": (c_int, [c_void, P(c_int)]),
+        "gcmc_stream": (c_void, [c_void]),
+        "gcmc_destroy": (c_int, [c_void]),
+        "gcmc_energy_poses": (c_int, [c_void, c_int, c_void, c_void, c_void, c_int, c_void, c_void, c_int,
+                                      c_void, c_void]),
+        "gcmc_synth_chain_sphere": (c_int, [c_int, c_void, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_uint64, c_void, P(ctypes.c_int)]),
+        "gcmc_synth_chain_slab": (c_int, [c_int] + [ctypes.c_float] * 12 + [ctypes.c_uint64, c_void,
+                                                                           P(ctypes.c_int)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def ptr(a):
+    """Data pointer of a C-contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(c_void)
+
+
+def check(status, what):
+    if status != 0:
+        raise GcmcError(status, what)
+
+
+def default_options(**kw):
+    o = Options()
+    lib().gcmc_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
+           "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
+           "gcmc_device_error", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses", "gcmc_synth_chain_sphere",
+           "gcmc_synth_chain_slab"]

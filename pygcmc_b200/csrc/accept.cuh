@@ -1,0 +1,447 @@
+// Accept/update kernel: the host halves of move_add / move_del / move_trn /
+// move_rot (gcmc/cpp/gcmc_move_add.h:103-198, gcmc_move_del.h:334-389,
+// gcmc_move_trn.h:159-250, gcmc_move_rot.h:437-527) moved onto the device,
+// plus the preparation of the next step's proposals.
+//
+// One CTA per replica.  For clustering moves the CTA
+//   1. sums each pose's slab partials (FP64) and precomputes per pose the
+//      Boltzmann weight relative to the step's lowest energy, the Gumbel key
+//      -beta*E + G (Gumbel-max picks pose i with probability w_i / sum w, the
+//      law of the reference's roulette selection) and ln u of the acceptance
+//      draw; it stages the pose-pose bit matrix in shared memory;
+//   2. warp 0 walks the clusters in pose-index order: seed = lowest unused
+//      pose, members = unused poses within the cutoff of the seed (one 32-bit
+//      word per lane), W and the argmax key by butterfly reductions, the
+//      Rosenbluth / Metropolis acceptance in FP64; an accepted cluster also
+//      removes the unused poses within the cutoff of its chosen pose;
+//   3. all warps write the accepted poses into their slots, then one thread
+//      applies the cell-list and count updates in acceptance order.
+#pragma once
+#include "energy.cuh"
+
+namespace gcmc {
+
+constexpr int kAcceptThreads = 1024;
+
+struct AcceptSmem {
+    double E[kMaxPoses];
+    double w[kMaxPoses];
+    double key[kMaxPoses];
+    double lnu[kMaxPoses];
+    float4 c[kMaxPoses];
+    uint32_t nb[kMaxPoses * kMaxWords];
+    int acc_list[kMaxPoses];
+    int acc_slot[kMaxPoses];
+    double red[32];
+    int misc[8];
+};
+
+// ---- cell list maintenance (single thread) ----
+__device__ __forceinline__ void cell_add(const RepDev& R, int g, float x, float y, float z) {
+    int c = cell_of(R, x, y, z);
+    int pos = R.cell_count[c];
+    if (pos >= R.cap) {
+        atomicOr(R.err, ERR_CELL_OVERFLOW);
+        R.gcell[g] = -1;
+        return;
+    }
+    R.cell_ent[c * R.cap + pos] = g;
+    R.cell_count[c] = pos + 1;
+    R.gcell[g] = c * R.cap + pos;
+}
+__device__ __forceinline__ void cell_remove(const RepDev& R, int g) {
+    int cp = R.gcell[g];
+    if (cp < 0) return;
+    int c = cp / R.cap;
+    int last = R.cell_count[c] - 1;
+    int gl = R.cell_ent[c * R.cap + last];
+    R.cell_ent[cp] = gl;
+    R.gcell[gl] = cp;
+    R.cell_count[c] = last;
+    R.gcell[g] = -1;
+}
+// the cell entry of group `from` now stands for group `to`
+__device__ __forceinline__ void cell_rename(const RepDev& R, int from, int to) {
+    int cp = R.gcell[from];
+    R.gcell[from] = -1;
+    R.gcell[to] = cp;
+    if (cp >= 0) R.cell_ent[cp] = to;
+}
+
+// ---- block reductions ----
+__device__ __forceinline__ double block_min(double v, double* red) {
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, off));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : INFINITY;
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, off));
+    return v;
+}
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    return v;
+}
+
+// ---- next-step preparation (whole CTA) ----
+__device__ void prepare_step(const RepDev& R, int step) {
+    __shared__ StepDesc Dsh;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) {
+        StepDesc D{};
+        D.step = step;
+        D.move = MV_NONE;
+        D.del_slot = -1;
+        D.nslab = R.span[2];
+        if (step < R.run_end && step < R.mcsteps) {
+            const int mv = R.moves[step];
+            D.ftype = mv >> 2;
+            D.move = mv & 3;
+            const FragDev& F = R.frag[D.ftype];
+            const int n = R.totalNum[D.ftype];
+            D.n = n;
+            if (D.move == MV_INSERT) {
+                D.k = (n >= F.maxNum) ? 0 : F.confBias;
+                D.nvar = 1;
+            } else if (D.move == MV_DELETE) {
+                D.k = n > 0 ? 1 : 0;
+                D.nvar = 1;
+                if (n > 0) {
+                    U4 r = rng(R.seed, R.replica, (uint32_t)step, 0u, RP_DELETE, 0);
+                    D.del_slot = (int)(r.x % (uint32_t)n);
+                }
+            } else {
+                D.k = min(F.confBias, n);
+                D.nvar = 2;
+                D.perm_key = rng(R.seed, R.replica, (uint32_t)step, 0u, RP_PERM, 0);
+                D.perm_h = perm_bits(n);
+            }
+            if (D.k > kMaxPoses) {
+                atomicOr(R.err, ERR_POSES);
+                D.k = 0;
+            }
+            D.nw = (D.move == MV_DELETE) ? 0 : (D.k + 31) >> 5;
+            D.items = D.k * D.nvar * D.nslab;
+        }
+        Dsh = D;
+    }
+    __syncthreads();
+    const StepDesc D = Dsh;
+    if (D.move == MV_INSERT) {
+        for (int i = tid; i < D.k; i += nt) {
+            float x, y, z;
+            insert_centre(R, step, i, x, y, z);
+            R.pcen[i] = make_float4(x, y, z, 0.0f);
+        }
+    } else if (D.move == MV_DELETE) {
+        if (tid == 0 && D.k > 0) R.pcen[0] = R.gcen[R.frag[D.ftype].startRes + D.del_slot];
+    } else if (D.move != MV_NONE) {
+        const int startRes = R.frag[D.ftype].startRes;
+        for (int i = tid; i < D.k; i += nt) {
+            const int slot = perm_slot(D.perm_key, D.perm_h, i, D.n);
+            R.pslot[i] = slot;
+            float4 c = R.gcen[startRes + slot];
+            if (D.move == MV_TRANSLATE) {
+                U4 r = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_MOVE, 0);
+                c.x = fadd(c.x, trn_shift(R, r.x, 0, c.x));
+                c.y = fadd(c.y, trn_shift(R, r.y, 1, c.y));
+                c.z = fadd(c.z, trn_shift(R, r.z, 2, c.z));
+            }
+            c.w = 0.0f;
+            R.pcen[i] = c;
+        }
+    }
+    if (tid == 0) *R.desc = D;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kAcceptThreads) k_prepare(const RepDev* __restrict__ reps, int nrep) {
+    const RepDev& R = reps[blockIdx.x];
+    const StepDesc D = *R.desc;
+    __syncthreads();
+    if (D.move == MV_NONE) prepare_step(R, D.step);
+}
+
+__global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep) {
+        long long e = (long long)reps[r].run_end + nsteps;
+        reps[r].run_end = (int)(e < reps[r].mcsteps ? e : reps[r].mcsteps);
+    }
+}
+
+// Initial cell lists: fixed groups, then each type's occupied slots, in index order.
+__global__ void k_build_cells(const RepDev* __restrict__ reps, int nrep) {
+    const RepDev& R = reps[blockIdx.x];
+    if (threadIdx.x != 0) return;
+    for (int g = 0; g < R.nfixed; ++g) {
+        float4 c = R.gcen[g];
+        cell_add(R, g, c.x, c.y, c.z);
+    }
+    for (int t = 0; t < R.ntypes; ++t) {
+        const int s0 = R.frag[t].startRes, n = R.totalNum[t];
+        for (int s = 0; s < n; ++s) {
+            float4 c = R.gcen[s0 + s];
+            cell_add(R, s0 + s, c.x, c.y, c.z);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    AcceptSmem& S = *reinterpret_cast<AcceptSmem*>(smem_raw);
+    const RepDev& R = reps[blockIdx.x];
+    const StepDesc D = *R.desc;
+    if (D.move == MV_NONE) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, nwarps = nt >> 5;
+    const FragDev& F = R.frag[D.ftype];
+    const int k = D.k, ns = F.nsites;
+
+    // ---- phase 0: pose energies (sum of slab partials; dE for translate/rotate)
+    for (int i = tid; i < k; i += nt) {
+        double e = 0.0;
+        for (int z = 0; z < D.nslab; ++z) e += R.epart[(i * D.nvar) * D.nslab + z];
+        if (D.nvar == 2) {
+            double eo = 0.0;
+            for (int z = 0; z < D.nslab; ++z) eo += R.epart[(i * 2 + 1) * D.nslab + z];
+            e = e - eo;
+        }
+        S.E[i] = e;
+    }
+    if (tid == 0) { S.misc[0] = 0; S.misc[1] = 0; S.misc[2] = -1; S.misc[3] = D.n; }
+    __syncthreads();
+    const bool logging = R.log != nullptr && D.step < R.log_cap;
+    double esum = 0.0;
+    if (logging) {
+        double v = 0.0;
+        for (int i = tid; i < k; i += nt) v += S.E[i];
+        esum = block_sum(v, S.red);
+        const int kl = min(k, R.log_kmax);
+        for (int i = tid; i < kl; i += nt) R.logE[(size_t)D.step * R.log_kmax + i] = S.E[i];
+    }
+
+    if (D.move == MV_DELETE) {
+        if (tid == 0 && k == 1) {
+            const double E = S.E[0];
+            const int n = D.n;
+            const double lnp = log((double)n) - F.B + kBeta * E;
+            const U4 r = rng(R.seed, R.replica, (uint32_t)D.step, 0u, RP_DELETE, 0);
+            const double u = u53(r.y, r.z);
+            const bool acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+            if (acc) {
+                const int slot = D.del_slot, last = n - 1;
+                const int gs = F.startRes + slot, gl = F.startRes + last;
+                cell_remove(R, gs);
+                if (slot != last) {
+                    const int2 ss = R.gspan[gs], sl = R.gspan[gl];
+                    for (int s = 0; s < ns; ++s) {
+                        float4 a = R.xyzq[sl.x + s];
+                        float4 b = R.xyzq[ss.x + s];
+                        R.xyzq[ss.x + s] = make_float4(a.x, a.y, a.z, b.w);
+                    }
+                    R.gcen[gs] = R.gcen[gl];
+                    cell_rename(R, gl, gs);
+                }
+                R.totalNum[D.ftype] = n - 1;
+            }
+            S.misc[0] = acc ? 1 : 0;
+            S.misc[1] = 1;
+            S.misc[2] = acc ? 0 : -1;
+            S.misc[3] = acc ? n - 1 : n;
+        }
+    } else if (k > 0) {
+        // ---- phase 1: per-pose weights, Gumbel keys, acceptance draws, bit rows
+        double emin_loc = INFINITY;
+        for (int i = tid; i < k; i += nt)
+            if (isfinite(S.E[i])) emin_loc = fmin(emin_loc, S.E[i]);
+        const double Eref = block_min(emin_loc, S.red);
+        for (int i = tid; i < k; i += nt) {
+            const double e = S.E[i];
+            const bool fin = isfinite(e);
+            S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
+            const U4 g = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
+            S.key[i] = fin ? (-kBeta * e - log(-log(u53_open(g.x, g.y)))) : -INFINITY;
+            const U4 ua = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
+            S.lnu[i] = log(u53(ua.x, ua.y));
+            S.c[i] = R.pcen[i];
+        }
+        const int nw = D.nw;
+        for (int x = tid; x < k * nw; x += nt) S.nb[x] = R.nbr[x];
+        __syncthreads();
+
+        // ---- phase 2: sequential cluster walk (warp 0)
+        const bool ins = (D.move == MV_INSERT);
+        if (warp == 0) {
+            uint32_t u = 0u;
+            if (lane < nw) {
+                const int rem = k - 32 * lane;
+                u = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+            }
+            int n = D.n, na = 0, nc = 0, fa = -1;
+            const double lnconst = ins ? (R.lncav + F.B) : 0.0;
+            double ln_n1 = ins ? log((double)n + 1.0) : 0.0;
+            for (;;) {
+                const unsigned nz = __ballot_sync(kFull, u != 0u);
+                if (nz == 0u) break;
+                const int L = __ffs(nz) - 1;
+                const uint32_t uw = __shfl_sync(kFull, u, L);
+                const int s = 32 * L + __ffs(uw) - 1;
+                uint32_t m = (lane < nw) ? (u & S.nb[s * nw + lane]) : 0u;
+                if (lane == L) m |= 1u << (s & 31);
+                const int cnt = __reduce_add_sync(kFull, (unsigned)__popc(m));
+                double wsum = 0.0, best = -INFINITY;
+                int bi = 0x7fffffff;
+                for (uint32_t mm = m; mm; mm &= mm - 1u) {
+                    const int i = 32 * lane + __ffs(mm) - 1;
+                    wsum += S.w[i];
+                    const double kk = S.key[i];
+                    if (kk > best) { best = kk; bi = i; }
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    wsum += __shfl_xor_sync(kFull, wsum, off);
+                    const double ob = __shfl_xor_sync(kFull, best, off);
+                    const int oi = __shfl_xor_sync(kFull, bi, off);
+                    if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+                }
+                bool acc = false;
+                int chosen = s;
+                if (bi != 0x7fffffff) {
+                    chosen = bi;
+                    double lnW;
+                    if (wsum > 1e-300) {
+                        lnW = log(wsum) - kBeta * Eref;
+                    } else {  // every member far above Eref: weights relative to the cluster minimum
+                        double em = INFINITY;
+                        for (uint32_t mm = m; mm; mm &= mm - 1u) {
+                            const double e = S.E[32 * lane + __ffs(mm) - 1];
+                            if (isfinite(e)) em = fmin(em, e);
+                        }
+                        for (int off = 16; off > 0; off >>= 1) em = fmin(em, __shfl_xor_sync(kFull, em, off));
+                        double w2 = 0.0;
+                        for (uint32_t mm = m; mm; mm &= mm - 1u) {
+                            const double e = S.E[32 * lane + __ffs(mm) - 1];
+                            if (isfinite(e)) w2 += exp(-kBeta * (e - em));
+                        }
+                        for (int off = 16; off > 0; off >>= 1) w2 += __shfl_xor_sync(kFull, w2, off);
+                        lnW = log(w2) - kBeta * em;
+                    }
+                    double lnp = lnW - log((double)cnt);
+                    if (ins) lnp += lnconst - ln_n1;
+                    acc = !isnan(lnp) && (lnp >= 0.0 || S.lnu[s] < lnp);
+                }
+                u &= ~m;
+                if (acc) {
+                    if (lane < nw) u &= ~S.nb[chosen * nw + lane];
+                    int slot = 0;
+                    if (ins) {
+                        if (n < F.maxNum) {
+                            slot = n;
+                            ++n;
+                            ln_n1 = log((double)n + 1.0);
+                        } else {
+                            slot = -1;
+                        }
+                    }
+                    if (lane == 0) { S.acc_list[na] = chosen; S.acc_slot[na] = slot; }
+                    ++na;
+                    if (fa < 0) fa = chosen;
+                }
+                ++nc;
+            }
+            if (lane == 0) { S.misc[0] = na; S.misc[1] = nc; S.misc[2] = fa; S.misc[3] = n; }
+        }
+        __syncthreads();
+
+        // ---- phase 3: write accepted poses, then cell lists and counts
+        const int na = S.misc[0];
+        if (ins) {
+            for (int a = warp; a < na; a += nwarps) {
+                const int slot = S.acc_slot[a];
+                if (slot < 0) continue;
+                const int i = S.acc_list[a];
+                const int res = F.startRes + slot;
+                const int2 sp = R.gspan[res];
+                const float4 c = S.c[i];
+                const Mat3 Rm = insert_rotation(R, D.step, i);
+                if (lane < ns) {
+                    const float4 t = F.site[lane];
+                    float x, y, z;
+                    rotate(Rm, t.x, t.y, t.z, x, y, z);
+                    R.xyzq[sp.x + lane] = make_float4(fadd(x, c.x), fadd(y, c.y), fadd(z, c.z), t.w);
+                    R.atype[sp.x + lane] = F.stype[lane];
+                }
+                if (lane == 0) R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int a = 0; a < na; ++a) {
+                    const int slot = S.acc_slot[a];
+                    if (slot < 0) continue;
+                    const float4 c = S.c[S.acc_list[a]];
+                    cell_add(R, F.startRes + slot, c.x, c.y, c.z);
+                }
+                R.totalNum[D.ftype] = S.misc[3];
+            }
+        } else {
+            for (int a = warp; a < na; a += nwarps) {
+                const int i = S.acc_list[a];
+                const int res = F.startRes + R.pslot[i];
+                const int2 sp = R.gspan[res];
+                const float4 gc = R.gcen[res];
+                float px = 0.f, py = 0.f, pz = 0.f, qw = 0.f;
+                if (lane < ns) {
+                    const float4 at = R.xyzq[sp.x + lane];
+                    px = at.x; py = at.y; pz = at.z; qw = at.w;
+                }
+                moved_site(R, D, i, gc, ns, lane, px, py, pz);
+                if (lane < ns) R.xyzq[sp.x + lane] = make_float4(px, py, pz, qw);
+            }
+            __syncthreads();
+            if (tid == 0 && D.move == MV_TRANSLATE) {
+                for (int a = 0; a < na; ++a) {
+                    const int i = S.acc_list[a];
+                    const int res = F.startRes + R.pslot[i];
+                    const float4 c = S.c[i];
+                    R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
+                    const int cp = R.gcell[res];
+                    if (cp < 0 || cp / R.cap != cell_of(R, c.x, c.y, c.z)) {
+                        cell_remove(R, res);
+                        cell_add(R, res, c.x, c.y, c.z);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        R.counters[0] += 1ull;
+        R.counters[1] += (unsigned long long)(k * D.nvar);
+        if (logging) {
+            gcmc_step_log L;
+            L.step = D.step;
+            L.move = D.move;
+            L.ftype = D.ftype;
+            L.k = k;
+            L.n_before = D.n;
+            L.n_after = S.misc[3];
+            L.n_clusters = S.misc[1];
+            L.n_accept = S.misc[0];
+            L.first_accept = S.misc[2];
+            L.slot = (D.move == MV_DELETE && k > 0) ? D.del_slot : -1;
+            L.e_sum = esum;
+            R.log[D.step] = L;
+        }
+    }
+    __syncthreads();
+    prepare_step(R, D.step + 1);
+}
+
+}  // namespace gcmc

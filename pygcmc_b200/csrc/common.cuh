@@ -1,0 +1,353 @@
+// Shared device definitions: constants, exact-rounding float helpers, the
+// counter-based RNG, the deterministic sin/cos, pose construction and the two
+// FP32 distance forms.  Everything a proposal or an inclusion decision depends
+// on is built from correctly rounded operations (explicit __f*_rn intrinsics,
+// which the compiler never fuses or reorders), so every result here is
+// reproducible bit for bit by a CPU implementation of the same formulas.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/gcmc_b200.h"
+
+namespace gcmc {
+
+// gcmc/cpp/gcmc.h:28-41
+constexpr double kBeta = 1.0 / (0.0083115 * 300.0);
+constexpr double kMolesToMolecules = 0.0006023;
+constexpr double kKcalToKJ = 4.184;
+constexpr float kCoulomb = 1388.431112f;  // gcmc/cpp/gcmc_energy.h:137
+constexpr float kTwoPiF = 6.28318530717958647692f;
+constexpr int kMaxSites = 20;
+constexpr int kMaxPoses = 1024;  // poses per step (confBias limit)
+constexpr int kMaxWords = kMaxPoses / 32;
+
+// RNG purposes: high half of the third counter word.
+enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6 };
+enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
+enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8 };
+
+// ---------------------------------------------------------------------------
+// exact-rounding float helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+
+// fast_round of gcmc/cpp/gcmc_energy.h:110-112: round half away from zero via
+// truncation to int, returned as float.
+__device__ __forceinline__ float fast_round(float a) {
+    return a >= 0.0f ? __int2float_rn(__float2int_rz(fadd(a, 0.5f)))
+                     : __int2float_rn(__float2int_rz(fsub(a, 0.5f)));
+}
+
+// Group-inclusion distance: the reference's device distanceP
+// (gcmc/cpp/gcmc_energy.h:115-122) with its multiply-adds fused.
+__device__ __forceinline__ float dist_group(float ax, float ay, float az, float bx, float by, float bz,
+                                            const float* L) {
+    float dx = fsub(ax, bx), dy = fsub(ay, by), dz = fsub(az, bz);
+    dx = ffma(-fast_round(fdiv(dx, L[0])), L[0], dx);
+    dy = ffma(-fast_round(fdiv(dy, L[1])), L[1], dy);
+    dz = ffma(-fast_round(fdiv(dz, L[2])), L[2], dz);
+    float s = fmul(dx, dx);
+    s = ffma(dy, dy, s);
+    s = ffma(dz, dz, s);
+    return fsqrt(s);
+}
+
+// Clustering distance: the reference's host distanceP (unfused), used by the
+// pose clustering of gcmc/cpp/gcmc_move_add.h:129 and gcmc_move_trn.h:180.
+__device__ __forceinline__ float dist_host(float ax, float ay, float az, float bx, float by, float bz,
+                                           const float* L) {
+    float dx = fsub(ax, bx), dy = fsub(ay, by), dz = fsub(az, bz);
+    dx = fsub(dx, fmul(fast_round(fdiv(dx, L[0])), L[0]));
+    dy = fsub(dy, fmul(fast_round(fdiv(dy, L[1])), L[1]));
+    dz = fsub(dz, fmul(fast_round(fdiv(dz, L[2])), L[2]));
+    float s = fadd(fmul(dx, dx), fmul(dy, dy));
+    s = fadd(s, fmul(dz, dz));
+    return fsqrt(s);
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter (step, index,
+// purpose<<16 | draw, 0), key (seed, replica).
+// ---------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                     uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    return {c0, c1, c2, c3};
+}
+
+__device__ __forceinline__ U4 rng(uint32_t seed, uint32_t replica, uint32_t step, uint32_t index,
+                                  uint32_t purpose, uint32_t draw) {
+    return philox(step, index, (purpose << 16) | draw, 0u, seed, replica);
+}
+
+__device__ __forceinline__ float u01_oc(uint32_t x) { return fmul(__uint2float_rn((x >> 8) + 1u), 5.9604644775390625e-08f); }
+__device__ __forceinline__ float u01_co(uint32_t x) { return fmul(__uint2float_rn(x >> 8), 5.9604644775390625e-08f); }
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    unsigned long long m = ((unsigned long long)(a >> 5) << 26) | (unsigned long long)(b >> 6);
+    return (double)m * 1.1102230246251565e-16;
+}
+__device__ __forceinline__ double u53_open(uint32_t a, uint32_t b) {
+    unsigned long long m = ((unsigned long long)(a >> 5) << 26) | (unsigned long long)(b >> 6);
+    return ((double)m + 0.5) * 1.1102230246251565e-16;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic sin/cos: reduction by pi/2 with a two-part constant, then the
+// Taylor polynomials of sin (through r^9) and cos (through r^10) on
+// |r| <= pi/4; absolute error below 4e-7 on [-2pi, 2pi].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void det_sincos(float x, float& s_out, float& c_out) {
+    const float two_over_pi = 0.636619772367581343f;
+    const float pio2_hi = 1.57079637050628662109375f;
+    const float pio2_lo = -4.37113900018624283e-8f;
+    float kf = rintf(fmul(x, two_over_pi));
+    float r = ffma(-kf, pio2_hi, x);
+    r = ffma(-kf, pio2_lo, r);
+    float r2 = fmul(r, r);
+    float ps = ffma(r2, 2.75573192239858925e-6f, -1.98412698412698413e-4f);
+    ps = ffma(r2, ps, 8.33333333333333333e-3f);
+    ps = ffma(r2, ps, -1.66666666666666667e-1f);
+    float sr = ffma(fmul(r, r2), ps, r);
+    float pc = ffma(r2, -2.75573192239858925e-7f, 2.48015873015873016e-5f);
+    pc = ffma(r2, pc, -1.38888888888888889e-3f);
+    pc = ffma(r2, pc, 4.16666666666666667e-2f);
+    pc = ffma(r2, pc, -0.5f);
+    float cr = ffma(r2, pc, 1.0f);
+    int q = __float2int_rz(kf) & 3;
+    float s, c;
+    if (q == 0) { s = sr; c = cr; }
+    else if (q == 1) { s = cr; c = -sr; }
+    else if (q == 2) { s = -sr; c = -cr; }
+    else { s = -cr; c = sr; }
+    s_out = s;
+    c_out = c;
+}
+
+struct Mat3 { float m[3][3]; };
+
+// Rodrigues rotation about a (normalised here) by the angle with (sn, cs);
+// gcmc/cpp/gcmc_energy.h:39-58 with the fused form fixed.
+__device__ __forceinline__ Mat3 rodrigues(float a0, float a1, float a2, float sn, float cs) {
+    float nn = fmul(a0, a0);
+    nn = ffma(a1, a1, nn);
+    nn = ffma(a2, a2, nn);
+    float norm = fsqrt(nn);
+    a0 = fdiv(a0, norm); a1 = fdiv(a1, norm); a2 = fdiv(a2, norm);
+    float C = fsub(1.0f, cs);
+    Mat3 R;
+    R.m[0][0] = ffma(fmul(a0, a0), C, cs);
+    R.m[0][1] = ffma(fmul(a0, a1), C, -fmul(a2, sn));
+    R.m[0][2] = ffma(fmul(a0, a2), C, fmul(a1, sn));
+    R.m[1][0] = ffma(fmul(a1, a0), C, fmul(a2, sn));
+    R.m[1][1] = ffma(fmul(a1, a1), C, cs);
+    R.m[1][2] = ffma(fmul(a1, a2), C, -fmul(a0, sn));
+    R.m[2][0] = ffma(fmul(a2, a0), C, -fmul(a1, sn));
+    R.m[2][1] = ffma(fmul(a2, a1), C, fmul(a0, sn));
+    R.m[2][2] = ffma(fmul(a2, a2), C, cs);
+    return R;
+}
+
+// Uniform random rotation from three uniforms (Shoemake, Graphics Gems III, 1992).
+__device__ __forceinline__ Mat3 shoemake(float u1, float u2, float u3) {
+    float s2, c2, s3, c3;
+    det_sincos(fmul(u2, kTwoPiF), s2, c2);
+    det_sincos(fmul(u3, kTwoPiF), s3, c3);
+    float r1 = fsqrt(fsub(1.0f, u1)), r2 = fsqrt(u1);
+    float x = fmul(r1, s2), y = fmul(r1, c2), z = fmul(r2, s3), w = fmul(r2, c3);
+    float xx = fmul(x, x), yy = fmul(y, y), zz = fmul(z, z);
+    float xy = fmul(x, y), xz = fmul(x, z), yz = fmul(y, z), xw = fmul(x, w), yw = fmul(y, w), zw = fmul(z, w);
+    Mat3 R;
+    R.m[0][0] = fsub(1.0f, fmul(2.0f, fadd(yy, zz)));
+    R.m[0][1] = fmul(2.0f, fsub(xy, zw));
+    R.m[0][2] = fmul(2.0f, fadd(xz, yw));
+    R.m[1][0] = fmul(2.0f, fadd(xy, zw));
+    R.m[1][1] = fsub(1.0f, fmul(2.0f, fadd(xx, zz)));
+    R.m[1][2] = fmul(2.0f, fsub(yz, xw));
+    R.m[2][0] = fmul(2.0f, fsub(xz, yw));
+    R.m[2][1] = fmul(2.0f, fadd(yz, xw));
+    R.m[2][2] = fsub(1.0f, fmul(2.0f, fadd(xx, yy)));
+    return R;
+}
+
+// p' = R p in the accumulation order of gcmc/cpp/gcmc_energy.h:62-71, fused.
+__device__ __forceinline__ void rotate(const Mat3& R, float p0, float p1, float p2, float& o0, float& o1,
+                                       float& o2) {
+    float x = fmul(p0, R.m[0][0]); x = ffma(p1, R.m[0][1], x); x = ffma(p2, R.m[0][2], x);
+    float y = fmul(p0, R.m[1][0]); y = ffma(p1, R.m[1][1], y); y = ffma(p2, R.m[1][2], y);
+    float z = fmul(p0, R.m[2][0]); z = ffma(p1, R.m[2][1], z); z = ffma(p2, R.m[2][2], z);
+    o0 = x; o1 = y; o2 = z;
+}
+
+// Keyed permutation of [0,n) (4-round Feistel on 2h bits, cycle walking;
+// round function = the MurmurHash3 32-bit finaliser).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ int perm_slot(const U4& rk, int h, int i, int n) {
+    uint32_t mask = (1u << h) - 1u;
+    uint32_t x = (uint32_t)i;
+    do {
+        uint32_t Lh = x >> h, Rh = x & mask;
+        uint32_t nl;
+        nl = Rh; Rh = Lh ^ (fmix32(Rh ^ rk.x) & mask); Lh = nl;
+        nl = Rh; Rh = Lh ^ (fmix32(Rh ^ rk.y) & mask); Lh = nl;
+        nl = Rh; Rh = Lh ^ (fmix32(Rh ^ rk.z) & mask); Lh = nl;
+        nl = Rh; Rh = Lh ^ (fmix32(Rh ^ rk.w) & mask); Lh = nl;
+        x = (Lh << h) | Rh;
+    } while (x >= (uint32_t)n);
+    return (int)x;
+}
+__host__ __device__ __forceinline__ int perm_bits(int n) {
+    int h = 1;
+    while ((1u << (2 * h)) < (uint32_t)n) ++h;
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// device-resident state
+// ---------------------------------------------------------------------------
+struct FragDev {
+    int startRes, maxNum, confBias, nsites;
+    double B;                  // beta*muex_eff + ln(V*conc*6.023e-4)
+    float4 site[kMaxSites];    // template x, y, z, charge
+    int stype[kMaxSites];      // template type
+};
+
+struct StepDesc {
+    int step;      // step index this descriptor describes
+    int move;      // MV_*
+    int ftype;
+    int k;         // poses
+    int n;         // totalNum at the start of the step
+    int nvar;      // 1, or 2 for translate/rotate (new, old)
+    int nslab;     // z-slabs per pose
+    int nw;        // neighbour-row words (0 = no clustering)
+    int items;     // k * nvar * nslab
+    int del_slot;
+    int perm_h;
+    int pad;
+    U4 perm_key;
+};
+
+struct RepDev {
+    // geometry and physics
+    float L[3], start[3];
+    float invLc[3];
+    int nc[3];          // cells per axis
+    int span[3];        // cells visited per axis (min(2R+1, nc))
+    int range;          // R
+    int cap;            // cell capacity
+    float cutoff, grid_dx, trn_step, rot_max;
+    double lncav;
+    int proposal;
+    int pair_image;     // 1: per-pair minimum image (small boxes); 0: per-group image shift
+    float invL[3];
+    int nfixed, ntypes, ffY, G;
+    int mcsteps;
+    uint32_t seed, replica;
+    int run_end;        // steps below this index are executed
+    int log_cap, log_kmax;
+    // state
+    float4* xyzq;       // atom x, y, z, charge
+    int* atype;         // atom type (column of the LJ table)
+    float4* gcen;       // group centre
+    int2* gspan;        // (atomStart, atomNum)
+    int* cell_count;
+    int* cell_ent;      // [ncell * cap] group ids
+    int* gcell;         // [ngroups] cell*cap + position, or -1
+    float4* grid;       // insertion base points
+    float2* lj;         // [ffX * ffY] (100*sigma^2 [nm^2 -> A^2], 4*eps)
+    const int* moves;
+    FragDev* frag;
+    int* totalNum;      // [ntypes]
+    // per-step scratch
+    StepDesc* desc;
+    float4* pcen;       // [kMaxPoses] pose centres (w unused)
+    int* pslot;         // [kMaxPoses]
+    double* epart;      // [kMaxPoses * 2 * nslab_max]
+    uint32_t* nbr;      // [kMaxPoses * kMaxWords]
+    // logs and counters
+    gcmc_step_log* log;
+    double* logE;
+    unsigned long long* counters;  // steps, poses, pairs
+    int* err;
+};
+
+__device__ __forceinline__ int wrapi(int c, int n) {
+    c %= n;
+    return c < 0 ? c + n : c;
+}
+__device__ __forceinline__ int cell_coord(float x, float start, float invLc, int nc) {
+    return wrapi(__float2int_rd(fmul(fsub(x, start), invLc)), nc);
+}
+__device__ __forceinline__ int cell_of(const RepDev& R, float x, float y, float z) {
+    int cx = cell_coord(x, R.start[0], R.invLc[0], R.nc[0]);
+    int cy = cell_coord(y, R.start[1], R.invLc[1], R.nc[1]);
+    int cz = cell_coord(z, R.start[2], R.invLc[2], R.nc[2]);
+    return (cz * R.nc[1] + cy) * R.nc[0] + cx;
+}
+
+// Centre of insertion pose i (gcmc/cpp/gcmc_energy.h:82-93): grid point + U(0,1]*dx.
+__device__ __forceinline__ void insert_centre(const RepDev& R, int step, int i, float& x, float& y,
+                                              float& z) {
+    U4 r0 = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 0);
+    int g = (int)(r0.x % (uint32_t)R.G);
+    float4 gp = R.grid[g];
+    x = fadd(fmul(u01_oc(r0.y), R.grid_dx), gp.x);
+    y = fadd(fmul(u01_oc(r0.z), R.grid_dx), gp.y);
+    z = fadd(fmul(u01_oc(r0.w), R.grid_dx), gp.z);
+}
+
+__device__ __forceinline__ Mat3 insert_rotation(const RepDev& R, int step, int i) {
+    U4 r1 = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 1);
+    if (R.proposal == 0) {
+        float sn, cs;
+        det_sincos(fmul(u01_oc(r1.w), kTwoPiF), sn, cs);
+        return rodrigues(u01_oc(r1.x), u01_oc(r1.y), u01_oc(r1.z), sn, cs);
+    }
+    return shoemake(u01_co(r1.x), u01_co(r1.y), u01_co(r1.z));
+}
+
+// Translate shift of pose i with the box wrap of gcmc/cpp/gcmc_move_trn.h:57-66.
+__device__ __forceinline__ float trn_shift(const RepDev& R, uint32_t r, int axis, float c) {
+    float sh = R.proposal == 0 ? fmul(u01_oc(r), R.grid_dx) : fmul(fsub(u01_co(r), 0.5f), R.trn_step);
+    float hi = fadd(R.L[axis], R.start[axis]);
+    if (fadd(c, sh) > hi) sh = fsub(sh, R.L[axis]);
+    if (fadd(c, sh) < R.start[axis]) sh = fadd(sh, R.L[axis]);
+    return sh;
+}
+
+__device__ __forceinline__ Mat3 move_rotation(const RepDev& R, const U4& r) {
+    if (R.proposal == 0) {
+        float sn, cs;
+        det_sincos(fmul(u01_oc(r.w), kTwoPiF), sn, cs);
+        return rodrigues(u01_oc(r.x), u01_oc(r.y), u01_oc(r.z), sn, cs);
+    }
+    float z = fsub(fmul(2.0f, u01_co(r.x)), 1.0f);
+    float sp, cp;
+    det_sincos(fmul(u01_co(r.y), kTwoPiF), sp, cp);
+    float rxy = fsqrt(fmaxf(0.0f, fsub(1.0f, fmul(z, z))));
+    float theta = fmul(R.rot_max, fsub(fmul(2.0f, u01_co(r.z)), 1.0f));
+    float sn, cs;
+    det_sincos(theta, sn, cs);
+    return rodrigues(fmul(rxy, cp), fmul(rxy, sp), z, sn, cs);
+}
+
+}  // namespace gcmc

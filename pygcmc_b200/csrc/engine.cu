@@ -1,0 +1,698 @@
+// Host engine and C ABI (include/gcmc_b200.h).
+//
+// A context owns the device-resident state of nrep independent replicas
+// (structure-of-arrays, float4 atoms and group centres, a cell grid over group
+// centres) and a CUDA graph of `kGraphSteps` MC steps; each step is one
+// k_energy launch (every replica's pose items) and one k_accept launch (one
+// CTA per replica) that also prepares the next step, so the whole step loop
+// runs without host round trips.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "accept.cuh"
+
+using namespace gcmc;
+
+namespace {
+
+constexpr int kGraphSteps = 32;
+constexpr int kMaxRep = 256;
+thread_local int g_last_status = GCMC_OK;
+
+struct RepHost {
+    int natoms = 0, ngroups = 0, ncell = 0, cap = 0, ntypes = 0, G = 0, ffX = 0, ffY = 0, mcsteps = 0;
+    int nslab = 0, log_cap = 0, log_kmax = 0;
+    int host_end = 0;
+    std::vector<int> startRes, maxNum, moves_host;
+    // device allocations (owned)
+    float4* xyzq = nullptr;
+    int* atype = nullptr;
+    float4* gcen = nullptr;
+    int2* gspan = nullptr;
+    int* cell_count = nullptr;
+    int* cell_ent = nullptr;
+    int* gcell = nullptr;
+    float4* grid = nullptr;
+    float2* lj = nullptr;
+    int* moves = nullptr;
+    FragDev* frag = nullptr;
+    int* totalNum = nullptr;
+    StepDesc* desc = nullptr;
+    float4* pcen = nullptr;
+    int* pslot = nullptr;
+    double* epart = nullptr;
+    uint32_t* nbr = nullptr;
+    gcmc_step_log* log = nullptr;
+    double* logE = nullptr;
+    unsigned long long* counters = nullptr;
+    int* err = nullptr;
+};
+
+}  // namespace
+
+struct gcmc_ctx {
+    int nrep = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<RepHost> reps;
+    std::vector<RepDev> repdev;
+    RepDev* d_reps = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int gridE = 0;
+};
+
+namespace {
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            std::fprintf(stderr, "gcmc_b200: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+            return GCMC_ERR_CUDA;                                                       \
+        }                                                                               \
+    } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc((void**)p, n * sizeof(T)));
+    return GCMC_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+void free_rep(RepHost& h) {
+    dfree(h.xyzq); dfree(h.atype); dfree(h.gcen); dfree(h.gspan); dfree(h.cell_count); dfree(h.cell_ent);
+    dfree(h.gcell); dfree(h.grid); dfree(h.lj); dfree(h.moves); dfree(h.frag); dfree(h.totalNum);
+    dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
+    dfree(h.logE); dfree(h.counters); dfree(h.err);
+}
+
+// Host copy of the device cell index function (floor((x - start) * invLc) mod nc),
+// used only to size the cell capacity.
+int host_cell(float x, float start, float invLc, int nc) {
+    volatile float d = x - start;
+    volatile float f = d * invLc;
+    int c = (int)std::floor((float)f);
+    c %= nc;
+    return c < 0 ? c + nc : c;
+}
+
+int validate(const gcmc_replica_in& in) {
+    const InfoStruct* I = in.info;
+    if (!I || !in.fragmentInfo || !in.residueInfo || !in.atomInfo || !in.ff) return GCMC_ERR_ARG;
+    if (I->fragTypeNum < 1 || I->totalResNum < 0 || I->totalAtomNum < 0 || I->mcsteps < 0) return GCMC_ERR_ARG;
+    if (I->mcsteps > 0 && !in.moveArray) return GCMC_ERR_ARG;
+    if (!(I->cutoff > 0.0f) || !(I->grid_dx > 0.0f)) return GCMC_ERR_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!(I->cryst[d] > 0.0f)) return GCMC_ERR_ARG;
+    if (I->ffXNum < 1 || I->ffYNum < 1) return GCMC_ERR_ARG;
+    if (I->totalAtomNum >= (1 << 26) || I->totalResNum >= (1 << 26)) return GCMC_ERR_LIMIT;
+    const AtomArray* F = in.fragmentInfo;
+    const residue* R = in.residueInfo;
+    int prev_end = F[0].startRes;
+    if (prev_end < 0) return GCMC_ERR_ARG;
+    bool any_insert = false;
+    for (int t = 0; t < I->fragTypeNum; ++t) {
+        const AtomArray& f = F[t];
+        if (f.num_atoms < 1 || f.num_atoms > kMaxSites) return GCMC_ERR_LIMIT;
+        if (f.confBias < 1) return GCMC_ERR_ARG;
+        if (f.confBias > kMaxPoses) return GCMC_ERR_LIMIT;
+        if (f.totalNum < 0 || f.maxNum < f.totalNum) return GCMC_ERR_ARG;
+        if (f.startRes != prev_end || f.startRes + f.maxNum > I->totalResNum) return GCMC_ERR_ARG;
+        prev_end = f.startRes + f.maxNum;
+        for (int s = 0; s < f.num_atoms; ++s)
+            if (f.atoms[s].type < 0 || f.atoms[s].type >= I->ffXNum) return GCMC_ERR_ARG;
+        for (int j = 0; j < f.maxNum; ++j) {
+            const residue& r = R[f.startRes + j];
+            if (r.atomNum != f.num_atoms || r.atomStart < 0 || r.atomStart + r.atomNum > I->totalAtomNum)
+                return GCMC_ERR_ARG;
+        }
+        for (int j = 0; j < f.totalNum; ++j) {
+            const residue& r = R[f.startRes + j];
+            for (int s = 0; s < r.atomNum; ++s) {
+                int ty = in.atomInfo[r.atomStart + s].type;
+                if (ty < 0 || ty >= I->ffYNum) return GCMC_ERR_ARG;
+            }
+        }
+    }
+    for (int g = 0; g < F[0].startRes; ++g) {
+        const residue& r = R[g];
+        if (r.atomNum < 0 || r.atomStart < 0 || r.atomStart + r.atomNum > I->totalAtomNum) return GCMC_ERR_ARG;
+        for (int s = 0; s < r.atomNum; ++s) {
+            int ty = in.atomInfo[r.atomStart + s].type;
+            if (ty < 0 || ty >= I->ffYNum) return GCMC_ERR_ARG;
+        }
+    }
+    for (int s = 0; s < I->mcsteps; ++s) {
+        int mv = in.moveArray[s];
+        if (mv < 0 || mv >= 4 * I->fragTypeNum) return GCMC_ERR_ARG;
+        if ((mv & 3) == 0) any_insert = true;
+    }
+    if (any_insert && (I->totalGridNum < 1 || !in.grid)) return GCMC_ERR_ARG;
+    return GCMC_OK;
+}
+
+int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
+    const InfoStruct* I = in.info;
+    RepHost& h = ctx->reps[r];
+    RepDev& d = ctx->repdev[r];
+    std::memset(&d, 0, sizeof(d));
+    h.natoms = I->totalAtomNum;
+    h.ngroups = I->totalResNum;
+    h.ntypes = I->fragTypeNum;
+    h.G = I->totalGridNum;
+    h.ffX = I->ffXNum;
+    h.ffY = I->ffYNum;
+    h.mcsteps = I->mcsteps;
+
+    // geometry: cells of edge >= cutoff/R, with a 1e-4 margin so rounding in the
+    // cell index can never push an included group outside the +-R window
+    const int Rc = opt.cells_per_cutoff > 0 ? opt.cells_per_cutoff : 2;
+    for (int a = 0; a < 3; ++a) {
+        d.L[a] = I->cryst[a];
+        d.start[a] = I->startxyz[a];
+        int nc = (int)std::floor((double)I->cryst[a] * Rc / I->cutoff * (1.0 - 1e-4));
+        nc = std::max(1, nc);
+        d.nc[a] = nc;
+        d.invLc[a] = (float)nc / I->cryst[a];
+        d.span[a] = std::min(2 * Rc + 1, nc);
+    }
+    d.range = Rc;
+    h.nslab = d.span[2];
+    h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
+    d.cutoff = I->cutoff;
+    d.grid_dx = I->grid_dx;
+    d.trn_step = opt.trn_step;
+    d.rot_max = opt.rot_max;
+    d.proposal = opt.proposal;
+    d.lncav = std::log((double)I->cavityFactor);
+    d.nfixed = in.fragmentInfo[0].startRes;
+    d.ntypes = I->fragTypeNum;
+    d.ffY = I->ffYNum;
+    d.G = I->totalGridNum;
+    d.mcsteps = I->mcsteps;
+    d.seed = I->seed;
+    d.replica = opt.replica + (uint32_t)r;
+    d.run_end = 0;
+
+    // the per-group periodic image is exact when every pair of an included
+    // group lies within half a box: cutoff + group radius + fragment radius < L/2
+    double rg = 0.0, rf = 0.0;
+    for (int g = 0; g < d.nfixed; ++g) {
+        const residue& rs = in.residueInfo[g];
+        for (int s = 0; s < rs.atomNum; ++s) {
+            const Atom& a = in.atomInfo[rs.atomStart + s];
+            double dx = a.position[0] - rs.position[0], dy = a.position[1] - rs.position[1],
+                   dz = a.position[2] - rs.position[2];
+            rg = std::max(rg, std::sqrt(dx * dx + dy * dy + dz * dz));
+        }
+    }
+    for (int t = 0; t < h.ntypes; ++t) {
+        const AtomArray& f = in.fragmentInfo[t];
+        for (int s = 0; s < f.num_atoms; ++s) {
+            double x = f.atoms[s].position[0], y = f.atoms[s].position[1], z = f.atoms[s].position[2];
+            rf = std::max(rf, std::sqrt(x * x + y * y + z * z));
+        }
+    }
+    rf += 0.5;
+    const double reach = (double)I->cutoff + std::max(rg, rf) + rf;
+    d.pair_image = 0;
+    for (int a = 0; a < 3; ++a) {
+        d.invL[a] = 1.0f / I->cryst[a];
+        if (reach >= 0.5 * I->cryst[a]) d.pair_image = 1;
+    }
+
+    // cell capacity from the initial occupancy
+    std::vector<int> counts(h.ncell, 0);
+    auto cell_host = [&](const float* p) {
+        int cx = host_cell(p[0], d.start[0], d.invLc[0], d.nc[0]);
+        int cy = host_cell(p[1], d.start[1], d.invLc[1], d.nc[1]);
+        int cz = host_cell(p[2], d.start[2], d.invLc[2], d.nc[2]);
+        return (cz * d.nc[1] + cy) * d.nc[0] + cx;
+    };
+    int maxcount = 0;
+    for (int g = 0; g < d.nfixed; ++g) maxcount = std::max(maxcount, ++counts[cell_host(in.residueInfo[g].position)]);
+    for (int t = 0; t < h.ntypes; ++t)
+        for (int j = 0; j < in.fragmentInfo[t].totalNum; ++j)
+            maxcount = std::max(maxcount, ++counts[cell_host(in.residueInfo[in.fragmentInfo[t].startRes + j].position)]);
+    int cap = 32;
+    while (cap < 2 * maxcount + 16) cap *= 2;
+    if (cap > 4096) return GCMC_ERR_LIMIT;
+    h.cap = d.cap = cap;
+
+    // host-side SoA conversion
+    std::vector<float4> xyzq(std::max(1, h.natoms));
+    std::vector<int> atype(std::max(1, h.natoms));
+    for (int a = 0; a < h.natoms; ++a) {
+        const Atom& A = in.atomInfo[a];
+        xyzq[a] = make_float4(A.position[0], A.position[1], A.position[2], A.charge);
+        atype[a] = A.type;
+    }
+    std::vector<float4> gcen(std::max(1, h.ngroups));
+    std::vector<int2> gspan(std::max(1, h.ngroups));
+    for (int g = 0; g < h.ngroups; ++g) {
+        const residue& rs = in.residueInfo[g];
+        gcen[g] = make_float4(rs.position[0], rs.position[1], rs.position[2], 0.0f);
+        gspan[g] = make_int2(rs.atomStart, rs.atomNum);
+    }
+    std::vector<float4> grid(std::max(1, h.G));
+    for (int i = 0; i < h.G; ++i) grid[i] = make_float4(in.grid[3 * i], in.grid[3 * i + 1], in.grid[3 * i + 2], 0.0f);
+    std::vector<float2> lj((size_t)h.ffX * h.ffY);
+    for (size_t x = 0; x < lj.size(); ++x) {
+        float sigma = in.ff[2 * x], eps = in.ff[2 * x + 1];
+        lj[x] = make_float2(sigma * sigma * 100.0f, 4.0f * eps);  // gcmc_energy.h:128-130
+    }
+    std::vector<FragDev> frag(h.ntypes);
+    std::vector<int> tot(h.ntypes);
+    const double V = (double)I->cryst[0] * (double)I->cryst[1] * (double)I->cryst[2];
+    for (int t = 0; t < h.ntypes; ++t) {
+        const AtomArray& f = in.fragmentInfo[t];
+        FragDev& F = frag[t];
+        std::memset(&F, 0, sizeof(F));
+        F.startRes = f.startRes;
+        F.maxNum = f.maxNum;
+        F.confBias = f.confBias;
+        F.nsites = f.num_atoms;
+        double mu = (double)f.muex * (opt.muex_kcal ? kKcalToKJ : 1.0);
+        F.B = kBeta * mu + std::log(V * (double)f.conc * kMolesToMolecules);
+        for (int s = 0; s < f.num_atoms; ++s) {
+            F.site[s] = make_float4(f.atoms[s].position[0], f.atoms[s].position[1], f.atoms[s].position[2],
+                                    f.atoms[s].charge);
+            F.stype[s] = f.atoms[s].type;
+        }
+        tot[t] = f.totalNum;
+        h.startRes.push_back(f.startRes);
+        h.maxNum.push_back(f.maxNum);
+    }
+
+    int st;
+#define AL(ptr, n) if ((st = dalloc(&(ptr), (size_t)(n))) != GCMC_OK) return st
+    AL(h.xyzq, h.natoms); AL(h.atype, h.natoms); AL(h.gcen, h.ngroups); AL(h.gspan, h.ngroups);
+    AL(h.cell_count, h.ncell); AL(h.cell_ent, (size_t)h.ncell * cap); AL(h.gcell, h.ngroups);
+    AL(h.grid, h.G); AL(h.lj, lj.size()); AL(h.moves, h.mcsteps); AL(h.frag, h.ntypes);
+    AL(h.totalNum, h.ntypes); AL(h.desc, 1); AL(h.pcen, kMaxPoses); AL(h.pslot, kMaxPoses);
+    AL(h.epart, (size_t)kMaxPoses * 2 * h.nslab); AL(h.nbr, (size_t)kMaxPoses * kMaxWords);
+    AL(h.counters, 4); AL(h.err, 1);
+    h.log_cap = std::max(0, std::min(opt.log_steps, h.mcsteps));
+    h.log_kmax = std::max(1, std::min(opt.log_kmax > 0 ? opt.log_kmax : 1, kMaxPoses));
+    if (h.log_cap > 0) {
+        AL(h.log, h.log_cap);
+        AL(h.logE, (size_t)h.log_cap * h.log_kmax);
+    }
+#undef AL
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(h.xyzq, xyzq.data(), sizeof(float4) * h.natoms, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h.atype, atype.data(), sizeof(int) * h.natoms, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h.gcen, gcen.data(), sizeof(float4) * h.ngroups, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h.gspan, gspan.data(), sizeof(int2) * h.ngroups, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h.cell_count, 0, sizeof(int) * h.ncell, s));
+    CK(cudaMemsetAsync(h.gcell, 0xff, sizeof(int) * std::max(1, h.ngroups), s));
+    CK(cudaMemcpyAsync(h.grid, grid.data(), sizeof(float4) * std::max(1, h.G), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h.lj, lj.data(), sizeof(float2) * lj.size(), cudaMemcpyHostToDevice, s));
+    if (h.mcsteps > 0) {
+        CK(cudaMemcpyAsync(h.moves, in.moveArray, sizeof(int) * h.mcsteps, cudaMemcpyHostToDevice, s));
+        h.moves_host.assign(in.moveArray, in.moveArray + h.mcsteps);
+    }
+    CK(cudaMemcpyAsync(h.frag, frag.data(), sizeof(FragDev) * h.ntypes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h.totalNum, tot.data(), sizeof(int) * h.ntypes, cudaMemcpyHostToDevice, s));
+    StepDesc d0{};
+    d0.step = 0;
+    d0.move = MV_NONE;
+    CK(cudaMemcpyAsync(h.desc, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 4, s));
+    CK(cudaMemsetAsync(h.err, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
+
+    d.xyzq = h.xyzq; d.atype = h.atype; d.gcen = h.gcen; d.gspan = h.gspan;
+    d.cell_count = h.cell_count; d.cell_ent = h.cell_ent; d.gcell = h.gcell;
+    d.grid = h.grid; d.lj = h.lj; d.moves = h.moves; d.frag = h.frag; d.totalNum = h.totalNum;
+    d.desc = h.desc; d.pcen = h.pcen; d.pslot = h.pslot; d.epart = h.epart; d.nbr = h.nbr;
+    d.log = h.log; d.logE = h.logE; d.log_cap = h.log_cap; d.log_kmax = h.log_kmax;
+    d.counters = h.counters; d.err = h.err;
+    return GCMC_OK;
+}
+
+int build_graph(gcmc_ctx* ctx) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < kGraphSteps; ++s) {
+        k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);
+    }
+    CK(cudaStreamEndCapture(ctx->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    return GCMC_OK;
+}
+
+int destroy_impl(gcmc_ctx* ctx) {
+    if (!ctx) return GCMC_OK;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    for (auto& h : ctx->reps) free_rep(h);
+    if (ctx->d_reps) cudaFree(ctx->d_reps);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GCMC_OK;
+}
+
+int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, void* stream, gcmc_ctx** out) {
+    if (!out || !ins || nrep < 1) return GCMC_ERR_ARG;
+    if (nrep > kMaxRep) return GCMC_ERR_LIMIT;
+    *out = nullptr;
+    gcmc_options opt;
+    if (optp) opt = *optp; else gcmc_default_options(&opt);
+    if (opt.proposal < 0 || opt.proposal > 1) return GCMC_ERR_ARG;
+    for (int r = 0; r < nrep; ++r) {
+        int st = validate(ins[r]);
+        if (st != GCMC_OK) return st;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return GCMC_ERR_NODEVICE;
+    }
+    gcmc_ctx* ctx = new gcmc_ctx();
+    ctx->nrep = nrep;
+    cudaGetDevice(&ctx->device);
+    int st = GCMC_OK;
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return GCMC_ERR_CUDA;
+        }
+        ctx->own_stream = true;
+    }
+    ctx->reps.resize(nrep);
+    ctx->repdev.resize(nrep);
+    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
+    if (st == GCMC_OK) {
+        if (cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess ||
+            cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice,
+                            ctx->stream) != cudaSuccess)
+            st = GCMC_ERR_CUDA;
+    }
+    if (st == GCMC_OK) {
+        if (cudaFuncSetAttribute(k_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(AcceptSmem)) != cudaSuccess)
+            st = GCMC_ERR_CUDA;
+    }
+    if (st == GCMC_OK) {
+        int sms = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy, kWarpsE * 32, 0);
+        ctx->gridE = std::max(1, sms) * std::max(1, per_sm);
+        k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
+        if (cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
+    }
+    if (st == GCMC_OK) st = build_graph(ctx);
+    if (st == GCMC_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (st == GCMC_OK) {
+        int32_t err = 0;
+        gcmc_device_error(ctx, &err);
+        if (err) st = GCMC_ERR_DEVICE;
+    }
+    if (st != GCMC_OK) {
+        cudaGetLastError();
+        destroy_impl(ctx);
+        return st;
+    }
+    *out = ctx;
+    return GCMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gcmc_default_options(gcmc_options* opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->proposal = 0;
+    opt->muex_kcal = 0;
+    opt->trn_step = 1.0f;
+    opt->rot_max = 15.0f * 3.14159265358979f / 180.0f;
+    opt->replica = 0;
+    opt->cells_per_cutoff = 2;
+    opt->log_steps = 0;
+    opt->log_kmax = 1;
+}
+
+const char* gcmc_status_string(int status) {
+    switch (status) {
+        case GCMC_OK: return "ok";
+        case GCMC_ERR_CUDA: return "CUDA runtime error";
+        case GCMC_ERR_ARG: return "invalid or inconsistent input";
+        case GCMC_ERR_LIMIT: return "a size limit of the engine is exceeded";
+        case GCMC_ERR_DEVICE: return "the device raised an error flag";
+        case GCMC_ERR_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int gcmc_create(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* opt, void* stream,
+                gcmc_ctx** out) {
+    return create_impl(nrep, reps, opt, stream, out);
+}
+
+int gcmc_destroy(gcmc_ctx* ctx) { return destroy_impl(ctx); }
+
+void* gcmc_stream(gcmc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int gcmc_run(gcmc_ctx* ctx, int32_t nsteps) {
+    if (!ctx) return GCMC_ERR_ARG;
+    if (nsteps <= 0) return GCMC_OK;
+    int need = 0;
+    for (auto& h : ctx->reps) {
+        long long e = std::min<long long>((long long)h.host_end + nsteps, h.mcsteps);
+        need = std::max(need, (int)(e - h.host_end));
+        h.host_end = (int)e;
+    }
+    if (need == 0) return GCMC_OK;
+    k_set_run_end<<<(ctx->nrep + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, nsteps);
+    k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+    CK(cudaGetLastError());
+    for (int done = 0; done < need; done += kGraphSteps) CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+    return GCMC_OK;
+}
+
+int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms_accept, int32_t* move) {
+    if (!ctx || nsteps < 0) return GCMC_ERR_ARG;
+    if (nsteps == 0) return GCMC_OK;
+    const int first = ctx->reps[0].host_end;
+    int need = 0;
+    for (auto& h : ctx->reps) {
+        long long e = std::min<long long>((long long)h.host_end + nsteps, h.mcsteps);
+        need = std::max(need, (int)(e - h.host_end));
+        h.host_end = (int)e;
+    }
+    if (need == 0) return GCMC_OK;
+    k_set_run_end<<<(ctx->nrep + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, nsteps);
+    k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+    CK(cudaGetLastError());
+    std::vector<cudaEvent_t> ev(3 * (size_t)need);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int i = 0; i < need; ++i) {
+        CK(cudaEventRecord(ev[3 * i], ctx->stream));
+        k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
+        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        CK(cudaEventRecord(ev[3 * i + 2], ctx->stream));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < need; ++i) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+        if (ms_energy) ms_energy[i] = a;
+        if (ms_accept) ms_accept[i] = b;
+        if (move) {
+            const auto& mh = ctx->reps[0].moves_host;
+            move[i] = (first + i < (int)mh.size()) ? mh[first + i] : -1;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return GCMC_OK;
+}
+
+int gcmc_device_error(gcmc_ctx* ctx, int32_t* err) {
+    if (!ctx || !err) return GCMC_ERR_ARG;
+    int acc = 0;
+    for (auto& h : ctx->reps) {
+        int e = 0;
+        CK(cudaMemcpy(&e, h.err, sizeof(int), cudaMemcpyDeviceToHost));
+        acc |= e;
+    }
+    *err = acc;
+    return GCMC_OK;
+}
+
+int gcmc_sync(gcmc_ctx* ctx) {
+    if (!ctx) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    int32_t err = 0;
+    int st = gcmc_device_error(ctx, &err);
+    if (st) return st;
+    if (err) {
+        std::fprintf(stderr, "gcmc_b200: device error flags 0x%x\n", err);
+        return GCMC_ERR_DEVICE;
+    }
+    return GCMC_OK;
+}
+
+int gcmc_download(gcmc_ctx* ctx, int32_t rep, AtomArray* fragmentInfo, residue* residueInfo, Atom* atomInfo) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    RepHost& h = ctx->reps[rep];
+    std::vector<int> tot(h.ntypes);
+    CK(cudaMemcpy(tot.data(), h.totalNum, sizeof(int) * h.ntypes, cudaMemcpyDeviceToHost));
+    if (fragmentInfo)
+        for (int t = 0; t < h.ntypes; ++t) fragmentInfo[t].totalNum = tot[t];
+    if (residueInfo && h.ngroups > 0) {
+        std::vector<float4> gcen(h.ngroups);
+        CK(cudaMemcpy(gcen.data(), h.gcen, sizeof(float4) * h.ngroups, cudaMemcpyDeviceToHost));
+        for (int g = 0; g < h.ngroups; ++g) {
+            residueInfo[g].position[0] = gcen[g].x;
+            residueInfo[g].position[1] = gcen[g].y;
+            residueInfo[g].position[2] = gcen[g].z;
+        }
+    }
+    if (atomInfo && h.natoms > 0) {
+        std::vector<float4> xyzq(h.natoms);
+        std::vector<int> atype(h.natoms);
+        CK(cudaMemcpy(xyzq.data(), h.xyzq, sizeof(float4) * h.natoms, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(atype.data(), h.atype, sizeof(int) * h.natoms, cudaMemcpyDeviceToHost));
+        for (int a = 0; a < h.natoms; ++a) {
+            atomInfo[a].position[0] = xyzq[a].x;
+            atomInfo[a].position[1] = xyzq[a].y;
+            atomInfo[a].position[2] = xyzq[a].z;
+            atomInfo[a].charge = xyzq[a].w;
+            atomInfo[a].type = atype[a];
+        }
+    }
+    return GCMC_OK;
+}
+
+int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energies, int32_t max_steps,
+                  int32_t* n_steps) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    RepHost& h = ctx->reps[rep];
+    int n = std::min(std::min(max_steps, h.log_cap), h.host_end);
+    if (n_steps) *n_steps = n;
+    if (n <= 0) return GCMC_OK;
+    if (logs) CK(cudaMemcpy(logs, h.log, sizeof(gcmc_step_log) * n, cudaMemcpyDeviceToHost));
+    if (energies) CK(cudaMemcpy(energies, h.logE, sizeof(double) * (size_t)n * h.log_kmax, cudaMemcpyDeviceToHost));
+    return GCMC_OK;
+}
+
+int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, int64_t* pairs) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long c[4];
+    CK(cudaMemcpy(c, ctx->reps[rep].counters, sizeof(c), cudaMemcpyDeviceToHost));
+    if (steps) *steps = (int64_t)c[0];
+    if (poses) *poses = (int64_t)c[1];
+    if (pairs) *pairs = (int64_t)c[2];
+    return GCMC_OK;
+}
+
+int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float* site_q,
+                      const int32_t* site_type, int32_t nsites, const float* centres, const int32_t* self,
+                      int32_t nposes, double* out, int32_t* n_groups) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !xyz || !site_q || !site_type || !centres || !out) return GCMC_ERR_ARG;
+    if (nsites < 1 || nsites > kMaxSites) return GCMC_ERR_LIMIT;
+    if (nposes <= 0) return GCMC_OK;
+    RepHost& h = ctx->reps[rep];
+    for (int s = 0; s < nsites; ++s)
+        if (site_type[s] < 0 || site_type[s] >= h.ffX) return GCMC_ERR_ARG;
+    const int nslab = h.nslab;
+    float *dxyz = nullptr, *dq = nullptr, *dc = nullptr;
+    int *dt = nullptr, *dself = nullptr, *dng = nullptr;
+    double* dout = nullptr;
+    int st = GCMC_OK;
+    std::vector<int> selfv(nposes, -1);
+    if (self) std::copy(self, self + nposes, selfv.begin());
+    std::vector<double> part((size_t)nposes * nslab);
+    std::vector<int> ngp((size_t)nposes * nslab);
+    do {
+        if ((st = dalloc(&dxyz, (size_t)nposes * nsites * 3)) || (st = dalloc(&dq, nsites)) ||
+            (st = dalloc(&dt, nsites)) || (st = dalloc(&dc, (size_t)nposes * 3)) || (st = dalloc(&dself, nposes)) ||
+            (st = dalloc(&dout, (size_t)nposes * nslab)) || (st = dalloc(&dng, (size_t)nposes * nslab)))
+            break;
+        cudaStream_t s = ctx->stream;
+        if (cudaMemcpyAsync(dxyz, xyz, sizeof(float) * nposes * nsites * 3, cudaMemcpyHostToDevice, s) ||
+            cudaMemcpyAsync(dq, site_q, sizeof(float) * nsites, cudaMemcpyHostToDevice, s) ||
+            cudaMemcpyAsync(dt, site_type, sizeof(int) * nsites, cudaMemcpyHostToDevice, s) ||
+            cudaMemcpyAsync(dc, centres, sizeof(float) * nposes * 3, cudaMemcpyHostToDevice, s) ||
+            cudaMemcpyAsync(dself, selfv.data(), sizeof(int) * nposes, cudaMemcpyHostToDevice, s)) {
+            st = GCMC_ERR_CUDA;
+            break;
+        }
+        k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->d_reps + rep, dxyz, dq, dt, nsites, dc, dself,
+                                                              nposes, nslab, dout, dng);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(part.data(), dout, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s) ||
+            cudaMemcpyAsync(ngp.data(), dng, sizeof(int) * ngp.size(), cudaMemcpyDeviceToHost, s) ||
+            cudaStreamSynchronize(s)) {
+            st = GCMC_ERR_CUDA;
+            break;
+        }
+        for (int p = 0; p < nposes; ++p) {
+            double e = 0.0;
+            int ng = 0;
+            for (int z = 0; z < nslab; ++z) {
+                e += part[(size_t)p * nslab + z];
+                ng += ngp[(size_t)p * nslab + z];
+            }
+            out[p] = e;
+            if (n_groups) n_groups[p] = ng;
+        }
+    } while (0);
+    dfree(dxyz); dfree(dq); dfree(dt); dfree(dc); dfree(dself); dfree(dout); dfree(dng);
+    if (st == GCMC_OK) {
+        int32_t err = 0;
+        gcmc_device_error(ctx, &err);
+        if (err) st = GCMC_ERR_DEVICE;
+    }
+    return st;
+}
+
+int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo, Atom* atomInfo,
+                  const float* grid, const float* ff, const int* moveArray, const gcmc_options* opt) {
+    if (!info) return GCMC_ERR_ARG;
+    gcmc_replica_in in{info, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray};
+    gcmc_ctx* ctx = nullptr;
+    int st = create_impl(1, &in, opt, nullptr, &ctx);
+    if (st != GCMC_OK) return st;
+    st = gcmc_run(ctx, info->mcsteps);
+    if (st == GCMC_OK) st = gcmc_sync(ctx);
+    if (st == GCMC_OK) st = gcmc_download(ctx, 0, fragmentInfo, residueInfo, atomInfo);
+    destroy_impl(ctx);
+    return st;
+}
+
+void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo, Atom* atomInfo,
+                  const float* grid, const float* ff, const int* moveArray) {
+    g_last_status = gcmc_run_gcmc(info, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, nullptr);
+}
+
+int gcmc_last_status(void) { return g_last_status; }
+
+}  // extern "C"

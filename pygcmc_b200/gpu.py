@@ -1,0 +1,97 @@
+"""Drop-in replacement of pyGCMC's native module ``gcmc.gpu``.
+
+``runGCMC(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)``
+has the signature, argument meaning and in-place semantics of the reference
+binding (gcmc/cpp/gcmc.cpp:162-197, called from gcmc/python/gcmc.py:41-49):
+it runs ``SimInfo[0]['mcsteps']`` steps of ``moveArray`` and writes
+``fragmentInfo['totalNum']``, ``residueInfo`` and ``atomInfo`` back in place,
+returning ``None``.  Unlike the reference it checks the arrays first and raises
+(``TypeError``/``ValueError`` for bad arrays, :class:`GcmcError` for engine
+failures) instead of running on undefined input.
+"""
+import numpy as np
+
+from . import values as V
+from ._native import GcmcError, check, default_options, lib, ptr
+
+__all__ = ["runGCMC", "GcmcError", "validate_arrays"]
+
+
+def validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray):
+    """Dtype, contiguity and size checks against the sizes recorded in SimInfo."""
+    spec = [("SimInfo", SimInfo, V.Info_dtype), ("fragmentInfo", fragmentInfo, V.AtomArray_dtype),
+            ("residueInfo", residueInfo, V.Residue_dtype), ("atomInfo", atomInfo, V.Atom_dtype),
+            ("grid", grid, np.dtype(np.float32)), ("ff", ff, np.dtype(np.float32)),
+            ("moveArray", moveArray, np.dtype(np.int32))]
+    for name, a, dt in spec:
+        if not isinstance(a, np.ndarray):
+            raise TypeError(f"{name} must be a numpy array")
+        if a.dtype != dt:
+            raise TypeError(f"{name} has dtype {a.dtype}, expected {dt}")
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"{name} must be C-contiguous")
+    info = SimInfo[0]
+    need = [("fragmentInfo", fragmentInfo, int(info["fragTypeNum"])),
+            ("residueInfo", residueInfo, int(info["totalResNum"])),
+            ("atomInfo", atomInfo, int(info["totalAtomNum"])),
+            ("grid", grid, 3 * int(info["totalGridNum"])),
+            ("ff", ff, 2 * int(info["ffXNum"]) * int(info["ffYNum"])),
+            ("moveArray", moveArray, int(info["mcsteps"]))]
+    for name, a, n in need:
+        if a.size < n:
+            raise ValueError(f"{name} holds {a.size} entries, SimInfo requires {n}")
+
+
+def print_all_info(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray):
+    """The state dump printed when SimInfo['showInfo'] > 0 (gcmc/cpp/gcmc.cpp:16-156)."""
+    info = SimInfo[0]
+    print("\n\nPrinting InfoStruct:\n")
+    print(f"Mcsteps: {info['mcsteps']}\nCutoff: {info['cutoff']}\nGrid_dx: {info['grid_dx']}")
+    print("Startxyz: (%g, %g, %g)" % tuple(info["startxyz"]))
+    print("Cryst: (%g, %g, %g)" % tuple(info["cryst"]))
+    print(f"CavityFactor: {info['cavityFactor']}\nFragTypeNum: {info['fragTypeNum']}")
+    print(f"TotalGridNum: {info['totalGridNum']}\nTotalResNum: {info['totalResNum']}")
+    print(f"TotalAtomNum: {info['totalAtomNum']}")
+    print("\n\nPrinting FragmentInfo:\n")
+    for i, f in enumerate(fragmentInfo):
+        print(f"AtomArray {i + 1}:\nName: {f['name'].decode(errors='replace')}\nMuex: {f['muex']}")
+        print(f"Conc: {f['conc']}\nConfBias: {f['confBias']}\nMcTime: {f['mcTime']}\nStartRes: {f['startRes']}")
+        print(f"TotalNum: {f['totalNum']}\nMaxNum: {f['maxNum']}\nNum_atoms: {f['num_atoms']}")
+        for j in range(f["num_atoms"]):
+            a = f["atoms"][j]
+            print(f"Atom {j + 1}:\n  Position: ({a['position'][0]:g}, {a['position'][1]:g}, {a['position'][2]:g})"
+                  f"\t  Charge: {a['charge']:g}\t  Type: {a['type']}")
+        print()
+    print("\n\nPrinting Grid:\n")
+    for i in range(int(info["totalGridNum"])):
+        print(f"Grid {i + 1}: {grid[3 * i]:g}, {grid[3 * i + 1]:g}, {grid[3 * i + 2]:g}")
+    print("\n\nPrinting FF:\n")
+    X, Y = int(info["ffXNum"]), int(info["ffYNum"])
+    for i in range(X):
+        for j in range(Y):
+            k = i * Y + j
+            print(f"FF {i + 1}, {j + 1}:  sigma {ff[2 * k]:g},  epsilon {ff[2 * k + 1]:g}")
+    print("\n\nPrinting MoveArray:\n")
+    for i in range(int(info["mcsteps"])):
+        f, m = divmod(int(moveArray[i]), 4)
+        print(f"Move {i + 1}:\tFragType: {fragmentInfo[f]['name'].decode(errors='replace')}\tMoveType: {m}")
+
+
+def runGCMC(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, options=None):
+    """Run ``mcsteps`` GCMC steps on the GPU, updating the state arrays in place.
+
+    ``options`` (optional, not part of the reference signature) is a
+    :class:`pygcmc_b200._native.Options`; the default is the reference's
+    semantics (``proposal=0``, ``muex_kcal=0``).
+    """
+    validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
+    show = int(SimInfo[0]["showInfo"]) > 0
+    if show:
+        print_all_info(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
+    opt = options if options is not None else default_options()
+    st = lib().gcmc_run_gcmc(ptr(SimInfo), ptr(fragmentInfo), ptr(residueInfo), ptr(atomInfo), ptr(grid),
+                             ptr(ff), ptr(moveArray), __import__("ctypes").byref(opt))
+    check(st, "runGCMC")
+    if show:
+        print_all_info(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
+    return None

@@ -1,0 +1,170 @@
+"""CUDA engine vs the CPU oracle on the same seeded inputs (needs a B200).
+
+* pose energies: FP64 sums of FP32 pair terms on the GPU vs the oracle's FP64
+  restatement of calcEnergy, per pose within 1e-5 relative or 1e-4 kcal/mol
+  (relative to |E| for these poses), with bit-identical group-inclusion counts;
+* trajectories: the oracle replays the engine's logged energies; every step's
+  move, pose count, cluster count, accepts, first accepted pose and counts
+  must be identical, the oracle's own FP64 energies must agree with the
+  engine's within 1e-5 of the sum of |pair terms| (both energies' pairs for a
+  translate/rotate dE) or 1e-4 kcal/mol, and the final coordinates of every
+  occupied slot must be bit-identical.
+"""
+import numpy as np
+import pytest
+
+from conftest import energy_close
+
+pytestmark = pytest.mark.gpu
+
+LOG_KMAX = 1024
+LOG_FIELDS = ("step", "move", "ftype", "k", "n_before", "n_after", "n_clusters", "n_accept", "first_accept", "slot")
+
+
+def engine_trajectory(system, nsteps, **opt):
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, **opt)
+    with Engine(system.copy(), opts) as eng:
+        eng.run(nsteps)
+        eng.sync()
+        logs, E = eng.logs()
+        final = eng.download()
+        counters = eng.counters()
+    return logs, E, final, counters
+
+
+def occupied_atoms(s):
+    idx = []
+    for f in s.fragmentInfo:
+        for j in range(int(f["totalNum"])):
+            r = s.residueInfo[int(f["startRes"]) + j]
+            idx.extend(range(int(r["atomStart"]), int(r["atomStart"]) + int(r["atomNum"])))
+    return np.array(idx, dtype=np.int64)
+
+
+def occupied_res(s):
+    return np.concatenate([np.arange(int(f["startRes"]), int(f["startRes"]) + int(f["totalNum"]))
+                           for f in s.fragmentInfo])
+
+
+def check_trajectory(oracle, system, nsteps, proposal=0, muex_kcal=0):
+    logs_g, E_g, final_g, counters = engine_trajectory(system, nsteps, proposal=proposal, muex_kcal=muex_kcal)
+    assert len(logs_g) == nsteps
+    s_o = system.copy()
+    opts = oracle.options(proposal=proposal, muex_kcal=muex_kcal)
+    logs_o, E_o, SC = oracle.run(s_o, nsteps, opts=opts, kmax=LOG_KMAX, replay=E_g, want_scale=True)
+    for f in LOG_FIELDS:
+        bad = np.flatnonzero(logs_g[f] != logs_o[f])
+        assert bad.size == 0, (f, bad[:5], logs_g[bad[:3]], logs_o[bad[:3]])
+    mask = np.arange(LOG_KMAX)[None, :] < logs_g["k"][:, None]
+    ok = energy_close(E_g[mask], E_o[mask], SC[mask])
+    assert ok.all(), (np.flatnonzero(~ok)[:10], E_g[mask][~ok][:5], E_o[mask][~ok][:5])
+    # and the errors sit far inside the bound
+    rel = np.abs(E_g[mask] - E_o[mask]) / np.maximum(SC[mask], 1e-30)
+    assert rel.max() < 1e-6, rel.max()
+    assert (final_g.fragmentInfo["totalNum"] == s_o.fragmentInfo["totalNum"]).all()
+    a = occupied_atoms(s_o)
+    assert np.array_equal(final_g.atomInfo["position"][a], s_o.atomInfo["position"][a])
+    r = occupied_res(s_o)
+    assert np.array_equal(final_g.residueInfo["position"][r], s_o.residueInfo["position"][r])
+    assert counters["steps"] == nsteps
+    return logs_g
+
+
+def explicit_poses(oracle, system, per_type=64):
+    """Insertion poses of every type plus the current pose of occupied slots."""
+    out = []
+    for t, f in enumerate(system.fragmentInfo):
+        ns = int(f["num_atoms"])
+        xyz, cen, self_res = [], [], []
+        for i in range(per_type):
+            p, c = oracle.insert_pose(system, t, 5, i)
+            xyz.append(p)
+            cen.append(c)
+            self_res.append(-1)
+        for j in range(min(int(f["totalNum"]), per_type)):
+            r = system.residueInfo[int(f["startRes"]) + j]
+            a0 = int(r["atomStart"])
+            xyz.append(system.atomInfo["position"][a0:a0 + ns])
+            cen.append(r["position"])
+            self_res.append(int(f["startRes"]) + j)
+        out.append((t, np.array(xyz, np.float32), np.array(cen, np.float32), np.array(self_res, np.int32),
+                    f["atoms"]["charge"][:ns].copy(), f["atoms"]["type"][:ns].copy()))
+    return out
+
+
+@pytest.mark.parametrize("which", ["water_small", "protein_small"])
+def test_pose_energies_match_oracle(request, oracle_lib, which):
+    from pygcmc_b200.engine import Engine
+    s = request.getfixturevalue(which)
+    with Engine(s.copy()) as eng:
+        for t, xyz, cen, self_res, q, ty in explicit_poses(oracle_lib, s):
+            e_g, ng_g = eng.energy_poses(xyz, q, ty, cen, self_res)
+            e_o, ng_o, _, l1 = oracle_lib.energy_batch(s, xyz, q, ty, cen, self_res, mode=0, want_l1=True)
+            assert np.array_equal(ng_g, ng_o), (t, np.flatnonzero(ng_g != ng_o)[:5])
+            ok = energy_close(e_g, e_o, l1) & energy_close(e_g, e_o)
+            assert ok.all(), (t, e_g[~ok][:5], e_o[~ok][:5])
+
+
+def test_trajectory_protein_reference_mode(oracle_lib, protein_small):
+    logs = check_trajectory(oracle_lib, protein_small, 240)
+    assert (logs["n_accept"] > 0).any()
+    assert set(np.unique(logs["move"])) == {0, 1, 2, 3}
+
+
+def test_trajectory_water_reference_mode(oracle_lib, water_small):
+    check_trajectory(oracle_lib, water_small, 120)
+
+
+def test_trajectory_protein_symmetric_mode(oracle_lib, protein_small):
+    check_trajectory(oracle_lib, protein_small, 160, proposal=1, muex_kcal=1)
+
+
+def test_runGCMC_dropin_matches_engine(protein_small):
+    """gpu.runGCMC (drop-in for gcmc.gpu.runGCMC) == an Engine run of mcsteps steps."""
+    from pygcmc_b200.gpu import runGCMC
+    s = protein_small.copy()
+    n = int(s.SimInfo[0]["mcsteps"])
+    assert runGCMC(*s.arrays()) is None
+    _, _, final, _ = engine_trajectory(protein_small, n)
+    assert (s.fragmentInfo["totalNum"] == final.fragmentInfo["totalNum"]).all()
+    a = occupied_atoms(s)
+    assert np.array_equal(s.atomInfo["position"][a], final.atomInfo["position"][a])
+
+
+def test_replicas_in_one_context_match_single(protein_small, water_small):
+    """Several replicas advanced together give each replica's solo result."""
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    systems = [protein_small.copy(), water_small.copy(), protein_small.copy()]
+    n = 100
+    with Engine([x.copy() for x in systems], default_options()) as eng:
+        eng.run(n)
+        eng.sync()
+        finals = [eng.download(r) for r in range(3)]
+    for r, s in enumerate(systems):
+        solo = Engine(s.copy(), default_options(replica=r))
+        solo.run(n)
+        solo.sync()
+        f1 = solo.download()
+        solo.close()
+        assert (f1.fragmentInfo["totalNum"] == finals[r].fragmentInfo["totalNum"]).all()
+        a = occupied_atoms(f1)
+        assert np.array_equal(f1.atomInfo["position"][a], finals[r].atomInfo["position"][a])
+
+
+def test_run_in_chunks_equals_one_run(protein_small):
+    from pygcmc_b200.engine import Engine
+    with Engine(protein_small.copy()) as e1:
+        e1.run(150)
+        e1.sync()
+        f1 = e1.download()
+    with Engine(protein_small.copy()) as e2:
+        for n in (7, 33, 1, 64, 45):
+            e2.run(n)
+        e2.sync()
+        f2 = e2.download()
+    assert (f1.fragmentInfo["totalNum"] == f2.fragmentInfo["totalNum"]).all()
+    a = occupied_atoms(f1)
+    assert np.array_equal(f1.atomInfo["position"][a], f2.atomInfo["position"][a])
