@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark: MC trial moves/s of the GCMC hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one replica per GPU): the synthetic protein system -- 6000 fixed
+atoms of a confined random-walk chain in a 64 A periodic box, eight rigid
+fragments of 4-12 sites starting at their bulk-concentration counts, confBias
+1000, cutoff 12 A, the reference's move schedule and acceptance semantics.
+A bench step is CHUNK MC steps (moveArray entries); `value` is MC steps/s with
+the state resident on the GPU, `e2e` the same through the runGCMC drop-in
+with host arrays (upload, run, download inside the timed region).
+
+--impl reference times the reference's own runGCMC_cuda (built unmodified
+from its sources into oracle/_ref) on the same workload.
+Under torchrun every rank runs an independent replica (its own seed) on its
+own GPU; times are the max over ranks ("replicas only", weak scaling).
+"""
+import argparse
+import contextlib
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC trial moves/sec on 1 B200: batched/force-bias vs plain, ΔE rel err ≤1e-5"
+FLOPS_PER_PAIR = 19  # fixed algorithmic count per atom-site pair
+WORKLOAD = ("synthetic protein: 6000-atom random-walk chain in a 24 A sphere, 64 A periodic box, "
+            "8 rigid fragments (4-12 sites) at bulk counts, confBias 1000, cutoff 12 A, reference semantics")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_system(seed, mcsteps):
+    from pygcmc_b200 import system as S
+    return S.protein_system(seed=seed, mcsteps=mcsteps)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(gpu_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Silence C-level stdout (the reference prints a newline per call)."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    try:
+        yield
+    finally:
+        os.dup2(saved, 1)
+        os.close(null)
+        os.close(saved)
+
+
+def cpu_baseline(seed, budget_s=15.0):
+    """The CPU oracle (C restatement, OpenMP over trial poses) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    s = make_system(seed, 4000)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    oracle.run(s, 20, step0=0, threads=threads, want_energies=False)
+    dt = time.perf_counter() - t0
+    n = int(min(2000, max(20, budget_s / max(dt / 20, 1e-6))))
+    t0 = time.perf_counter()
+    oracle.run(s, n, step0=20, threads=threads, want_energies=False)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "moves/s", "cores": threads, "kind": "port",
+            "sample": f"MC steps 20..{20 + n} of the same workload on the oracle (FP64, OpenMP over poses)"}
+
+
+def nominal_fp32_tflops(sm_max_mhz):
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    return sms * 128 * 2 * sm_max_mhz * 1e6 / 1e12, sms
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "k_energy_cfg1.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    from pygcmc_b200.gpu import runGCMC
+    torch.cuda.set_device(local)
+    chunk = args.chunk
+    seed = args.seed + rank
+    prof_steps = 256
+    total = (args.warmup + args.steps) * chunk + prof_steps + 64
+    sysm = make_system(seed, total)
+    eng = Engine(sysm.copy(), default_options(cells_per_cutoff=args.cells))
+    stream = torch.cuda.ExternalStream(eng.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    for _ in range(args.warmup):
+        eng.run(chunk)
+    eng.sync()
+    c0 = eng.counters()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    for a, b in evs:
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a.record(stream)
+        eng.run(chunk)
+        b.record(stream)
+    eng.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    ms = max_over_ranks(ms, ws)
+    barrier(ws)
+    c1 = eng.counters()
+    # live per-kernel durations on the same trajectory (kernels launched one by one)
+    te, ta, mv = eng.run_profiled(prof_steps)
+    c2 = eng.counters()
+    eng.sync()
+    eng.close()
+    # end to end through the drop-in API with host arrays
+    e2e_state = sysm.copy()
+    e2e_chunk = args.e2e_chunk
+    h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * e2e_chunk
+    d2h = e2e_state.fragmentInfo.nbytes + e2e_state.residueInfo.nbytes + e2e_state.atomInfo.nbytes
+    info = e2e_state.SimInfo
+    info[0]["mcsteps"] = e2e_chunk
+    moves = e2e_state.moveArray
+    runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
+            e2e_state.ff, np.ascontiguousarray(moves[:e2e_chunk]))  # warm-up call
+    e2e_times = []
+    for k in range(args.e2e_reps):
+        info[0]["seed"] = (seed * 7 + k) & 0xFFFFFFFF
+        mv = np.ascontiguousarray(moves[(k + 1) * e2e_chunk:(k + 2) * e2e_chunk])
+        barrier(ws)
+        t0 = time.perf_counter()
+        runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
+                e2e_state.ff, mv)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(e2e_times) * 1e3, ws) / 1e3
+    steps_all = args.steps * chunk * ws
+    value = steps_all / (ms / 1e3)
+    e2e_val = args.e2e_reps * e2e_chunk * ws / e2e_s
+    pairs_prof = c2["pairs"] - c1["pairs"]
+    e_ms = float(te.sum())
+    a_ms = float(ta.sum())
+    sm_max = (clk or {}).get("sm_max_mhz") or 1965.0
+    peak, sms = nominal_fp32_tflops(sm_max)
+    achieved = pairs_prof * FLOPS_PER_PAIR / (e_ms / 1e3) / 1e12
+    traffic = load_traffic()
+    launches = args.steps * (2 + 2 * 32 * ((chunk + 31) // 32))
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair terms, fp64 sums/acceptance",
+        "data": "synthetic (seeded generator; no public dataset)",
+        "config": {"workload": WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
+                   "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
+                   "cells_per_cutoff": args.cells},
+        "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": e2e_chunk,
+                "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
+        "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies)",
+                     "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 5),
+                     "peak_source": f"nominal FP32: {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                                    "(MEASURED_PEAKS.json has no FP32 figure)",
+                     "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_prof / prof_steps,
+                     "avg_launch_us": e_ms / prof_steps * 1e3,
+                     "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3),
+                     "accept_kernel_avg_us": a_ms / prof_steps * 1e3},
+        "pose_energies_per_s": round((c1["poses"] - c0["poses"]) / (ms / 1e3), 1),
+        "pairs_per_s": round((c1["pairs"] - c0["pairs"]) / (ms / 1e3), 1),
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(seed)
+    return out
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return None
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libgcmc_ref.so")
+    if not os.path.exists(lib_path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libgcmc_ref.so not built (make -C oracle ref)"}
+    import torch
+    torch.cuda.set_device(local)
+    L = ctypes.CDLL(lib_path)
+    L.runGCMC_cuda.restype = None
+    L.runGCMC_cuda.argtypes = [ctypes.c_void_p] * 7
+    chunk = args.ref_chunk
+    seed = args.seed
+    s = make_system(seed, (args.warmup + args.steps + 2) * chunk + 16)
+    info = s.SimInfo.copy()
+    moves = s.moveArray
+    skipped = [0]
+
+    def call(mv):
+        info[0]["mcsteps"] = len(mv)
+        with quiet_stdout():
+            L.runGCMC_cuda(info.ctypes.data, s.fragmentInfo.ctypes.data, s.residueInfo.ctypes.data,
+                           s.atomInfo.ctypes.data, s.grid.ctypes.data, s.ff.ctypes.data, mv.ctypes.data)
+
+    def run_range(a, b):
+        """Steps [a, b) in slices; a delete on an empty fragment type (where the
+        reference divides by zero, gcmc_move_del.h:316) is skipped."""
+        calls = 0
+        pos = a
+        while pos < b:
+            tot = s.fragmentInfo["totalNum"].astype(np.int64).copy()
+            q = pos
+            while q < b:
+                f, m = divmod(int(moves[q]), 4)
+                if m == 1:
+                    if tot[f] <= 0:
+                        break
+                    tot[f] -= 1
+                q += 1
+            if q == pos:
+                skipped[0] += 1
+                pos += 1
+                continue
+            info[0]["seed"] = (seed * 131 + pos) & 0xFFFFFFFF
+            call(np.ascontiguousarray(moves[pos:q]))
+            calls += 1
+            pos = q
+        return calls
+
+    # fixed per-call cost (allocation, copies, RNG set-up) from zero-step calls
+    t_fix = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        call(np.zeros(1, np.int32)[:0])
+        torch.cuda.synchronize()
+        t_fix.append(time.perf_counter() - t0)
+    fixed = float(np.median(t_fix))
+    pos = 0
+    for _ in range(args.warmup):
+        run_range(pos, pos + chunk)
+        pos += chunk
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    t_raw, t_adj, n = 0.0, 0.0, 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        calls = run_range(pos, pos + chunk)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        t_raw += dt
+        t_adj += max(dt - calls * fixed, 1e-9)
+        pos += chunk
+        n += chunk
+    clk = clocks.stop()
+    value = n / t_adj
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_adj / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (reference kernels)", "impl": "reference",
+        "data": "synthetic (seeded generator; no public dataset)",
+        "config": {"workload": WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
+                   "parallelism": "replicas x1"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "moves/s", "cores": 1, "kind": "reference",
+                         "sample": f"reference runGCMC_cuda (unmodified pyGCMC gcmc.cu, sm_100a) on the B200, "
+                                   f"{n} MC steps; the reference has no CPU implementation of this path; "
+                                   f"per-call set-up ({fixed * 1e3:.2f} ms) subtracted"},
+        "e2e": {"value": round(n / t_raw, 1), "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "skipped_deletes_on_empty_types": skipped[0],
+        "clocks": clk,
+    }
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--chunk", type=int, default=2048, help="MC steps per bench step (ours)")
+    ap.add_argument("--ref-chunk", type=int, default=0,
+                    help="MC steps per bench step for the reference arm (default: --chunk, same step range)")
+    ap.add_argument("--e2e-chunk", type=int, default=2048)
+    ap.add_argument("--e2e-reps", type=int, default=3)
+    ap.add_argument("--cells", type=int, default=2)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.ref_chunk <= 0:
+        args.ref_chunk = args.chunk
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        out = run_reference(args, ws, rank, local) if args.impl == "reference" else run_ours(args, ws, rank, local)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -141,6 +141,11 @@ int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energ
                   int32_t max_steps, int32_t* n_steps);
 /* Counters: steps done, pose energies evaluated, atom-site pairs evaluated. */
 int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, int64_t* pairs);
+/* SM cycles spent by replica `rep`'s accept kernel in its phases, summed over
+ * steps: [0] pose energies, [1] per-pose weights and bit rows, [2] cluster
+ * walk, [3] state update, [4] next-step preparation; [5] number of
+ * speculative cluster rounds; [6..7] reserved. */
+int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8);
 /* Device error word (bit 0 cell overflow, bit 1 periodic image > 1 box,
  * bit 2 slot overflow, bit 3 pose limit). */
 int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);

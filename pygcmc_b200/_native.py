@@ -64,6 +64,7 @@ def lib():
         "gcmc_get_logs": (c_int, [c_void, c_int, c_void, c_void, c_int, P(c_int)]),
         "gcmc_counters": (c_int, [c_void, c_int, P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
         "gcmc_device_error": (c_int, [c_void, P(c_int)]),
+        "gcmc_phase_cycles": (c_int, [c_void, c_int, c_void]),
         "gcmc_stream": (c_void, [c_void]),
         "gcmc_destroy": (c_int, [c_void]),
         "gcmc_energy_poses": (c_int, [c_void, c_int, c_void, c_void, c_void, c_int, c_void, c_void, c_int,
@@ -107,5 +108,5 @@ def default_options(**kw):
 
 EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
-           "gcmc_device_error", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses", "gcmc_synth_chain_sphere",
+           "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses", "gcmc_synth_chain_sphere",
            "gcmc_synth_chain_slab"]

@@ -26,14 +26,21 @@ constexpr int kAcceptThreads = 1024;
 struct AcceptSmem {
     double E[kMaxPoses];
     double w[kMaxPoses];
-    double key[kMaxPoses];
-    double lnu[kMaxPoses];
+    unsigned long long key[kMaxPoses];  // order-preserving encoding of the Gumbel key
+    double lnu[kMaxPoses];              // ln of the acceptance draw of the cluster seeded by pose i
     float4 c[kMaxPoses];
     uint32_t nb[kMaxPoses * kMaxWords];
     int acc_list[kMaxPoses];
     int acc_slot[kMaxPoses];
     double red[32];
     int misc[8];
+    // one round of speculative clusters (seeded in order assuming no acceptance)
+    uint32_t spec_mask[32][kMaxWords];
+    int spec_seed[32];
+    int spec_cnt[32];
+    int spec_chosen[32];  // Gumbel argmax, -1 if no member has a finite energy
+    double spec_lnq[32];  // ln(W) - ln(cnt), W = sum over members of exp(-beta E)
+    int spec_n;
 };
 
 // ---- cell list maintenance (single thread) ----
@@ -66,6 +73,15 @@ __device__ __forceinline__ void cell_rename(const RepDev& R, int from, int to) {
     R.gcell[from] = -1;
     R.gcell[to] = cp;
     if (cp >= 0) R.cell_ent[cp] = to;
+}
+
+// Order-preserving map of a double to uint64 (larger key -> larger integer);
+// 0 is reserved for "no candidate".
+__device__ __forceinline__ bool normal_positive(double a) { return a >= 2.2250738585072014e-308 && a <= 1.7976931348623157e308; }
+
+__device__ __forceinline__ unsigned long long key_order(double d) {
+    const long long b = __double_as_longlong(d);
+    return b >= 0 ? ((unsigned long long)b | 0x8000000000000000ull) : ~(unsigned long long)b;
 }
 
 // ---- block reductions ----
@@ -203,6 +219,16 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, nwarps = nt >> 5;
     const FragDev& F = R.frag[D.ftype];
     const int k = D.k, ns = F.nsites;
+    long long t_start = clock64(), t_mark = t_start;
+    // phase cycle sums (thread 0): 0 energies, 1 per-pose precompute, 2 cluster walk, 3 apply, 4 prepare
+#define PHASE(i)                                                                  \
+    do {                                                                          \
+        if (tid == 0) {                                                           \
+            long long t_ = clock64();                                             \
+            atomicAdd(&R.counters[4 + (i)], (unsigned long long)(t_ - t_mark));   \
+            t_mark = t_;                                                          \
+        }                                                                         \
+    } while (0)
 
     // ---- phase 0: pose energies (sum of slab partials; dE for translate/rotate)
     for (int i = tid; i < k; i += nt) {
@@ -217,6 +243,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     }
     if (tid == 0) { S.misc[0] = 0; S.misc[1] = 0; S.misc[2] = -1; S.misc[3] = D.n; }
     __syncthreads();
+    PHASE(0);
     const bool logging = R.log != nullptr && D.step < R.log_cap;
     double esum = 0.0;
     if (logging) {
@@ -267,7 +294,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             const bool fin = isfinite(e);
             S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
             const U4 g = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
-            S.key[i] = fin ? (-kBeta * e - log(-log(u53_open(g.x, g.y)))) : -INFINITY;
+            S.key[i] = fin ? key_order(-kBeta * e - log(-log(u53_open(g.x, g.y)))) : 0ull;
             const U4 ua = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
             S.lnu[i] = log(u53(ua.x, ua.y));
             S.c[i] = R.pcen[i];
@@ -275,46 +302,77 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         const int nw = D.nw;
         for (int x = tid; x < k * nw; x += nt) S.nb[x] = R.nbr[x];
         __syncthreads();
+        PHASE(1);
 
-        // ---- phase 2: sequential cluster walk (warp 0)
+        // ---- phase 2: cluster walk in speculative rounds
+        // The sequential definition: seed = lowest unused pose, members = unused
+        // poses within the cutoff of the seed, decision, then the members (and on
+        // acceptance the unused poses within the cutoff of the chosen pose) leave
+        // the unused set.  Each round, warp 0 seeds up to 32 clusters ahead
+        // assuming no acceptance; all warps evaluate them in parallel (member
+        // count, Gumbel argmax and ln(W) - ln(cnt) with W = sum of exp(-beta E));
+        // warp 0 then commits them in order.  A speculative cluster is exactly
+        // the sequential one while its seed and all its members are still unused
+        // (removing other poses can neither lower the seed nor change the member
+        // set); at the first cluster that fails this test the round ends and the
+        // next one reseeds from there.  The commit accepts iff
+        // ln u < ln(W) - ln(cnt) + K(n), K = ln(cavityFactor) + B - ln(n+1) for
+        // insertions and 0 for translate/rotate -- u < min(1, exp(lnp)) in log form.
         const bool ins = (D.move == MV_INSERT);
-        if (warp == 0) {
-            uint32_t u = 0u;
-            if (lane < nw) {
-                const int rem = k - 32 * lane;
-                u = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+        uint32_t u = 0u;  // warp 0: unused-pose word `lane`
+        if (warp == 0 && lane < nw) {
+            const int rem = k - 32 * lane;
+            u = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+        }
+        int wn = D.n, wna = 0, wnc = 0, wfa = -1;
+        const double K0 = ins ? (R.lncav + F.B) : 0.0;
+        double K = ins ? K0 - log((double)wn + 1.0) : 0.0;
+        int nrounds = 0;
+        for (int round = 0; round <= k; ++round) {
+            ++nrounds;
+            if (warp == 0) {  // speculative seeding
+                uint32_t us = u;
+                int nb = 0;
+                while (nb < 32) {
+                    const unsigned nz = __ballot_sync(kFull, us != 0u);
+                    if (nz == 0u) break;
+                    const int L = __ffs(nz) - 1;
+                    const uint32_t uw = __shfl_sync(kFull, us, L);
+                    const int sd = 32 * L + __ffs(uw) - 1;
+                    uint32_t m = (lane < nw) ? (us & S.nb[sd * nw + lane]) : 0u;
+                    if (lane == L) m |= 1u << (sd & 31);
+                    us &= ~m;
+                    S.spec_mask[nb][lane] = m;
+                    if (lane == 0) S.spec_seed[nb] = sd;
+                    ++nb;
+                }
+                if (lane == 0) S.spec_n = nb;
             }
-            int n = D.n, na = 0, nc = 0, fa = -1;
-            const double lnconst = ins ? (R.lncav + F.B) : 0.0;
-            double ln_n1 = ins ? log((double)n + 1.0) : 0.0;
-            for (;;) {
-                const unsigned nz = __ballot_sync(kFull, u != 0u);
-                if (nz == 0u) break;
-                const int L = __ffs(nz) - 1;
-                const uint32_t uw = __shfl_sync(kFull, u, L);
-                const int s = 32 * L + __ffs(uw) - 1;
-                uint32_t m = (lane < nw) ? (u & S.nb[s * nw + lane]) : 0u;
-                if (lane == L) m |= 1u << (s & 31);
+            __syncthreads();
+            const int nb = S.spec_n;
+            if (nb == 0) break;
+            if (warp < nb) {  // evaluation, one warp per speculative cluster
+                const uint32_t m = S.spec_mask[warp][lane];
                 const int cnt = __reduce_add_sync(kFull, (unsigned)__popc(m));
-                double wsum = 0.0, best = -INFINITY;
-                int bi = 0x7fffffff;
+                double wsum = 0.0;
+                unsigned long long best = 0ull;
+                int bi = -1;
                 for (uint32_t mm = m; mm; mm &= mm - 1u) {
                     const int i = 32 * lane + __ffs(mm) - 1;
                     wsum += S.w[i];
-                    const double kk = S.key[i];
+                    const unsigned long long kk = S.key[i];
                     if (kk > best) { best = kk; bi = i; }
                 }
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    wsum += __shfl_xor_sync(kFull, wsum, off);
-                    const double ob = __shfl_xor_sync(kFull, best, off);
-                    const int oi = __shfl_xor_sync(kFull, bi, off);
-                    if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-                }
-                bool acc = false;
-                int chosen = s;
-                if (bi != 0x7fffffff) {
-                    chosen = bi;
+                for (int off = 16; off > 0; off >>= 1) wsum += __shfl_xor_sync(kFull, wsum, off);
+                const unsigned hi = (unsigned)(best >> 32);
+                const unsigned mhi = __reduce_max_sync(kFull, hi);
+                const unsigned lo = (hi == mhi) ? (unsigned)best : 0u;
+                const unsigned mlo = __reduce_max_sync(kFull, lo);
+                const unsigned win = __ballot_sync(kFull, best != 0ull && hi == mhi && (unsigned)best == mlo);
+                const int chosen = win ? __shfl_sync(kFull, bi, __ffs(win) - 1) : -1;
+                double lnq = -INFINITY;
+                if (chosen >= 0) {
                     double lnW;
                     if (wsum > 1e-300) {
                         lnW = log(wsum) - kBeta * Eref;
@@ -333,32 +391,51 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                         for (int off = 16; off > 0; off >>= 1) w2 += __shfl_xor_sync(kFull, w2, off);
                         lnW = log(w2) - kBeta * em;
                     }
-                    double lnp = lnW - log((double)cnt);
-                    if (ins) lnp += lnconst - ln_n1;
-                    acc = !isnan(lnp) && (lnp >= 0.0 || S.lnu[s] < lnp);
+                    lnq = lnW - log((double)cnt);
                 }
-                u &= ~m;
-                if (acc) {
-                    if (lane < nw) u &= ~S.nb[chosen * nw + lane];
-                    int slot = 0;
-                    if (ins) {
-                        if (n < F.maxNum) {
-                            slot = n;
-                            ++n;
-                            ln_n1 = log((double)n + 1.0);
-                        } else {
-                            slot = -1;
-                        }
-                    }
-                    if (lane == 0) { S.acc_list[na] = chosen; S.acc_slot[na] = slot; }
-                    ++na;
-                    if (fa < 0) fa = chosen;
+                if (lane == 0) {
+                    S.spec_cnt[warp] = cnt;
+                    S.spec_lnq[warp] = lnq;
+                    S.spec_chosen[warp] = chosen;
                 }
-                ++nc;
             }
-            if (lane == 0) { S.misc[0] = na; S.misc[1] = nc; S.misc[2] = fa; S.misc[3] = n; }
+            __syncthreads();
+            if (warp == 0) {  // in-order commit
+                for (int j = 0; j < nb; ++j) {
+                    const uint32_t m = S.spec_mask[j][lane];
+                    if (__ballot_sync(kFull, (m & ~u) != 0u)) break;  // speculation no longer exact
+                    const int sd = S.spec_seed[j];
+                    int chosen = S.spec_chosen[j];
+                    const bool acc = chosen >= 0 && S.lnu[sd] < S.spec_lnq[j] + K;
+                    if (chosen < 0) chosen = sd;
+                    u &= ~m;
+                    if (acc) {
+                        if (lane < nw) u &= ~S.nb[chosen * nw + lane];
+                        int slot = 0;
+                        if (ins) {
+                            if (wn < F.maxNum) {
+                                slot = wn;
+                                ++wn;
+                                K = K0 - log((double)wn + 1.0);
+                            } else {
+                                slot = -1;
+                            }
+                        }
+                        if (lane == 0) { S.acc_list[wna] = chosen; S.acc_slot[wna] = slot; }
+                        ++wna;
+                        if (wfa < 0) wfa = chosen;
+                    }
+                    ++wnc;
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            S.misc[0] = wna; S.misc[1] = wnc; S.misc[2] = wfa; S.misc[3] = wn;
+            atomicAdd(&R.counters[12], (unsigned long long)nrounds);
         }
         __syncthreads();
+        PHASE(2);
 
         // ---- phase 3: write accepted poses, then cell lists and counts
         const int na = S.misc[0];
@@ -441,7 +518,10 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         }
     }
     __syncthreads();
+    PHASE(3);
     prepare_step(R, D.step + 1);
+    PHASE(4);
+#undef PHASE
 }
 
 }  // namespace gcmc

@@ -71,6 +71,28 @@ __device__ __forceinline__ float dist_host(float ax, float ay, float az, float b
     return fsqrt(s);
 }
 
+// Inclusion test equal to dist_group(...) <= cutoff.  When R.fast_incl is set
+// (cutoff below half of every box edge) a multiply-based squared distance
+// decides every case outside +-1e-4 of the cutoff: there both forms pick the
+// same periodic image (they can differ only at |d| ~ L/2, beyond the cutoff)
+// and their distances agree to a few ulps; only candidates inside the band take
+// the exact division form.
+template <bool Host>
+__device__ __forceinline__ bool within_cutoff(float ax, float ay, float az, float bx, float by, float bz,
+                                              const float* L, const float* invL, float cutoff, float lo2,
+                                              float hi2, bool fast) {
+    if (fast) {
+        float dx = ax - bx, dy = ay - by, dz = az - bz;
+        dx = fmaf(-rintf(dx * invL[0]), L[0], dx);
+        dy = fmaf(-rintf(dy * invL[1]), L[1], dy);
+        dz = fmaf(-rintf(dz * invL[2]), L[2], dz);
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        if (r2 < lo2) return true;
+        if (r2 > hi2) return false;
+    }
+    return (Host ? dist_host(ax, ay, az, bx, by, bz, L) : dist_group(ax, ay, az, bx, by, bz, L)) <= cutoff;
+}
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter (step, index,
 // purpose<<16 | draw, 0), key (seed, replica).
@@ -258,7 +280,9 @@ struct RepDev {
     double lncav;
     int proposal;
     int pair_image;     // 1: per-pair minimum image (small boxes); 0: per-group image shift
+    int fast_incl;      // 1: multiply-based prefilter decides away from the cutoff (cutoff < L/2)
     float invL[3];
+    float cut2_lo, cut2_hi;  // (cutoff*(1-1e-4))^2, (cutoff*(1+1e-4))^2
     int nfixed, ntypes, ffY, G;
     int mcsteps;
     uint32_t seed, replica;
@@ -286,7 +310,7 @@ struct RepDev {
     // logs and counters
     gcmc_step_log* log;
     double* logE;
-    unsigned long long* counters;  // steps, poses, pairs
+    unsigned long long* counters;  // steps, poses, pairs, then 8 accept-kernel phase cycle sums
     int* err;
 };
 

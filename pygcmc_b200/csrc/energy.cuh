@@ -95,29 +95,64 @@ __device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, i
     else flush_atoms_t<false>(R, B, na, ns, lane, cx, cy, cz, acc);
 }
 
-// Expand included groups B.glist[0, ng) into atoms and evaluate them.
+// Expand included groups B.glist[0, ng) into atoms and evaluate them.  Each
+// lane takes one group of a batch of 32, a warp scan of the atom counts gives
+// the write offsets; groups larger than the buffer are streamed in pieces.
 __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int ng, int ns, int lane,
                                                double cx, double cy, double cz, double& acc, long long& npair) {
     int na = 0;
-    for (int gi = 0; gi < ng; ++gi) {
-        uint32_t ge = B.glist[gi];
-        int g = (int)(ge & 0x3FFFFFFu);
-        uint32_t code = ge >> 26;
-        int2 sp = __ldg(&R.gspan[g]);
-        npair += (long long)sp.y * ns;
-        int done = 0;
-        while (done < sp.y) {
-            int take = min(sp.y - done, kACap - na);
-            if (take == 0) {
+    for (int base = 0; base < ng; base += 32) {
+        const int gi = base + lane;
+        int start = 0, cnt = 0;
+        uint32_t code = 0;
+        if (gi < ng) {
+            const uint32_t ge = B.glist[gi];
+            const int2 sp = __ldg(&R.gspan[(int)(ge & 0x3FFFFFFu)]);
+            start = sp.x;
+            cnt = sp.y;
+            code = ge >> 26;
+        }
+        npair += (long long)cnt * ns;
+        int incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        const int maxcnt = __reduce_max_sync(kFull, (unsigned)cnt);
+        if (maxcnt <= kACap / 2) {
+            if (na + total > kACap) {
                 __syncwarp();
                 flush_atoms(R, B, na, ns, lane, cx, cy, cz, acc);
                 __syncwarp();
                 na = 0;
+            }
+            if (total <= kACap) {
+                const int off0 = na + incl - cnt;
+                for (int j = 0; j < cnt; ++j) B.alist[off0 + j] = (uint32_t)(start + j) | (code << 26);
+                na += total;
                 continue;
             }
-            for (int j = lane; j < take; j += 32) B.alist[na + j] = (uint32_t)(sp.x + done + j) | (code << 26);
-            na += take;
-            done += take;
+        }
+        // large groups: one group at a time, in buffer-sized pieces
+        for (int l = 0; l < 32; ++l) {
+            const int s0 = __shfl_sync(kFull, start, l), c0 = __shfl_sync(kFull, cnt, l);
+            const uint32_t cd = __shfl_sync(kFull, code, l);
+            int done = 0;
+            while (done < c0) {
+                const int take = min(c0 - done, kACap - na);
+                if (take == 0) {
+                    __syncwarp();
+                    flush_atoms(R, B, na, ns, lane, cx, cy, cz, acc);
+                    __syncwarp();
+                    na = 0;
+                    continue;
+                }
+                for (int j = lane; j < take; j += 32) B.alist[na + j] = (uint32_t)(s0 + done + j) | (cd << 26);
+                na += take;
+                done += take;
+            }
         }
     }
     __syncwarp();
@@ -156,7 +191,8 @@ __device__ __noinline__ void energy_slab(const RepDev& R, WarpBuf& B, int ns, fl
                 int g = R.cell_ent[cell * R.cap + e];
                 if (g != self) {
                     float4 gc = R.gcen[g];
-                    inc = dist_group(cx, cy, cz, gc.x, gc.y, gc.z, R.L) <= R.cutoff;
+                    inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                               R.cut2_hi, R.fast_incl);
                     if (inc) {
                         // image of the group relative to the pose (same rounding as dist_group)
                         float rx = fast_round(fdiv(fsub(gc.x, cx), R.L[0]));
@@ -272,7 +308,7 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
 }
 
 // One launch per MC step: every replica's (pose, variant, slab) items.
-__global__ void __launch_bounds__(kWarpsE * 32) k_energy(const RepDev* __restrict__ reps, int nrep) {
+__global__ void __launch_bounds__(kWarpsE * 32, 3) k_energy(const RepDev* __restrict__ reps, int nrep) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -314,7 +350,8 @@ __global__ void __launch_bounds__(kWarpsE * 32) k_energy(const RepDev* __restric
                 bool b = false;
                 if (j < D.k) {
                     float4 cj = R.pcen[j];
-                    b = dist_host(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L) <= R.cutoff;
+                    b = within_cutoff<true>(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                            R.cut2_hi, R.fast_incl);
                 }
                 unsigned m = __ballot_sync(kFull, b);
                 if (lane == 0) R.nbr[i * D.nw + w] = m;

@@ -228,10 +228,14 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     rf += 0.5;
     const double reach = (double)I->cutoff + std::max(rg, rf) + rf;
     d.pair_image = 0;
+    d.fast_incl = 1;
     for (int a = 0; a < 3; ++a) {
         d.invL[a] = 1.0f / I->cryst[a];
         if (reach >= 0.5 * I->cryst[a]) d.pair_image = 1;
+        if ((double)I->cutoff * (1.0 + 1e-3) >= 0.5 * I->cryst[a]) d.fast_incl = 0;
     }
+    d.cut2_lo = (float)(((double)I->cutoff * (1.0 - 1e-4)) * ((double)I->cutoff * (1.0 - 1e-4)));
+    d.cut2_hi = (float)(((double)I->cutoff * (1.0 + 1e-4)) * ((double)I->cutoff * (1.0 + 1e-4)));
 
     // cell capacity from the initial occupancy
     std::vector<int> counts(h.ncell, 0);
@@ -303,7 +307,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.grid, h.G); AL(h.lj, lj.size()); AL(h.moves, h.mcsteps); AL(h.frag, h.ntypes);
     AL(h.totalNum, h.ntypes); AL(h.desc, 1); AL(h.pcen, kMaxPoses); AL(h.pslot, kMaxPoses);
     AL(h.epart, (size_t)kMaxPoses * 2 * h.nslab); AL(h.nbr, (size_t)kMaxPoses * kMaxWords);
-    AL(h.counters, 4); AL(h.err, 1);
+    AL(h.counters, 16); AL(h.err, 1);
     h.log_cap = std::max(0, std::min(opt.log_steps, h.mcsteps));
     h.log_kmax = std::max(1, std::min(opt.log_kmax > 0 ? opt.log_kmax : 1, kMaxPoses));
     if (h.log_cap > 0) {
@@ -330,7 +334,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d0.step = 0;
     d0.move = MV_NONE;
     CK(cudaMemcpyAsync(h.desc, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 4, s));
+    CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 16, s));
     CK(cudaMemsetAsync(h.err, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
 
@@ -610,6 +614,17 @@ int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, in
     if (steps) *steps = (int64_t)c[0];
     if (poses) *poses = (int64_t)c[1];
     if (pairs) *pairs = (int64_t)c[2];
+    return GCMC_OK;
+}
+
+int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !out8) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long c[16];
+    CK(cudaMemcpy(c, ctx->reps[rep].counters, sizeof(c), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 5; ++i) out8[i] = (int64_t)c[4 + i];
+    out8[5] = (int64_t)c[12];  // speculative cluster rounds
+    out8[6] = out8[7] = 0;
     return GCMC_OK;
 }
 

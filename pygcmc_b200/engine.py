@@ -76,6 +76,13 @@ class Engine:
         check(lib().gcmc_counters(self._h, rep, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "gcmc_counters")
         return {"steps": a.value, "poses": b.value, "pairs": c.value}
 
+    def phase_cycles(self, rep: int = 0):
+        """Accept-kernel SM cycles per phase (energies, precompute, cluster walk,
+        update, prepare) and the number of speculative cluster rounds."""
+        out = np.zeros(8, np.int64)
+        check(lib().gcmc_phase_cycles(self._h, rep, ptr(out)), "gcmc_phase_cycles")
+        return out[:6]
+
     def device_error(self) -> int:
         e = ctypes.c_int32(0)
         check(lib().gcmc_device_error(self._h, ctypes.byref(e)), "gcmc_device_error")
