@@ -181,29 +181,28 @@ def run_ours(args, ws, rank, local):
     c2 = eng.counters()
     eng.sync()
     eng.close()
-    # end to end through the drop-in API with host arrays
+    # end to end through the drop-in API with host arrays, over the same step range:
+    # warm-up calls advance the host state through the first `warmup` chunks
     e2e_state = sysm.copy()
-    e2e_chunk = args.e2e_chunk
-    h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * e2e_chunk
+    h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * chunk
     d2h = e2e_state.fragmentInfo.nbytes + e2e_state.residueInfo.nbytes + e2e_state.atomInfo.nbytes
     info = e2e_state.SimInfo
-    info[0]["mcsteps"] = e2e_chunk
+    info[0]["mcsteps"] = chunk
     moves = e2e_state.moveArray
-    runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
-            e2e_state.ff, np.ascontiguousarray(moves[:e2e_chunk]))  # warm-up call
     e2e_times = []
-    for k in range(args.e2e_reps):
+    for k in range(args.warmup + args.steps):
         info[0]["seed"] = (seed * 7 + k) & 0xFFFFFFFF
-        mv = np.ascontiguousarray(moves[(k + 1) * e2e_chunk:(k + 2) * e2e_chunk])
+        mv = np.ascontiguousarray(moves[k * chunk:(k + 1) * chunk])
         barrier(ws)
         t0 = time.perf_counter()
         runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
                 e2e_state.ff, mv)
-        e2e_times.append(time.perf_counter() - t0)
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(e2e_times) * 1e3, ws) / 1e3
     steps_all = args.steps * chunk * ws
     value = steps_all / (ms / 1e3)
-    e2e_val = args.e2e_reps * e2e_chunk * ws / e2e_s
+    e2e_val = args.steps * chunk * ws / e2e_s
     pairs_prof = c2["pairs"] - c1["pairs"]
     e_ms = float(te.sum())
     a_ms = float(ta.sum())
@@ -221,7 +220,7 @@ def run_ours(args, ws, rank, local):
                    "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
                    "cells_per_cutoff": args.cells},
         "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": e2e_chunk,
+                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
                 "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
@@ -360,8 +359,6 @@ def main():
     ap.add_argument("--chunk", type=int, default=2048, help="MC steps per bench step (ours)")
     ap.add_argument("--ref-chunk", type=int, default=0,
                     help="MC steps per bench step for the reference arm (default: --chunk, same step range)")
-    ap.add_argument("--e2e-chunk", type=int, default=2048)
-    ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--cells", type=int, default=2)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")

@@ -78,6 +78,8 @@ typedef struct {
     int32_t cells_per_cutoff; /* cell-grid resolution R (cells of >= cutoff/R); 0 = 2 */
     int32_t log_steps;   /* record per-step logs for this many steps (0 = off)      */
     int32_t log_kmax;    /* per-step pose energies recorded (<= 1024)               */
+    int32_t split_items; /* target pose-energy work items per step: each pose's cell
+                            window is split into ~split_items/poses ranges; 0 = 2048 */
 } gcmc_options;
 
 /* One per-step record (48 bytes). */

@@ -18,7 +18,7 @@ class Options(ctypes.Structure):
     """gcmc_options (include/gcmc_b200.h)."""
     _fields_ = [("proposal", c_int), ("muex_kcal", c_int), ("trn_step", ctypes.c_float),
                 ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("cells_per_cutoff", c_int),
-                ("log_steps", c_int), ("log_kmax", c_int)]
+                ("log_steps", c_int), ("log_kmax", c_int), ("split_items", c_int)]
 
 
 class ReplicaIn(ctypes.Structure):

@@ -115,7 +115,7 @@ __device__ void prepare_step(const RepDev& R, int step) {
         D.step = step;
         D.move = MV_NONE;
         D.del_slot = -1;
-        D.nslab = R.span[2];
+        D.nslab = 1;
         if (step < R.run_end && step < R.mcsteps) {
             const int mv = R.moves[step];
             D.ftype = mv >> 2;
@@ -144,6 +144,9 @@ __device__ void prepare_step(const RepDev& R, int step) {
                 D.k = 0;
             }
             D.nw = (D.move == MV_DELETE) ? 0 : (D.k + 31) >> 5;
+            // split each pose's cell window so a step has about split_items work items
+            const int kv = max(1, D.k * D.nvar);
+            D.nslab = max(1, min(R.max_split, (R.split_items + kv - 1) / kv));
             D.items = D.k * D.nvar * D.nslab;
         }
         Dsh = D;
@@ -328,12 +331,13 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         const double K0 = ins ? (R.lncav + F.B) : 0.0;
         double K = ins ? K0 - log((double)wn + 1.0) : 0.0;
         int nrounds = 0;
+        int depth = 32;  // speculation depth: halves after a round cut short, doubles after a full one
         for (int round = 0; round <= k; ++round) {
             ++nrounds;
             if (warp == 0) {  // speculative seeding
                 uint32_t us = u;
                 int nb = 0;
-                while (nb < 32) {
+                while (nb < depth) {
                     const unsigned nz = __ballot_sync(kFull, us != 0u);
                     if (nz == 0u) break;
                     const int L = __ffs(nz) - 1;
@@ -401,7 +405,8 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             }
             __syncthreads();
             if (warp == 0) {  // in-order commit
-                for (int j = 0; j < nb; ++j) {
+                int j = 0;
+                for (; j < nb; ++j) {
                     const uint32_t m = S.spec_mask[j][lane];
                     if (__ballot_sync(kFull, (m & ~u) != 0u)) break;  // speculation no longer exact
                     const int sd = S.spec_seed[j];
@@ -427,6 +432,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     }
                     ++wnc;
                 }
+                depth = (j < nb) ? max(1, min(depth, 2 * j) / 2 + 1) : min(32, 2 * depth);
             }
             __syncthreads();
         }

@@ -259,7 +259,7 @@ struct StepDesc {
     int k;         // poses
     int n;         // totalNum at the start of the step
     int nvar;      // 1, or 2 for translate/rotate (new, old)
-    int nslab;     // z-slabs per pose
+    int nslab;     // work items per pose variant (each covers a contiguous range of window cells)
     int nw;        // neighbour-row words (0 = no clustering)
     int items;     // k * nvar * nslab
     int del_slot;
@@ -275,6 +275,8 @@ struct RepDev {
     int nc[3];          // cells per axis
     int span[3];        // cells visited per axis (min(2R+1, nc))
     int range;          // R
+    int split_items;    // target work items per step (pose splits = target / poses)
+    int max_split;      // splits per pose cap (window cells / 8)
     int cap;            // cell capacity
     float cutoff, grid_dx, trn_step, rot_max;
     double lncav;
@@ -319,7 +321,8 @@ __device__ __forceinline__ int wrapi(int c, int n) {
     return c < 0 ? c + n : c;
 }
 __device__ __forceinline__ int cell_coord(float x, float start, float invLc, int nc) {
-    return wrapi(__float2int_rd(fmul(fsub(x, start), invLc)), nc);
+    const int c = __float2int_rd(fmul(fsub(x, start), invLc));
+    return (unsigned)c < (unsigned)nc ? c : wrapi(c, nc);
 }
 __device__ __forceinline__ int cell_of(const RepDev& R, float x, float y, float z) {
     int cx = cell_coord(x, R.start[0], R.invLc[0], R.nc[0]);

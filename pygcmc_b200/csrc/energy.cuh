@@ -23,65 +23,96 @@ namespace gcmc {
 constexpr int kWarpsE = 8;
 constexpr int kGCap = 128;
 constexpr int kACap = 512;
+constexpr int kCCap = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct WarpBuf {
-    float4 site[kMaxSites];  // x, y, z, Coulomb constant * charge
+    float4 site[kMaxSites];  // x, y, z relative to the pose centre, Coulomb constant * charge
     int srow[kMaxSites];     // template type * ffY
     uint32_t glist[kGCap];   // group id | image code << 26
     uint32_t alist[kACap];   // atom id  | image code << 26
+    int cand[kCCap];         // candidate group ids gathered from the cells
+    float cs_hi[3][4];       // pose centre + image shift (code 0: 0, 1: +L, 2: -L), high part
+    float cs_lo[3][4];       //   and its exact rounding error (TwoSum)
 };
+
+// Exact split of c + t into hi + lo (Knuth's TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float& hi, float& lo) {
+    hi = __fadd_rn(a, b);
+    const float bb = __fsub_rn(hi, a);
+    lo = __fadd_rn(__fsub_rn(a, __fsub_rn(hi, bb)), __fsub_rn(b, bb));
+}
+
+// Per item: the pose centre plus each periodic image shift as an exact
+// (hi, lo) pair, so an atom's centre-relative offset (a - hi) - lo carries a
+// single rounding of the offset itself.
+__device__ __forceinline__ void set_centre(const RepDev& R, WarpBuf& B, float cx, float cy, float cz, int lane) {
+    if (lane < 9) {
+        const int ax = lane / 3, code = lane - 3 * (lane / 3);
+        const float c = ax == 0 ? cx : (ax == 1 ? cy : cz);
+        const float t = code == 0 ? 0.0f : (code == 1 ? R.L[ax] : -R.L[ax]);
+        float hi, lo;
+        two_sum(c, t, hi, lo);
+        B.cs_hi[ax][code] = hi;
+        B.cs_lo[ax][code] = lo;
+    }
+    __syncwarp();
+}
 
 __device__ __forceinline__ float image_shift(uint32_t code2, float L) {
     return code2 == 1u ? L : (code2 == 2u ? -L : 0.0f);
 }
 
 // Pair energies of the atoms buffered in B.alist[0, na) with the pose sites.
-// Geometry is centre-relative: each atom's offset from the pose centre is
-// formed in FP64 (including its periodic image) and rounded once to FP32, and
-// the sites in B.site are stored relative to the same centre, so the FP32
-// pair differences carry ~1e-7 A of rounding instead of the ~1e-6 A of
-// absolute-coordinate differences.  PairImage = false: the atom takes its
-// group's image (exact when every pair of an included group lies within half
-// a box, checked at set-up); true: per-pair minimum image as in
-// gcmc_energy.h:115-122.  1/r is rsqrt refined by one Newton step.
+// Geometry is centre-relative: an atom's offset from the pose centre (with its
+// group's periodic image) is (a - hi) - lo with hi + lo = centre + image
+// exactly, i.e. one rounding of the offset, and the sites in B.site are stored
+// relative to the same centre, so the FP32 pair differences carry ~1e-7 A of
+// rounding instead of the ~1e-6 A of absolute-coordinate differences.
+// PairImage = false: the atom takes its group's image (exact when every pair
+// of an included group lies within half a box, checked at set-up); true:
+// per-pair minimum image as in gcmc_energy.h:115-122.  1/r is rsqrt refined by
+// one Newton step; each atom's site terms are summed in FP32, atoms in FP64.
 template <bool PairImage>
 __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
-                                              double cx, double cy, double cz, double& acc) {
+                                              double& acc) {
     for (int f = lane; f < na; f += 32) {
-        uint32_t u = B.alist[f];
-        int idx = (int)(u & 0x3FFFFFFu);
-        uint32_t code = u >> 26;
-        float4 a = __ldg(&R.xyzq[idx]);
-        int ta = __ldg(&R.atype[idx]);
-        double ox = (double)a.x - cx, oy = (double)a.y - cy, oz = (double)a.z - cz;
-        if (PairImage) {
-            ox -= (double)R.L[0] * rint(ox * (double)R.invL[0]);
-            oy -= (double)R.L[1] * rint(oy * (double)R.invL[1]);
-            oz -= (double)R.L[2] * rint(oz * (double)R.invL[2]);
+        const uint32_t u = B.alist[f];
+        const int idx = (int)(u & 0x3FFFFFFu);
+        const float4 a = __ldg(&R.xyzq[idx]);
+        const int ta = __ldg(&R.atype[idx]);
+        uint32_t c0, c1, c2;
+        if (PairImage) {  // the atom's image nearest the pose centre
+            const float kx = rintf((a.x - B.cs_hi[0][0]) * R.invL[0]);
+            const float ky = rintf((a.y - B.cs_hi[1][0]) * R.invL[1]);
+            const float kz = rintf((a.z - B.cs_hi[2][0]) * R.invL[2]);
+            c0 = kx > 0.0f ? 1u : (kx < 0.0f ? 2u : 0u);
+            c1 = ky > 0.0f ? 1u : (ky < 0.0f ? 2u : 0u);
+            c2 = kz > 0.0f ? 1u : (kz < 0.0f ? 2u : 0u);
         } else {
-            ox -= (double)image_shift(code & 3u, R.L[0]);
-            oy -= (double)image_shift((code >> 2) & 3u, R.L[1]);
-            oz -= (double)image_shift((code >> 4) & 3u, R.L[2]);
+            const uint32_t code = u >> 26;
+            c0 = code & 3u; c1 = (code >> 2) & 3u; c2 = (code >> 4) & 3u;
         }
-        const float ax = (float)ox, ay = (float)oy, az = (float)oz;
+        const float ax = (a.x - B.cs_hi[0][c0]) - B.cs_lo[0][c0];
+        const float ay = (a.y - B.cs_hi[1][c1]) - B.cs_lo[1][c1];
+        const float az = (a.z - B.cs_hi[2][c2]) - B.cs_lo[2][c2];
         float e = 0.0f;
 #pragma unroll 4
         for (int s = 0; s < ns; ++s) {
-            float4 sp = B.site[s];
+            const float4 sp = B.site[s];
             float dx = ax - sp.x, dy = ay - sp.y, dz = az - sp.z;
             if (PairImage) {
                 dx = fmaf(-rintf(dx * R.invL[0]), R.L[0], dx);
                 dy = fmaf(-rintf(dy * R.invL[1]), R.L[1], dy);
                 dz = fmaf(-rintf(dz * R.invL[2]), R.L[2], dz);
             }
-            float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
             float ir = rsqrtf(r2);
             ir = ir * fmaf(-0.5f * r2 * ir, ir, 1.5f);
-            float ir2 = ir * ir;
-            float2 p = __ldg(&R.lj[B.srow[s] + ta]);
-            float s2 = p.x * ir2;
-            float s6 = s2 * s2 * s2;
+            const float ir2 = ir * ir;
+            const float2 p = __ldg(&R.lj[B.srow[s] + ta]);
+            const float s2 = p.x * ir2;
+            const float s6 = s2 * s2 * s2;
             e = fmaf(p.y, fmaf(s6, s6, -s6), e);
             e = fmaf(sp.w * a.w, ir, e);
         }
@@ -90,16 +121,16 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
 }
 
 __device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
-                                            double cx, double cy, double cz, double& acc) {
-    if (R.pair_image) flush_atoms_t<true>(R, B, na, ns, lane, cx, cy, cz, acc);
-    else flush_atoms_t<false>(R, B, na, ns, lane, cx, cy, cz, acc);
+                                            double& acc) {
+    if (R.pair_image) flush_atoms_t<true>(R, B, na, ns, lane, acc);
+    else flush_atoms_t<false>(R, B, na, ns, lane, acc);
 }
 
 // Expand included groups B.glist[0, ng) into atoms and evaluate them.  Each
 // lane takes one group of a batch of 32, a warp scan of the atom counts gives
 // the write offsets; groups larger than the buffer are streamed in pieces.
 __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int ng, int ns, int lane,
-                                               double cx, double cy, double cz, double& acc, long long& npair) {
+                                               double& acc, long long& npair) {
     int na = 0;
     for (int base = 0; base < ng; base += 32) {
         const int gi = base + lane;
@@ -124,7 +155,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
         if (maxcnt <= kACap / 2) {
             if (na + total > kACap) {
                 __syncwarp();
-                flush_atoms(R, B, na, ns, lane, cx, cy, cz, acc);
+                flush_atoms(R, B, na, ns, lane, acc);
                 __syncwarp();
                 na = 0;
             }
@@ -144,7 +175,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
                 const int take = min(c0 - done, kACap - na);
                 if (take == 0) {
                     __syncwarp();
-                    flush_atoms(R, B, na, ns, lane, cx, cy, cz, acc);
+                    flush_atoms(R, B, na, ns, lane, acc);
                     __syncwarp();
                     na = 0;
                     continue;
@@ -156,75 +187,115 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
         }
     }
     __syncwarp();
-    flush_atoms(R, B, na, ns, lane, cx, cy, cz, acc);
+    flush_atoms(R, B, na, ns, lane, acc);
     __syncwarp();
 }
 
-// Energy of the pose in B.site against the groups whose cells lie in z-slab
-// `slab` around the pose centre; returns this lane's FP64 partial.  ngroups
-// (warp-uniform) counts the included groups.
-__device__ __noinline__ void energy_slab(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
-                                         int self, int slab, int lane, double& acc, int& ngroups,
-                                         long long& npair) {
-    const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
-    const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
-    const int pcz = cell_coord(cz, R.start[2], R.invLc[2], R.nc[2]);
-    const int z = (R.span[2] == R.nc[2]) ? slab : wrapi(pcz - R.range + slab, R.nc[2]);
-    const int nxy = R.span[0] * R.span[1];
+// Energy of the pose in B.site against the groups whose cells lie in the
+// z-layers [z0, z1) of the +-R window around the pose centre; returns this
+// lane's FP64 partial.  ngroups (warp-uniform) counts the included groups.
+// Cells are visited 32 at a time; their entries are first copied into a warp
+// candidate list, then every lane tests one candidate at a time.
+__device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
+    return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+__device__ __forceinline__ void test_candidates(const RepDev& R, WarpBuf& B, int nc, int self, float cx, float cy,
+                                                float cz, int lane, int& ng, int& ngroups, int ns, double& acc,
+                                                long long& npair) {
     const unsigned lt = (1u << lane) - 1u;
-    int ng = 0;
-    for (int base = 0; base < nxy; base += 32) {
-        int j = base + lane;
-        int cell = 0, cnt = 0;
-        if (j < nxy) {
-            int jx = j % R.span[0], jy = j / R.span[0];
-            int x = (R.span[0] == R.nc[0]) ? jx : wrapi(pcx - R.range + jx, R.nc[0]);
-            int y = (R.span[1] == R.nc[1]) ? jy : wrapi(pcy - R.range + jy, R.nc[1]);
-            cell = (z * R.nc[1] + y) * R.nc[0] + x;
-            cnt = R.cell_count[cell];
-        }
-        int maxc = __reduce_max_sync(kFull, cnt);
-        for (int e = 0; e < maxc; ++e) {
-            bool inc = false;
-            uint32_t packed = 0;
-            if (e < cnt) {
-                int g = R.cell_ent[cell * R.cap + e];
-                if (g != self) {
-                    float4 gc = R.gcen[g];
-                    inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
-                                               R.cut2_hi, R.fast_incl);
-                    if (inc) {
-                        // image of the group relative to the pose (same rounding as dist_group)
-                        float rx = fast_round(fdiv(fsub(gc.x, cx), R.L[0]));
-                        float ry = fast_round(fdiv(fsub(gc.y, cy), R.L[1]));
-                        float rz = fast_round(fdiv(fsub(gc.z, cz), R.L[2]));
-                        if (R.pair_image) {
-                            packed = (uint32_t)g;
-                        } else if (fabsf(rx) > 1.0f || fabsf(ry) > 1.0f || fabsf(rz) > 1.0f) {
+    for (int base = 0; base < nc; base += 32) {
+        const int t = base + lane;
+        bool inc = false;
+        uint32_t packed = 0;
+        if (t < nc) {
+            const int g = B.cand[t];
+            if (g != self) {
+                const float4 gc = R.gcen[g];
+                inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                           R.cut2_hi, R.fast_incl);
+                if (inc) {
+                    packed = (uint32_t)g;
+                    if (!R.pair_image) {  // the group's periodic image relative to the pose centre
+                        const float rx = rintf((gc.x - cx) * R.invL[0]);
+                        const float ry = rintf((gc.y - cy) * R.invL[1]);
+                        const float rz = rintf((gc.z - cz) * R.invL[2]);
+                        if (fabsf(rx) > 1.0f || fabsf(ry) > 1.0f || fabsf(rz) > 1.0f) {
                             atomicOr(R.err, ERR_IMAGE);
                             inc = false;
                         } else {
-                            uint32_t code = (rx > 0.0f ? 1u : (rx < 0.0f ? 2u : 0u)) |
-                                            ((ry > 0.0f ? 1u : (ry < 0.0f ? 2u : 0u)) << 2) |
-                                            ((rz > 0.0f ? 1u : (rz < 0.0f ? 2u : 0u)) << 4);
-                            packed = (uint32_t)g | (code << 26);
+                            const uint32_t code = (rx > 0.0f ? 1u : (rx < 0.0f ? 2u : 0u)) |
+                                                  ((ry > 0.0f ? 1u : (ry < 0.0f ? 2u : 0u)) << 2) |
+                                                  ((rz > 0.0f ? 1u : (rz < 0.0f ? 2u : 0u)) << 4);
+                            packed |= code << 26;
                         }
                     }
                 }
             }
-            unsigned m = __ballot_sync(kFull, inc);
-            if (inc) B.glist[ng + __popc(m & lt)] = packed;
-            ng += __popc(m);
-            ngroups += __popc(m);
-            if (ng > kGCap - 32) {
-                __syncwarp();
-                process_groups(R, B, ng, ns, lane, (double)cx, (double)cy, (double)cz, acc, npair);
-                ng = 0;
+        }
+        const unsigned m = __ballot_sync(kFull, inc);
+        if (inc) B.glist[ng + __popc(m & lt)] = packed;
+        ng += __popc(m);
+        ngroups += __popc(m);
+        if (ng > kGCap - 32) {
+            __syncwarp();
+            process_groups(R, B, ng, ns, lane, acc, npair);
+            ng = 0;
+        }
+    }
+}
+
+__device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
+                                             int self, int c0, int c1, int lane, double& acc, int& ngroups,
+                                             long long& npair) {
+    // cells [c0, c1) of the window, flattened as ((z * span1) + y) * span0 + x
+    set_centre(R, B, cx, cy, cz, lane);
+    const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
+    const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
+    const int pcz = cell_coord(cz, R.start[2], R.invLc[2], R.nc[2]);
+    const int sxy = R.span[0] * R.span[1];
+    const float inv_s0 = 1.0f / (float)R.span[0], inv_sxy = 1.0f / (float)sxy;
+    int ng = 0;
+    for (int base = c0; base < c1; base += 32) {
+        const int j = base + lane;
+        int cell = 0, cnt = 0;
+        if (j < c1) {
+            const int jz = (int)(((float)j + 0.5f) * inv_sxy), jxy = j - jz * sxy;
+            const int jy = (int)(((float)jxy + 0.5f) * inv_s0), jx = jxy - jy * R.span[0];
+            const int x = (R.span[0] == R.nc[0]) ? jx : wrap_near(pcx - R.range + jx, R.nc[0]);
+            const int y = (R.span[1] == R.nc[1]) ? jy : wrap_near(pcy - R.range + jy, R.nc[1]);
+            const int z = (R.span[2] == R.nc[2]) ? jz : wrap_near(pcz - R.range + jz, R.nc[2]);
+            cell = (z * R.nc[1] + y) * R.nc[0] + x;
+            cnt = R.cell_count[cell];
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        if (total <= kCCap) {
+            const int* ent = R.cell_ent + (size_t)cell * R.cap;
+            for (int e = 0, o = incl - cnt; e < cnt; ++e) B.cand[o + e] = ent[e];
+            __syncwarp();
+            test_candidates(R, B, total, self, cx, cy, cz, lane, ng, ngroups, ns, acc, npair);
+            __syncwarp();
+        } else {  // more candidates than the buffer holds: one cell at a time
+            for (int l = 0; l < 32; ++l) {
+                const int cl = __shfl_sync(kFull, cell, l), cn = __shfl_sync(kFull, cnt, l);
+                const int* ent = R.cell_ent + (size_t)cl * R.cap;
+                for (int e0 = 0; e0 < cn; e0 += kCCap) {
+                    const int m = min(kCCap, cn - e0);
+                    for (int e = lane; e < m; e += 32) B.cand[e] = ent[e0 + e];
+                    __syncwarp();
+                    test_candidates(R, B, m, self, cx, cy, cz, lane, ng, ngroups, ns, acc, npair);
+                    __syncwarp();
+                }
             }
         }
     }
     __syncwarp();
-    process_groups(R, B, ng, ns, lane, (double)cx, (double)cy, (double)cz, acc, npair);
+    process_groups(R, B, ng, ns, lane, acc, npair);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -308,7 +379,10 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
 }
 
 // One launch per MC step: every replica's (pose, variant, slab) items.
-__global__ void __launch_bounds__(kWarpsE * 32, 3) k_energy(const RepDev* __restrict__ reps, int nrep) {
+#ifndef GCMC_ENERGY_MIN_BLOCKS
+#define GCMC_ENERGY_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy(const RepDev* __restrict__ reps, int nrep) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -329,21 +403,23 @@ __global__ void __launch_bounds__(kWarpsE * 32, 3) k_energy(const RepDev* __rest
         const int per_pose = D.nvar * D.nslab;
         const int i = local / per_pose;
         const int rem = local - i * per_pose;
-        const int v = rem / D.nslab, z = rem - v * D.nslab;
+        const int v = rem / D.nslab, zi = rem - v * D.nslab;
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
         double acc = 0.0;
         int ng = 0;
         long long npair = 0;
-        energy_slab(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, z, lane, acc, ng, npair);
+        const int nwin = R.span[0] * R.span[1] * R.span[2];
+        energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi * nwin / D.nslab,
+                     (zi + 1) * nwin / D.nslab, lane, acc, ng, npair);
         acc = warp_sum(acc);
         if (lane == 0) {
-            R.epart[(i * D.nvar + v) * D.nslab + z] = acc;
+            R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
         if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
-            const int w0 = z * D.nw / D.nslab, w1 = (z + 1) * D.nw / D.nslab;
+            const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
             const float4 ci = R.pcen[i];
             for (int w = w0; w < w1; ++w) {
                 int j = 32 * w + lane;
@@ -385,8 +461,9 @@ __global__ void __launch_bounds__(kWarpsE * 32)
         double acc = 0.0;
         int ng = 0;
         long long npair = 0;
-        energy_slab(R, B, ns, centres[3 * p], centres[3 * p + 1], centres[3 * p + 2], self ? self[p] : -1, z,
-                    lane, acc, ng, npair);
+        const int nwin = R.span[0] * R.span[1] * R.span[2];
+        energy_cells(R, B, ns, centres[3 * p], centres[3 * p + 1], centres[3 * p + 2], self ? self[p] : -1,
+                     z * nwin / nslab, (z + 1) * nwin / nslab, lane, acc, ng, npair);
         acc = warp_sum(acc);
         if (lane == 0) {
             out[it] = acc;

@@ -189,7 +189,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         d.span[a] = std::min(2 * Rc + 1, nc);
     }
     d.range = Rc;
-    h.nslab = d.span[2];
+    d.max_split = std::max(1, d.span[0] * d.span[1] * d.span[2] / 8);
+    d.split_items = opt.split_items > 0 ? opt.split_items : 2048;
+    h.nslab = std::max(d.span[2], d.max_split);
     h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
     d.cutoff = I->cutoff;
     d.grid_dx = I->grid_dx;
@@ -454,6 +456,7 @@ void gcmc_default_options(gcmc_options* opt) {
     opt->cells_per_cutoff = 2;
     opt->log_steps = 0;
     opt->log_kmax = 1;
+    opt->split_items = 2048;
 }
 
 const char* gcmc_status_string(int status) {

@@ -28,8 +28,8 @@ def main():
         eng.run(a.warm)
         eng.sync()
         te, ta, mv = eng.run_profiled(a.steps)
-        print(json.dumps({"move": (mv % 4).tolist(), "energy_us": [round(x * 1e3, 2) for x in te],
-                          "accept_us": [round(x * 1e3, 2) for x in ta], "counters": eng.counters()}))
+        print(json.dumps({"move": (mv % 4).tolist(), "energy_us": [round(float(x) * 1e3, 2) for x in te],
+                          "accept_us": [round(float(x) * 1e3, 2) for x in ta], "counters": eng.counters()}))
 
 
 if __name__ == "__main__":
