@@ -230,8 +230,11 @@ def run_ours(args, ws, rank, local):
                      "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_prof / prof_steps,
                      "avg_launch_us": e_ms / prof_steps * 1e3,
                      "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3),
-                     "accept_kernel_avg_us": a_ms / prof_steps * 1e3},
+                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3)},
+        "roofline_accept": {"kernel": "k_accept (cluster walk, accept/update; 1 CTA per replica)",
+                            "bound": "latency (sequential greedy clustering on one SM)",
+                            "avg_launch_us": a_ms / prof_steps * 1e3,
+                            "share_of_step_time": round(a_ms / (e_ms + a_ms), 3)},
         "pose_energies_per_s": round((c1["poses"] - c0["poses"]) / (ms / 1e3), 1),
         "pairs_per_s": round((c1["pairs"] - c0["pairs"]) / (ms / 1e3), 1),
         "gpu_launches": launches,
