@@ -164,6 +164,35 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
                       const int32_t* site_type, int32_t nsites, const float* centres,
                       const int32_t* self, int32_t nposes, double* out, int32_t* n_groups);
 
+/* Allocation-free variant of gcmc_energy_poses (no counterpart in the reference).
+ *
+ * For callers that cannot allocate GPU memory at the point where they need
+ * trial energies: a host program that hands the whole device budget to its own
+ * memory pool and forbids allocations by third-party code, or one running an
+ * asynchronous pipeline that must not stall -- cudaMalloc/cudaFree (which
+ * gcmc_energy_poses uses for its staging buffers) can block or synchronise the
+ * device.  This entry point takes DEVICE pointers the caller already owns
+ * (inputs as in gcmc_energy_poses; out[nposes] doubles; ngroups[nposes] ints,
+ * optional; self optional = none skipped), launches on `stream` (NULL = the
+ * context's stream), returns without waiting, and calls no allocator.
+ *
+ * Its intermediate per-(pose, split) sums live in a fixed 2 MiB device array
+ * inside the library, reserved on every GPU that loads the library until the
+ * process exits.  Limit: nposes x splits <= 174762, where splits is the
+ * context's number of work items per pose (at most ~11,600 poses for the
+ * default cell grid); larger requests return GCMC_ERR_LIMIT and launch
+ * nothing.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array and it keeps the last call's contents; every
+ * entry a call reads is first written by that call, so nothing needs clearing,
+ * but calls that overlap on the GPU (different streams, or different contexts
+ * on the same device) race on it and must be serialised by the caller.
+ * Device-side error flags are reported by the next gcmc_sync. */
+int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float* d_site_q,
+                              const int32_t* d_site_type, int32_t nsites, const float* d_centres,
+                              const int32_t* d_self, int32_t nposes, double* d_out, int32_t* d_ngroups,
+                              void* stream);
+
 /* ---- synthetic fixed-atom generators (host) ---- */
 int gcmc_synth_chain_sphere(int n, const float centre[3], float radius, float step, float excl,
                             uint64_t seed, float* out_xyz, int* n_breaks);

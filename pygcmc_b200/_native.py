@@ -69,6 +69,8 @@ def lib():
         "gcmc_destroy": (c_int, [c_void]),
         "gcmc_energy_poses": (c_int, [c_void, c_int, c_void, c_void, c_void, c_int, c_void, c_void, c_int,
                                       c_void, c_void]),
+        "gcmc_energy_poses_noalloc": (c_int, [c_void, c_int, c_void, c_void, c_void, c_int, c_void, c_void,
+                                              c_int, c_void, c_void, c_void]),
         "gcmc_synth_chain_sphere": (c_int, [c_int, c_void, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_uint64, c_void, P(ctypes.c_int)]),
         "gcmc_synth_chain_slab": (c_int, [c_int] + [ctypes.c_float] * 12 + [ctypes.c_uint64, c_void,
@@ -108,5 +110,6 @@ def default_options(**kw):
 
 EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
-           "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses", "gcmc_synth_chain_sphere",
+           "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",
+           "gcmc_energy_poses_noalloc", "gcmc_synth_chain_sphere",
            "gcmc_synth_chain_slab"]

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -441,6 +442,59 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     return GCMC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free pose energies (gcmc_energy_poses_noalloc).
+//
+// The per-(pose, split) partial sums live in this file-scope device array
+// instead of a cudaMalloc'd buffer.  It is reserved when the library is loaded
+// and stays resident on every GPU that loads the library until the process
+// exits.  In host code `g_noalloc_scratch` names a host-side stand-in, not the
+// device array, so its device address is looked up once per device with
+// cudaGetSymbolAddress and cached.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = 2u << 20;  // 2 MiB
+constexpr int kNoAllocPartBytes = sizeof(double) + sizeof(int);
+constexpr int kNoAllocMaxParts = (int)(kNoAllocScratchBytes / kNoAllocPartBytes);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (set up on first use).
+int noalloc_scratch(int device, void** out) {
+    if (device < 0 || device >= kMaxDevices) return GCMC_ERR_LIMIT;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            std::fprintf(stderr, "gcmc_b200: cudaGetSymbolAddress(scratch) failed on device %d: %s\n", device,
+                         cudaGetErrorString(e));
+            return GCMC_ERR_CUDA;
+        }
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return GCMC_OK;
+}
+
+// out[p] = sum of the pose's split partials in split order (the order the
+// host-side sum of gcmc_energy_poses uses), ngroups[p] likewise.
+__global__ void k_sum_parts(const double* __restrict__ part, const int* __restrict__ ngpart, int nposes, int nslab,
+                            double* __restrict__ out, int* __restrict__ ngroups) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nposes) return;
+    double e = 0.0;
+    int ng = 0;
+    for (int z = 0; z < nslab; ++z) {
+        e += part[(size_t)p * nslab + z];
+        ng += ngpart[(size_t)p * nslab + z];
+    }
+    out[p] = e;
+    if (ngroups) ngroups[p] = ng;
+}
+
 }  // namespace
 
 extern "C" {
@@ -712,5 +766,37 @@ void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* resi
 }
 
 int gcmc_last_status(void) { return g_last_status; }
+
+int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float* d_site_q,
+                              const int32_t* d_site_type, int32_t nsites, const float* d_centres,
+                              const int32_t* d_self, int32_t nposes, double* d_out, int32_t* d_ngroups,
+                              void* stream) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !d_xyz || !d_site_q || !d_site_type || !d_centres || !d_out)
+        return GCMC_ERR_ARG;
+    if (nsites < 1 || nsites > kMaxSites) return GCMC_ERR_LIMIT;
+    if (nposes <= 0) return GCMC_OK;
+    const int nslab = ctx->reps[rep].nslab;
+    if ((long long)nposes * nslab > kNoAllocMaxParts) {
+        std::fprintf(stderr,
+                     "gcmc_b200: gcmc_energy_poses_noalloc: %d poses x %d splits exceed the %d partials of its "
+                     "fixed %zu-byte scratch (at most %d poses per call for this context)\n",
+                     nposes, nslab, kNoAllocMaxParts, kNoAllocScratchBytes, kNoAllocMaxParts / nslab);
+        return GCMC_ERR_LIMIT;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev != ctx->device) return GCMC_ERR_ARG;
+    void* scratch = nullptr;
+    int st = noalloc_scratch(dev, &scratch);
+    if (st != GCMC_OK) return st;
+    double* part = reinterpret_cast<double*>(scratch);
+    int* ngpart = reinterpret_cast<int*>(part + kNoAllocMaxParts);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->d_reps + rep, d_xyz, d_site_q, d_site_type, nsites,
+                                                          d_centres, d_self, nposes, nslab, part, ngpart);
+    k_sum_parts<<<(nposes + 255) / 256, 256, 0, s>>>(part, ngpart, nposes, nslab, d_out, d_ngroups);
+    CK(cudaGetLastError());
+    return GCMC_OK;
+}
 
 }  // extern "C"
