@@ -111,10 +111,17 @@ typedef struct {
 void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo,
                   Atom* atomInfo, const float* grid, const float* ff, const int* moveArray);
 
-/* Same as runGCMC_cuda with options, returning the status. */
+/* Same as runGCMC_cuda with options, returning the status.  Unlike the
+ * reference (which allocates and frees all device buffers on every call,
+ * gcmc/cpp/gcmc.cu:31-43,107-115), the device context of the last call is
+ * kept and refilled by the next call on the same device (buffers grown only
+ * when a larger system arrives); gcmc_release_cache() frees it.  Calls are
+ * serialised by a lock. */
 int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo,
                   Atom* atomInfo, const float* grid, const float* ff, const int* moveArray,
                   const gcmc_options* opt);
+/* Free the device context kept between runGCMC_cuda / gcmc_run_gcmc calls. */
+int gcmc_release_cache(void);
 
 /* Status of the last runGCMC_cuda call in this thread. */
 int gcmc_last_status(void);

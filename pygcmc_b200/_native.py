@@ -54,6 +54,7 @@ def lib():
         "runGCMC_cuda": (None, [c_void] * 7),
         "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
         "gcmc_last_status": (c_int, []),
+        "gcmc_release_cache": (c_int, []),
         "gcmc_status_string": (ctypes.c_char_p, [c_int]),
         "gcmc_default_options": (None, [P(Options)]),
         "gcmc_create": (c_int, [c_int, P(ReplicaIn), P(Options), c_void, P(c_void)]),
@@ -108,7 +109,7 @@ def default_options(**kw):
     return o
 
 
-EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
+EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",
            "gcmc_energy_poses_noalloc", "gcmc_synth_chain_sphere",

@@ -29,6 +29,7 @@ struct RepHost {
     int nslab = 0, log_cap = 0, log_kmax = 0;
     int host_end = 0;
     std::vector<int> startRes, maxNum, moves_host;
+    size_t capn[24] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
     // device allocations (owned)
     float4* xyzq = nullptr;
     int* atype = nullptr;
@@ -92,11 +93,24 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
+// (Re)allocate *p for n elements unless it already holds at least n.
+template <typename T>
+int ensure(T** p, size_t* cap, size_t n) {
+    if (n == 0) n = 1;
+    if (*p && *cap >= n) return GCMC_OK;
+    dfree(*p);
+    *cap = 0;
+    int st = dalloc(p, n);
+    if (st == GCMC_OK) *cap = n;
+    return st;
+}
+
 void free_rep(RepHost& h) {
     dfree(h.xyzq); dfree(h.atype); dfree(h.gcen); dfree(h.gspan); dfree(h.cell_count); dfree(h.cell_ent);
     dfree(h.gcell); dfree(h.grid); dfree(h.lj); dfree(h.moves); dfree(h.frag); dfree(h.totalNum);
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
+    for (auto& c : h.capn) c = 0;
 }
 
 // Host copy of the device cell index function (floor((x - start) * invLc) mod nc),
@@ -169,6 +183,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     RepHost& h = ctx->reps[r];
     RepDev& d = ctx->repdev[r];
     std::memset(&d, 0, sizeof(d));
+    h.startRes.clear();
+    h.maxNum.clear();
+    h.host_end = 0;
     h.natoms = I->totalAtomNum;
     h.ngroups = I->totalResNum;
     h.ntypes = I->fragTypeNum;
@@ -304,7 +321,8 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     }
 
     int st;
-#define AL(ptr, n) if ((st = dalloc(&(ptr), (size_t)(n))) != GCMC_OK) return st
+    int bi = 0;
+#define AL(ptr, n) if ((st = ensure(&(ptr), &h.capn[bi++], (size_t)(n))) != GCMC_OK) return st
     AL(h.xyzq, h.natoms); AL(h.atype, h.natoms); AL(h.gcen, h.ngroups); AL(h.gspan, h.ngroups);
     AL(h.cell_count, h.ncell); AL(h.cell_ent, (size_t)h.ncell * cap); AL(h.gcell, h.ngroups);
     AL(h.grid, h.G); AL(h.lj, lj.size()); AL(h.moves, h.mcsteps); AL(h.frag, h.ntypes);
@@ -441,6 +459,32 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     *out = ctx;
     return GCMC_OK;
 }
+
+// Load a new single-replica input into an existing context: buffers are reused
+// where large enough, the captured graph is kept (kernels reach every buffer
+// through d_reps), cells are rebuilt and the run state reset.
+int refill_impl(gcmc_ctx* ctx, const gcmc_replica_in& in, const gcmc_options* optp) {
+    if (ctx->nrep != 1) return GCMC_ERR_ARG;
+    gcmc_options opt;
+    if (optp) opt = *optp; else gcmc_default_options(&opt);
+    if (opt.proposal < 0 || opt.proposal > 1) return GCMC_ERR_ARG;
+    int st = validate(in);
+    if (st != GCMC_OK) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    st = setup_rep(ctx, 0, in, opt);
+    if (st != GCMC_OK) return st;
+    CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev), cudaMemcpyHostToDevice, ctx->stream));
+    k_build_cells<<<1, 32, 0, ctx->stream>>>(ctx->d_reps, 1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    int32_t err = 0;
+    gcmc_device_error(ctx, &err);
+    return err ? GCMC_ERR_DEVICE : GCMC_OK;
+}
+
+// The context kept by gcmc_run_gcmc / runGCMC_cuda between calls.
+std::mutex g_cache_mutex;
+gcmc_ctx* g_cache = nullptr;
 
 // ---------------------------------------------------------------------------
 // Allocation-free pose energies (gcmc_energy_poses_noalloc).
@@ -750,14 +794,46 @@ int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* resi
                   const float* grid, const float* ff, const int* moveArray, const gcmc_options* opt) {
     if (!info) return GCMC_ERR_ARG;
     gcmc_replica_in in{info, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray};
-    gcmc_ctx* ctx = nullptr;
-    int st = create_impl(1, &in, opt, nullptr, &ctx);
-    if (st != GCMC_OK) return st;
-    st = gcmc_run(ctx, info->mcsteps);
-    if (st == GCMC_OK) st = gcmc_sync(ctx);
-    if (st == GCMC_OK) st = gcmc_download(ctx, 0, fragmentInfo, residueInfo, atomInfo);
-    destroy_impl(ctx);
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return GCMC_ERR_NODEVICE;
+    }
+    int st = GCMC_OK;
+    if (g_cache && g_cache->device == dev) {
+        st = refill_impl(g_cache, in, opt);
+        if (st != GCMC_OK) {  // drop the cached context and start afresh
+            destroy_impl(g_cache);
+            g_cache = nullptr;
+            if (st == GCMC_ERR_ARG || st == GCMC_ERR_LIMIT) return st;
+        }
+    } else if (g_cache) {
+        destroy_impl(g_cache);
+        g_cache = nullptr;
+    }
+    if (!g_cache) {
+        st = create_impl(1, &in, opt, nullptr, &g_cache);
+        if (st != GCMC_OK) {
+            g_cache = nullptr;
+            return st;
+        }
+    }
+    st = gcmc_run(g_cache, info->mcsteps);
+    if (st == GCMC_OK) st = gcmc_sync(g_cache);
+    if (st == GCMC_OK) st = gcmc_download(g_cache, 0, fragmentInfo, residueInfo, atomInfo);
+    if (st != GCMC_OK) {
+        destroy_impl(g_cache);
+        g_cache = nullptr;
+    }
     return st;
+}
+
+int gcmc_release_cache(void) {
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    if (g_cache) destroy_impl(g_cache);
+    g_cache = nullptr;
+    return GCMC_OK;
 }
 
 void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo, Atom* atomInfo,

@@ -167,3 +167,19 @@ def test_run_in_chunks_equals_one_run(protein_small):
     assert (f1.fragmentInfo["totalNum"] == f2.fragmentInfo["totalNum"]).all()
     a = occupied_atoms(f1)
     assert np.array_equal(f1.atomInfo["position"][a], f2.atomInfo["position"][a])
+
+
+def test_runGCMC_consecutive_calls_reuse_context(protein_small, water_small):
+    """runGCMC keeps its device context between calls; a refill with a different
+    system (other sizes) must give the same result as a fresh engine."""
+    from pygcmc_b200._native import lib
+    from pygcmc_b200.gpu import runGCMC
+    for sysm in (water_small, protein_small, water_small, protein_small):
+        s = sysm.copy()
+        n = int(s.SimInfo[0]["mcsteps"])
+        runGCMC(*s.arrays())
+        _, _, final, _ = engine_trajectory(sysm, n)
+        assert (s.fragmentInfo["totalNum"] == final.fragmentInfo["totalNum"]).all()
+        a = occupied_atoms(s)
+        assert np.array_equal(s.atomInfo["position"][a], final.atomInfo["position"][a])
+    assert lib().gcmc_release_cache() == 0
