@@ -170,6 +170,21 @@ def lj_pair_table(frag_types: Sequence[str], env_types: Sequence[str], nb: dict,
     return t1, t2, ff
 
 
+def group_centres(xyz: np.ndarray, starts: np.ndarray, counts: np.ndarray) -> np.ndarray:
+    """Unweighted group centres with the reference's arithmetic (dataset.py:248-300
+    under its numpy<2 dependency): each coordinate is added in float64 to a
+    float32 running sum that is rounded back to float32, then divided by the
+    count in float64 and stored as float32."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    starts = np.asarray(starts, dtype=np.int64)
+    counts = np.asarray(counts, dtype=np.int64)
+    acc = np.zeros((len(starts), 3), dtype=np.float32)
+    for j in range(int(counts.max()) if len(counts) else 0):
+        m = counts > j
+        acc[m] = (acc[m].astype(np.float64) + xyz[starts[m] + j]).astype(np.float32)
+    return (acc.astype(np.float64) / np.maximum(counts, 1)[:, None]).astype(np.float32)
+
+
 def charmm_to_nb(eps_kcal: float, rmin_half: float):
     """CHARMM (epsilon [kcal/mol], Rmin/2 [A]) -> (sigma [nm], epsilon [kJ/mol])."""
     return (2.0 * rmin_half / 2.0 ** (1.0 / 6.0) / 10.0, V.KCAL_TO_KJ * eps_kcal)
@@ -184,8 +199,7 @@ def assemble(*, names: Sequence[str], templates: Sequence[dict], initial: Sequen
 
     ``templates[i]`` = ``{"xyz": (n,3), "q": (n,), "type": (n,)}`` (type = column
     index of ff); ``initial[i]`` = list of (n,3) site arrays already in the box.
-    Group centres are accumulated in float32, as the reference's numpy field
-    arithmetic does.
+    Group centres follow the reference's arithmetic (see :func:`group_centres`).
     """
     nt = len(names)
     volume = float(cryst[0]) * float(cryst[1]) * float(cryst[2])
@@ -194,7 +208,7 @@ def assemble(*, names: Sequence[str], templates: Sequence[dict], initial: Sequen
     for i in range(nt):
         t = templates[i]
         xyz = np.asarray(t["xyz"], dtype=np.float64)
-        xyz = xyz - xyz.mean(axis=0)
+        xyz = xyz - np.cumsum(xyz, axis=0)[-1] / len(xyz)  # sequential sum, as dataset.py:219-222
         frag[i]["name"] = names[i].ljust(4)[:4].encode()
         frag[i]["muex"] = muex[i]
         frag[i]["conc"] = conc[i]
@@ -221,12 +235,9 @@ def assemble(*, names: Sequence[str], templates: Sequence[dict], initial: Sequen
         bounds = np.flatnonzero(np.diff(fixed_group)) + 1
         starts = np.concatenate([[0], bounds])
         ends = np.concatenate([bounds, [nfix]])
-        f32 = np.asarray(fixed_xyz, dtype=np.float32)
-        for g, (a, b) in enumerate(zip(starts, ends)):
-            res[g]["atomStart"] = a
-            res[g]["atomNum"] = b - a
-            acc = np.cumsum(f32[a:b], axis=0, dtype=np.float32)[-1]  # sequential float32 sum
-            res[g]["position"] = acc / np.float32(b - a)
+        res["atomStart"][:len(starts)] = starts
+        res["atomNum"][:len(starts)] = ends - starts
+        res["position"][:len(starts)] = group_centres(fixed_xyz, starts, ends - starts)
     seq = ngroups_fixed
     next_atom = nfix
     for i in range(nt):
@@ -236,12 +247,11 @@ def assemble(*, names: Sequence[str], templates: Sequence[dict], initial: Sequen
             res[seq]["atomNum"] = na
             res[seq]["atomStart"] = next_atom
             if j < len(initial[i]):
-                p = np.asarray(initial[i][j], dtype=np.float32)
+                p = np.asarray(initial[i][j], dtype=np.float64)
                 atoms["position"][next_atom:next_atom + na] = p
                 atoms["charge"][next_atom:next_atom + na] = templates[i]["q"]
                 atoms["type"][next_atom:next_atom + na] = templates[i]["type"]
-                acc = np.cumsum(p, axis=0, dtype=np.float32)[-1]
-                res[seq]["position"] = acc / np.float32(na)
+                res[seq]["position"] = group_centres(p, [0], [na])[0]
             next_atom += na
             seq += 1
     info = np.zeros(1, dtype=V.Info_dtype)
