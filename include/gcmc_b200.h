@@ -206,6 +206,11 @@ int gcmc_synth_chain_sphere(int n, const float centre[3], float radius, float st
 int gcmc_synth_chain_slab(int n, float lo0, float hi0, float lo1, float hi1, float zc, float half,
                           float px, float py, float pore, float step, float excl, uint64_t seed,
                           float* out_xyz, int* n_breaks);
+/* count random non-clashing copies (sites >= min_dist from all atoms) of a rigid
+ * template in the periodic box [lo, lo+L); out_xyz[count*nsites*3]. */
+int gcmc_synth_place(int n_existing, const float* existing_xyz, const float lo[3], const float L[3],
+                     const float* tpl_xyz, int nsites, int count, float min_dist, uint64_t seed,
+                     float* out_xyz);
 
 #ifdef __cplusplus
 }

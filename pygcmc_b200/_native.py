@@ -76,6 +76,8 @@ def lib():
                                             ctypes.c_uint64, c_void, P(ctypes.c_int)]),
         "gcmc_synth_chain_slab": (c_int, [c_int] + [ctypes.c_float] * 12 + [ctypes.c_uint64, c_void,
                                                                            P(ctypes.c_int)]),
+        "gcmc_synth_place": (c_int, [c_int, c_void, c_void, c_void, c_void, c_int, c_int, ctypes.c_float,
+                                     ctypes.c_uint64, c_void]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -112,5 +114,5 @@ def default_options(**kw):
 EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",
-           "gcmc_energy_poses_noalloc", "gcmc_synth_chain_sphere",
+           "gcmc_energy_poses_noalloc", "gcmc_synth_place", "gcmc_synth_chain_sphere",
            "gcmc_synth_chain_slab"]

@@ -6,6 +6,7 @@
 // (bonded = the two preceding atoms).  When a step cannot be placed after a
 // bounded number of trials the chain restarts at a random free point (a chain
 // break).  A cell hash of side `excl` makes each trial O(1).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <unordered_map>
@@ -123,9 +124,95 @@ int grow_chain(const Region& reg, int n, double step, double excl, uint64_t seed
     return 0;
 }
 
+// Periodic cell hash over a box (for rigid-body placement).
+struct PeriodicHash {
+    double lo[3], L[3], h;
+    int n[3];
+    std::vector<std::vector<double>> cells;  // xyz triples per cell
+    PeriodicHash(const double lo_[3], const double L_[3], double side) : h(side) {
+        for (int i = 0; i < 3; ++i) {
+            lo[i] = lo_[i];
+            L[i] = L_[i];
+            n[i] = std::max(1, (int)std::floor(L[i] / side));
+        }
+        cells.resize((size_t)n[0] * n[1] * n[2]);
+    }
+    int idx(int a, int i) const { return ((a % n[i]) + n[i]) % n[i]; }
+    int coord(double x, int i) const { return idx((int)std::floor((x - lo[i]) / L[i] * n[i]), i); }
+    void add(const double p[3]) {
+        auto& c = cells[((size_t)coord(p[2], 2) * n[1] + coord(p[1], 1)) * n[0] + coord(p[0], 0)];
+        c.insert(c.end(), p, p + 3);
+    }
+    bool clear(const double p[3], double r) const {
+        const int cx = coord(p[0], 0), cy = coord(p[1], 1), cz = coord(p[2], 2);
+        const int rx = std::min(n[0], 3), ry = std::min(n[1], 3), rz = std::min(n[2], 3);
+        for (int dz = 0; dz < rz; ++dz)
+            for (int dy = 0; dy < ry; ++dy)
+                for (int dx = 0; dx < rx; ++dx) {
+                    const auto& c = cells[((size_t)idx(cz + dz - (rz > 1), 2) * n[1] + idx(cy + dy - (ry > 1), 1)) * n[0] +
+                                          idx(cx + dx - (rx > 1), 0)];
+                    for (size_t k = 0; k < c.size(); k += 3) {
+                        double d2 = 0.0;
+                        for (int i = 0; i < 3; ++i) {
+                            double d = c[k + i] - p[i];
+                            d -= L[i] * std::round(d / L[i]);
+                            d2 += d * d;
+                        }
+                        if (d2 < r * r) return false;
+                    }
+                }
+        return true;
+    }
+};
+
 }  // namespace
 
 extern "C" {
+
+// `count` copies of a rigid template (nsites x 3, centred) at uniformly random
+// positions and orientations in the periodic box [lo, lo+L), each site at
+// least min_dist from every atom already present (existing atoms and earlier
+// copies).  Returns 0, or -1 when a copy cannot be placed.
+int gcmc_synth_place(int n_existing, const float* existing_xyz, const float lo[3], const float L[3],
+                     const float* tpl_xyz, int nsites, int count, float min_dist, uint64_t seed,
+                     float* out_xyz) {
+    double lo_d[3] = {lo[0], lo[1], lo[2]}, L_d[3] = {L[0], L[1], L[2]};
+    PeriodicHash hash(lo_d, L_d, std::max(1e-3, (double)min_dist));
+    for (int a = 0; a < n_existing; ++a) {
+        double p[3] = {existing_xyz[3 * a], existing_xyz[3 * a + 1], existing_xyz[3 * a + 2]};
+        hash.add(p);
+    }
+    SplitMix64 r(seed);
+    std::vector<double> site((size_t)nsites * 3);
+    for (int c = 0; c < count; ++c) {
+        bool placed = false;
+        for (int t = 0; t < 200000 && !placed; ++t) {
+            // uniform rotation (Shoemake) and uniform position
+            const double u1 = r.uniform(), u2 = 2 * M_PI * r.uniform(), u3 = 2 * M_PI * r.uniform();
+            const double a = std::sqrt(1 - u1), b = std::sqrt(u1);
+            const double x = a * std::sin(u2), y = a * std::cos(u2), z = b * std::sin(u3), w = b * std::cos(u3);
+            const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)},
+                                    {2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)},
+                                    {2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)}};
+            double cen[3];
+            for (int i = 0; i < 3; ++i) cen[i] = lo_d[i] + r.uniform() * L_d[i];
+            placed = true;
+            for (int s = 0; s < nsites && placed; ++s) {
+                for (int i = 0; i < 3; ++i)
+                    site[3 * s + i] = cen[i] + R[i][0] * tpl_xyz[3 * s] + R[i][1] * tpl_xyz[3 * s + 1] +
+                                      R[i][2] * tpl_xyz[3 * s + 2];
+                placed = hash.clear(&site[3 * s], min_dist);
+            }
+        }
+        if (!placed) return -1;
+        for (int s = 0; s < nsites; ++s) {
+            hash.add(&site[3 * s]);
+            for (int i = 0; i < 3; ++i) out_xyz[((size_t)c * nsites + s) * 3 + i] = (float)site[3 * s + i];
+        }
+    }
+    return 0;
+}
+
 
 // Chain of n atoms inside a sphere; returns 0, or -1 when the sphere cannot hold it.
 int gcmc_synth_chain_sphere(int n, const float centre[3], float radius, float step, float excl,

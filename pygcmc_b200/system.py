@@ -441,15 +441,21 @@ def protein_system(seed: int = 1, n_atoms: int = 6000, box: float = 64.0, radius
     if n_initial is None:
         n_initial = int(round(conc * float(np.prod(L)) * V.MOLES_TO_MOLECULES))
     initial = []
-    existing = xyz.astype(np.float64)
+    existing = np.ascontiguousarray(xyz, dtype=np.float32)
+    lo = np.zeros(3, np.float32)
+    Lf = L.astype(np.float32)
     for f in range(n_frag):
-        tx = templates[f]["xyz"] - templates[f]["xyz"].mean(axis=0)
-        start0 = np.zeros(3)
-        placed = _place_rigid(g, tx, n_initial, L, start0, existing, 2.0)
-        initial.append(placed)
-        if placed:
-            existing = np.concatenate([existing] + placed)
-    all_xyz = existing
+        tx = np.ascontiguousarray(templates[f]["xyz"] - templates[f]["xyz"].mean(axis=0), dtype=np.float32)
+        ns = len(tx)
+        out = np.zeros((n_initial, ns, 3), np.float32)
+        if n_initial:
+            rc = lib().gcmc_synth_place(len(existing), ptr(existing), ptr(lo), ptr(Lf), ptr(tx), ns, n_initial, 2.0,
+                                        int(seed) * 104729 + 31 * f + 7, ptr(out))
+            if rc != 0:
+                raise RuntimeError("could not place the initial fragment copies")
+            existing = np.ascontiguousarray(np.concatenate([existing, out.reshape(-1, 3)]))
+        initial.append([out[c].astype(np.float64) for c in range(n_initial)])
+    all_xyz = existing.astype(np.float64)
     start, grid, cav, dx = cavity_grid(all_xyz, L, grid_dx)
     groups = fix_groups(xyz, 6.0)
     if moves is None:
