@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark: MC trial moves/s of the GCMC hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload protein|batched]
 
 Workload (one replica per GPU): the synthetic protein system -- 6000 fixed
 atoms of a confined random-walk chain in a 64 A periodic box, eight rigid
@@ -11,8 +11,13 @@ A bench step is CHUNK MC steps (moveArray entries); `value` is MC steps/s with
 the state resident on the GPU, `e2e` the same through the runGCMC drop-in
 with host arrays (upload, run, download inside the timed region).
 
+--workload batched: 64 replicas of uneven size (2000-40000 atoms, a muex scan)
+advanced together in one context, with the launch shape from the autotuner;
+`e2e` through the batched drop-in runGCMC_batch.
+
 --impl reference times the reference's own runGCMC_cuda (built unmodified
-from its sources into oracle/_ref) on the same workload.
+from its sources into oracle/_ref) on the same workload (batched: one
+replica after another, as the reference has no batched form).
 Under torchrun every rank runs an independent replica (its own seed) on its
 own GPU; times are the max over ranks ("replicas only", weak scaling).
 """
@@ -245,33 +250,144 @@ def run_ours(args, ws, rank, local):
     return out
 
 
-def run_reference(args, ws, rank, local):
-    if rank != 0:
-        return None
-    lib_path = os.path.join(ROOT, "oracle", "_ref", "libgcmc_ref.so")
-    if not os.path.exists(lib_path):
-        return {"impl": "reference", "unavailable": "oracle/_ref/libgcmc_ref.so not built (make -C oracle ref)"}
+BATCH_WORKLOAD = ("64 replicas of uneven size in one context: synthetic proteins of 2000-40000 atoms "
+                  "(log-uniform), box 40-100 A at constant protein density, 8 fragments each, muex scan "
+                  "-8..0 kcal/mol, own seeds, confBias 1000, cutoff 12 A, reference semantics")
+
+
+def make_batch(seed, mcsteps, n_rep):
+    from pygcmc_b200 import system as S
+    return S.replica_batch(n_rep=n_rep, seed=seed, mcsteps=mcsteps)
+
+
+def run_ours_batched(args, ws, rank, local):
+    """All replicas of the batch advance in one context (one pose-energy and one
+    accept launch per MC step, replayed from a CUDA graph); the launch shape
+    comes from the autotuner, run before the timed region."""
     import torch
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine, autotune
+    from pygcmc_b200.gpu import runGCMC_batch
     torch.cuda.set_device(local)
-    L = ctypes.CDLL(lib_path)
-    L.runGCMC_cuda.restype = None
-    L.runGCMC_cuda.argtypes = [ctypes.c_void_p] * 7
-    chunk = args.ref_chunk
-    seed = args.seed
-    s = make_system(seed, (args.warmup + args.steps + 2) * chunk + 16)
-    info = s.SimInfo.copy()
-    moves = s.moveArray
-    skipped = [0]
+    chunk = args.chunk
+    seed = args.seed + 1000 * rank
+    prof_steps = 64
+    total = (args.warmup + args.steps) * chunk + prof_steps + 256
+    t0 = time.perf_counter()
+    systems = make_batch(seed, total, args.replicas)
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    best, trials = autotune(systems, default_options(), trial_steps=64)
+    t_tune = time.perf_counter() - t0
+    nrep = len(systems)
+    eng = Engine([x.copy() for x in systems], best)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        eng.run(chunk)
+    eng.sync()
+    c0 = [eng.counters(r) for r in range(nrep)]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    for a, b in evs:
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a.record(stream)
+        eng.run(chunk)
+        b.record(stream)
+    eng.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), ws)
+    barrier(ws)
+    c1 = [eng.counters(r) for r in range(nrep)]
+    te, ta, _ = eng.run_profiled(prof_steps)
+    c2 = [eng.counters(r) for r in range(nrep)]
+    eng.close()
+    # end to end: the batched drop-in with host arrays (upload, run, download per call)
+    state = [x.copy() for x in systems]
+    h2d = sum(sum(a.nbytes for a in s.arrays()[:6]) + 4 * chunk for s in state)
+    d2h = sum(s.fragmentInfo.nbytes + s.residueInfo.nbytes + s.atomInfo.nbytes for s in state)
+    full_moves = [s.moveArray for s in systems]
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        for r, s in enumerate(state):
+            s.SimInfo[0]["mcsteps"] = chunk
+            s.SimInfo[0]["seed"] = (seed * 7 + 131 * r + k) & 0xFFFFFFFF
+            s.moveArray = np.ascontiguousarray(full_moves[r][k * chunk:(k + 1) * chunk])
+        barrier(ws)
+        t0 = time.perf_counter()
+        runGCMC_batch(state, best)
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(e2e_times) * 1e3, ws) / 1e3
+    moves_all = args.steps * chunk * nrep * ws
+    pairs_prof = sum(b["pairs"] - a["pairs"] for a, b in zip(c1, c2))
+    e_ms, a_ms = float(te.sum()), float(ta.sum())
+    sm_max = (clk or {}).get("sm_max_mhz") or 1965.0
+    peak, sms = nominal_fp32_tflops(sm_max)
+    achieved = pairs_prof * FLOPS_PER_PAIR / (e_ms / 1e3) / 1e12
+    launches = args.steps * (2 + 2 * 32 * best.branches * ((chunk + 31) // 32))
+    out = {
+        "metric": METRIC, "value": round(moves_all / (ms / 1e3), 1), "unit": "moves/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair terms, fp64 sums/acceptance", "data": "synthetic (seeded generator; no public dataset)",
+        "config": {"workload": BATCH_WORKLOAD, "replicas_per_gpu": nrep, "mc_steps_per_bench_step": chunk,
+                   "atoms_per_replica": [int(s.info["totalAtomNum"]) for s in systems][:nrep],
+                   "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
+                   "autotuned": {"cells_per_cutoff": best.cells_per_cutoff, "split_items": best.split_items,
+                                 "branches": best.branches, "energy_blocks_per_sm": best.energy_blocks_per_sm,
+                                 "trials": len(trials), "tune_s": round(t_tune, 2),
+                                 "trial_ms_per_step": [[*t[:4], round(t[4], 4)] for t in trials]},
+                   "generate_s": round(t_gen, 2)},
+        "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
+                "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+        "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies, all replicas)",
+                     "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 5),
+                     "peak_source": f"nominal FP32: {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                                    "(MEASURED_PEAKS.json has no FP32 figure)",
+                     "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_prof / prof_steps,
+                     "avg_launch_us": e_ms / prof_steps * 1e3, "traffic": None,
+                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3),
+                     "timing": "kernels launched one by one (no graph, one branch) over the next 64 steps"},
+        "roofline_accept": {"kernel": "k_accept (1 CTA per replica)", "avg_launch_us": a_ms / prof_steps * 1e3,
+                            "share_of_step_time": round(a_ms / (e_ms + a_ms), 3)},
+        "pairs_per_s": round(sum(b["pairs"] - a["pairs"] for a, b in zip(c0, c1)) / (ms / 1e3), 1),
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(seed)
+        out["cpu_baseline"]["sample"] += " (one 6000-atom replica; replicas are independent, so the CPU rate " \
+                                         "for the batch is this rate at the same cores)"
+    return out
 
-    def call(mv):
-        info[0]["mcsteps"] = len(mv)
+
+class RefRunner:
+    """The reference's runGCMC_cuda driven over a step range of one system."""
+
+    def __init__(self, L, system, seed):
+        self.L, self.s, self.seed = L, system, seed
+        self.info = system.SimInfo.copy()
+        self.skipped = 0
+
+    def call(self, mv):
+        s = self.s
+        self.info[0]["mcsteps"] = len(mv)
         with quiet_stdout():
-            L.runGCMC_cuda(info.ctypes.data, s.fragmentInfo.ctypes.data, s.residueInfo.ctypes.data,
-                           s.atomInfo.ctypes.data, s.grid.ctypes.data, s.ff.ctypes.data, mv.ctypes.data)
+            self.L.runGCMC_cuda(self.info.ctypes.data, s.fragmentInfo.ctypes.data, s.residueInfo.ctypes.data,
+                                s.atomInfo.ctypes.data, s.grid.ctypes.data, s.ff.ctypes.data, mv.ctypes.data)
 
-    def run_range(a, b):
+    def run_range(self, a, b):
         """Steps [a, b) in slices; a delete on an empty fragment type (where the
-        reference divides by zero, gcmc_move_del.h:316) is skipped."""
+        reference divides by zero, gcmc_move_del.h:316) is skipped.  Returns the
+        number of calls made."""
+        s, moves = self.s, self.s.moveArray
         calls = 0
         pos = a
         while pos < b:
@@ -285,54 +401,84 @@ def run_reference(args, ws, rank, local):
                     tot[f] -= 1
                 q += 1
             if q == pos:
-                skipped[0] += 1
+                self.skipped += 1
                 pos += 1
                 continue
-            info[0]["seed"] = (seed * 131 + pos) & 0xFFFFFFFF
-            call(np.ascontiguousarray(moves[pos:q]))
+            self.info[0]["seed"] = (self.seed * 131 + pos) & 0xFFFFFFFF
+            self.call(np.ascontiguousarray(moves[pos:q]))
             calls += 1
             pos = q
         return calls
 
-    # fixed per-call cost (allocation, copies, RNG set-up) from zero-step calls
-    t_fix = []
-    for _ in range(3):
-        t0 = time.perf_counter()
-        call(np.zeros(1, np.int32)[:0])
-        torch.cuda.synchronize()
-        t_fix.append(time.perf_counter() - t0)
-    fixed = float(np.median(t_fix))
+    def fixed_cost(self):
+        """Per-call set-up time (allocation, copies, RNG set-up) from zero-step calls."""
+        import torch
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            self.call(np.zeros(1, np.int32)[:0])
+            torch.cuda.synchronize()
+            t.append(time.perf_counter() - t0)
+        return float(np.median(t))
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return None
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libgcmc_ref.so")
+    if not os.path.exists(lib_path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libgcmc_ref.so not built (make -C oracle ref)"}
+    import torch
+    torch.cuda.set_device(local)
+    L = ctypes.CDLL(lib_path)
+    L.runGCMC_cuda.restype = None
+    L.runGCMC_cuda.argtypes = [ctypes.c_void_p] * 7
+    chunk = args.ref_chunk
+    seed = args.seed
+    batched = args.workload == "batched"
+    if batched:
+        systems = make_batch(seed, (args.warmup + args.steps + 2) * chunk + 16, args.replicas)
+    else:
+        systems = [make_system(seed, (args.warmup + args.steps + 2) * chunk + 16)]
+    runners = [RefRunner(L, s, seed + 7 * r) for r, s in enumerate(systems)]
+    fixed = runners[0].fixed_cost()
     pos = 0
     for _ in range(args.warmup):
-        run_range(pos, pos + chunk)
+        for rr in runners:
+            rr.run_range(pos, pos + chunk)
         pos += chunk
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     t_raw, t_adj, n = 0.0, 0.0, 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        calls = run_range(pos, pos + chunk)
+        calls = 0
+        for rr in runners:
+            calls += rr.run_range(pos, pos + chunk)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         t_raw += dt
         t_adj += max(dt - calls * fixed, 1e-9)
         pos += chunk
-        n += chunk
+        n += chunk * len(runners)
     clk = clocks.stop()
     value = n / t_adj
+    workload = BATCH_WORKLOAD if batched else WORKLOAD
+    how = (f"each of the {len(runners)} replicas in turn, {chunk} steps per replica per bench step"
+           if batched else f"{chunk} steps per bench step")
     return {
         "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_adj / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (reference kernels)", "impl": "reference",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
-                   "parallelism": "replicas x1"},
+        "config": {"workload": workload, "mc_steps_per_bench_step": chunk * len(runners),
+                   "replicas_per_gpu": len(runners), "parallelism": "replicas x1", "schedule": how},
         "cpu_baseline": {"value": round(value, 1), "unit": "moves/s", "cores": 1, "kind": "reference",
                          "sample": f"reference runGCMC_cuda (unmodified pyGCMC gcmc.cu, sm_100a) on the B200, "
-                                   f"{n} MC steps; the reference has no CPU implementation of this path; "
-                                   f"per-call set-up ({fixed * 1e3:.2f} ms) subtracted"},
+                                   f"{n} MC steps ({how}); the reference has no CPU implementation of this "
+                                   f"path; per-call set-up ({fixed * 1e3:.2f} ms) subtracted"},
         "e2e": {"value": round(n / t_raw, 1), "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "skipped_deletes_on_empty_types": skipped[0],
+        "skipped_deletes_on_empty_types": sum(rr.skipped for rr in runners),
         "clocks": clk,
     }
 
@@ -359,7 +505,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--chunk", type=int, default=2048, help="MC steps per bench step (ours)")
+    ap.add_argument("--workload", choices=["protein", "batched"], default="protein",
+                    help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU")
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--chunk", type=int, default=0, help="MC steps per bench step (default 2048; batched 256)")
     ap.add_argument("--ref-chunk", type=int, default=0,
                     help="MC steps per bench step for the reference arm (default: --chunk, same step range)")
     ap.add_argument("--cells", type=int, default=2)
@@ -367,8 +516,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.chunk <= 0:
+        args.chunk = 256 if args.workload == "batched" else 2048
     if args.ref_chunk <= 0:
-        args.ref_chunk = args.chunk
+        args.ref_chunk = 16 if args.workload == "batched" else args.chunk
     ws, rank, local = dist_env()
     if ws > 1:
         import datetime
@@ -377,7 +528,12 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        out = run_reference(args, ws, rank, local) if args.impl == "reference" else run_ours(args, ws, rank, local)
+        if args.impl == "reference":
+            out = run_reference(args, ws, rank, local)
+        elif args.workload == "batched":
+            out = run_ours_batched(args, ws, rank, local)
+        else:
+            out = run_ours(args, ws, rank, local)
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

@@ -80,7 +80,19 @@ typedef struct {
     int32_t log_kmax;    /* per-step pose energies recorded (<= 1024)               */
     int32_t split_items; /* target pose-energy work items per step: each pose's cell
                             window is split into ~split_items/poses ranges; 0 = 2048 */
+    int32_t branches;    /* independent chains of the captured step loop: the
+                            replicas are split into this many contiguous groups
+                            (balanced by atom count) whose kernels run
+                            concurrently; 0 = 1                                     */
+    int32_t energy_blocks_per_sm; /* pose-energy kernel CTAs per SM (0 = the
+                            occupancy limit)                                        */
 } gcmc_options;
+
+/* One autotuner trial (gcmc_autotune). */
+typedef struct {
+    int32_t cells_per_cutoff, split_items, branches, energy_blocks_per_sm;
+    float ms_per_step;   /* device time per MC step (all replicas)                  */
+} gcmc_tune_trial;
 
 /* One per-step record (48 bytes). */
 typedef struct {
@@ -120,8 +132,18 @@ void runGCMC_cuda(const InfoStruct* info, AtomArray* fragmentInfo, residue* resi
 int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* residueInfo,
                   Atom* atomInfo, const float* grid, const float* ff, const int* moveArray,
                   const gcmc_options* opt);
-/* Free the device context kept between runGCMC_cuda / gcmc_run_gcmc calls. */
+/* Free the device contexts kept between runGCMC_cuda / gcmc_run_gcmc /
+ * gcmc_run_batch calls. */
 int gcmc_release_cache(void);
+
+/* Batched drop-in (no counterpart in the reference, which runs one system per
+ * runGCMC_cuda call): runs each replica's info->mcsteps steps in ONE device
+ * context -- all replicas advance together, one pose-energy launch and one
+ * accept launch per MC step -- and writes every replica's totalNum,
+ * residueInfo and atomInfo back in place (the arrays behind reps[r] are
+ * written although the struct holds const pointers).  The context is kept
+ * between calls with the same replica count, like gcmc_run_gcmc's. */
+int gcmc_run_batch(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* opt);
 
 /* Status of the last runGCMC_cuda call in this thread. */
 int gcmc_last_status(void);
@@ -161,6 +183,18 @@ int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);
 /* The cudaStream_t the context launches on. */
 void* gcmc_stream(gcmc_ctx* ctx);
 int gcmc_destroy(gcmc_ctx* ctx);
+
+/* Launch-shape autotuner (no counterpart in the reference).  For the given
+ * replicas, times trial_steps MC steps (after 8 warm-up steps) on temporary
+ * contexts for a coordinate-descent sequence of candidates -- cell-grid
+ * resolution (cells_per_cutoff 1..3), pose-energy work split (split_items
+ * 512..8192), graph branches (1, 2, 4) and pose-energy CTAs per SM -- and
+ * writes the base options with the fastest shape into *best.  trials
+ * (optional, max_trials entries) receives each trial; *ntrials their number.
+ * The inputs are not modified; the trajectories of a context created with
+ * *best are the same MC chain up to FP32 summation order. */
+int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* base, int32_t trial_steps,
+                  gcmc_options* best, gcmc_tune_trial* trials, int32_t max_trials, int32_t* ntrials);
 
 /* Energies of explicit poses against replica `rep`'s current state
  * (the calcEnergy of gcmc/cpp/gcmc_energy.h:142-204, batched).

@@ -65,7 +65,10 @@ struct gcmc_ctx {
     std::vector<RepDev> repdev;
     RepDev* d_reps = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    int gridE = 0;
+    int gridE = 0;       // pose-energy CTAs for all replicas
+    int branches = 1;    // independent chains in the captured step loop
+    int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
+    std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
 };
 
 namespace {
@@ -368,18 +371,91 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     return GCMC_OK;
 }
 
-int build_graph(gcmc_ctx* ctx) {
-    cudaGraph_t graph;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < kGraphSteps; ++s) {
-        k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
-        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);
-    }
-    CK(cudaStreamEndCapture(ctx->stream, &graph));
-    cudaError_t e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    CK(e);
+// Pose-energy grid: SMs x min(occupancy limit, requested CTAs per SM).
+int set_energy_grid(gcmc_ctx* ctx, int ebps) {
+    int sms = 0, per_sm = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy, kWarpsE * 32, 0));
+    per_sm = std::max(1, per_sm);
+    if (ebps > 0) per_sm = std::min(per_sm, ebps);
+    ctx->ebps = ebps;
+    ctx->gridE = std::max(1, sms) * per_sm;
     return GCMC_OK;
+}
+
+// Split the replicas into `nb` contiguous groups of about equal atom count.
+void split_branches(gcmc_ctx* ctx, int nb) {
+    nb = std::max(1, std::min(nb, ctx->nrep));
+    std::vector<double> pre(ctx->nrep + 1, 0.0);
+    for (int r = 0; r < ctx->nrep; ++r) pre[r + 1] = pre[r] + (double)ctx->reps[r].natoms + 1.0;
+    ctx->br_off.assign(nb + 1, 0);
+    ctx->br_off[nb] = ctx->nrep;
+    for (int b = 1; b < nb; ++b) {
+        const double target = pre[ctx->nrep] * b / nb;
+        int r = ctx->br_off[b - 1] + 1;
+        while (r < ctx->nrep - (nb - b) && pre[r] < target) ++r;
+        ctx->br_off[b] = r;
+    }
+    ctx->branches = nb;
+}
+
+// kGraphSteps MC steps.  With several branches, each branch is its own chain
+// of (pose-energy, accept) launches over its replicas, forked from and joined
+// to the context's stream, so one branch's accept kernel (a CTA per replica)
+// overlaps another's pose energies; each branch gets a share of the
+// pose-energy grid in proportion to its atoms.
+int build_graph(gcmc_ctx* ctx) {
+    if (ctx->gexec) {
+        cudaGraphExecDestroy(ctx->gexec);
+        ctx->gexec = nullptr;
+    }
+    const int nb = ctx->branches;
+    std::vector<cudaStream_t> side(nb, nullptr);
+    std::vector<cudaEvent_t> ev(nb, nullptr);
+    int st = GCMC_OK;
+    for (int b = 1; b < nb && st == GCMC_OK; ++b)
+        if (cudaStreamCreateWithFlags(&side[b], cudaStreamNonBlocking) != cudaSuccess) st = GCMC_ERR_CUDA;
+    for (int b = 0; b < nb && st == GCMC_OK; ++b)
+        if (cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming) != cudaSuccess) st = GCMC_ERR_CUDA;
+    cudaGraph_t graph = nullptr;
+    if (st == GCMC_OK && cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        st = GCMC_ERR_CUDA;
+    if (st == GCMC_OK) {
+        side[0] = ctx->stream;
+        double tot = 0.0;
+        for (int r = 0; r < ctx->nrep; ++r) tot += (double)ctx->reps[r].natoms + 1.0;
+        cudaError_t e = cudaEventRecord(ev[0], ctx->stream);
+        for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(side[b], ev[0], 0);
+        for (int b = 0; b < nb && e == cudaSuccess; ++b) {
+            const int r0 = ctx->br_off[b], cnt = ctx->br_off[b + 1] - r0;
+            double part = 0.0;
+            for (int r = r0; r < r0 + cnt; ++r) part += (double)ctx->reps[r].natoms + 1.0;
+            const int grid = nb == 1 ? ctx->gridE : std::max(1, (int)std::ceil(ctx->gridE * part / tot));
+            for (int s = 0; s < kGraphSteps; ++s) {
+                k_energy<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
+                k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt);
+            }
+            e = cudaGetLastError();
+        }
+        for (int b = 1; b < nb && e == cudaSuccess; ++b) {
+            e = cudaEventRecord(ev[b], side[b]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ev[b], 0);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            std::fprintf(stderr, "gcmc_b200: graph capture failed: %s\n",
+                         cudaGetErrorString(e != cudaSuccess ? e : e2));
+            st = GCMC_ERR_CUDA;
+        }
+    }
+    if (st == GCMC_OK && cudaGraphInstantiate(&ctx->gexec, graph, 0) != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+    for (int b = 1; b < nb; ++b)
+        if (side[b]) cudaStreamDestroy(side[b]);
+    for (int b = 0; b < nb; ++b)
+        if (ev[b]) cudaEventDestroy(ev[b]);
+    if (st != GCMC_OK) cudaGetLastError();
+    return st;
 }
 
 int destroy_impl(gcmc_ctx* ctx) {
@@ -436,11 +512,9 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
                                  (int)sizeof(AcceptSmem)) != cudaSuccess)
             st = GCMC_ERR_CUDA;
     }
+    if (st == GCMC_OK) st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
     if (st == GCMC_OK) {
-        int sms = 0, per_sm = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy, kWarpsE * 32, 0);
-        ctx->gridE = std::max(1, sms) * std::max(1, per_sm);
+        split_branches(ctx, opt.branches > 0 ? opt.branches : 1);
         k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
         if (cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
     }
@@ -460,31 +534,85 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     return GCMC_OK;
 }
 
-// Load a new single-replica input into an existing context: buffers are reused
-// where large enough, the captured graph is kept (kernels reach every buffer
-// through d_reps), cells are rebuilt and the run state reset.
-int refill_impl(gcmc_ctx* ctx, const gcmc_replica_in& in, const gcmc_options* optp) {
-    if (ctx->nrep != 1) return GCMC_ERR_ARG;
+// Load new inputs (same replica count) into an existing context: buffers are
+// reused where large enough, the captured graph is kept when the launch shape
+// is unchanged (kernels reach every buffer through d_reps), cells are rebuilt
+// and the run state reset.
+int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_options* optp) {
+    if (ctx->nrep != nrep) return GCMC_ERR_ARG;
     gcmc_options opt;
     if (optp) opt = *optp; else gcmc_default_options(&opt);
     if (opt.proposal < 0 || opt.proposal > 1) return GCMC_ERR_ARG;
-    int st = validate(in);
+    int st = GCMC_OK;
+    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = validate(ins[r]);
     if (st != GCMC_OK) return st;
     CK(cudaStreamSynchronize(ctx->stream));
-    st = setup_rep(ctx, 0, in, opt);
+    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
     if (st != GCMC_OK) return st;
-    CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev), cudaMemcpyHostToDevice, ctx->stream));
-    k_build_cells<<<1, 32, 0, ctx->stream>>>(ctx->d_reps, 1);
+    CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
     CK(cudaGetLastError());
+    const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
+    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps) {
+        st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
+        if (st != GCMC_OK) return st;
+        split_branches(ctx, nb);
+        st = build_graph(ctx);
+        if (st != GCMC_OK) return st;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     int32_t err = 0;
     gcmc_device_error(ctx, &err);
     return err ? GCMC_ERR_DEVICE : GCMC_OK;
 }
 
-// The context kept by gcmc_run_gcmc / runGCMC_cuda between calls.
+// The contexts kept by gcmc_run_gcmc / runGCMC_cuda (one replica) and by
+// gcmc_run_batch between calls.
 std::mutex g_cache_mutex;
 gcmc_ctx* g_cache = nullptr;
+gcmc_ctx* g_batch = nullptr;
+
+// Refill *slot (or create it) for these inputs, run every replica's mcsteps
+// steps and download the results in place.  Called under g_cache_mutex.
+int cached_run(gcmc_ctx** slot, int nrep, const gcmc_replica_in* ins, const gcmc_options* opt) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return GCMC_ERR_NODEVICE;
+    }
+    int st = GCMC_OK;
+    if (*slot && (*slot)->device == dev && (*slot)->nrep == nrep) {
+        st = refill_impl(*slot, nrep, ins, opt);
+        if (st != GCMC_OK) {  // drop the cached context and start afresh
+            destroy_impl(*slot);
+            *slot = nullptr;
+            if (st == GCMC_ERR_ARG || st == GCMC_ERR_LIMIT) return st;
+        }
+    } else if (*slot) {
+        destroy_impl(*slot);
+        *slot = nullptr;
+    }
+    if (!*slot) {
+        st = create_impl(nrep, ins, opt, nullptr, slot);
+        if (st != GCMC_OK) {
+            *slot = nullptr;
+            return st;
+        }
+    }
+    int most = 0;
+    for (int r = 0; r < nrep; ++r) most = std::max(most, (int)ins[r].info->mcsteps);
+    st = gcmc_run(*slot, most);
+    if (st == GCMC_OK) st = gcmc_sync(*slot);
+    for (int r = 0; r < nrep && st == GCMC_OK; ++r)
+        st = gcmc_download(*slot, r, const_cast<AtomArray*>(ins[r].fragmentInfo),
+                           const_cast<residue*>(ins[r].residueInfo), const_cast<Atom*>(ins[r].atomInfo));
+    if (st != GCMC_OK) {
+        destroy_impl(*slot);
+        *slot = nullptr;
+    }
+    return st;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free pose energies (gcmc_energy_poses_noalloc).
@@ -555,6 +683,8 @@ void gcmc_default_options(gcmc_options* opt) {
     opt->log_steps = 0;
     opt->log_kmax = 1;
     opt->split_items = 2048;
+    opt->branches = 1;
+    opt->energy_blocks_per_sm = 0;
 }
 
 const char* gcmc_status_string(int status) {
@@ -575,6 +705,99 @@ int gcmc_create(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* o
 }
 
 int gcmc_destroy(gcmc_ctx* ctx) { return destroy_impl(ctx); }
+
+int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* base, int32_t trial_steps,
+                  gcmc_options* best, gcmc_tune_trial* trials, int32_t max_trials, int32_t* ntrials) {
+    if (!reps || nrep < 1 || !best || trial_steps < 1) return GCMC_ERR_ARG;
+    if (nrep > kMaxRep) return GCMC_ERR_LIMIT;
+    constexpr int kWarm = 8;
+    int avail = INT32_MAX;
+    for (int r = 0; r < nrep; ++r) {
+        if (!reps[r].info) return GCMC_ERR_ARG;
+        avail = std::min(avail, (int)reps[r].info->mcsteps - kWarm);
+    }
+    const int steps = std::min(trial_steps, avail);
+    if (steps < 1) return GCMC_ERR_ARG;
+    gcmc_options opt;
+    if (base) opt = *base; else gcmc_default_options(&opt);
+    if (opt.cells_per_cutoff <= 0) opt.cells_per_cutoff = 2;
+    if (opt.split_items <= 0) opt.split_items = 2048;
+    if (opt.branches <= 0) opt.branches = 1;
+    opt.log_steps = 0;
+    int n = 0;
+    float best_ms = INFINITY;
+    gcmc_options cur = opt;
+    // time one candidate on a fresh context: kWarm steps, then the best of two runs of `steps`
+    auto trial = [&](gcmc_options o, float* ms) -> int {
+        gcmc_ctx* c = nullptr;
+        int st = create_impl(nrep, reps, &o, nullptr, &c);
+        if (st != GCMC_OK) return st;
+        cudaEvent_t a = nullptr, b = nullptr;
+        float t = INFINITY;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) st = GCMC_ERR_CUDA;
+        if (st == GCMC_OK) st = gcmc_run(c, kWarm);
+        const int half = std::max(1, steps / 2);
+        for (int k = 0; k < 2 && st == GCMC_OK; ++k) {
+            cudaEventRecord(a, c->stream);
+            st = gcmc_run(c, half);
+            cudaEventRecord(b, c->stream);
+            if (st == GCMC_OK) st = gcmc_sync(c);
+            float x = 0.f;
+            if (st == GCMC_OK && cudaEventElapsedTime(&x, a, b) == cudaSuccess) t = std::min(t, x / half);
+        }
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+        destroy_impl(c);
+        *ms = t;
+        return st;
+    };
+    auto consider = [&](gcmc_options o) -> int {
+        float ms = INFINITY;
+        int st = trial(o, &ms);
+        if (st != GCMC_OK) return st;
+        if (trials && n < max_trials)
+            trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items, o.branches, o.energy_blocks_per_sm, ms};
+        ++n;
+        if (ms < best_ms) {
+            best_ms = ms;
+            cur = o;
+        }
+        return GCMC_OK;
+    };
+    int st = GCMC_OK;
+    // coordinate descent: cell grid, then work split, then branches, then energy CTAs per SM
+    for (int R : {1, 2, 3}) {
+        gcmc_options o = cur;
+        o.cells_per_cutoff = R;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    const int base_split = cur.split_items;
+    for (int sp : {512, 1024, 2048, 4096, 8192}) {
+        if (sp == base_split) continue;
+        gcmc_options o = cur;
+        o.split_items = sp;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    const int base_br = cur.branches;
+    for (int nb : {1, 2, 4}) {
+        if (nb == base_br || nb > nrep) continue;
+        gcmc_options o = cur;
+        o.branches = nb;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    const int base_e = cur.energy_blocks_per_sm;
+    for (int e : {0, 2, 1}) {
+        if (e == base_e) continue;
+        gcmc_options o = cur;
+        o.energy_blocks_per_sm = e;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    if (ntrials) *ntrials = n;
+    if (st != GCMC_OK) return st;
+    cur.log_steps = base ? base->log_steps : 0;
+    *best = cur;
+    return GCMC_OK;
+}
 
 void* gcmc_stream(gcmc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
@@ -795,44 +1018,24 @@ int gcmc_run_gcmc(const InfoStruct* info, AtomArray* fragmentInfo, residue* resi
     if (!info) return GCMC_ERR_ARG;
     gcmc_replica_in in{info, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray};
     std::lock_guard<std::mutex> lock(g_cache_mutex);
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return GCMC_ERR_NODEVICE;
-    }
-    int st = GCMC_OK;
-    if (g_cache && g_cache->device == dev) {
-        st = refill_impl(g_cache, in, opt);
-        if (st != GCMC_OK) {  // drop the cached context and start afresh
-            destroy_impl(g_cache);
-            g_cache = nullptr;
-            if (st == GCMC_ERR_ARG || st == GCMC_ERR_LIMIT) return st;
-        }
-    } else if (g_cache) {
-        destroy_impl(g_cache);
-        g_cache = nullptr;
-    }
-    if (!g_cache) {
-        st = create_impl(1, &in, opt, nullptr, &g_cache);
-        if (st != GCMC_OK) {
-            g_cache = nullptr;
-            return st;
-        }
-    }
-    st = gcmc_run(g_cache, info->mcsteps);
-    if (st == GCMC_OK) st = gcmc_sync(g_cache);
-    if (st == GCMC_OK) st = gcmc_download(g_cache, 0, fragmentInfo, residueInfo, atomInfo);
-    if (st != GCMC_OK) {
-        destroy_impl(g_cache);
-        g_cache = nullptr;
-    }
-    return st;
+    return cached_run(&g_cache, 1, &in, opt);
+}
+
+int gcmc_run_batch(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options* opt) {
+    if (!reps || nrep < 1) return GCMC_ERR_ARG;
+    if (nrep > kMaxRep) return GCMC_ERR_LIMIT;
+    for (int r = 0; r < nrep; ++r)
+        if (!reps[r].info) return GCMC_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    return cached_run(&g_batch, nrep, reps, opt);
 }
 
 int gcmc_release_cache(void) {
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     if (g_cache) destroy_impl(g_cache);
+    if (g_batch) destroy_impl(g_batch);
     g_cache = nullptr;
+    g_batch = nullptr;
     return GCMC_OK;
 }
 

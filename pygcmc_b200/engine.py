@@ -10,7 +10,34 @@ import ctypes
 import numpy as np
 
 from . import values as V
-from ._native import Options, ReplicaIn, check, default_options, lib, ptr
+from ._native import Options, ReplicaIn, TuneTrial, check, default_options, lib, ptr
+
+
+def _replica_array(systems):
+    arr = (ReplicaIn * len(systems))()
+    for i, s in enumerate(systems):
+        arr[i] = ReplicaIn(*[ptr(x) for x in s.arrays()])
+    return arr
+
+
+def autotune(systems, options: Options = None, trial_steps: int = 64):
+    """Pick the launch shape (cell-grid resolution, pose-energy work split,
+    graph branches, pose-energy CTAs per SM) for these replicas by timing
+    short runs on temporary contexts (gcmc_autotune).  Returns the options to
+    create the :class:`Engine` with and the list of trials
+    ``(cells_per_cutoff, split_items, branches, energy_blocks_per_sm, ms_per_step)``."""
+    if not isinstance(systems, (list, tuple)):
+        systems = [systems]
+    base = options if options is not None else default_options()
+    arr = _replica_array(systems)
+    best = Options()
+    trials = (TuneTrial * 32)()
+    n = ctypes.c_int32(0)
+    check(lib().gcmc_autotune(len(systems), arr, ctypes.byref(base), int(trial_steps), ctypes.byref(best), trials,
+                              32, ctypes.byref(n)), "gcmc_autotune")
+    out = [(t.cells_per_cutoff, t.split_items, t.branches, t.energy_blocks_per_sm, float(t.ms_per_step))
+           for t in trials[: min(n.value, 32)]]
+    return best, out
 
 
 class Engine:
@@ -22,10 +49,7 @@ class Engine:
             systems = [systems]
         self.systems = list(systems)
         self.options = options if options is not None else default_options()
-        arr = (ReplicaIn * len(self.systems))()
-        for i, s in enumerate(self.systems):
-            a = s.arrays()
-            arr[i] = ReplicaIn(*[ptr(x) for x in a])
+        arr = _replica_array(self.systems)
         self._in = arr
         h = ctypes.c_void_p()
         check(lib().gcmc_create(len(self.systems), arr, ctypes.byref(self.options),

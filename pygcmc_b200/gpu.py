@@ -95,3 +95,22 @@ def runGCMC(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, o
     if show:
         print_all_info(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
     return None
+
+
+def runGCMC_batch(replicas, options=None):
+    """Batched form of :func:`runGCMC` (no counterpart in the reference): every
+    replica -- a :class:`pygcmc_b200.system.System` or a 7-tuple of the
+    runGCMC arrays -- runs its ``mcsteps`` steps in one device context (one
+    pose-energy launch and one accept launch per MC step for all of them), and
+    each replica's fragmentInfo/residueInfo/atomInfo are updated in place."""
+    import ctypes
+    from ._native import ReplicaIn
+    arrays = [r.arrays() if hasattr(r, "arrays") else tuple(r) for r in replicas]
+    for a in arrays:
+        validate_arrays(*a)
+    arr = (ReplicaIn * len(arrays))()
+    for i, a in enumerate(arrays):
+        arr[i] = ReplicaIn(*[ptr(x) for x in a])
+    opt = options if options is not None else default_options()
+    check(lib().gcmc_run_batch(len(arrays), arr, ctypes.byref(opt)), "runGCMC_batch")
+    return None

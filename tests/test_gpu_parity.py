@@ -183,3 +183,78 @@ def test_runGCMC_consecutive_calls_reuse_context(protein_small, water_small):
         a = occupied_atoms(s)
         assert np.array_equal(s.atomInfo["position"][a], final.atomInfo["position"][a])
     assert lib().gcmc_release_cache() == 0
+
+
+def _solo_final(s, n, replica):
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    with Engine(s.copy(), default_options(replica=replica)) as e:
+        e.run(n)
+        e.sync()
+        return e.download()
+
+
+@pytest.mark.parametrize("branches,ebps", [(2, 0), (3, 1), (4, 2)])
+def test_graph_branches_match_single(protein_small, water_small, branches, ebps):
+    """Replicas split over concurrent graph branches (and a reduced pose-energy
+    grid) give each replica's solo result."""
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    systems = [protein_small.copy(), water_small.copy(), water_small.copy(), protein_small.copy(),
+               water_small.copy()]
+    n = 96
+    with Engine([x.copy() for x in systems], default_options(branches=branches, energy_blocks_per_sm=ebps)) as eng:
+        for k in (40, 56):
+            eng.run(k)
+        eng.sync()
+        finals = [eng.download(r) for r in range(len(systems))]
+    for r, s in enumerate(systems):
+        f1 = _solo_final(s, n, r)
+        assert (f1.fragmentInfo["totalNum"] == finals[r].fragmentInfo["totalNum"]).all()
+        a = occupied_atoms(f1)
+        assert np.array_equal(f1.atomInfo["position"][a], finals[r].atomInfo["position"][a])
+
+
+def test_runGCMC_batch_matches_runGCMC(protein_small, water_small):
+    """The batched drop-in advances each replica exactly as its own runGCMC call
+    (replica r on RNG stream r), and keeps its context between calls."""
+    from pygcmc_b200._native import default_options, lib
+    from pygcmc_b200.gpu import runGCMC, runGCMC_batch
+    for order in ((protein_small, water_small, water_small), (water_small, protein_small, protein_small)):
+        batch = [x.copy() for x in order]
+        for i, b in enumerate(batch):
+            b.SimInfo[0]["mcsteps"] = 60 + 20 * i
+            b.SimInfo[0]["seed"] = 1000 + i
+        runGCMC_batch(batch, default_options(branches=2))
+        for r, src in enumerate(order):
+            s = src.copy()
+            s.SimInfo[0]["mcsteps"] = 60 + 20 * r
+            s.SimInfo[0]["seed"] = 1000 + r
+            runGCMC(*s.arrays(), options=default_options(replica=r))
+            assert (s.fragmentInfo["totalNum"] == batch[r].fragmentInfo["totalNum"]).all()
+            assert np.array_equal(s.atomInfo, batch[r].atomInfo)
+            assert np.array_equal(s.residueInfo, batch[r].residueInfo)
+    assert lib().gcmc_release_cache() == 0
+
+
+def test_autotune_picks_the_fastest_trial(protein_small, water_small):
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine, autotune
+    systems = [protein_small.copy(), water_small.copy(), protein_small.copy()]
+    before = [s.copy() for s in systems]
+    best, trials = autotune(systems, default_options(), trial_steps=32)
+    assert len(trials) >= 8
+    ms = [t[4] for t in trials]
+    assert all(np.isfinite(ms)) and min(ms) > 0
+    k = int(np.argmin(ms))
+    assert (best.cells_per_cutoff, best.split_items, best.branches, best.energy_blocks_per_sm) == trials[k][:4]
+    for s, b in zip(systems, before):  # inputs untouched
+        assert np.array_equal(s.atomInfo, b.atomInfo)
+        assert (s.fragmentInfo["totalNum"] == b.fragmentInfo["totalNum"]).all()
+    # the tuned shape runs the same chain (check one replica against its solo run)
+    with Engine([x.copy() for x in systems], best) as eng:
+        eng.run(64)
+        eng.sync()
+        f = eng.download(1)
+    solo = _solo_final(systems[1], 64, 1)
+    assert (solo.fragmentInfo["totalNum"] == f.fragmentInfo["totalNum"]).all()
