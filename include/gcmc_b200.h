@@ -205,6 +205,31 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
                       const int32_t* site_type, int32_t nsites, const float* centres,
                       const int32_t* self, int32_t nposes, double* out, int32_t* n_groups);
 
+/* Pose energies and their gradients (no counterpart in the reference, whose
+ * calcEnergy, gcmc/cpp/gcmc_energy.h:142-204, has no derivative).  All arrays
+ * are DEVICE pointers except site_type, a host copy of d_site_type used for
+ * validation; launches on `stream` (NULL = the context's stream) and returns
+ * without waiting (scratch comes from the stream-ordered allocator).
+ *   d_xyz[p*nsites*3], d_centres[p*3], d_self[p] (optional), d_site_q /
+ *   d_site_type[nsites]: as gcmc_energy_poses;
+ *   d_ff: pair table in the reference's layout (sigma [nm], eps [kJ/mol] per
+ *     (site type, atom type), ffX*ffY*2 floats) used instead of the
+ *     context's; NULL = the context's table;
+ *   d_energy[p] (optional): E_p with that table (FP64 sums of FP32 terms, the
+ *     arithmetic of gcmc_energy_poses);
+ *   d_gxyz[p*nsites*3] (optional): dE_p / dx_{p,s};
+ *   d_gq[p*nsites] (optional): dE_p / dq_s;
+ *   d_gff[ffX*ffY*2] (optional; needs d_ff and d_gout): ADDS
+ *     sum_p d_gout[p] * dE_p / dff.
+ * Gradients are FP32 pair terms summed per lane in FP32 and across lanes and
+ * cell ranges in FP64 (the table gradient per block in FP32).  Group
+ * inclusion is by pose centre, as in the energy, so E is piecewise smooth in
+ * the site coordinates and the centre carries no gradient. */
+int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float* d_site_q,
+                     const int32_t* d_site_type, const int32_t* site_type, int32_t nsites, const float* d_centres,
+                     const int32_t* d_self, int32_t nposes, const float* d_ff, const double* d_gout,
+                     double* d_energy, double* d_gxyz, double* d_gq, double* d_gff, void* stream);
+
 /* Allocation-free variant of gcmc_energy_poses (no counterpart in the reference).
  *
  * For callers that cannot allocate GPU memory at the point where they need

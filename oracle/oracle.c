@@ -713,6 +713,194 @@ int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_
     return total;
 }
 
+/* ------------------------------------------------------------------------- */
+/* FP64 inputs and analytic gradients of calcEnergy's pair sum.               */
+/*                                                                            */
+/* Same group inclusion as or_pose_energy (the FP32 group-centre distance of  */
+/* gcmc_energy.h:160-176 against the float pose centre), but sites, site      */
+/* charges and the pair table are double, so that central finite differences  */
+/* of these energies resolve steps of 1e-4 A / 1e-5 relative.  The gradient    */
+/* of each pair term (minimum-image d = atom - site, d2 = |d|^2):             */
+/*   U = 4 eps (s6^2 - s6) + K q_s q_a / r,  s6 = (100 sigma^2 / d2)^3         */
+/*   dU/dd2 = -12 eps s6 (2 s6 - 1) / d2 - U_el / (2 d2)                      */
+/*   dU/dx_s = -2 dU/dd2 d,  dU/dq_s = K q_a / r,                             */
+/*   dU/dsigma = 24 eps (2 s6 - 1) s6 / sigma,  dU/deps = 4 (s6^2 - s6).        */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    const or_info* info;
+    const or_atomarray* frag;
+    const or_residue* res;
+    const or_atom* atoms;
+    const double* ff;
+    const double (*sx)[3];
+    const double* sq;
+    const int32_t* st;
+    int ns;
+} pose64;
+
+/* Visit every included group of a pose (fixed groups, then occupied slots). */
+#define OR_FOR_INCLUDED(P, centre, self, ...)                                          \
+    do {                                                                               \
+        const int nfixed_ = (P)->frag[0].startRes;                                     \
+        for (int t_ = -1; t_ < (P)->info->fragTypeNum; ++t_) {                         \
+            const int g0_ = t_ < 0 ? 0 : (P)->frag[t_].startRes;                       \
+            const int g1_ = t_ < 0 ? nfixed_ : g0_ + (P)->frag[t_].totalNum;          \
+            for (int g = g0_; g < g1_; ++g) {                                          \
+                if (g == (self)) continue;                                             \
+                if (or_dist_group((centre), (P)->res[g].position, (P)->info->cryst) >   \
+                    (P)->info->cutoff)                                                 \
+                    continue;                                                          \
+                __VA_ARGS__                                                            \
+            }                                                                          \
+        }                                                                              \
+    } while (0)
+
+static double pose_energy64(const pose64* P, const float centre[3], int self, int32_t* ngroups) {
+    const double L[3] = {P->info->cryst[0], P->info->cryst[1], P->info->cryst[2]};
+    double e = 0.0;
+    int ng = 0;
+    OR_FOR_INCLUDED(P, centre, self, {
+        ng++;
+        for (int a = P->res[g].atomStart; a < P->res[g].atomStart + P->res[g].atomNum; ++a) {
+            const or_atom* A = &P->atoms[a];
+            for (int s = 0; s < P->ns; ++s) {
+                double d2 = 0.0;
+                for (int i = 0; i < 3; ++i) {
+                    double d = (double)A->position[i] - P->sx[s][i];
+                    d -= fast_round_d(d / L[i]) * L[i];
+                    d2 += d * d;
+                }
+                const int tij = P->st[s] * P->info->ffYNum + A->type;
+                const double sig = P->ff[2 * tij], eps = P->ff[2 * tij + 1];
+                const double s2 = sig * sig * 100.0 / d2, s6 = s2 * s2 * s2;
+                e += 4.0 * eps * (s6 * s6 - s6) + OR_COULOMB * P->sq[s] * (double)A->charge / sqrt(d2);
+            }
+        }
+    });
+    if (ngroups) *ngroups = ng;
+    return e;
+}
+
+/* gxyz[ns*3], gq[ns] of one pose; gff (+= w * dE/dff) and the l1 scales
+ * (sums of |terms|: per site over its three components, per site charge, per
+ * table entry). */
+static void pose_grad64(const pose64* P, const float centre[3], int self, double w, double* gxyz, double* gq,
+                        double* gff, double* gxyz_l1, double* gq_l1, double* gff_l1) {
+    const double L[3] = {P->info->cryst[0], P->info->cryst[1], P->info->cryst[2]};
+    for (int s = 0; s < P->ns; ++s) {
+        gxyz[3 * s] = gxyz[3 * s + 1] = gxyz[3 * s + 2] = 0.0;
+        gq[s] = 0.0;
+        if (gxyz_l1) gxyz_l1[s] = 0.0;
+        if (gq_l1) gq_l1[s] = 0.0;
+    }
+    OR_FOR_INCLUDED(P, centre, self, {
+        for (int a = P->res[g].atomStart; a < P->res[g].atomStart + P->res[g].atomNum; ++a) {
+            const or_atom* A = &P->atoms[a];
+            for (int s = 0; s < P->ns; ++s) {
+                double d[3], d2 = 0.0;
+                for (int i = 0; i < 3; ++i) {
+                    d[i] = (double)A->position[i] - P->sx[s][i];
+                    d[i] -= fast_round_d(d[i] / L[i]) * L[i];
+                    d2 += d[i] * d[i];
+                }
+                const int tij = P->st[s] * P->info->ffYNum + A->type;
+                const double sig = P->ff[2 * tij], eps = P->ff[2 * tij + 1];
+                const double s2 = sig * sig * 100.0 / d2, s6 = s2 * s2 * s2;
+                const double r = sqrt(d2);
+                const double el = OR_COULOMB * P->sq[s] * (double)A->charge / r;
+                const double dd2 = -12.0 * eps * s6 * (2.0 * s6 - 1.0) / d2 - 0.5 * el / d2;
+                for (int i = 0; i < 3; ++i) {
+                    const double gi = -2.0 * dd2 * d[i];
+                    gxyz[3 * s + i] += gi;
+                    if (gxyz_l1) gxyz_l1[s] += fabs(gi);
+                }
+                const double gqi = OR_COULOMB * (double)A->charge / r;
+                gq[s] += gqi;
+                if (gq_l1) gq_l1[s] += fabs(gqi);
+                if (gff) {
+                    /* dU/dsigma = 24 eps s6 (2 s6 - 1) / sigma, written without the division */
+                    const double c3 = 100.0 / d2 * (100.0 / d2) * (100.0 / d2);
+                    const double s5 = sig * sig * sig * sig * sig;
+                    const double gs = w * 4.0 * eps * (2.0 * s6 - 1.0) * 6.0 * s5 * c3;
+                    const double ge = w * 4.0 * (s6 * s6 - s6);
+                    gff[2 * tij] += gs;
+                    gff[2 * tij + 1] += ge;
+                    if (gff_l1) {
+                        gff_l1[2 * tij] += fabs(gs);
+                        gff_l1[2 * tij + 1] += fabs(ge);
+                    }
+                }
+            }
+        }
+    });
+}
+
+int64_t or_energy_batch64(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                          const or_atom* atoms, const double* ff64, const double* xyz64, const double* q64,
+                          const int32_t* site_type, int32_t nsites, const float* centres, const int32_t* self,
+                          int32_t nposes, double* out, int32_t* n_groups, int32_t threads) {
+    if (threads <= 0) threads = 1;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
+    for (int p = 0; p < nposes; ++p) {
+        pose64 P = {info, frag, res, atoms, ff64, (const double (*)[3])(xyz64 + (size_t)p * nsites * 3), q64,
+                    site_type, nsites};
+        int32_t ng = 0;
+        out[p] = pose_energy64(&P, centres + 3 * p, self ? self[p] : -1, &ng);
+        if (n_groups) n_groups[p] = ng;
+    }
+    return 0;
+}
+
+int64_t or_grad_batch(const or_info* info, const or_atomarray* frag, const or_residue* res, const or_atom* atoms,
+                      const double* ff64, const double* xyz64, const double* q64, const int32_t* site_type,
+                      int32_t nsites, const float* centres, const int32_t* self, int32_t nposes,
+                      const double* gout, double* gxyz, double* gq, double* gff, double* gxyz_l1, double* gq_l1,
+                      double* gff_l1, int32_t threads) {
+    if (threads <= 0) threads = 1;
+    const size_t nff = (size_t)2 * info->ffXNum * info->ffYNum;
+    double* tff = NULL;
+    double* tff1 = NULL;
+    if (gff) {
+        tff = calloc(nff * (size_t)threads, sizeof(double));
+        tff1 = calloc(nff * (size_t)threads, sizeof(double));
+        if (!tff || !tff1) {
+            free(tff);
+            free(tff1);
+            return -1;
+        }
+    }
+#pragma omp parallel num_threads(threads)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+        for (int p = 0; p < nposes; ++p) {
+            pose64 P = {info, frag, res, atoms, ff64, (const double (*)[3])(xyz64 + (size_t)p * nsites * 3), q64,
+                        site_type, nsites};
+            pose_grad64(&P, centres + 3 * p, self ? self[p] : -1, gout ? gout[p] : 1.0,
+                        gxyz + (size_t)p * nsites * 3, gq + (size_t)p * nsites, tff ? tff + nff * tid : NULL,
+                        gxyz_l1 ? gxyz_l1 + (size_t)p * nsites : NULL, gq_l1 ? gq_l1 + (size_t)p * nsites : NULL,
+                        tff1 ? tff1 + nff * tid : NULL);
+        }
+    }
+    if (gff) {
+        for (size_t j = 0; j < nff; ++j) {
+            double a = 0.0, b = 0.0;
+            for (int t = 0; t < threads; ++t) {
+                a += tff[nff * t + j];
+                b += tff1[nff * t + j];
+            }
+            gff[j] = a;
+            if (gff_l1) gff_l1[j] = b;
+        }
+    }
+    free(tff);
+    free(tff1);
+    return 0;
+}
+
 /* Rotation of one point by the Rodrigues matrix of (axis, angle) -- exposes the
  * pose rotation for the known-answer test of the reference notebook. */
 void or_rotate_point(const float axis[3], float angle, const float p[3], float out[3], float R_out[9]) {

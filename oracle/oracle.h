@@ -144,6 +144,23 @@ int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_
                         const float* centres, const int32_t* self, int32_t nposes,
                         int32_t mode, double* out, int32_t* n_groups, double* l1, int32_t threads);
 
+/* FP64 energies of explicit poses with FP64 sites, charges and pair table
+ * (same inclusion as or_energy_batch; for finite differences). */
+int64_t or_energy_batch64(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                          const or_atom* atoms, const double* ff64, const double* xyz64, const double* q64,
+                          const int32_t* site_type, int32_t nsites, const float* centres, const int32_t* self,
+                          int32_t nposes, double* out, int32_t* n_groups, int32_t threads);
+
+/* FP64 analytic gradients of those energies: gxyz[p][s][3] = dE_p/dx_s,
+ * gq[p][s] = dE_p/dq_s, gff[ffX*ffY*2] = sum_p gout[p] dE_p/dff (sigma, eps)
+ * (gff optional; gout NULL = all ones), with the l1 scales of each (sums of
+ * |pair terms|; optional). */
+int64_t or_grad_batch(const or_info* info, const or_atomarray* frag, const or_residue* res, const or_atom* atoms,
+                      const double* ff64, const double* xyz64, const double* q64, const int32_t* site_type,
+                      int32_t nsites, const float* centres, const int32_t* self, int32_t nposes,
+                      const double* gout, double* gxyz, double* gq, double* gff, double* gxyz_l1, double* gq_l1,
+                      double* gff_l1, int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,12 @@ def lib():
         L.or_energy_batch.restype = ctypes.c_int64
         L.or_energy_batch.argtypes = [c_void] * 8 + [ctypes.c_int32, c_void, c_void, ctypes.c_int32, ctypes.c_int32,
                                                      c_void, c_void, c_void, ctypes.c_int32]
+        L.or_energy_batch64.restype = ctypes.c_int64
+        L.or_energy_batch64.argtypes = [c_void] * 7 + [c_void, ctypes.c_int32, c_void, c_void, ctypes.c_int32,
+                                                       c_void, c_void, ctypes.c_int32]
+        L.or_grad_batch.restype = ctypes.c_int64
+        L.or_grad_batch.argtypes = [c_void] * 7 + [c_void, ctypes.c_int32, c_void, c_void, ctypes.c_int32] + \
+            [c_void] * 7 + [ctypes.c_int32]
         L.or_philox.argtypes = [c_void, c_void, c_void]
         L.or_det_sincos.argtypes = [ctypes.c_float, c_void, c_void]
         L.or_dist_group.restype = ctypes.c_float
@@ -136,3 +142,46 @@ def rotate_point(axis, angle, p):
     R = np.zeros(9, np.float32)
     lib().or_rotate_point(_p(a), ctypes.c_float(angle), _p(x), _p(out), _p(R))
     return out, R.reshape(3, 3)
+
+
+def energy_batch64(system, xyz, q, types, centres, ff=None, self_res=None, threads=None):
+    """FP64 energies of poses given by FP64 sites ``xyz[P, ns, 3]``, FP64 site
+    charges ``q[ns]`` and an FP64 pair table ``ff`` (default: the system's)."""
+    threads = threads or os.cpu_count() or 1
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n, ns = xyz.shape[0], xyz.shape[1]
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    c = np.ascontiguousarray(centres, dtype=np.float32)
+    f = np.ascontiguousarray(system.ff if ff is None else ff, dtype=np.float64)
+    sr = None if self_res is None else np.ascontiguousarray(self_res, dtype=np.int32)
+    out = np.zeros(n, dtype=np.float64)
+    ng = np.zeros(n, dtype=np.int32)
+    s = system
+    lib().or_energy_batch64(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), _p(f), _p(xyz),
+                            _p(q), _p(t), ns, _p(c), _p(sr), n, _p(out), _p(ng), threads)
+    return out, ng
+
+
+def grad_batch(system, xyz, q, types, centres, ff=None, self_res=None, gout=None, threads=None):
+    """FP64 analytic gradients of :func:`energy_batch64`: returns a dict with
+    gxyz [P, ns, 3], gq [P, ns], gff [ffX*ffY*2] (weighted by gout) and their
+    l1 scales gxyz_l1 [P, ns], gq_l1 [P, ns], gff_l1."""
+    threads = threads or os.cpu_count() or 1
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n, ns = xyz.shape[0], xyz.shape[1]
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    c = np.ascontiguousarray(centres, dtype=np.float32)
+    f = np.ascontiguousarray(system.ff if ff is None else ff, dtype=np.float64)
+    sr = None if self_res is None else np.ascontiguousarray(self_res, dtype=np.int32)
+    go = None if gout is None else np.ascontiguousarray(gout, dtype=np.float64)
+    r = {"gxyz": np.zeros((n, ns, 3)), "gq": np.zeros((n, ns)), "gff": np.zeros(len(f)),
+         "gxyz_l1": np.zeros((n, ns)), "gq_l1": np.zeros((n, ns)), "gff_l1": np.zeros(len(f))}
+    s = system
+    rc = lib().or_grad_batch(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), _p(f), _p(xyz),
+                             _p(q), _p(t), ns, _p(c), _p(sr), n, _p(go), _p(r["gxyz"]), _p(r["gq"]), _p(r["gff"]),
+                             _p(r["gxyz_l1"]), _p(r["gq_l1"]), _p(r["gff_l1"]), threads)
+    if rc != 0:
+        raise MemoryError("or_grad_batch")
+    return r

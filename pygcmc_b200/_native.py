@@ -62,6 +62,7 @@ def lib():
         "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
         "gcmc_last_status": (c_int, []),
         "gcmc_release_cache": (c_int, []),
+        "gcmc_energy_grad": (c_int, [c_void, c_int] + [c_void] * 4 + [c_int, c_void, c_void, c_int] + [c_void] * 7),
         "gcmc_run_batch": (c_int, [c_int, c_void, P(Options)]),
         "gcmc_autotune": (c_int, [c_int, c_void, P(Options), c_int, P(Options), c_void, c_int, P(c_int)]),
         "gcmc_status_string": (ctypes.c_char_p, [c_int]),
@@ -120,7 +121,7 @@ def default_options(**kw):
     return o
 
 
-EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
+EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",
            "gcmc_energy_poses_noalloc", "gcmc_synth_place", "gcmc_synth_chain_sphere",

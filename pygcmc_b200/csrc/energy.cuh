@@ -126,11 +126,21 @@ __device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, i
     else flush_atoms_t<false>(R, B, na, ns, lane, acc);
 }
 
+// What the cell walk does with each buffer of included atoms: the energy
+// sink sums pair energies; the gradient kernel supplies its own sink.
+struct EnergySink {
+    double acc = 0.0;
+    __device__ __forceinline__ void flush(const RepDev& R, WarpBuf& B, int na, int ns, int lane) {
+        flush_atoms(R, B, na, ns, lane, acc);
+    }
+};
+
 // Expand included groups B.glist[0, ng) into atoms and evaluate them.  Each
 // lane takes one group of a batch of 32, a warp scan of the atom counts gives
 // the write offsets; groups larger than the buffer are streamed in pieces.
+template <class Sink>
 __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int ng, int ns, int lane,
-                                               double& acc, long long& npair) {
+                                               Sink& sink, long long& npair) {
     int na = 0;
     for (int base = 0; base < ng; base += 32) {
         const int gi = base + lane;
@@ -155,7 +165,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
         if (maxcnt <= kACap / 2) {
             if (na + total > kACap) {
                 __syncwarp();
-                flush_atoms(R, B, na, ns, lane, acc);
+                sink.flush(R, B, na, ns, lane);
                 __syncwarp();
                 na = 0;
             }
@@ -175,7 +185,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
                 const int take = min(c0 - done, kACap - na);
                 if (take == 0) {
                     __syncwarp();
-                    flush_atoms(R, B, na, ns, lane, acc);
+                    sink.flush(R, B, na, ns, lane);
                     __syncwarp();
                     na = 0;
                     continue;
@@ -187,7 +197,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
         }
     }
     __syncwarp();
-    flush_atoms(R, B, na, ns, lane, acc);
+    sink.flush(R, B, na, ns, lane);
     __syncwarp();
 }
 
@@ -199,8 +209,9 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
 __device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
     return c < 0 ? c + n : (c >= n ? c - n : c);
 }
+template <class Sink>
 __device__ __forceinline__ void test_candidates(const RepDev& R, WarpBuf& B, int nc, int self, float cx, float cy,
-                                                float cz, int lane, int& ng, int& ngroups, int ns, double& acc,
+                                                float cz, int lane, int& ng, int& ngroups, int ns, Sink& sink,
                                                 long long& npair) {
     const unsigned lt = (1u << lane) - 1u;
     for (int base = 0; base < nc; base += 32) {
@@ -238,15 +249,16 @@ __device__ __forceinline__ void test_candidates(const RepDev& R, WarpBuf& B, int
         ngroups += __popc(m);
         if (ng > kGCap - 32) {
             __syncwarp();
-            process_groups(R, B, ng, ns, lane, acc, npair);
+            process_groups(R, B, ng, ns, lane, sink, npair);
             ng = 0;
         }
     }
 }
 
-__device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
-                                             int self, int c0, int c1, int lane, double& acc, int& ngroups,
-                                             long long& npair) {
+template <class Sink>
+__device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
+                                           int self, int c0, int c1, int lane, Sink& sink, int& ngroups,
+                                           long long& npair) {
     // cells [c0, c1) of the window, flattened as ((z * span1) + y) * span0 + x
     set_centre(R, B, cx, cy, cz, lane);
     const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
@@ -278,7 +290,7 @@ __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns
             const int* ent = R.cell_ent + (size_t)cell * R.cap;
             for (int e = 0, o = incl - cnt; e < cnt; ++e) B.cand[o + e] = ent[e];
             __syncwarp();
-            test_candidates(R, B, total, self, cx, cy, cz, lane, ng, ngroups, ns, acc, npair);
+            test_candidates(R, B, total, self, cx, cy, cz, lane, ng, ngroups, ns, sink, npair);
             __syncwarp();
         } else {  // more candidates than the buffer holds: one cell at a time
             for (int l = 0; l < 32; ++l) {
@@ -288,14 +300,23 @@ __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns
                     const int m = min(kCCap, cn - e0);
                     for (int e = lane; e < m; e += 32) B.cand[e] = ent[e0 + e];
                     __syncwarp();
-                    test_candidates(R, B, m, self, cx, cy, cz, lane, ng, ngroups, ns, acc, npair);
+                    test_candidates(R, B, m, self, cx, cy, cz, lane, ng, ngroups, ns, sink, npair);
                     __syncwarp();
                 }
             }
         }
     }
     __syncwarp();
-    process_groups(R, B, ng, ns, lane, acc, npair);
+    process_groups(R, B, ng, ns, lane, sink, npair);
+}
+
+__device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
+                                             int self, int c0, int c1, int lane, double& acc, int& ngroups,
+                                             long long& npair) {
+    EnergySink sink;
+    sink.acc = acc;
+    walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair);
+    acc = sink.acc;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -438,14 +459,15 @@ __global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy
 }
 
 // Energies of caller-supplied poses (gcmc_energy_poses): item = (pose, slab).
+// The replica descriptor is passed by value so that callers can substitute
+// the pair table (R.lj).
 __global__ void __launch_bounds__(kWarpsE * 32)
-    k_energy_explicit(const RepDev* __restrict__ rep, const float* __restrict__ xyz,
+    k_energy_explicit(const RepDev R, const float* __restrict__ xyz,
                       const float* __restrict__ q, const int* __restrict__ type, int ns,
                       const float* __restrict__ centres, const int* __restrict__ self, int nposes,
                       int nslab, double* __restrict__ out, int* __restrict__ ngout) {
     __shared__ WarpBuf bufs[kWarpsE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const RepDev& R = *rep;
     WarpBuf& B = bufs[warp];
     const int total = nposes * nslab;
     for (int it = blockIdx.x * kWarpsE + warp; it < total; it += gridDim.x * kWarpsE) {

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "accept.cuh"
+#include "grad.cuh"
 
 using namespace gcmc;
 
@@ -984,7 +985,7 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
             st = GCMC_ERR_CUDA;
             break;
         }
-        k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->d_reps + rep, dxyz, dq, dt, nsites, dc, dself,
+        k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->repdev[rep], dxyz, dq, dt, nsites, dc, dself,
                                                               nposes, nslab, dout, dng);
         if (cudaGetLastError() != cudaSuccess ||
             cudaMemcpyAsync(part.data(), dout, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s) ||
@@ -1010,6 +1011,78 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
         gcmc_device_error(ctx, &err);
         if (err) st = GCMC_ERR_DEVICE;
     }
+    return st;
+}
+
+int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float* d_site_q,
+                     const int32_t* d_site_type, const int32_t* site_type, int32_t nsites, const float* d_centres,
+                     const int32_t* d_self, int32_t nposes, const float* d_ff, const double* d_gout,
+                     double* d_energy, double* d_gxyz, double* d_gq, double* d_gff, void* stream) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !d_xyz || !d_site_q || !d_site_type || !site_type || !d_centres)
+        return GCMC_ERR_ARG;
+    if (nsites < 1 || nsites > kMaxSites) return GCMC_ERR_LIMIT;
+    if (d_gff && (!d_ff || !d_gout)) return GCMC_ERR_ARG;
+    if (nposes <= 0) return GCMC_OK;
+    RepHost& h = ctx->reps[rep];
+    for (int s = 0; s < nsites; ++s)
+        if (site_type[s] < 0 || site_type[s] >= h.ffX) return GCMC_ERR_ARG;
+    const int nslab = h.nslab;
+    const size_t ntab = (size_t)h.ffX * h.ffY;
+    const size_t tab_smem = d_gff ? (size_t)nsites * h.ffY * 2 * sizeof(float) : 0;
+    if (tab_smem > 160 * 1024) return GCMC_ERR_LIMIT;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    RepDev R = ctx->repdev[rep];
+    float2* lj = nullptr;
+    double *epart = nullptr, *glj = nullptr;
+    int* ngpart = nullptr;
+    float4* gpart = nullptr;
+    int st = GCMC_OK;
+    auto amalloc = [&](void** p, size_t bytes) {
+        if (st == GCMC_OK && cudaMallocAsync(p, bytes, s) != cudaSuccess) st = GCMC_ERR_CUDA;
+    };
+    if (d_ff) {
+        amalloc((void**)&lj, sizeof(float2) * ntab);
+        if (st == GCMC_OK) {
+            k_ff_to_lj<<<(int)((ntab + 255) / 256), 256, 0, s>>>(d_ff, lj, (int)ntab);
+            R.lj = lj;
+        }
+    }
+    if (d_energy) {
+        amalloc((void**)&epart, sizeof(double) * nposes * nslab);
+        amalloc((void**)&ngpart, sizeof(int) * nposes * nslab);
+        if (st == GCMC_OK) {
+            k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(R, d_xyz, d_site_q, d_site_type, nsites, d_centres,
+                                                                  d_self, nposes, nslab, epart, ngpart);
+            k_sum_parts<<<(nposes + 255) / 256, 256, 0, s>>>(epart, ngpart, nposes, nslab, d_energy, nullptr);
+        }
+    }
+    if (d_gxyz || d_gq || d_gff) {
+        amalloc((void**)&gpart, sizeof(float4) * nposes * nslab * nsites);
+        if (d_gff) {
+            amalloc((void**)&glj, sizeof(double) * ntab * 2);
+            if (st == GCMC_OK && cudaMemsetAsync(glj, 0, sizeof(double) * ntab * 2, s) != cudaSuccess)
+                st = GCMC_ERR_CUDA;
+        }
+        if (st == GCMC_OK && tab_smem > 0 &&
+            cudaFuncSetAttribute(k_energy_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_smem) !=
+                cudaSuccess)
+            st = GCMC_ERR_CUDA;
+        if (st == GCMC_OK) {
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+            k_energy_grad<<<std::max(1, sms) * 4, kWarpsG * 32, tab_smem, s>>>(
+                R, d_xyz, d_site_q, d_site_type, nsites, d_centres, d_self, nposes, nslab, d_gout, gpart, glj);
+            if (d_gxyz || d_gq)
+                k_sum_grad<<<(nposes * nsites + 255) / 256, 256, 0, s>>>(gpart, nposes, nslab, nsites, d_gxyz, d_gq);
+            if (d_gff) k_glj_to_gff<<<(int)((ntab + 255) / 256), 256, 0, s>>>(glj, d_ff, d_gff, (int)ntab);
+        }
+    }
+    if (st == GCMC_OK && cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (lj) cudaFreeAsync(lj, s);
+    if (epart) cudaFreeAsync(epart, s);
+    if (ngpart) cudaFreeAsync(ngpart, s);
+    if (gpart) cudaFreeAsync(gpart, s);
+    if (glj) cudaFreeAsync(glj, s);
     return st;
 }
 
@@ -1071,7 +1144,7 @@ int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, co
     double* part = reinterpret_cast<double*>(scratch);
     int* ngpart = reinterpret_cast<int*>(part + kNoAllocMaxParts);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->d_reps + rep, d_xyz, d_site_q, d_site_type, nsites,
+    k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->repdev[rep], d_xyz, d_site_q, d_site_type, nsites,
                                                           d_centres, d_self, nposes, nslab, part, ngpart);
     k_sum_parts<<<(nposes + 255) / 256, 256, 0, s>>>(part, ngpart, nposes, nslab, d_out, d_ngroups);
     CK(cudaGetLastError());

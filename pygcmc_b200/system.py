@@ -465,7 +465,10 @@ def protein_system(seed: int = 1, n_atoms: int = 6000, box: float = 64.0, radius
                  conf_bias=[conf_bias] * n_frag, mctime=[1.0] * n_frag, cryst=L, cutoff=cutoff, grid_dx=dx,
                  start=start, grid=grid, cavity_factor=cav, ff=ff, n_frag_types_ff=len(t1), n_types_ff=len(t2),
                  moves=moves, seed=seed)
-    s.meta.update({"chain_breaks": int(nbreak.value), "n_fixed": n_atoms, "box": box})
+    s.meta.update({"chain_breaks": int(nbreak.value), "n_fixed": n_atoms, "box": box,
+                   # per-type CHARMM parameters in the ff column order (t2); rows are t2[:ffX]
+                   "lj_types": {"names": list(t2), "eps_kcal": np.array([eps[tnames.index(n)] for n in t2]),
+                                "rmin_half": np.array([rmin2[tnames.index(n)] for n in t2])}})
     return s
 
 

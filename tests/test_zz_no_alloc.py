@@ -52,7 +52,7 @@ def test_noalloc_matches_allocating_entry_point(oracle_lib, protein_small):
             stream = torch.cuda.current_stream()
             st = L.gcmc_energy_poses_noalloc(eng.handle, 0, d_xyz.data_ptr(), d_q.data_ptr(), d_t.data_ptr(), ns,
                                              d_c.data_ptr(), None, n, d_out.data_ptr(), d_ng.data_ptr(),
-                                             ctypes.c_void_p(stream.cuda_stream))
+                                             ctypes.c_void_p(stream.cuda_stream or 1))  # 1: cudaStreamLegacy
             assert st == 0
             torch.cuda.synchronize()
             eng.sync()
