@@ -69,7 +69,15 @@ typedef struct {
                             octant, translate by U(0,grid_dx] per axis (gcmc_energy.h:84,
                             gcmc_move_trn.h:58); 1: symmetric -- uniform SO(3)
                             insertion, translate in a cube of edge trn_step,
-                            rotate about a uniform axis by up to rot_max             */
+                            rotate about a uniform axis by up to rot_max;
+                            2: force-biased (no counterpart in the reference) --
+                            uniform SO(3) insertion; translate by
+                            d = (sigma_t^2 beta / 2) F + sigma_t z and rotate by the
+                            rotation vector (sigma_r^2 beta / 2) tau + sigma_r z,
+                            z ~ N(0, I3), F / tau the force / torque about the site
+                            centroid at the old pose, accepted with the
+                            Metropolis-Hastings ratio of the two Gaussian
+                            proposal densities (forces at the old and new pose) */
     int32_t muex_kcal;   /* 0: beta*muex with beta in mol/kJ and muex as given
                             (gcmc_move_add.h:105); 1: muex in kcal/mol (x4.184)     */
     float trn_step;      /* symmetric translate cube edge, A                        */
@@ -86,6 +94,8 @@ typedef struct {
                             concurrently; 0 = 1                                     */
     int32_t energy_blocks_per_sm; /* pose-energy kernel CTAs per SM (0 = the
                             occupancy limit)                                        */
+    float fb_trn;        /* proposal 2: translate step sigma_t, A (0 = 0.5)          */
+    float fb_rot;        /* proposal 2: rotation step sigma_r, rad (0 = 10 degrees)  */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
@@ -94,13 +104,15 @@ typedef struct {
     float ms_per_step;   /* device time per MC step (all replicas)                  */
 } gcmc_tune_trial;
 
-/* One per-step record (48 bytes). */
+/* One per-step record (56 bytes). */
 typedef struct {
     int32_t step, move, ftype, k;
     int32_t n_before, n_after, n_clusters, n_accept;
     int32_t first_accept;  /* pose index of the first accepted cluster, -1 if none */
     int32_t slot;          /* delete: chosen slot; otherwise -1                     */
     double e_sum;          /* sum of pose E (insert/delete) or dE (translate/rotate) */
+    double e_total;        /* running sum of the accepted energy changes since the
+                              context was created (kJ/mol, FP64), after this step   */
 } gcmc_step_log;
 
 typedef struct gcmc_ctx gcmc_ctx;
@@ -170,6 +182,12 @@ int gcmc_download(gcmc_ctx* ctx, int32_t rep, AtomArray* fragmentInfo, residue* 
  * (optional) receives log_kmax doubles per step. */
 int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energies,
                   int32_t max_steps, int32_t* n_steps);
+/* Force-biased runs with logs: per step, log_kmax x 12 floats -- the force and
+ * torque at the old pose, then at the new pose, of each translate/rotate pose
+ * (as used by the proposal and the acceptance). */
+int gcmc_get_forces(gcmc_ctx* ctx, int32_t rep, float* forces, int32_t max_steps, int32_t* n_steps);
+/* Running sum of the accepted moves' energy changes since creation (FP64). */
+int gcmc_energy_total(gcmc_ctx* ctx, int32_t rep, double* e_total);
 /* Counters: steps done, pose energies evaluated, atom-site pairs evaluated. */
 int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, int64_t* pairs);
 /* SM cycles spent by replica `rep`'s accept kernel in its phases, summed over

@@ -24,7 +24,7 @@
 #define OR_TWO_PI_F 6.28318530717958647692f
 
 /* RNG purposes (third counter word, high half). */
-enum { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6 };
+enum { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6, RP_FB = 7 };
 
 /* ------------------------------------------------------------------------- */
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as    */
@@ -101,6 +101,45 @@ void or_det_sincos(float x, float* s_out, float* c_out) {
     }
     *s_out = s;
     *c_out = c;
+}
+
+/* Own natural logarithm (engine: det_log in common.cuh): x = m 2^e with m in
+ * [sqrt(1/2), sqrt(2)), ln m = 2 atanh((m-1)/(m+1)) as an odd series. */
+float or_det_log(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+    float m;
+    memcpy(&m, &mb, 4);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = s2 * 0.0909090936f + 0.111111112f;
+    p = s2 * p + 0.142857149f;
+    p = s2 * p + 0.200000003f;
+    p = s2 * p + 0.333333343f;
+    p = s2 * p + 1.0f;
+    const float lnm = (2.0f * s) * p;
+    const float ef = (float)e;
+    return ef * 0.693145751953125f + (ef * 1.42860677e-06f + lnm);
+}
+
+void or_fb_normals(uint32_t seed, uint32_t replica, int32_t step, int32_t i, float z[4]) {
+    uint32_t r[4];
+    rng(seed, replica, (uint32_t)step, (uint32_t)i, RP_FB, 0, r);
+    const float ra = sqrtf(-2.0f * or_det_log(u01_oc(r[0])));
+    const float rb = sqrtf(-2.0f * or_det_log(u01_oc(r[2])));
+    float sa, ca, sb, cb;
+    or_det_sincos(u01_co(r[1]) * OR_TWO_PI_F, &sa, &ca);
+    or_det_sincos(u01_co(r[3]) * OR_TWO_PI_F, &sb, &cb);
+    z[0] = ra * ca;
+    z[1] = ra * sa;
+    z[2] = rb * cb;
+    z[3] = rb * sb;
 }
 
 /* Rodrigues matrix about axis a (normalised here) by angle with (sin, cos);
@@ -499,221 +538,6 @@ static int cluster_pass(const or_info* info, const or_options* opt, int step, in
 }
 
 /* ------------------------------------------------------------------------- */
-/* Moves and the step loop.                                                   */
-/* ------------------------------------------------------------------------- */
-typedef struct {
-    const or_info* info;
-    or_atomarray* frag;
-    or_residue* res;
-    or_atom* atoms;
-    const float* grid;
-    const float* ff;
-    const or_options* opt;
-} sysref;
-
-static double beta_muex(const or_options* opt, const or_atomarray* F) {
-    double mu = (double)F->muex;
-    if (opt->muex_kcal) mu *= OR_KCAL_TO_KJ;
-    return OR_BETA * mu;
-}
-
-static double ln_nbar(const or_info* info, const or_atomarray* F) {
-    double V = (double)info->cryst[0] * (double)info->cryst[1] * (double)info->cryst[2];
-    return log(V * (double)F->conc * OR_MOLES_TO_MOLECULES);
-}
-
-static void template_sites(const or_atomarray* F, float* q, int32_t* t) {
-    for (int s = 0; s < F->num_atoms; ++s) { q[s] = F->atoms[s].charge; t[s] = F->atoms[s].type; }
-}
-
-static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_log* L, double* Eout,
-                       double* Escale, const double* Ereplay, int kmax, int threads) {
-    const or_info* info = S->info;
-    int mv = moves[step];
-    int f = mv / 4, m = mv % 4;
-    or_atomarray* F = &S->frag[f];
-    const int ns = F->num_atoms;
-    float sq[20];
-    int32_t st[20];
-    template_sites(F, sq, st);
-    int n0 = F->totalNum;
-    if (L) {
-        memset(L, 0, sizeof(*L));
-        L->step = step; L->move = m; L->ftype = f; L->n_before = n0;
-        L->first_accept = -1; L->slot = -1;
-    }
-    int k = 0;
-    if (m == 0) {
-        if (F->totalNum == F->maxNum) goto done;
-        k = F->confBias;
-        if (Eout && k > kmax) return -3;
-        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
-        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
-        double* E = malloc(sizeof(double) * (size_t)k);
-        double* l1 = malloc(sizeof(double) * (size_t)k);
-#pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
-        for (int i = 0; i < k; ++i) {
-            or_insert_pose(info, S->frag, S->grid, S->opt, f, step, i, xyz[i], cen[i]);
-            E[i] = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
-                                     sq, st, ns, cen[i], -1, 0, NULL, NULL, &l1[i]);
-        }
-        double esum = 0.0;
-        for (int i = 0; i < k; ++i) {
-            esum += E[i];
-            if (Eout) Eout[i] = E[i];
-            if (Escale) Escale[i] = l1[i];
-        }
-        free(l1);
-        const double* Ed = Ereplay ? Ereplay : E;
-        int n = F->totalNum;
-        cluster_par P = {0, log((double)info->cavityFactor), beta_muex(S->opt, F) + ln_nbar(info, F), &n,
-                         F->maxNum};
-        int* acc = malloc(sizeof(int) * (size_t)k);
-        int* ins = malloc(sizeof(int) * (size_t)k);
-        int na = 0, fa = -1;
-        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
-        for (int a = 0; a < na; ++a) {
-            if (!ins[a]) continue;
-            int i = acc[a];
-            int slot = F->totalNum++;
-            or_residue* R = &S->res[F->startRes + slot];
-            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
-            for (int s = 0; s < ns; ++s) {
-                or_atom* A = &S->atoms[R->atomStart + s];
-                for (int j = 0; j < 3; ++j) A->position[j] = xyz[i][s][j];
-                A->charge = F->atoms[s].charge;
-                A->type = F->atoms[s].type;
-            }
-        }
-        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
-        free(acc); free(ins); free(xyz); free(cen); free(E);
-    } else if (m == 1) {
-        if (F->totalNum == 0) goto done; /* the reference divides by zero here */
-        k = 1;
-        uint32_t r[4];
-        rng(info->seed, S->opt->replica, (uint32_t)step, 0u, RP_DELETE, 0, r);
-        int slot = (int)(r[0] % (uint32_t)F->totalNum);
-        or_residue* R = &S->res[F->startRes + slot];
-        float xyz[20][3];
-        for (int s = 0; s < ns; ++s)
-            for (int j = 0; j < 3; ++j) xyz[s][j] = S->atoms[R->atomStart + s].position[j];
-        double l1 = 0.0;
-        double E = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz, sq, st,
-                                     ns, R->position, F->startRes + slot, 0, NULL, NULL, &l1);
-        if (Eout) Eout[0] = E;
-        if (Escale) Escale[0] = l1;
-        double Ed = Ereplay ? Ereplay[0] : E;
-        int n = F->totalNum;
-        double lnp = log((double)n) - (beta_muex(S->opt, F) + ln_nbar(info, F)) + OR_BETA * Ed;
-        double u = u53(r[1], r[2]);
-        int acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
-        if (acc) {
-            int last = n - 1;
-            or_residue* RL = &S->res[F->startRes + last];
-            for (int j = 0; j < 3; ++j) R->position[j] = RL->position[j];
-            for (int s = 0; s < R->atomNum; ++s)
-                for (int j = 0; j < 3; ++j)
-                    S->atoms[R->atomStart + s].position[j] = S->atoms[RL->atomStart + s].position[j];
-            F->totalNum -= 1;
-        }
-        if (L) {
-            L->n_clusters = 1; L->n_accept = acc; L->first_accept = acc ? 0 : -1;
-            L->slot = slot; L->e_sum = E;
-        }
-    } else {
-        int n = F->totalNum;
-        k = F->confBias < n ? F->confBias : n;
-        if (k == 0) goto done;
-        if (Eout && k > kmax) return -3;
-        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
-        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
-        int* slots = malloc(sizeof(int) * (size_t)k);
-        double* dE = malloc(sizeof(double) * (size_t)k);
-        double* sc = malloc(sizeof(double) * (size_t)k);
-#pragma omp parallel for num_threads(threads) schedule(dynamic, 2)
-        for (int i = 0; i < k; ++i) {
-            int slot = or_perm_slot(S->opt, info->seed, step, i, n);
-            slots[i] = slot;
-            const or_residue* R = &S->res[F->startRes + slot];
-            float old[20][3];
-            for (int s = 0; s < ns; ++s)
-                for (int j = 0; j < 3; ++j) old[s][j] = S->atoms[R->atomStart + s].position[j];
-            double lo = 0.0, ln = 0.0;
-            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
-                                          st, ns, R->position, F->startRes + slot, 0, NULL, NULL, &lo);
-            or_move_pose(info, S->frag, S->res, S->atoms, S->opt, f, m, step, i, slot, xyz[i], cen[i]);
-            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
-                                          sq, st, ns, cen[i], F->startRes + slot, 0, NULL, NULL, &ln);
-            dE[i] = En - Eo;
-            sc[i] = ln + lo;
-        }
-        double esum = 0.0;
-        for (int i = 0; i < k; ++i) {
-            esum += dE[i];
-            if (Eout) Eout[i] = dE[i];
-            if (Escale) Escale[i] = sc[i];
-        }
-        const double* Ed = Ereplay ? Ereplay : dE;
-        cluster_par P = {1, 0.0, 0.0, NULL, 0};
-        int* acc = malloc(sizeof(int) * (size_t)k);
-        int* ins = malloc(sizeof(int) * (size_t)k);
-        int na = 0, fa = -1;
-        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
-        for (int a = 0; a < na; ++a) {
-            int i = acc[a];
-            or_residue* R = &S->res[F->startRes + slots[i]];
-            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
-            for (int s = 0; s < ns; ++s)
-                for (int j = 0; j < 3; ++j) S->atoms[R->atomStart + s].position[j] = xyz[i][s][j];
-        }
-        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
-        free(acc); free(ins); free(xyz); free(cen); free(slots); free(dE); free(sc);
-    }
-done:
-    if (L) { L->k = k; L->n_after = F->totalNum; }
-    return 0;
-}
-
-int32_t or_run(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
-               const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
-               int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
-               const double* replay, int32_t kmax, int32_t threads) {
-    if (threads <= 0) threads = 1;
-    sysref S = {info, frag, res, atoms, grid, ff, opt};
-    for (int s = 0; s < nsteps; ++s) {
-        int step = step0 + s;
-        int rc = do_step(&S, moves, step, log ? &log[s] : NULL, energies ? energies + (size_t)s * kmax : NULL,
-                         escale ? escale + (size_t)s * kmax : NULL, replay ? replay + (size_t)s * kmax : NULL,
-                         kmax, threads);
-        if (rc) return rc;
-    }
-    return 0;
-}
-
-int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_residue* res,
-                        const or_atom* atoms, const float* ff, const float* poses_xyz,
-                        const float* site_q, const int32_t* site_type, int32_t nsites,
-                        const float* centres, const int32_t* self, int32_t nposes, int32_t mode,
-                        double* out, int32_t* n_groups, double* l1, int32_t threads) {
-    if (threads <= 0) threads = 1;
-    int64_t total = 0;
-#pragma omp parallel for num_threads(threads) schedule(dynamic, 4) reduction(+ : total)
-    for (int p = 0; p < nposes; ++p) {
-        int32_t ng = 0;
-        int64_t np = 0;
-        double m1 = 0.0;
-        out[p] = or_pose_energy_l1(info, frag, res, atoms, ff,
-                                   (const float (*)[3])(poses_xyz + (size_t)p * nsites * 3), site_q,
-                                   site_type, nsites, centres + 3 * p, self ? self[p] : -1, mode, &ng, &np,
-                                   &m1);
-        if (l1) l1[p] = m1;
-        if (n_groups) n_groups[p] = ng;
-        total += np;
-    }
-    return total;
-}
-
-/* ------------------------------------------------------------------------- */
 /* FP64 inputs and analytic gradients of calcEnergy's pair sum.               */
 /*                                                                            */
 /* Same group inclusion as or_pose_energy (the FP32 group-centre distance of  */
@@ -833,6 +657,415 @@ static void pose_grad64(const pose64* P, const float centre[3], int self, double
             }
         }
     });
+}
+
+/* ------------------------------------------------------------------------- */
+/* Moves and the step loop.                                                   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    const or_info* info;
+    or_atomarray* frag;
+    or_residue* res;
+    or_atom* atoms;
+    const float* grid;
+    const float* ff;
+    const or_options* opt;
+    /* or_run_ext extensions (per call; the step pointers are advanced per step) */
+    double* e_total;
+    double* forces;
+    double* fscale;
+    const float* replay_forces;
+} sysref;
+
+/* FP64 force and torque (about the site centroid) on a pose of float sites:
+ * f = (F, tau) with F = -sum_s dE/dx_s, tau = -sum_s (x_s - m) x dE/dx_s;
+ * sc = (sum of |force terms|, sum of |x_s - m| |force terms of s|). */
+static void pose_force64(const sysref* S, const double* ff64, const float (*sx)[3], const float* sq,
+                         const int32_t* st, int ns, const float centre[3], int self, double f[6], double sc[2]) {
+    double x64[20][3], q64[20], g[60], gq[20], gl1[20];
+    for (int s = 0; s < ns; ++s) {
+        for (int j = 0; j < 3; ++j) x64[s][j] = sx[s][j];
+        q64[s] = sq[s];
+    }
+    pose64 P = {S->info, S->frag, S->res, S->atoms, ff64, (const double (*)[3])x64, q64, st, ns};
+    pose_grad64(&P, centre, self, 1.0, g, gq, NULL, gl1, NULL, NULL);
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int s = 0; s < ns; ++s)
+        for (int j = 0; j < 3; ++j) m[j] += x64[s][j] / ns;
+    for (int c = 0; c < 6; ++c) f[c] = 0.0;
+    sc[0] = sc[1] = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const double r[3] = {x64[s][0] - m[0], x64[s][1] - m[1], x64[s][2] - m[2]};
+        const double* gs = g + 3 * s;
+        f[0] -= gs[0]; f[1] -= gs[1]; f[2] -= gs[2];
+        f[3] -= r[1] * gs[2] - r[2] * gs[1];
+        f[4] -= r[2] * gs[0] - r[0] * gs[2];
+        f[5] -= r[0] * gs[1] - r[1] * gs[0];
+        sc[0] += gl1[s];
+        sc[1] += sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) * gl1[s];
+    }
+}
+
+/* Force-biased proposal steps (engine: fb_* in energy.cuh). */
+static inline float fb_shift(const or_info* info, float d, int axis, float c) {
+    const float invL = 1.0f / info->cryst[axis];
+    const float k = floorf(((c + d) - info->startxyz[axis]) * invL);
+    return d - k * info->cryst[axis];
+}
+static void fb_params(const or_options* opt, int trn, float* c1, float* sg) {
+    const float st = opt->fb_trn > 0.0f ? opt->fb_trn : 0.5f;
+    const float sr = opt->fb_rot > 0.0f ? opt->fb_rot : (float)(10.0 * 3.14159265358979323846 / 180.0);
+    *sg = trn ? st : sr;
+    *c1 = (float)(0.5 * (double)*sg * (double)*sg * OR_BETA);
+}
+static double fb_ln_ratio(const float d[3], const float z[3], const float* g, float c1f, float sgf) {
+    const double c1 = c1f, sg = sgf;
+    double fwd = 0.0, rev = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        fwd = fwd + (double)z[a] * (double)z[a];
+        const double e = (-(double)d[a] - c1 * (double)g[a]) / sg;
+        rev = rev + e * e;
+    }
+    return -0.5 * (rev - fwd);
+}
+
+static double beta_muex(const or_options* opt, const or_atomarray* F) {
+    double mu = (double)F->muex;
+    if (opt->muex_kcal) mu *= OR_KCAL_TO_KJ;
+    return OR_BETA * mu;
+}
+
+static double ln_nbar(const or_info* info, const or_atomarray* F) {
+    double V = (double)info->cryst[0] * (double)info->cryst[1] * (double)info->cryst[2];
+    return log(V * (double)F->conc * OR_MOLES_TO_MOLECULES);
+}
+
+static void template_sites(const or_atomarray* F, float* q, int32_t* t) {
+    for (int s = 0; s < F->num_atoms; ++s) { q[s] = F->atoms[s].charge; t[s] = F->atoms[s].type; }
+}
+
+static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_log* L, double* Eout,
+                       double* Escale, const double* Ereplay, int kmax, int threads) {
+    const or_info* info = S->info;
+    int mv = moves[step];
+    int f = mv / 4, m = mv % 4;
+    or_atomarray* F = &S->frag[f];
+    const int ns = F->num_atoms;
+    float sq[20];
+    int32_t st[20];
+    template_sites(F, sq, st);
+    int n0 = F->totalNum;
+    if (L) {
+        memset(L, 0, sizeof(*L));
+        L->step = step; L->move = m; L->ftype = f; L->n_before = n0;
+        L->first_accept = -1; L->slot = -1;
+    }
+    int k = 0;
+    if (m == 0) {
+        if (F->totalNum == F->maxNum) goto done;
+        k = F->confBias;
+        if (Eout && k > kmax) return -3;
+        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
+        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        double* E = malloc(sizeof(double) * (size_t)k);
+        double* l1 = malloc(sizeof(double) * (size_t)k);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
+        for (int i = 0; i < k; ++i) {
+            or_insert_pose(info, S->frag, S->grid, S->opt, f, step, i, xyz[i], cen[i]);
+            E[i] = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
+                                     sq, st, ns, cen[i], -1, 0, NULL, NULL, &l1[i]);
+        }
+        double esum = 0.0;
+        for (int i = 0; i < k; ++i) {
+            esum += E[i];
+            if (Eout) Eout[i] = E[i];
+            if (Escale) Escale[i] = l1[i];
+        }
+        free(l1);
+        const double* Ed = Ereplay ? Ereplay : E;
+        int n = F->totalNum;
+        cluster_par P = {0, log((double)info->cavityFactor), beta_muex(S->opt, F) + ln_nbar(info, F), &n,
+                         F->maxNum};
+        int* acc = malloc(sizeof(int) * (size_t)k);
+        int* ins = malloc(sizeof(int) * (size_t)k);
+        int na = 0, fa = -1;
+        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
+        for (int a = 0; a < na; ++a) {
+            if (!ins[a]) continue;
+            int i = acc[a];
+            if (S->e_total) *S->e_total += Ed[i];
+            int slot = F->totalNum++;
+            or_residue* R = &S->res[F->startRes + slot];
+            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
+            for (int s = 0; s < ns; ++s) {
+                or_atom* A = &S->atoms[R->atomStart + s];
+                for (int j = 0; j < 3; ++j) A->position[j] = xyz[i][s][j];
+                A->charge = F->atoms[s].charge;
+                A->type = F->atoms[s].type;
+            }
+        }
+        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
+        free(acc); free(ins); free(xyz); free(cen); free(E);
+    } else if (m == 1) {
+        if (F->totalNum == 0) goto done; /* the reference divides by zero here */
+        k = 1;
+        uint32_t r[4];
+        rng(info->seed, S->opt->replica, (uint32_t)step, 0u, RP_DELETE, 0, r);
+        int slot = (int)(r[0] % (uint32_t)F->totalNum);
+        or_residue* R = &S->res[F->startRes + slot];
+        float xyz[20][3];
+        for (int s = 0; s < ns; ++s)
+            for (int j = 0; j < 3; ++j) xyz[s][j] = S->atoms[R->atomStart + s].position[j];
+        double l1 = 0.0;
+        double E = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz, sq, st,
+                                     ns, R->position, F->startRes + slot, 0, NULL, NULL, &l1);
+        if (Eout) Eout[0] = E;
+        if (Escale) Escale[0] = l1;
+        double Ed = Ereplay ? Ereplay[0] : E;
+        int n = F->totalNum;
+        double lnp = log((double)n) - (beta_muex(S->opt, F) + ln_nbar(info, F)) + OR_BETA * Ed;
+        double u = u53(r[1], r[2]);
+        int acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+        if (acc) {
+            int last = n - 1;
+            or_residue* RL = &S->res[F->startRes + last];
+            for (int j = 0; j < 3; ++j) R->position[j] = RL->position[j];
+            for (int s = 0; s < R->atomNum; ++s)
+                for (int j = 0; j < 3; ++j)
+                    S->atoms[R->atomStart + s].position[j] = S->atoms[RL->atomStart + s].position[j];
+            F->totalNum -= 1;
+            if (S->e_total) *S->e_total -= Ed;
+        }
+        if (L) {
+            L->n_clusters = 1; L->n_accept = acc; L->first_accept = acc ? 0 : -1;
+            L->slot = slot; L->e_sum = E;
+        }
+    } else if (S->opt->proposal == 2) {
+        /* force-biased translate/rotate with the Metropolis-Hastings correction */
+        int n = F->totalNum;
+        k = F->confBias < n ? F->confBias : n;
+        if (k == 0) goto done;
+        if (Eout && k > kmax) return -3;
+        const int trn = (m == 2);
+        float c1, sg;
+        fb_params(S->opt, trn, &c1, &sg);
+        const size_t nff = (size_t)2 * info->ffXNum * info->ffYNum;
+        double* ff64 = malloc(sizeof(double) * nff);
+        for (size_t j = 0; j < nff; ++j) ff64[j] = S->ff[j];
+        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
+        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        float (*pd)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        float (*pz)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        float (*fnu)[6] = malloc(sizeof(float) * 6 * (size_t)k);
+        int* okv = malloc(sizeof(int) * (size_t)k);
+        int* slots = malloc(sizeof(int) * (size_t)k);
+        double* dE = malloc(sizeof(double) * (size_t)k);
+        double* sc = malloc(sizeof(double) * (size_t)k);
+        double* Eeff = malloc(sizeof(double) * (size_t)k);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 2)
+        for (int i = 0; i < k; ++i) {
+            int slot = or_perm_slot(S->opt, info->seed, step, i, n);
+            slots[i] = slot;
+            const int self = F->startRes + slot;
+            const or_residue* R = &S->res[self];
+            float old[20][3];
+            for (int s2 = 0; s2 < ns; ++s2)
+                for (int j = 0; j < 3; ++j) old[s2][j] = S->atoms[R->atomStart + s2].position[j];
+            double lo = 0.0, ln = 0.0, fo64[6], fn64[6], so[2], sn2[2];
+            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
+                                          st, ns, R->position, self, 0, NULL, NULL, &lo);
+            pose_force64(S, ff64, (const float (*)[3])old, sq, st, ns, R->position, self, fo64, so);
+            float fo[6];
+            for (int c = 0; c < 6; ++c)
+                fo[c] = S->replay_forces ? S->replay_forces[(size_t)i * 12 + c] : (float)fo64[c];
+            float z[4];
+            or_fb_normals(info->seed, S->opt->replica, step, i, z);
+            const float* g = trn ? fo : fo + 3;
+            const int ok = isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]);
+            okv[i] = ok;
+            for (int a = 0; a < 3; ++a) {
+                pd[i][a] = (ok ? c1 * g[a] : 0.0f) + sg * z[a];
+                pz[i][a] = z[a];
+            }
+            if (trn) {
+                for (int j = 0; j < 3; ++j) {
+                    const float sh = fb_shift(info, pd[i][j], j, R->position[j]);
+                    cen[i][j] = R->position[j] + sh;
+                    for (int s2 = 0; s2 < ns; ++s2) xyz[i][s2][j] = old[s2][j] + sh;
+                }
+            } else {
+                for (int s2 = 0; s2 < ns; ++s2)
+                    for (int j = 0; j < 3; ++j) xyz[i][s2][j] = old[s2][j];
+                for (int j = 0; j < 3; ++j) cen[i][j] = R->position[j];
+                const float* d = pd[i];
+                float nn = d[0] * d[0];
+                nn = fmaf(d[1], d[1], nn);
+                nn = fmaf(d[2], d[2], nn);
+                if (nn > 0.0f) {
+                    float ang = sqrtf(nn);
+                    ang = ang - floorf(ang * 0.159154943f) * OR_TWO_PI_F;
+                    float sn, cs, Rm[3][3];
+                    or_det_sincos(ang, &sn, &cs);
+                    rodrigues(d, sn, cs, Rm);
+                    float mc[3] = {0.0f, 0.0f, 0.0f};
+                    for (int j = 0; j < 3; ++j)
+                        for (int s2 = 0; s2 < ns; ++s2) mc[j] = mc[j] + xyz[i][s2][j] / (float)ns;
+                    for (int s2 = 0; s2 < ns; ++s2) {
+                        float q[3] = {xyz[i][s2][0] - mc[0], xyz[i][s2][1] - mc[1], xyz[i][s2][2] - mc[2]};
+                        float pr[3];
+                        rotate(Rm, q, pr);
+                        for (int j = 0; j < 3; ++j) xyz[i][s2][j] = pr[j] + mc[j];
+                    }
+                }
+            }
+            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i], sq,
+                                          st, ns, cen[i], self, 0, NULL, NULL, &ln);
+            pose_force64(S, ff64, (const float (*)[3])xyz[i], sq, st, ns, cen[i], self, fn64, sn2);
+            for (int c = 0; c < 6; ++c)
+                fnu[i][c] = S->replay_forces ? S->replay_forces[(size_t)i * 12 + 6 + c] : (float)fn64[c];
+            if (S->forces)
+                for (int c = 0; c < 6; ++c) {
+                    S->forces[(size_t)i * 12 + c] = fo64[c];
+                    S->forces[(size_t)i * 12 + 6 + c] = fn64[c];
+                }
+            if (S->fscale) {
+                S->fscale[(size_t)i * 4] = so[0]; S->fscale[(size_t)i * 4 + 1] = so[1];
+                S->fscale[(size_t)i * 4 + 2] = sn2[0]; S->fscale[(size_t)i * 4 + 3] = sn2[1];
+            }
+            dE[i] = En - Eo;
+            sc[i] = ln + lo;
+        }
+        double esum = 0.0;
+        for (int i = 0; i < k; ++i) {
+            esum += dE[i];
+            if (Eout) Eout[i] = dE[i];
+            if (Escale) Escale[i] = sc[i];
+        }
+        const double* Ed = Ereplay ? Ereplay : dE;
+        for (int i = 0; i < k; ++i) {
+            const float* gn = trn ? fnu[i] : fnu[i] + 3;
+            Eeff[i] = (!okv[i] || !isfinite(Ed[i])) ? INFINITY
+                                                    : Ed[i] - fb_ln_ratio(pd[i], pz[i], gn, c1, sg) / OR_BETA;
+        }
+        cluster_par P = {1, 0.0, 0.0, NULL, 0};
+        int* acc = malloc(sizeof(int) * (size_t)k);
+        int* ins = malloc(sizeof(int) * (size_t)k);
+        int na = 0, fa = -1;
+        int nc = cluster_pass(info, S->opt, step, k, Eeff, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
+        for (int a = 0; a < na; ++a) {
+            int i = acc[a];
+            or_residue* R = &S->res[F->startRes + slots[i]];
+            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
+            for (int s2 = 0; s2 < ns; ++s2)
+                for (int j = 0; j < 3; ++j) S->atoms[R->atomStart + s2].position[j] = xyz[i][s2][j];
+            if (S->e_total) *S->e_total += Ed[i];
+        }
+        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
+        free(acc); free(ins); free(xyz); free(cen); free(pd); free(pz); free(fnu); free(okv); free(slots);
+        free(dE); free(sc); free(Eeff); free(ff64);
+    } else {
+        int n = F->totalNum;
+        k = F->confBias < n ? F->confBias : n;
+        if (k == 0) goto done;
+        if (Eout && k > kmax) return -3;
+        float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
+        float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        int* slots = malloc(sizeof(int) * (size_t)k);
+        double* dE = malloc(sizeof(double) * (size_t)k);
+        double* sc = malloc(sizeof(double) * (size_t)k);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 2)
+        for (int i = 0; i < k; ++i) {
+            int slot = or_perm_slot(S->opt, info->seed, step, i, n);
+            slots[i] = slot;
+            const or_residue* R = &S->res[F->startRes + slot];
+            float old[20][3];
+            for (int s = 0; s < ns; ++s)
+                for (int j = 0; j < 3; ++j) old[s][j] = S->atoms[R->atomStart + s].position[j];
+            double lo = 0.0, ln = 0.0;
+            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
+                                          st, ns, R->position, F->startRes + slot, 0, NULL, NULL, &lo);
+            or_move_pose(info, S->frag, S->res, S->atoms, S->opt, f, m, step, i, slot, xyz[i], cen[i]);
+            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
+                                          sq, st, ns, cen[i], F->startRes + slot, 0, NULL, NULL, &ln);
+            dE[i] = En - Eo;
+            sc[i] = ln + lo;
+        }
+        double esum = 0.0;
+        for (int i = 0; i < k; ++i) {
+            esum += dE[i];
+            if (Eout) Eout[i] = dE[i];
+            if (Escale) Escale[i] = sc[i];
+        }
+        const double* Ed = Ereplay ? Ereplay : dE;
+        cluster_par P = {1, 0.0, 0.0, NULL, 0};
+        int* acc = malloc(sizeof(int) * (size_t)k);
+        int* ins = malloc(sizeof(int) * (size_t)k);
+        int na = 0, fa = -1;
+        int nc = cluster_pass(info, S->opt, step, k, Ed, (const float (*)[3])cen, &P, acc, ins, &na, &fa);
+        for (int a = 0; a < na; ++a) {
+            int i = acc[a];
+            or_residue* R = &S->res[F->startRes + slots[i]];
+            for (int j = 0; j < 3; ++j) R->position[j] = cen[i][j];
+            for (int s = 0; s < ns; ++s)
+                for (int j = 0; j < 3; ++j) S->atoms[R->atomStart + s].position[j] = xyz[i][s][j];
+            if (S->e_total) *S->e_total += Ed[i];
+        }
+        if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
+        free(acc); free(ins); free(xyz); free(cen); free(slots); free(dE); free(sc);
+    }
+done:
+    if (L) { L->k = k; L->n_after = F->totalNum; L->e_total = S->e_total ? *S->e_total : 0.0; }
+    return 0;
+}
+
+int32_t or_run(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
+               const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
+               int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
+               const double* replay, int32_t kmax, int32_t threads) {
+    return or_run_ext(info, frag, res, atoms, grid, ff, moves, opt, step0, nsteps, log, energies, escale, replay,
+                      kmax, threads, NULL, NULL, NULL, NULL);
+}
+
+int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
+                   const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
+                   int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
+                   const double* replay, int32_t kmax, int32_t threads, double* e_total,
+                   double* forces, double* fscale, const float* replay_forces) {
+    if (threads <= 0) threads = 1;
+    for (int s = 0; s < nsteps; ++s) {
+        int step = step0 + s;
+        sysref S = {info, frag, res, atoms, grid, ff, opt, e_total,
+                    forces ? forces + (size_t)s * kmax * 12 : NULL, fscale ? fscale + (size_t)s * kmax * 4 : NULL,
+                    replay_forces ? replay_forces + (size_t)s * kmax * 12 : NULL};
+        int rc = do_step(&S, moves, step, log ? &log[s] : NULL, energies ? energies + (size_t)s * kmax : NULL,
+                         escale ? escale + (size_t)s * kmax : NULL, replay ? replay + (size_t)s * kmax : NULL,
+                         kmax, threads);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                        const or_atom* atoms, const float* ff, const float* poses_xyz,
+                        const float* site_q, const int32_t* site_type, int32_t nsites,
+                        const float* centres, const int32_t* self, int32_t nposes, int32_t mode,
+                        double* out, int32_t* n_groups, double* l1, int32_t threads) {
+    if (threads <= 0) threads = 1;
+    int64_t total = 0;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4) reduction(+ : total)
+    for (int p = 0; p < nposes; ++p) {
+        int32_t ng = 0;
+        int64_t np = 0;
+        double m1 = 0.0;
+        out[p] = or_pose_energy_l1(info, frag, res, atoms, ff,
+                                   (const float (*)[3])(poses_xyz + (size_t)p * nsites * 3), site_q,
+                                   site_type, nsites, centres + 3 * p, self ? self[p] : -1, mode, &ng, &np,
+                                   &m1);
+        if (l1) l1[p] = m1;
+        if (n_groups) n_groups[p] = ng;
+        total += np;
+    }
+    return total;
 }
 
 int64_t or_energy_batch64(const or_info* info, const or_atomarray* frag, const or_residue* res,

@@ -64,12 +64,14 @@ typedef struct { float position[3]; int32_t atomNum; int32_t atomStart; } or_res
 
 /* ---- engine options (same meaning as gcmc_options in include/gcmc_b200.h) ---- */
 typedef struct {
-    int32_t proposal;   /* 0: reference proposals, 1: symmetric proposals      */
+    int32_t proposal;   /* 0: reference, 1: symmetric, 2: force-biased proposals */
     int32_t muex_kcal;  /* 0: beta*muex with muex as given, 1: muex in kcal/mol */
     float trn_step;     /* symmetric translate: cube edge (A)                   */
     float rot_max;      /* symmetric rotate: max angle (rad)                    */
     uint32_t replica;   /* RNG stream id                                        */
-    int32_t reserved[3];
+    float fb_trn;       /* proposal 2: translate step sigma_t (A)               */
+    float fb_rot;       /* proposal 2: rotation step sigma_r (rad)              */
+    int32_t reserved;
 } or_options;
 
 /* Per-step record; identical layout to gcmc_step_log in include/gcmc_b200.h. */
@@ -79,6 +81,7 @@ typedef struct {
     int32_t first_accept;   /* pose index of the first accepted cluster, -1 if none */
     int32_t slot;           /* delete: chosen slot; otherwise -1                    */
     double e_sum;           /* sum over poses of E (insert/delete) or dE (trn/rot)  */
+    double e_total;         /* running sum of accepted energy changes after the step */
 } or_step_log;
 
 /* Counter-based RNG: Philox4x32-10. */
@@ -135,6 +138,25 @@ int32_t or_run(const or_info* info, or_atomarray* frag, or_residue* res, or_atom
                const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
                int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
                const double* replay_energies, int32_t kmax, int32_t threads);
+
+/* or_run with the force-biased (proposal 2) and running-energy extensions:
+ * e_total (in/out, optional): running sum of the accepted moves' energy
+ * changes (the energies decisions use); forces (optional, [s*kmax + i][12]):
+ * the oracle's FP64 force and torque at the old and at the new pose of each
+ * force-biased translate/rotate pose; fscale ([s*kmax + i][4], optional): their
+ * l1 scales (sum of |pair terms| of the force, and of |r| times them for the
+ * torque); replay_forces ([s*kmax + i][12], optional): forces to use instead
+ * of the oracle's own (as float, the values another engine used). */
+int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
+                   const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
+                   int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
+                   const double* replay_energies, int32_t kmax, int32_t threads, double* e_total,
+                   double* forces, double* fscale, const float* replay_forces);
+
+/* Own float log and the four Box-Muller normals of a force-biased proposal
+ * (identical to the engine's). */
+float or_det_log(float x);
+void or_fb_normals(uint32_t seed, uint32_t replica, int32_t step, int32_t i, float z[4]);
 
 /* Energies of many explicit poses (OpenMP over poses): poses_xyz[p*nsites*3],
  * centres[p*3], self[p]; returns pair count. */

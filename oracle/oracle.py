@@ -16,7 +16,8 @@ c_void = ctypes.c_void_p
 
 class OrOptions(ctypes.Structure):
     _fields_ = [("proposal", ctypes.c_int32), ("muex_kcal", ctypes.c_int32), ("trn_step", ctypes.c_float),
-                ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("reserved", ctypes.c_int32 * 3)]
+                ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("fb_trn", ctypes.c_float),
+                ("fb_rot", ctypes.c_float), ("reserved", ctypes.c_int32)]
 
 
 def build():
@@ -33,6 +34,12 @@ def lib():
         if not os.path.exists(LIB):
             build()
         L = ctypes.CDLL(LIB)
+        L.or_run_ext.restype = ctypes.c_int32
+        L.or_run_ext.argtypes = [c_void] * 8 + [ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void,
+                                                ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void]
+        L.or_det_log.restype = ctypes.c_float
+        L.or_det_log.argtypes = [ctypes.c_float]
+        L.or_fb_normals.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, c_void]
         L.or_run.restype = ctypes.c_int32
         L.or_run.argtypes = [c_void] * 8 + [ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void,
                                             ctypes.c_int32, ctypes.c_int32]
@@ -65,8 +72,41 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(c_void)
 
 
-def options(proposal=0, muex_kcal=0, trn_step=1.0, rot_max=np.radians(15.0), replica=0):
-    return OrOptions(proposal, muex_kcal, trn_step, rot_max, replica)
+def options(proposal=0, muex_kcal=0, trn_step=1.0, rot_max=np.radians(15.0), replica=0, fb_trn=0.5,
+            fb_rot=np.radians(10.0)):
+    return OrOptions(proposal, muex_kcal, trn_step, rot_max, replica, fb_trn, fb_rot, 0)
+
+
+def run_ext(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, replay_forces=None,
+            e_total=0.0):
+    """:func:`run` with the running energy and the force-biased extensions.
+    Returns a dict: logs, energies, scale, forces [n, kmax, 12] (the oracle's
+    FP64 old/new force and torque of force-biased poses), fscale [n, kmax, 4]
+    and e_total (the running energy after the last step)."""
+    from pygcmc_b200.values import StepLog_dtype
+    opts = opts or options()
+    threads = threads or os.cpu_count() or 1
+    out = {"logs": np.zeros(nsteps, dtype=StepLog_dtype), "energies": np.zeros((nsteps, kmax)),
+           "scale": np.zeros((nsteps, kmax)), "forces": np.zeros((nsteps, kmax, 12)),
+           "fscale": np.zeros((nsteps, kmax, 4))}
+    rp = None if replay is None else np.ascontiguousarray(replay, dtype=np.float64)
+    rf = None if replay_forces is None else np.ascontiguousarray(replay_forces, dtype=np.float32)
+    et = ctypes.c_double(e_total)
+    s = system
+    rc = lib().or_run_ext(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), _p(s.grid),
+                          _p(s.ff), _p(s.moveArray), ctypes.byref(opts), step0, nsteps, _p(out["logs"]),
+                          _p(out["energies"]), _p(out["scale"]), _p(rp), kmax, threads, ctypes.byref(et),
+                          _p(out["forces"]), _p(out["fscale"]), _p(rf))
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed ({rc})")
+    out["e_total"] = et.value
+    return out
+
+
+def fb_normals(seed, replica, step, i):
+    z = np.zeros(4, np.float32)
+    lib().or_fb_normals(seed, replica, step, i, _p(z))
+    return z
 
 
 def run(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, want_energies=True,

@@ -19,7 +19,7 @@ class Options(ctypes.Structure):
     _fields_ = [("proposal", c_int), ("muex_kcal", c_int), ("trn_step", ctypes.c_float),
                 ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("cells_per_cutoff", c_int),
                 ("log_steps", c_int), ("log_kmax", c_int), ("split_items", c_int), ("branches", c_int),
-                ("energy_blocks_per_sm", c_int)]
+                ("energy_blocks_per_sm", c_int), ("fb_trn", ctypes.c_float), ("fb_rot", ctypes.c_float)]
 
 
 class TuneTrial(ctypes.Structure):
@@ -62,6 +62,8 @@ def lib():
         "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
         "gcmc_last_status": (c_int, []),
         "gcmc_release_cache": (c_int, []),
+        "gcmc_get_forces": (c_int, [c_void, c_int, c_void, c_int, P(c_int)]),
+        "gcmc_energy_total": (c_int, [c_void, c_int, P(ctypes.c_double)]),
         "gcmc_energy_grad": (c_int, [c_void, c_int] + [c_void] * 4 + [c_int, c_void, c_void, c_int] + [c_void] * 7),
         "gcmc_run_batch": (c_int, [c_int, c_void, P(Options)]),
         "gcmc_autotune": (c_int, [c_int, c_void, P(Options), c_int, P(Options), c_void, c_int, P(c_int)]),
@@ -121,7 +123,8 @@ def default_options(**kw):
     return o
 
 
-EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
+EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_get_forces",
+           "gcmc_energy_total", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",
            "gcmc_energy_poses_noalloc", "gcmc_synth_place", "gcmc_synth_chain_sphere",

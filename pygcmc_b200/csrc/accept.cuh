@@ -24,7 +24,8 @@ namespace gcmc {
 constexpr int kAcceptThreads = 1024;
 
 struct AcceptSmem {
-    double E[kMaxPoses];
+    double E[kMaxPoses];      // energy entering the acceptance (force-biased: dE - ln(q ratio) / beta)
+    double ephys[kMaxPoses];  // the pose's energy (insert/delete) or energy change (translate/rotate)
     double w[kMaxPoses];
     unsigned long long key[kMaxPoses];  // order-preserving encoding of the Gumbel key
     double lnu[kMaxPoses];              // ln of the acceptance draw of the cluster seeded by pose i
@@ -138,6 +139,7 @@ __device__ void prepare_step(const RepDev& R, int step) {
                 D.nvar = 2;
                 D.perm_key = rng(R.seed, R.replica, (uint32_t)step, 0u, RP_PERM, 0);
                 D.perm_h = perm_bits(n);
+                D.fb = R.fb;
             }
             if (D.k > kMaxPoses) {
                 atomicOr(R.err, ERR_POSES);
@@ -147,7 +149,8 @@ __device__ void prepare_step(const RepDev& R, int step) {
             // split each pose's cell window so a step has about split_items work items
             const int kv = max(1, D.k * D.nvar);
             D.nslab = max(1, min(R.max_split, (R.split_items + kv - 1) / kv));
-            D.items = D.k * D.nvar * D.nslab;
+            D.items = D.fb ? D.k * D.nslab : D.k * D.nvar * D.nslab;
+            D.items_pre = D.fb ? D.k * D.nslab : 0;
         }
         Dsh = D;
     }
@@ -167,7 +170,7 @@ __device__ void prepare_step(const RepDev& R, int step) {
             const int slot = perm_slot(D.perm_key, D.perm_h, i, D.n);
             R.pslot[i] = slot;
             float4 c = R.gcen[startRes + slot];
-            if (D.move == MV_TRANSLATE) {
+            if (D.move == MV_TRANSLATE && !D.fb) {  // force-biased: set by the old-pose launch
                 U4 r = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_MOVE, 0);
                 c.x = fadd(c.x, trn_shift(R, r.x, 0, c.x));
                 c.y = fadd(c.y, trn_shift(R, r.y, 1, c.y));
@@ -234,6 +237,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     } while (0)
 
     // ---- phase 0: pose energies (sum of slab partials; dE for translate/rotate)
+    const bool logging = R.log != nullptr && D.step < R.log_cap;
     for (int i = tid; i < k; i += nt) {
         double e = 0.0;
         for (int z = 0; z < D.nslab; ++z) e += R.epart[(i * D.nvar) * D.nslab + z];
@@ -242,19 +246,33 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             for (int z = 0; z < D.nslab; ++z) eo += R.epart[(i * 2 + 1) * D.nslab + z];
             e = e - eo;
         }
-        S.E[i] = e;
+        S.ephys[i] = e;
+        if (D.fb) {  // Metropolis-Hastings: exp(-beta dE) q(new -> old) / q(old -> new)
+            float fo[6], fn[6];
+            fb_force(R, D, i, 1, fo, false);
+            fb_force(R, D, i, 0, fn, false);
+            const float4 d = R.fbprop[2 * i], z = R.fbprop[2 * i + 1];
+            double eff = INFINITY;
+            if (d.w == 0.0f && isfinite(e)) eff = __dsub_rn(e, __ddiv_rn(fb_ln_ratio(R, D, d, z, fn), kBeta));
+            S.E[i] = eff;
+            if (logging && R.logF && i < R.log_kmax) {
+                float* o = R.logF + ((size_t)D.step * R.log_kmax + i) * 12;
+                for (int c = 0; c < 6; ++c) { o[c] = fo[c]; o[6 + c] = fn[c]; }
+            }
+        } else {
+            S.E[i] = e;
+        }
     }
     if (tid == 0) { S.misc[0] = 0; S.misc[1] = 0; S.misc[2] = -1; S.misc[3] = D.n; }
     __syncthreads();
     PHASE(0);
-    const bool logging = R.log != nullptr && D.step < R.log_cap;
     double esum = 0.0;
     if (logging) {
         double v = 0.0;
-        for (int i = tid; i < k; i += nt) v += S.E[i];
+        for (int i = tid; i < k; i += nt) v += S.ephys[i];
         esum = block_sum(v, S.red);
         const int kl = min(k, R.log_kmax);
-        for (int i = tid; i < kl; i += nt) R.logE[(size_t)D.step * R.log_kmax + i] = S.E[i];
+        for (int i = tid; i < kl; i += nt) R.logE[(size_t)D.step * R.log_kmax + i] = S.ephys[i];
     }
 
     if (D.move == MV_DELETE) {
@@ -280,6 +298,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     cell_rename(R, gl, gs);
                 }
                 R.totalNum[D.ftype] = n - 1;
+                *R.energy -= E;
             }
             S.misc[0] = acc ? 1 : 0;
             S.misc[1] = 1;
@@ -484,7 +503,8 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     const float4 at = R.xyzq[sp.x + lane];
                     px = at.x; py = at.y; pz = at.z; qw = at.w;
                 }
-                moved_site(R, D, i, gc, ns, lane, px, py, pz);
+                if (D.fb) fb_moved_site(R, D, i, gc, ns, lane, px, py, pz);
+                else moved_site(R, D, i, gc, ns, lane, px, py, pz);
                 if (lane < ns) R.xyzq[sp.x + lane] = make_float4(px, py, pz, qw);
             }
             __syncthreads();
@@ -505,6 +525,13 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     }
     __syncthreads();
     if (tid == 0) {
+        if (D.move != MV_DELETE) {  // running energy: accepted moves in commit order
+            double et = *R.energy;
+            const int na = S.misc[0];
+            for (int a = 0; a < na; ++a)
+                if (D.move != MV_INSERT || S.acc_slot[a] >= 0) et += S.ephys[S.acc_list[a]];
+            *R.energy = et;
+        }
         R.counters[0] += 1ull;
         R.counters[1] += (unsigned long long)(k * D.nvar);
         if (logging) {
@@ -520,6 +547,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             L.first_accept = S.misc[2];
             L.slot = (D.move == MV_DELETE && k > 0) ? D.del_slot : -1;
             L.e_sum = esum;
+            L.e_total = *R.energy;
             R.log[D.step] = L;
         }
     }

@@ -23,7 +23,7 @@ constexpr int kMaxPoses = 1024;  // poses per step (confBias limit)
 constexpr int kMaxWords = kMaxPoses / 32;
 
 // RNG purposes: high half of the third counter word.
-enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6 };
+enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6, RP_FB = 7 };
 enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
 enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8 };
 
@@ -216,6 +216,46 @@ __device__ __forceinline__ void rotate(const Mat3& R, float p0, float p1, float 
     o0 = x; o1 = y; o2 = z;
 }
 
+// Own natural logarithm for x > 0 (finite, normal), identical on the host
+// oracle: x = m 2^e with m in [sqrt(1/2), sqrt(2)), ln m = 2 atanh(s) with
+// s = (m - 1) / (m + 1) summed as the odd series s (1 + s^2/3 + ... + s^10/11)
+// (|s| <= 0.1716, truncation < 1e-9 relative), ln x = e ln2_hi + (e ln2_lo + ln m).
+__device__ __forceinline__ float det_log(float x) {
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) {
+        m = fmul(m, 0.5f);
+        e += 1;
+    }
+    const float s = fdiv(fsub(m, 1.0f), fadd(m, 1.0f));
+    const float s2 = fmul(s, s);
+    float p = fadd(fmul(s2, 0.0909090936f), 0.111111112f);  // 1/11, 1/9
+    p = fadd(fmul(s2, p), 0.142857149f);                      // 1/7
+    p = fadd(fmul(s2, p), 0.200000003f);                      // 1/5
+    p = fadd(fmul(s2, p), 0.333333343f);                      // 1/3
+    p = fadd(fmul(s2, p), 1.0f);
+    const float lnm = fmul(fmul(2.0f, s), p);
+    const float ef = (float)e;
+    return fadd(fmul(ef, 0.693145751953125f), fadd(fmul(ef, 1.42860677e-06f), lnm));
+}
+
+// Four standard normal draws (Box-Muller on one Philox block) for the
+// force-biased proposal of pose i of a step.
+__device__ __forceinline__ void fb_normals(uint32_t seed, uint32_t replica, int step, int i, float z[4]) {
+    const U4 r = rng(seed, replica, (uint32_t)step, (uint32_t)i, RP_FB, 0);
+    const float ra = fsqrt(fmul(-2.0f, det_log(u01_oc(r.x))));
+    const float rb = fsqrt(fmul(-2.0f, det_log(u01_oc(r.z))));
+    float sa, ca, sb, cb;
+    det_sincos(fmul(u01_co(r.y), kTwoPiF), sa, ca);
+    det_sincos(fmul(u01_co(r.w), kTwoPiF), sb, cb);
+    z[0] = fmul(ra, ca);
+    z[1] = fmul(ra, sa);
+    z[2] = fmul(rb, cb);
+    z[3] = fmul(rb, sb);
+}
+
+
 // Keyed permutation of [0,n) (4-round Feistel on 2h bits, cycle walking;
 // round function = the MurmurHash3 32-bit finaliser).
 __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
@@ -261,10 +301,12 @@ struct StepDesc {
     int nvar;      // 1, or 2 for translate/rotate (new, old)
     int nslab;     // work items per pose variant (each covers a contiguous range of window cells)
     int nw;        // neighbour-row words (0 = no clustering)
-    int items;     // k * nvar * nslab
+    int items;     // k * nvar * nslab (force-biased steps: k * nslab, the new poses)
     int del_slot;
     int perm_h;
-    int pad;
+    int fb;        // 1: force-biased translate/rotate (old-pose forces first, then new poses)
+    int items_pre; // force-biased steps: k * nslab old-pose items of the first launch; else 0
+    int pad[3];
     U4 perm_key;
 };
 
@@ -290,6 +332,11 @@ struct RepDev {
     uint32_t seed, replica;
     int run_end;        // steps below this index are executed
     int log_cap, log_kmax;
+    // force-biased translate/rotate (proposal 2): displacement d = c1 f + sigma z,
+    // z ~ N(0, I3), f the force (translate) or torque (rotate) at the old pose
+    int fb;
+    float fb_c1t, fb_sig_t;  // translate: sigma_t^2 beta / 2 [A^2 mol/kJ], sigma_t [A]
+    float fb_c1r, fb_sig_r;  // rotate: sigma_r^2 beta / 2 [mol/kJ], sigma_r [rad]
     // state
     float4* xyzq;       // atom x, y, z, charge
     int* atype;         // atom type (column of the LJ table)
@@ -314,6 +361,12 @@ struct RepDev {
     double* logE;
     unsigned long long* counters;  // steps, poses, pairs, then 8 accept-kernel phase cycle sums
     int* err;
+    double* energy;     // running sum of the accepted moves' energy changes (FP64)
+    // force-biased moves
+    float* fpart;       // [kMaxPoses * 2 * nslab_max * 6] per-item force and torque partials
+    float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (z0, z1, z2, 0)
+    int* fbcnt;         // [kMaxPoses] old-pose items finished (reset by the last one)
+    float* logF;        // [log_cap * log_kmax * 12] F_old, tau_old, F_new, tau_new used
 };
 
 __device__ __forceinline__ int wrapi(int c, int n) {

@@ -351,6 +351,109 @@ __device__ __forceinline__ void moved_site(const RepDev& R, const StepDesc& D, i
     pz = fadd(z, mz);
 }
 
+// ---- force-biased translate/rotate (proposal 2) ----
+//
+// Pose i's displacement is d = c1 f + sigma z with f the force (translate) or
+// the torque about the site centroid (rotate) at the old pose and z ~ N(0, I3)
+// (fb_normals).  A translate moves the sites by d wrapped so the new centre
+// lies in the box; a rotate turns them about their centroid by the rotation
+// vector v = d.  The proposal density ratio q(new -> old) / q(old -> new) enters
+// the acceptance (fb_ln_ratio).  All float steps are explicit round-to-nearest
+// operations so the host oracle reproduces them bit for bit.
+
+// Force and torque partials of pose i, variant v, summed over the slabs in
+// order (FP64) and rounded to float.  cg: read through L2 only (partials
+// written by other CTAs of the running launch).
+__device__ __forceinline__ void fb_force(const RepDev& R, const StepDesc& D, int i, int v, float f[6], bool cg) {
+    for (int c = 0; c < 6; ++c) {
+        double a = 0.0;
+        for (int z = 0; z < D.nslab; ++z) {
+            const float* p = R.fpart + ((size_t)(i * 2 + v) * D.nslab + z) * 6 + c;
+            a += (double)(cg ? __ldcg(p) : *p);
+        }
+        f[c] = (float)a;
+    }
+}
+
+// Shift of the centre coordinate c by d, wrapped into [start, start + L).
+__device__ __forceinline__ float fb_shift(const RepDev& R, float d, int axis, float c) {
+    const float k = floorf(fmul(fsub(fadd(c, d), R.start[axis]), R.invL[axis]));
+    return fsub(d, fmul(k, R.L[axis]));
+}
+
+// Proposal of pose i from its old-pose force/torque f and group centre gc:
+// prop[0] = (d, invalid), prop[1] = (z, 0); returns the new centre.
+__device__ __forceinline__ float4 fb_propose(const RepDev& R, const StepDesc& D, int i, const float f[6],
+                                             float4 gc, float4* prop) {
+    float z[4];
+    fb_normals(R.seed, R.replica, D.step, i, z);
+    const bool trn = D.move == MV_TRANSLATE;
+    const float* g = trn ? f : f + 3;
+    const bool ok = isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]);
+    const float c1 = trn ? R.fb_c1t : R.fb_c1r, sg = trn ? R.fb_sig_t : R.fb_sig_r;
+    float d[3];
+    for (int a = 0; a < 3; ++a) d[a] = fadd(ok ? fmul(c1, g[a]) : 0.0f, fmul(sg, z[a]));
+    prop[0] = make_float4(d[0], d[1], d[2], ok ? 0.0f : 1.0f);
+    prop[1] = make_float4(z[0], z[1], z[2], 0.0f);
+    if (!trn) return gc;
+    return make_float4(fadd(gc.x, fb_shift(R, d[0], 0, gc.x)), fadd(gc.y, fb_shift(R, d[1], 1, gc.y)),
+                       fadd(gc.z, fb_shift(R, d[2], 2, gc.z)), 0.0f);
+}
+
+// New site of lane `lane` (old site p) under pose i's stored proposal.
+__device__ __forceinline__ void fb_moved_site(const RepDev& R, const StepDesc& D, int i, const float4& gc, int ns,
+                                              int lane, float& px, float& py, float& pz) {
+    const float4 d = R.fbprop[2 * i];
+    if (D.move == MV_TRANSLATE) {
+        px = fadd(px, fb_shift(R, d.x, 0, gc.x));
+        py = fadd(py, fb_shift(R, d.y, 1, gc.y));
+        pz = fadd(pz, fb_shift(R, d.z, 2, gc.z));
+        return;
+    }
+    float nn = fmul(d.x, d.x);
+    nn = ffma(d.y, d.y, nn);
+    nn = ffma(d.z, d.z, nn);
+    if (!(nn > 0.0f)) return;
+    float ang = fsqrt(nn);
+    ang = fsub(ang, fmul(floorf(fmul(ang, 0.159154943f)), kTwoPiF));  // same rotation, angle in [0, 2 pi)
+    float sn, cs;
+    det_sincos(ang, sn, cs);
+    const Mat3 Rm = rodrigues(d.x, d.y, d.z, sn, cs);
+    const float nsf = (float)ns;
+    float mx = 0.f, my = 0.f, mz = 0.f;
+    for (int s = 0; s < ns; ++s) {
+        mx = fadd(mx, fdiv(__shfl_sync(kFull, px, s), nsf));
+        my = fadd(my, fdiv(__shfl_sync(kFull, py, s), nsf));
+        mz = fadd(mz, fdiv(__shfl_sync(kFull, pz, s), nsf));
+    }
+    float x, y, z;
+    rotate(Rm, fsub(px, mx), fsub(py, my), fsub(pz, mz), x, y, z);
+    px = fadd(x, mx);
+    py = fadd(y, my);
+    pz = fadd(z, mz);
+}
+
+// ln q(new -> old) - ln q(old -> new) for pose i: the reverse displacement is
+// -d from the new pose with its force/torque fn; q is the N(c1 f, sigma^2 I3)
+// density of the displacement (the rotation-vector Jacobian is even in v and
+// cancels).  FP64 with explicit rounding.
+__device__ __forceinline__ double fb_ln_ratio(const RepDev& R, const StepDesc& D, const float4& d, const float4& z,
+                                              const float fn[6]) {
+    const bool trn = D.move == MV_TRANSLATE;
+    const float* g = trn ? fn : fn + 3;
+    const double c1 = trn ? (double)R.fb_c1t : (double)R.fb_c1r;
+    const double sg = trn ? (double)R.fb_sig_t : (double)R.fb_sig_r;
+    const double dd[3] = {(double)d.x, (double)d.y, (double)d.z};
+    const double zz[3] = {(double)z.x, (double)z.y, (double)z.z};
+    double fwd = 0.0, rev = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        fwd = __dadd_rn(fwd, __dmul_rn(zz[a], zz[a]));
+        const double e = __ddiv_rn(__dsub_rn(-dd[a], __dmul_rn(c1, (double)g[a])), sg);
+        rev = __dadd_rn(rev, __dmul_rn(e, e));
+    }
+    return __dmul_rn(-0.5, __dsub_rn(rev, fwd));
+}
+
 // Load the pose of item (i, variant v) of step D into B.site; returns the
 // pose centre and the residue to skip.
 __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, int i, int v, WarpBuf& B,
@@ -392,7 +495,10 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
         const float4 c = R.pcen[i];
         cx = c.x; cy = c.y; cz = c.z;
     }
-    if (D.move != MV_DELETE && v == 0) moved_site(R, D, i, gc, ns, lane, px, py, pz);
+    if (D.move != MV_DELETE && v == 0) {
+        if (D.fb) fb_moved_site(R, D, i, gc, ns, lane, px, py, pz);
+        else moved_site(R, D, i, gc, ns, lane, px, py, pz);
+    }
     if (lane < ns)
         B.site[lane] = make_float4((float)((double)px - (double)cx), (float)((double)py - (double)cy),
                                    (float)((double)pz - (double)cz), kCoulomb * F.site[lane].w);

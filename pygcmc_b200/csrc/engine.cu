@@ -30,7 +30,7 @@ struct RepHost {
     int nslab = 0, log_cap = 0, log_kmax = 0;
     int host_end = 0;
     std::vector<int> startRes, maxNum, moves_host;
-    size_t capn[24] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
+    size_t capn[32] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
     // device allocations (owned)
     float4* xyzq = nullptr;
     int* atype = nullptr;
@@ -53,6 +53,11 @@ struct RepHost {
     double* logE = nullptr;
     unsigned long long* counters = nullptr;
     int* err = nullptr;
+    double* energy = nullptr;
+    float* fpart = nullptr;
+    float4* fbprop = nullptr;
+    int* fbcnt = nullptr;
+    float* logF = nullptr;
 };
 
 }  // namespace
@@ -69,6 +74,8 @@ struct gcmc_ctx {
     int gridE = 0;       // pose-energy CTAs for all replicas
     int branches = 1;    // independent chains in the captured step loop
     int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
+    int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
+    int gridF = 0;       // k_energy_fb CTAs
     std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
 };
 
@@ -114,6 +121,7 @@ void free_rep(RepHost& h) {
     dfree(h.gcell); dfree(h.grid); dfree(h.lj); dfree(h.moves); dfree(h.frag); dfree(h.totalNum);
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
+    dfree(h.energy); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     for (auto& c : h.capn) c = 0;
 }
 
@@ -220,6 +228,14 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.trn_step = opt.trn_step;
     d.rot_max = opt.rot_max;
     d.proposal = opt.proposal;
+    d.fb = opt.proposal == 2 ? 1 : 0;
+    {
+        const double st = opt.fb_trn > 0.0f ? opt.fb_trn : 0.5, sr = opt.fb_rot > 0.0f ? opt.fb_rot : 10.0 * M_PI / 180.0;
+        d.fb_sig_t = (float)st;
+        d.fb_c1t = (float)(0.5 * (double)d.fb_sig_t * (double)d.fb_sig_t * kBeta);
+        d.fb_sig_r = (float)sr;
+        d.fb_c1r = (float)(0.5 * (double)d.fb_sig_r * (double)d.fb_sig_r * kBeta);
+    }
     d.lncav = std::log((double)I->cavityFactor);
     d.nfixed = in.fragmentInfo[0].startRes;
     d.ntypes = I->fragTypeNum;
@@ -326,18 +342,25 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
 
     int st;
     int bi = 0;
-#define AL(ptr, n) if ((st = ensure(&(ptr), &h.capn[bi++], (size_t)(n))) != GCMC_OK) return st
+#define AL(ptr, n)                                                                          \
+    do {                                                                                    \
+        if (bi >= (int)(sizeof(h.capn) / sizeof(h.capn[0]))) return GCMC_ERR_LIMIT;          \
+        if ((st = ensure(&(ptr), &h.capn[bi++], (size_t)(n))) != GCMC_OK) return st;        \
+    } while (0)
     AL(h.xyzq, h.natoms); AL(h.atype, h.natoms); AL(h.gcen, h.ngroups); AL(h.gspan, h.ngroups);
     AL(h.cell_count, h.ncell); AL(h.cell_ent, (size_t)h.ncell * cap); AL(h.gcell, h.ngroups);
     AL(h.grid, h.G); AL(h.lj, lj.size()); AL(h.moves, h.mcsteps); AL(h.frag, h.ntypes);
     AL(h.totalNum, h.ntypes); AL(h.desc, 1); AL(h.pcen, kMaxPoses); AL(h.pslot, kMaxPoses);
     AL(h.epart, (size_t)kMaxPoses * 2 * h.nslab); AL(h.nbr, (size_t)kMaxPoses * kMaxWords);
     AL(h.counters, 16); AL(h.err, 1);
+    AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
+    AL(h.fbcnt, kMaxPoses);
     h.log_cap = std::max(0, std::min(opt.log_steps, h.mcsteps));
     h.log_kmax = std::max(1, std::min(opt.log_kmax > 0 ? opt.log_kmax : 1, kMaxPoses));
     if (h.log_cap > 0) {
         AL(h.log, h.log_cap);
         AL(h.logE, (size_t)h.log_cap * h.log_kmax);
+        if (d.fb) AL(h.logF, (size_t)h.log_cap * h.log_kmax * 12);
     }
 #undef AL
     cudaStream_t s = ctx->stream;
@@ -362,6 +385,10 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 16, s));
     CK(cudaMemsetAsync(h.err, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
+    CK(cudaMemsetAsync(h.energy, 0, sizeof(double), s));
+    CK(cudaMemsetAsync(h.fpart, 0, sizeof(float) * kMaxPoses * 2 * h.nslab * 6, s));
+    CK(cudaMemsetAsync(h.fbprop, 0, sizeof(float4) * kMaxPoses * 2, s));
+    CK(cudaMemsetAsync(h.fbcnt, 0, sizeof(int) * kMaxPoses, s));
 
     d.xyzq = h.xyzq; d.atype = h.atype; d.gcen = h.gcen; d.gspan = h.gspan;
     d.cell_count = h.cell_count; d.cell_ent = h.cell_ent; d.gcell = h.gcell;
@@ -369,6 +396,8 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.desc = h.desc; d.pcen = h.pcen; d.pslot = h.pslot; d.epart = h.epart; d.nbr = h.nbr;
     d.log = h.log; d.logE = h.logE; d.log_cap = h.log_cap; d.log_kmax = h.log_kmax;
     d.counters = h.counters; d.err = h.err;
+    d.energy = h.energy; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
+    d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
     return GCMC_OK;
 }
 
@@ -381,6 +410,9 @@ int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     if (ebps > 0) per_sm = std::min(per_sm, ebps);
     ctx->ebps = ebps;
     ctx->gridE = std::max(1, sms) * per_sm;
+    int per_sm_f = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_energy_fb, kWarpsG * 32, 0));
+    ctx->gridF = std::max(1, sms) * std::max(1, per_sm_f);
     return GCMC_OK;
 }
 
@@ -432,8 +464,14 @@ int build_graph(gcmc_ctx* ctx) {
             double part = 0.0;
             for (int r = r0; r < r0 + cnt; ++r) part += (double)ctx->reps[r].natoms + 1.0;
             const int grid = nb == 1 ? ctx->gridE : std::max(1, (int)std::ceil(ctx->gridE * part / tot));
+            const int gridf = nb == 1 ? ctx->gridF : std::max(1, (int)std::ceil(ctx->gridF * part / tot));
             for (int s = 0; s < kGraphSteps; ++s) {
-                k_energy<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
+                if (ctx->fb) {
+                    k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
+                    k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
+                } else {
+                    k_energy<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
+                }
                 k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt);
             }
             e = cudaGetLastError();
@@ -476,7 +514,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     *out = nullptr;
     gcmc_options opt;
     if (optp) opt = *optp; else gcmc_default_options(&opt);
-    if (opt.proposal < 0 || opt.proposal > 1) return GCMC_ERR_ARG;
+    if (opt.proposal < 0 || opt.proposal > 2) return GCMC_ERR_ARG;
     for (int r = 0; r < nrep; ++r) {
         int st = validate(ins[r]);
         if (st != GCMC_OK) return st;
@@ -513,6 +551,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
                                  (int)sizeof(AcceptSmem)) != cudaSuccess)
             st = GCMC_ERR_CUDA;
     }
+    ctx->fb = opt.proposal == 2 ? 1 : 0;
     if (st == GCMC_OK) st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
     if (st == GCMC_OK) {
         split_branches(ctx, opt.branches > 0 ? opt.branches : 1);
@@ -543,7 +582,7 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     if (ctx->nrep != nrep) return GCMC_ERR_ARG;
     gcmc_options opt;
     if (optp) opt = *optp; else gcmc_default_options(&opt);
-    if (opt.proposal < 0 || opt.proposal > 1) return GCMC_ERR_ARG;
+    if (opt.proposal < 0 || opt.proposal > 2) return GCMC_ERR_ARG;
     int st = GCMC_OK;
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = validate(ins[r]);
     if (st != GCMC_OK) return st;
@@ -555,7 +594,9 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
     CK(cudaGetLastError());
     const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
-    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps) {
+    const int fb = opt.proposal == 2 ? 1 : 0;
+    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb) {
+        ctx->fb = fb;
         st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
         if (st != GCMC_OK) return st;
         split_branches(ctx, nb);
@@ -686,6 +727,8 @@ void gcmc_default_options(gcmc_options* opt) {
     opt->split_items = 2048;
     opt->branches = 1;
     opt->energy_blocks_per_sm = 0;
+    opt->fb_trn = 0.5f;
+    opt->fb_rot = (float)(10.0 * M_PI / 180.0);
 }
 
 const char* gcmc_status_string(int status) {
@@ -837,7 +880,12 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int i = 0; i < need; ++i) {
         CK(cudaEventRecord(ev[3 * i], ctx->stream));
-        k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        if (ctx->fb) {
+            k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
+            k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
+        } else {
+            k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        }
         CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
         k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);
         CK(cudaEventRecord(ev[3 * i + 2], ctx->stream));
@@ -928,6 +976,24 @@ int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energ
     if (n <= 0) return GCMC_OK;
     if (logs) CK(cudaMemcpy(logs, h.log, sizeof(gcmc_step_log) * n, cudaMemcpyDeviceToHost));
     if (energies) CK(cudaMemcpy(energies, h.logE, sizeof(double) * (size_t)n * h.log_kmax, cudaMemcpyDeviceToHost));
+    return GCMC_OK;
+}
+
+int gcmc_get_forces(gcmc_ctx* ctx, int32_t rep, float* forces, int32_t max_steps, int32_t* n_steps) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !forces) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    RepHost& h = ctx->reps[rep];
+    const int n = std::min(std::min(max_steps, h.log_cap), h.host_end);
+    if (n_steps) *n_steps = std::max(0, n);
+    if (n <= 0 || !ctx->repdev[rep].logF) return GCMC_OK;
+    CK(cudaMemcpy(forces, h.logF, sizeof(float) * (size_t)n * h.log_kmax * 12, cudaMemcpyDeviceToHost));
+    return GCMC_OK;
+}
+
+int gcmc_energy_total(gcmc_ctx* ctx, int32_t rep, double* e_total) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || !e_total) return GCMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(e_total, ctx->reps[rep].energy, sizeof(double), cudaMemcpyDeviceToHost));
     return GCMC_OK;
 }
 

@@ -30,12 +30,14 @@ struct GradStage {
     float4 red[32];     // per-lane site sums for the end-of-item reduction
 };
 
-struct GradSink {
+template <bool WithE>
+struct GradSinkT {
     GradStage* st;
     float* gtab;   // block shared [ns][ffY][2] (nullptr: no table gradient)
     float w;       // dL/dE of the current pose
     int ffY;
     float gx = 0.f, gy = 0.f, gz = 0.f, gq = 0.f;
+    float e = 0.f;  // WithE: this lane's FP32 sum of its pair energies
 
     template <bool PairImage>
     __device__ __forceinline__ void flush_t(const RepDev& R, WarpBuf& B, int na, int ns, int lane) {
@@ -96,6 +98,7 @@ struct GradSink {
                     gy = fmaf(m2, dy, gy);
                     gz = fmaf(m2, dz, gz);
                     gq = fmaf(kCoulomb * a.w, ir, gq);
+                    if (WithE) e = fmaf(p.y, fmaf(s6, s6, -s6), e) + uel;
                     if (gtab) {
                         float* g = gtab + ((size_t)s * ffY + ta) * 2;
                         atomicAdd(g, w * (3.0f * p.y * s2 * s2 * ir2 * fmaf(2.0f, s6, -1.0f)));
@@ -111,6 +114,7 @@ struct GradSink {
         else flush_t<false>(R, B, na, ns, lane);
     }
 };
+using GradSink = GradSinkT<false>;
 
 // item = (pose, slab) as in k_energy_explicit; part[(item * ns + s)] =
 // (dE/dx, dE/dy, dE/dz, dE/dq) of site s from this slab's atoms.
@@ -172,6 +176,135 @@ __global__ void __launch_bounds__(kWarpsG * 32)
                 atomicAdd(&glj[(size_t)type[s] * R.ffY * 2 + rem], (double)v);
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pose energies with forces for force-biased translate/rotate steps.
+//
+// phase 1: items (pose i, slab) of the OLD poses: energy partial (variant 1)
+//          and force/torque partials; the last item of a pose to finish (a
+//          per-pose counter after a fence) sums them in slab order and draws
+//          the pose's proposal (new centre, d, z).
+// phase 2: the step's ordinary items, except that a force-biased step's items
+//          are (pose i, slab) of the NEW poses (variant 0) with forces.
+// Non-force-biased steps have no phase-1 items and run the energy path.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __restrict__ reps, int nrep, int phase) {
+    __shared__ WarpBuf bufs[kWarpsG];
+    __shared__ GradStage stages[kWarpsG];
+    __shared__ int pre[257];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int r = 0; r < nrep; ++r) {
+            pre[r] = acc;
+            const StepDesc* d = reps[r].desc;
+            acc += phase == 1 ? d->items_pre : d->items;
+        }
+        pre[nrep] = acc;
+    }
+    __syncthreads();
+    const int total = pre[nrep];
+    WarpBuf& B = bufs[warp];
+    for (int it = blockIdx.x * kWarpsG + warp; it < total; it += gridDim.x * kWarpsG) {
+        int lo = 0, hi = nrep;
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
+        const RepDev& R = reps[lo];
+        const StepDesc D = *R.desc;
+        const int local = it - pre[lo];
+        const bool fbitem = phase == 1 || D.fb;
+        const int per_pose = fbitem ? D.nslab : D.nvar * D.nslab;
+        const int i = local / per_pose;
+        const int rem = local - i * per_pose;
+        const int v = fbitem ? (phase == 1 ? 1 : 0) : rem / D.nslab;
+        const int zi = fbitem ? rem : rem - v * D.nslab;
+        float cx, cy, cz;
+        int self;
+        build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
+        const int ns = R.frag[D.ftype].nsites;
+        const int nwin = R.span[0] * R.span[1] * R.span[2];
+        const int c0 = zi * nwin / D.nslab, c1 = (zi + 1) * nwin / D.nslab;
+        int ng = 0;
+        long long npair = 0;
+        double acc = 0.0;
+        if (!fbitem) {
+            EnergySink sink;
+            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair);
+            acc = warp_sum(sink.acc);
+        } else {
+            GradSinkT<true> sink;
+            sink.st = &stages[warp];
+            sink.gtab = nullptr;
+            sink.w = 1.0f;
+            sink.ffY = R.ffY;
+            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair);
+            acc = warp_sum((double)sink.e);
+            // per-site gradient (lanes < ns after summing the atom subsets), then
+            // force -sum g_s and torque -sum (x_s - m) x g_s about the site centroid
+            stages[warp].red[lane] = make_float4(sink.gx, sink.gy, sink.gz, 0.0f);
+            __syncwarp();
+            float g0 = 0.f, g1 = 0.f, g2 = 0.f, r0 = 0.f, r1 = 0.f, r2 = 0.f;
+            if (lane < ns) {
+                const int nsub = 32 / ns;
+                float4 gsum = stages[warp].red[lane];
+                for (int k = 1; k < nsub; ++k) {
+                    const float4 t = stages[warp].red[k * ns + lane];
+                    gsum.x += t.x; gsum.y += t.y; gsum.z += t.z;
+                }
+                g0 = gsum.x; g1 = gsum.y; g2 = gsum.z;
+                float mx = 0.f, my = 0.f, mz = 0.f;
+                for (int s = 0; s < ns; ++s) { mx += B.site[s].x; my += B.site[s].y; mz += B.site[s].z; }
+                const float inv = 1.0f / (float)ns;
+                r0 = B.site[lane].x - mx * inv;
+                r1 = B.site[lane].y - my * inv;
+                r2 = B.site[lane].z - mz * inv;
+            }
+            float f[6] = {-g0, -g1, -g2, -(r1 * g2 - r2 * g1), -(r2 * g0 - r0 * g2), -(r0 * g1 - r1 * g0)};
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                for (int off = 16; off > 0; off >>= 1) f[c] += __shfl_xor_sync(kFull, f[c], off);
+            if (lane == 0) {
+                float* out = R.fpart + ((size_t)(i * 2 + v) * D.nslab + zi) * 6;
+                for (int c = 0; c < 6; ++c) out[c] = f[c];
+            }
+        }
+        if (lane == 0) {
+            R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
+            atomicAdd(&R.counters[2], (unsigned long long)npair);
+        }
+        if (phase == 1) {  // the last item of pose i draws its proposal
+            int last = 0;
+            if (lane == 0) {
+                __threadfence();
+                const int done = atomicAdd(&R.fbcnt[i], 1);
+                last = done == D.nslab - 1;
+                if (last) R.fbcnt[i] = 0;
+            }
+            last = __shfl_sync(kFull, last, 0);
+            if (last && lane == 0) {
+                __threadfence();
+                float fo[6];
+                fb_force(R, D, i, 1, fo, true);
+                const float4 gc = R.gcen[R.frag[D.ftype].startRes + R.pslot[i]];
+                R.pcen[i] = fb_propose(R, D, i, fo, gc, R.fbprop + 2 * i);
+            }
+        } else if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
+            const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
+            const float4 ci = R.pcen[i];
+            for (int w = w0; w < w1; ++w) {
+                const int j = 32 * w + lane;
+                bool b = false;
+                if (j < D.k) {
+                    const float4 cj = R.pcen[j];
+                    b = within_cutoff<true>(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                            R.cut2_hi, R.fast_incl);
+                }
+                const unsigned m = __ballot_sync(kFull, b);
+                if (lane == 0) R.nbr[i * D.nw + w] = m;
+            }
+        }
+        __syncwarp();
     }
 }
 

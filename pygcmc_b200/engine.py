@@ -95,6 +95,22 @@ class Engine:
         check(lib().gcmc_get_logs(self._h, rep, ptr(logs), ptr(E), n, ctypes.byref(got)), "gcmc_get_logs")
         return logs[: got.value], E[: got.value]
 
+    def forces(self, rep: int = 0):
+        """Force-biased runs with logs: [steps, log_kmax, 12] float32 -- old-pose
+        force and torque, then new-pose force and torque, of each pose."""
+        n = int(self.options.log_steps)
+        km = max(1, int(self.options.log_kmax))
+        out = np.zeros((n, km, 12), dtype=np.float32)
+        got = ctypes.c_int32(0)
+        check(lib().gcmc_get_forces(self._h, rep, ptr(out), n, ctypes.byref(got)), "gcmc_get_forces")
+        return out[: got.value]
+
+    def energy_total(self, rep: int = 0) -> float:
+        """Running sum of the accepted energy changes since creation (kJ/mol)."""
+        e = ctypes.c_double(0.0)
+        check(lib().gcmc_energy_total(self._h, rep, ctypes.byref(e)), "gcmc_energy_total")
+        return e.value
+
     def counters(self, rep: int = 0):
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         check(lib().gcmc_counters(self._h, rep, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "gcmc_counters")

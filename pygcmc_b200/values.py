@@ -70,11 +70,11 @@ Residue_dtype = np.dtype([
 StepLog_dtype = np.dtype([
     ("step", np.int32), ("move", np.int32), ("ftype", np.int32), ("k", np.int32),
     ("n_before", np.int32), ("n_after", np.int32), ("n_clusters", np.int32), ("n_accept", np.int32),
-    ("first_accept", np.int32), ("slot", np.int32), ("e_sum", np.float64),
+    ("first_accept", np.int32), ("slot", np.int32), ("e_sum", np.float64), ("e_total", np.float64),
 ])
 
 assert Atom_dtype.itemsize == 20
 assert AtomArray_dtype.itemsize == 436
 assert Info_dtype.itemsize == 76
 assert Residue_dtype.itemsize == 20
-assert StepLog_dtype.itemsize == 48
+assert StepLog_dtype.itemsize == 56

@@ -53,10 +53,13 @@ def check_trajectory(oracle, system, nsteps, proposal=0, muex_kcal=0):
     assert len(logs_g) == nsteps
     s_o = system.copy()
     opts = oracle.options(proposal=proposal, muex_kcal=muex_kcal)
-    logs_o, E_o, SC = oracle.run(s_o, nsteps, opts=opts, kmax=LOG_KMAX, replay=E_g, want_scale=True)
+    r = oracle.run_ext(s_o, nsteps, opts=opts, kmax=LOG_KMAX, replay=E_g)
+    logs_o, E_o, SC = r["logs"], r["energies"], r["scale"]
     for f in LOG_FIELDS:
         bad = np.flatnonzero(logs_g[f] != logs_o[f])
         assert bad.size == 0, (f, bad[:5], logs_g[bad[:3]], logs_o[bad[:3]])
+    # the running energy (FP64 sum of the accepted energy changes) is the same sum
+    assert np.array_equal(logs_g["e_total"], logs_o["e_total"])
     mask = np.arange(LOG_KMAX)[None, :] < logs_g["k"][:, None]
     ok = energy_close(E_g[mask], E_o[mask], SC[mask])
     assert ok.all(), (np.flatnonzero(~ok)[:10], E_g[mask][~ok][:5], E_o[mask][~ok][:5])
