@@ -422,6 +422,155 @@ class RefRunner:
         return float(np.median(t))
 
 
+FB_WORKLOAD = ("force-biased vs plain translate/rotate on the synthetic protein (6000-atom chain, 64 A box, "
+               "8 fragments at their initial counts, confBias 1000, cutoff 12 A), a translate/rotate-only "
+               "schedule (fixed N, equal move probabilities): plain = symmetric moves (translate in a cube of "
+               "half-width 0.5 A, rotate about a uniform axis by <= 10 deg); force-biased = each component of "
+               "the displacement / rotation vector in [-0.5 A, 0.5 A] / [-10 deg, 10 deg] with density "
+               "~exp(beta f d / 2) from the force / torque (Pangali-Rao-Berne), Metropolis-Hastings corrected")
+
+
+def time_engine(eng, stream, flush, chunk, warmup, steps):
+    """Warm-up chunks, then `steps` timed chunks (CUDA events on the engine's
+    stream, L2 flushed before each); returns the summed milliseconds."""
+    import torch
+    for _ in range(warmup):
+        eng.run(chunk)
+    eng.sync()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for a, b in evs:
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a.record(stream)
+        eng.run(chunk)
+        b.record(stream)
+    eng.sync()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def gradient_throughput(sysm, batches=10, nposes=4096):
+    """Forward + backward of the pose energy for `nposes` random rigid poses
+    (uniform centre, uniform quaternion) through the autograd wrapper: poses/s."""
+    import torch
+    from pygcmc_b200 import poses as PZ
+    from pygcmc_b200.engine import Engine
+    from pygcmc_b200.grad import RigidFragment, lj_table
+    dev = torch.device("cuda")
+    lt = sysm.meta["lj_types"]
+    ffx = int(sysm.SimInfo[0]["ffXNum"])
+    with Engine(sysm.copy()) as eng:
+        frag = RigidFragment(eng, 0, 0, dtype=torch.float32)
+        eps = torch.tensor(lt["eps_kcal"], device=dev, requires_grad=True)
+        rmin = torch.tensor(lt["rmin_half"], device=dev, requires_grad=True)
+        data = []
+        for b in range(batches + 3):
+            com, quat = PZ.random_poses(sysm, nposes, seed=100 + b)
+            data.append((torch.tensor(com, device=dev, dtype=torch.float32, requires_grad=True),
+                         torch.tensor(quat, device=dev, dtype=torch.float32, requires_grad=True)))
+
+        def one(c, q):
+            e = frag.energy(c, q, lj_table(eps, rmin, ffx))
+            torch.nan_to_num(e, posinf=0.0, neginf=0.0).sum().backward()
+
+        for c, q in data[:3]:
+            one(c, q)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for c, q in data[3:]:
+            one(c, q)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+    return {"poses_per_s": round(batches * nposes / (ms / 1e3), 1), "batch": nposes, "batches": batches,
+            "ms_per_batch": round(ms / batches, 3),
+            "gradients": "centre of mass (3), quaternion (4), per-type eps and rmin/2 (24 + 24), site charges"}
+
+
+def run_ours_forcebias(args, ws, rank, local):
+    import torch
+    from pygcmc_b200 import analysis as A
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    from pygcmc_b200.gpu import runGCMC
+    torch.cuda.set_device(local)
+    chunk = args.chunk
+    seed = args.seed + rank
+    total = (args.warmup + args.steps) * chunk + 256
+    sysm = make_system(seed, total)
+    # translate/rotate-only schedule: fixed N, so the comparison isolates the proposals
+    g = np.random.default_rng(seed + 17)
+    ntype = len(sysm.fragmentInfo)
+    sysm.moveArray = (g.integers(0, ntype, total) * 4 + 2 + g.integers(0, 2, total)).astype(np.int32)
+    init = sysm.fragmentInfo["totalNum"].astype(np.int64).copy()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    arms = {"plain": default_options(proposal=1, trn_step=1.0, rot_max=float(np.radians(10.0)), log_steps=total),
+            "force_biased": default_options(proposal=2, fb_trn=0.5, fb_rot=float(np.radians(10.0)),
+                                            log_steps=total)}
+    res, ms_fb, clk = {}, None, None
+    for name, opt in arms.items():
+        eng = Engine(sysm.copy(), opt)
+        stream = torch.cuda.ExternalStream(eng.stream)
+        barrier(ws)
+        clocks = ClockSampler(local) if name == "force_biased" else None
+        ms = max_over_ranks(time_engine(eng, stream, flush, chunk, args.warmup, args.steps), ws)
+        if clocks is not None:
+            clk = clocks.stop()
+        logs, _ = eng.logs()
+        rate = args.steps * chunk / (ms / 1e3)
+        summ = A.sampling_summary(logs[: (args.warmup + args.steps) * chunk], init, rate, burn=args.warmup * chunk)
+        summ["moves_per_s"] = round(rate, 1)
+        if name == "force_biased":
+            ms_fb = ms
+            te, ta, _ = eng.run_profiled(128)
+            summ["avg_energy_launches_us"] = float(te.mean() * 1e3)
+            summ["avg_accept_us"] = float(ta.mean() * 1e3)
+        eng.close()
+        res[name] = summ
+    # end to end: the runGCMC drop-in with force-biased options, host arrays per call
+    e2e_state = sysm.copy()
+    info = e2e_state.SimInfo
+    info[0]["mcsteps"] = chunk
+    h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * chunk
+    d2h = e2e_state.fragmentInfo.nbytes + e2e_state.residueInfo.nbytes + e2e_state.atomInfo.nbytes
+    fbopt = default_options(proposal=2, fb_trn=0.5, fb_rot=float(np.radians(10.0)))
+    times = []
+    for k in range(args.warmup + args.steps):
+        info[0]["seed"] = (seed * 7 + k) & 0xFFFFFFFF
+        mv = np.ascontiguousarray(sysm.moveArray[k * chunk:(k + 1) * chunk])
+        barrier(ws)
+        t0 = time.perf_counter()
+        runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
+                e2e_state.ff, mv, options=fbopt)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(times) * 1e3, ws) / 1e3
+    value = args.steps * chunk * ws / (ms_fb / 1e3)
+    fb, pl = res["force_biased"], res["plain"]
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_fb / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair terms, fp64 sums/acceptance",
+        "data": "synthetic (seeded generator; no public dataset)",
+        "config": {"workload": FB_WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
+                   "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks"},
+        "e2e": {"value": round(args.steps * chunk * ws / e2e_s, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
+                "api": "pygcmc_b200.gpu.runGCMC(..., options=proposal 2)"},
+        "forcebias": {"plain": pl, "force_biased": fb,
+                      "decorrelated_samples_per_s_ratio": round(fb["decorrelated_samples_per_s"]
+                                                                / max(pl["decorrelated_samples_per_s"], 1e-30), 3),
+                      "tau": "integrated autocorrelation time (steps) of the total fragment count N and the "
+                             "running energy E, Sokal window c=5, over the timed steps"},
+        "gradient": gradient_throughput(sysm),
+        "gpu_launches": args.steps * (2 + 3 * 32 * ((chunk + 31) // 32)),
+        "clocks": clk,
+    }
+    return out
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
@@ -505,8 +654,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["protein", "batched"], default="protein",
-                    help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU")
+    ap.add_argument("--workload", choices=["protein", "batched", "forcebias"], default="protein",
+                    help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU; "
+                         "forcebias: force-biased vs plain translate/rotate on the protein system")
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--chunk", type=int, default=0, help="MC steps per bench step (default 2048; batched 256)")
     ap.add_argument("--ref-chunk", type=int, default=0,
@@ -517,7 +667,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.chunk <= 0:
-        args.chunk = 256 if args.workload == "batched" else 2048
+        args.chunk = {"batched": 256, "forcebias": 8192}.get(args.workload, 2048)
     if args.ref_chunk <= 0:
         args.ref_chunk = 16 if args.workload == "batched" else args.chunk
     ws, rank, local = dist_env()
@@ -532,6 +682,8 @@ def main():
             out = run_reference(args, ws, rank, local)
         elif args.workload == "batched":
             out = run_ours_batched(args, ws, rank, local)
+        elif args.workload == "forcebias":
+            out = run_ours_forcebias(args, ws, rank, local)
         else:
             out = run_ours(args, ws, rank, local)
         if rank == 0 and out is not None:

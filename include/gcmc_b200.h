@@ -71,13 +71,13 @@ typedef struct {
                             insertion, translate in a cube of edge trn_step,
                             rotate about a uniform axis by up to rot_max;
                             2: force-biased (no counterpart in the reference) --
-                            uniform SO(3) insertion; translate by
-                            d = (sigma_t^2 beta / 2) F + sigma_t z and rotate by the
-                            rotation vector (sigma_r^2 beta / 2) tau + sigma_r z,
-                            z ~ N(0, I3), F / tau the force / torque about the site
-                            centroid at the old pose, accepted with the
-                            Metropolis-Hastings ratio of the two Gaussian
-                            proposal densities (forces at the old and new pose) */
+                            uniform SO(3) insertion; translate by d and rotate by
+                            the rotation vector v (about the site centroid) whose
+                            components lie in [-h, h] with density
+                            ~ exp(beta f_c x / 2), f the force / torque at the old
+                            pose (Pangali, Rao and Berne 1978), accepted with the
+                            Metropolis-Hastings ratio of the proposal densities
+                            (forces at the old and at the new pose)              */
     int32_t muex_kcal;   /* 0: beta*muex with beta in mol/kJ and muex as given
                             (gcmc_move_add.h:105); 1: muex in kcal/mol (x4.184)     */
     float trn_step;      /* symmetric translate cube edge, A                        */
@@ -94,8 +94,8 @@ typedef struct {
                             concurrently; 0 = 1                                     */
     int32_t energy_blocks_per_sm; /* pose-energy kernel CTAs per SM (0 = the
                             occupancy limit)                                        */
-    float fb_trn;        /* proposal 2: translate step sigma_t, A (0 = 0.5)          */
-    float fb_rot;        /* proposal 2: rotation step sigma_r, rad (0 = 10 degrees)  */
+    float fb_trn;        /* proposal 2: translate half-width h_t, A (0 = 0.5)        */
+    float fb_rot;        /* proposal 2: rotation half-width h_r, rad (0 = 10 degrees)*/
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */

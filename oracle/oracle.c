@@ -128,18 +128,46 @@ float or_det_log(float x) {
     return ef * 0.693145751953125f + (ef * 1.42860677e-06f + lnm);
 }
 
-void or_fb_normals(uint32_t seed, uint32_t replica, int32_t step, int32_t i, float z[4]) {
-    uint32_t r[4];
-    rng(seed, replica, (uint32_t)step, (uint32_t)i, RP_FB, 0, r);
-    const float ra = sqrtf(-2.0f * or_det_log(u01_oc(r[0])));
-    const float rb = sqrtf(-2.0f * or_det_log(u01_oc(r[2])));
-    float sa, ca, sb, cb;
-    or_det_sincos(u01_co(r[1]) * OR_TWO_PI_F, &sa, &ca);
-    or_det_sincos(u01_co(r[3]) * OR_TWO_PI_F, &sb, &cb);
-    z[0] = ra * ca;
-    z[1] = ra * sa;
-    z[2] = rb * cb;
-    z[3] = rb * sb;
+/* Own exponential for x <= 0 (engine: det_exp_neg). */
+float or_det_exp_neg(float x) {
+    if (!(x > -87.0f)) return 0.0f;
+    const float kf = floorf(x * 1.44269502f + 0.5f);
+    const float r = (x - kf * 0.693145751953125f) - kf * 1.42860677e-06f;
+    float p = r * 1.98412701e-04f + 1.38888892e-03f;
+    p = r * p + 8.33333377e-03f;
+    p = r * p + 4.16666679e-02f;
+    p = r * p + 0.166666672f;
+    p = r * p + 0.5f;
+    p = r * p + 1.0f;
+    p = r * p + 1.0f;
+    const int k = (int)kf;
+    const uint32_t sb = (uint32_t)(k + 127) << 23;
+    float sc;
+    memcpy(&sc, &sb, 4);
+    return p * sc;
+}
+
+/* Tilted-uniform draw on [-h, h] with density a e^{ax} / (2 sinh(ah)) (force
+ * bias of Pangali, Rao and Berne 1978; engine: fb_tilted). */
+static float fb_tilted(float a, float h, float u) {
+    const float ah = a * h;
+    if (fabsf(ah) < 1e-4f) return h * (2.0f * u - 1.0f);
+    if (a > 0.0f) {
+        const float t = or_det_exp_neg(-2.0f * ah);
+        return h + or_det_log(u + (1.0f - u) * t) / a;
+    }
+    const float t = or_det_exp_neg(2.0f * ah);
+    return -h + or_det_log((1.0f - u) + u * t) / a;
+}
+
+/* ln(a / (2 sinh(ah))) (engine: fb_lnorm). */
+static float fb_lnorm(float a, float h) {
+    const float b = fabsf(a * h);
+    if (b < 1e-2f) {
+        const float b2 = b * b;
+        return (-or_det_log(2.0f * h) - b2 / 6.0f) + (b2 * b2) / 180.0f;
+    }
+    return (or_det_log(fabsf(a)) - b) - or_det_log(1.0f - or_det_exp_neg(-2.0f * b));
 }
 
 /* Rodrigues matrix about axis a (normalised here) by angle with (sin, cos);
@@ -712,21 +740,21 @@ static inline float fb_shift(const or_info* info, float d, int axis, float c) {
     const float k = floorf(((c + d) - info->startxyz[axis]) * invL);
     return d - k * info->cryst[axis];
 }
-static void fb_params(const or_options* opt, int trn, float* c1, float* sg) {
-    const float st = opt->fb_trn > 0.0f ? opt->fb_trn : 0.5f;
-    const float sr = opt->fb_rot > 0.0f ? opt->fb_rot : (float)(10.0 * 3.14159265358979323846 / 180.0);
-    *sg = trn ? st : sr;
-    *c1 = (float)(0.5 * (double)*sg * (double)*sg * OR_BETA);
+static void fb_params(const or_options* opt, int trn, float* lb, float* h) {
+    const float ht = opt->fb_trn > 0.0f ? opt->fb_trn : 0.5f;
+    const float hr = opt->fb_rot > 0.0f ? opt->fb_rot : (float)(10.0 * 3.14159265358979323846 / 180.0);
+    *h = trn ? ht : hr;
+    *lb = (float)(0.5 * OR_BETA);
 }
-static double fb_ln_ratio(const float d[3], const float z[3], const float* g, float c1f, float sgf) {
-    const double c1 = c1f, sg = sgf;
-    double fwd = 0.0, rev = 0.0;
-    for (int a = 0; a < 3; ++a) {
-        fwd = fwd + (double)z[a] * (double)z[a];
-        const double e = (-(double)d[a] - c1 * (double)g[a]) / sg;
-        rev = rev + e * e;
+/* sum over components of g(a') - g(a) - (a' + a) d (engine: fb_ln_ratio) */
+static double fb_ln_ratio(const float d[3], const float ao[3], const float* gn, float lb, float h) {
+    double s2 = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        const float an = lb * gn[c];
+        const double t = ((double)fb_lnorm(an, h) - (double)fb_lnorm(ao[c], h)) - ((double)an + (double)ao[c]) * (double)d[c];
+        s2 = s2 + t;
     }
-    return -0.5 * (rev - fwd);
+    return s2;
 }
 
 static double beta_muex(const or_options* opt, const or_atomarray* F) {
@@ -847,15 +875,15 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         if (k == 0) goto done;
         if (Eout && k > kmax) return -3;
         const int trn = (m == 2);
-        float c1, sg;
-        fb_params(S->opt, trn, &c1, &sg);
+        float lb, hh;
+        fb_params(S->opt, trn, &lb, &hh);
         const size_t nff = (size_t)2 * info->ffXNum * info->ffYNum;
         double* ff64 = malloc(sizeof(double) * nff);
         for (size_t j = 0; j < nff; ++j) ff64[j] = S->ff[j];
         float (*xyz)[20][3] = malloc(sizeof(float) * 60 * (size_t)k);
         float (*cen)[3] = malloc(sizeof(float) * 3 * (size_t)k);
         float (*pd)[3] = malloc(sizeof(float) * 3 * (size_t)k);
-        float (*pz)[3] = malloc(sizeof(float) * 3 * (size_t)k);
+        float (*pa)[3] = malloc(sizeof(float) * 3 * (size_t)k);
         float (*fnu)[6] = malloc(sizeof(float) * 6 * (size_t)k);
         int* okv = malloc(sizeof(int) * (size_t)k);
         int* slots = malloc(sizeof(int) * (size_t)k);
@@ -878,14 +906,14 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
             float fo[6];
             for (int c = 0; c < 6; ++c)
                 fo[c] = S->replay_forces ? S->replay_forces[(size_t)i * 12 + c] : (float)fo64[c];
-            float z[4];
-            or_fb_normals(info->seed, S->opt->replica, step, i, z);
+            uint32_t ru[4];
+            rng(info->seed, S->opt->replica, (uint32_t)step, (uint32_t)i, RP_FB, 0, ru);
             const float* g = trn ? fo : fo + 3;
             const int ok = isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]);
             okv[i] = ok;
             for (int a = 0; a < 3; ++a) {
-                pd[i][a] = (ok ? c1 * g[a] : 0.0f) + sg * z[a];
-                pz[i][a] = z[a];
+                pa[i][a] = ok ? lb * g[a] : 0.0f;
+                pd[i][a] = fb_tilted(pa[i][a], hh, u01_co(ru[a]));
             }
             if (trn) {
                 for (int j = 0; j < 3; ++j) {
@@ -945,7 +973,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         for (int i = 0; i < k; ++i) {
             const float* gn = trn ? fnu[i] : fnu[i] + 3;
             Eeff[i] = (!okv[i] || !isfinite(Ed[i])) ? INFINITY
-                                                    : Ed[i] - fb_ln_ratio(pd[i], pz[i], gn, c1, sg) / OR_BETA;
+                                                    : Ed[i] - fb_ln_ratio(pd[i], pa[i], gn, lb, hh) / OR_BETA;
         }
         cluster_par P = {1, 0.0, 0.0, NULL, 0};
         int* acc = malloc(sizeof(int) * (size_t)k);
@@ -961,7 +989,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
             if (S->e_total) *S->e_total += Ed[i];
         }
         if (L) { L->n_clusters = nc; L->n_accept = na; L->first_accept = fa; L->e_sum = esum; }
-        free(acc); free(ins); free(xyz); free(cen); free(pd); free(pz); free(fnu); free(okv); free(slots);
+        free(acc); free(ins); free(xyz); free(cen); free(pd); free(pa); free(fnu); free(okv); free(slots);
         free(dE); free(sc); free(Eeff); free(ff64);
     } else {
         int n = F->totalNum;

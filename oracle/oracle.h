@@ -153,10 +153,9 @@ int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_
                    const double* replay_energies, int32_t kmax, int32_t threads, double* e_total,
                    double* forces, double* fscale, const float* replay_forces);
 
-/* Own float log and the four Box-Muller normals of a force-biased proposal
- * (identical to the engine's). */
+/* Own float log and exp(x <= 0), identical to the engine's (force-biased proposals). */
 float or_det_log(float x);
-void or_fb_normals(uint32_t seed, uint32_t replica, int32_t step, int32_t i, float z[4]);
+float or_det_exp_neg(float x);
 
 /* Energies of many explicit poses (OpenMP over poses): poses_xyz[p*nsites*3],
  * centres[p*3], self[p]; returns pair count. */

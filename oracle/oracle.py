@@ -39,7 +39,8 @@ def lib():
                                                 ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void]
         L.or_det_log.restype = ctypes.c_float
         L.or_det_log.argtypes = [ctypes.c_float]
-        L.or_fb_normals.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, c_void]
+        L.or_det_exp_neg.restype = ctypes.c_float
+        L.or_det_exp_neg.argtypes = [ctypes.c_float]
         L.or_run.restype = ctypes.c_int32
         L.or_run.argtypes = [c_void] * 8 + [ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void,
                                             ctypes.c_int32, ctypes.c_int32]
@@ -102,11 +103,6 @@ def run_ext(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=
     out["e_total"] = et.value
     return out
 
-
-def fb_normals(seed, replica, step, i):
-    z = np.zeros(4, np.float32)
-    lib().or_fb_normals(seed, replica, step, i, _p(z))
-    return z
 
 
 def run(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, want_energies=True,

@@ -251,9 +251,9 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             float fo[6], fn[6];
             fb_force(R, D, i, 1, fo, false);
             fb_force(R, D, i, 0, fn, false);
-            const float4 d = R.fbprop[2 * i], z = R.fbprop[2 * i + 1];
+            const float4 d = R.fbprop[2 * i], ao = R.fbprop[2 * i + 1];
             double eff = INFINITY;
-            if (d.w == 0.0f && isfinite(e)) eff = __dsub_rn(e, __ddiv_rn(fb_ln_ratio(R, D, d, z, fn), kBeta));
+            if (d.w == 0.0f && isfinite(e)) eff = __dsub_rn(e, __ddiv_rn(fb_ln_ratio(R, D, d, ao, fn), kBeta));
             S.E[i] = eff;
             if (logging && R.logF && i < R.log_kmax) {
                 float* o = R.logF + ((size_t)D.step * R.log_kmax + i) * 12;

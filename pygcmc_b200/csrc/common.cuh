@@ -24,6 +24,8 @@ constexpr int kMaxWords = kMaxPoses / 32;
 
 // RNG purposes: high half of the third counter word.
 enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6, RP_FB = 7 };
+// force-bias tilt lambda (Pangali, Rao and Berne): density ~ exp(lambda beta f . d) in the step cube
+constexpr float kFbLambda = 0.5f;
 enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
 enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8 };
 
@@ -240,19 +242,50 @@ __device__ __forceinline__ float det_log(float x) {
     return fadd(fmul(ef, 0.693145751953125f), fadd(fmul(ef, 1.42860677e-06f), lnm));
 }
 
-// Four standard normal draws (Box-Muller on one Philox block) for the
-// force-biased proposal of pose i of a step.
-__device__ __forceinline__ void fb_normals(uint32_t seed, uint32_t replica, int step, int i, float z[4]) {
-    const U4 r = rng(seed, replica, (uint32_t)step, (uint32_t)i, RP_FB, 0);
-    const float ra = fsqrt(fmul(-2.0f, det_log(u01_oc(r.x))));
-    const float rb = fsqrt(fmul(-2.0f, det_log(u01_oc(r.z))));
-    float sa, ca, sb, cb;
-    det_sincos(fmul(u01_co(r.y), kTwoPiF), sa, ca);
-    det_sincos(fmul(u01_co(r.w), kTwoPiF), sb, cb);
-    z[0] = fmul(ra, ca);
-    z[1] = fmul(ra, sa);
-    z[2] = fmul(rb, cb);
-    z[3] = fmul(rb, sb);
+// Own exponential for x <= 0 (0 below -87), identical on the host oracle:
+// x = k ln2 + r with |r| <= ln2 / 2 (Cody-Waite split of ln2), e^r by its
+// Taylor polynomial to r^7 (truncation < 3e-9 relative), times 2^k.
+__device__ __forceinline__ float det_exp_neg(float x) {
+    if (!(x > -87.0f)) return 0.0f;
+    const float kf = floorf(fadd(fmul(x, 1.44269502f), 0.5f));
+    const float r = fsub(fsub(x, fmul(kf, 0.693145751953125f)), fmul(kf, 1.42860677e-06f));
+    float p = fadd(fmul(r, 1.98412701e-04f), 1.38888892e-03f);  // 1/5040, 1/720
+    p = fadd(fmul(r, p), 8.33333377e-03f);                      // 1/120
+    p = fadd(fmul(r, p), 4.16666679e-02f);                      // 1/24
+    p = fadd(fmul(r, p), 0.166666672f);                         // 1/6
+    p = fadd(fmul(r, p), 0.5f);
+    p = fadd(fmul(r, p), 1.0f);
+    p = fadd(fmul(r, p), 1.0f);
+    const int k = (int)kf;  // in [-126, 0]
+    return fmul(p, __int_as_float((k + 127) << 23));
+}
+
+// One tilted-uniform draw on [-h, h] with density a e^{a x} / (2 sinh(a h))
+// (the force-bias proposal of Pangali, Rao and Berne, Chem. Phys. Lett. 55
+// (1978) 413, per axis with a = lambda beta f), by inverting its CDF in the
+// overflow-free forms  x = h + ln(u + (1 - u) e^{-2ah}) / a  (a > 0) and
+// x = -h + ln(1 - u + u e^{2ah}) / a  (a < 0); uniform when |a| h < 1e-4.
+__device__ __forceinline__ float fb_tilted(float a, float h, float u) {
+    const float ah = fmul(a, h);
+    if (fabsf(ah) < 1e-4f) return fmul(h, fsub(fmul(2.0f, u), 1.0f));
+    if (a > 0.0f) {
+        const float t = det_exp_neg(fmul(-2.0f, ah));
+        return fadd(h, fdiv(det_log(fadd(u, fmul(fsub(1.0f, u), t))), a));
+    }
+    const float t = det_exp_neg(fmul(2.0f, ah));
+    return fadd(-h, fdiv(det_log(fadd(fsub(1.0f, u), fmul(u, t))), a));
+}
+
+// ln of the tilted-uniform normaliser a / (2 sinh(a h)) (even in a):
+// -ln(2h) - (ah)^2/6 + (ah)^4/180 for |a| h < 1e-2, else
+// ln|a| - |a| h - ln(1 - e^{-2|a| h}).
+__device__ __forceinline__ float fb_lnorm(float a, float h) {
+    const float b = fabsf(fmul(a, h));
+    if (b < 1e-2f) {
+        const float b2 = fmul(b, b);
+        return fadd(fsub(-det_log(fmul(2.0f, h)), fdiv(b2, 6.0f)), fdiv(fmul(b2, b2), 180.0f));
+    }
+    return fsub(fsub(det_log(fabsf(a)), b), det_log(fsub(1.0f, det_exp_neg(fmul(-2.0f, b)))));
 }
 
 
@@ -332,11 +365,12 @@ struct RepDev {
     uint32_t seed, replica;
     int run_end;        // steps below this index are executed
     int log_cap, log_kmax;
-    // force-biased translate/rotate (proposal 2): displacement d = c1 f + sigma z,
-    // z ~ N(0, I3), f the force (translate) or torque (rotate) at the old pose
+    // force-biased translate/rotate (proposal 2): each component of the
+    // displacement (rotation vector) lies in [-h, h] with density ~ exp(a d),
+    // a = lambda beta f, f the force (torque) at the old pose
     int fb;
-    float fb_c1t, fb_sig_t;  // translate: sigma_t^2 beta / 2 [A^2 mol/kJ], sigma_t [A]
-    float fb_c1r, fb_sig_r;  // rotate: sigma_r^2 beta / 2 [mol/kJ], sigma_r [rad]
+    float fb_at, fb_ht;  // translate: lambda beta [mol/kJ], half-width h_t [A]
+    float fb_ar, fb_hr;  // rotate: lambda beta [mol/kJ], half-width h_r [rad]
     // state
     float4* xyzq;       // atom x, y, z, charge
     int* atype;         // atom type (column of the LJ table)
@@ -364,7 +398,7 @@ struct RepDev {
     double* energy;     // running sum of the accepted moves' energy changes (FP64)
     // force-biased moves
     float* fpart;       // [kMaxPoses * 2 * nslab_max * 6] per-item force and torque partials
-    float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (z0, z1, z2, 0)
+    float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (a0, a1, a2, 0) of the old pose
     int* fbcnt;         // [kMaxPoses] old-pose items finished (reset by the last one)
     float* logF;        // [log_cap * log_kmax * 12] F_old, tau_old, F_new, tau_new used
 };

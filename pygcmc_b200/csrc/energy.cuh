@@ -353,12 +353,13 @@ __device__ __forceinline__ void moved_site(const RepDev& R, const StepDesc& D, i
 
 // ---- force-biased translate/rotate (proposal 2) ----
 //
-// Pose i's displacement is d = c1 f + sigma z with f the force (translate) or
-// the torque about the site centroid (rotate) at the old pose and z ~ N(0, I3)
-// (fb_normals).  A translate moves the sites by d wrapped so the new centre
-// lies in the box; a rotate turns them about their centroid by the rotation
-// vector v = d.  The proposal density ratio q(new -> old) / q(old -> new) enters
-// the acceptance (fb_ln_ratio).  All float steps are explicit round-to-nearest
+// Pose i's displacement d (translate) or rotation vector v (rotate, about the
+// site centroid) has independent components on [-h, h] with densities
+// a e^{a x} / (2 sinh(a h)), a = lambda beta f from the force (torque) f at the
+// old pose (fb_tilted).  A translate moves the sites by d wrapped so the new
+// centre lies in the box.  The reverse move is -d from the new pose with its
+// own force, and the ratio of the two proposal densities enters the
+// acceptance (fb_ln_ratio).  All float steps are explicit round-to-nearest
 // operations so the host oracle reproduces them bit for bit.
 
 // Force and torque partials of pose i, variant v, summed over the slabs in
@@ -382,19 +383,22 @@ __device__ __forceinline__ float fb_shift(const RepDev& R, float d, int axis, fl
 }
 
 // Proposal of pose i from its old-pose force/torque f and group centre gc:
-// prop[0] = (d, invalid), prop[1] = (z, 0); returns the new centre.
+// prop[0] = (d, invalid), prop[1] = (a, 0); returns the new centre.
 __device__ __forceinline__ float4 fb_propose(const RepDev& R, const StepDesc& D, int i, const float f[6],
                                              float4 gc, float4* prop) {
-    float z[4];
-    fb_normals(R.seed, R.replica, D.step, i, z);
+    const U4 r = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_FB, 0);
+    const float u[3] = {u01_co(r.x), u01_co(r.y), u01_co(r.z)};
     const bool trn = D.move == MV_TRANSLATE;
     const float* g = trn ? f : f + 3;
     const bool ok = isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]);
-    const float c1 = trn ? R.fb_c1t : R.fb_c1r, sg = trn ? R.fb_sig_t : R.fb_sig_r;
-    float d[3];
-    for (int a = 0; a < 3; ++a) d[a] = fadd(ok ? fmul(c1, g[a]) : 0.0f, fmul(sg, z[a]));
+    const float lb = trn ? R.fb_at : R.fb_ar, h = trn ? R.fb_ht : R.fb_hr;
+    float d[3], a[3];
+    for (int c = 0; c < 3; ++c) {
+        a[c] = ok ? fmul(lb, g[c]) : 0.0f;
+        d[c] = fb_tilted(a[c], h, u[c]);
+    }
     prop[0] = make_float4(d[0], d[1], d[2], ok ? 0.0f : 1.0f);
-    prop[1] = make_float4(z[0], z[1], z[2], 0.0f);
+    prop[1] = make_float4(a[0], a[1], a[2], 0.0f);
     if (!trn) return gc;
     return make_float4(fadd(gc.x, fb_shift(R, d[0], 0, gc.x)), fadd(gc.y, fb_shift(R, d[1], 1, gc.y)),
                        fadd(gc.z, fb_shift(R, d[2], 2, gc.z)), 0.0f);
@@ -433,25 +437,24 @@ __device__ __forceinline__ void fb_moved_site(const RepDev& R, const StepDesc& D
     pz = fadd(z, mz);
 }
 
-// ln q(new -> old) - ln q(old -> new) for pose i: the reverse displacement is
-// -d from the new pose with its force/torque fn; q is the N(c1 f, sigma^2 I3)
-// density of the displacement (the rotation-vector Jacobian is even in v and
-// cancels).  FP64 with explicit rounding.
-__device__ __forceinline__ double fb_ln_ratio(const RepDev& R, const StepDesc& D, const float4& d, const float4& z,
+// ln q(new -> old) - ln q(old -> new) for pose i: per component
+// g(a') - g(a) - (a' + a) d with g = fb_lnorm, a (stored) the old tilt and
+// a' = lambda beta f' from the new pose's force/torque fn; the rotation-vector
+// Jacobian is even in v and cancels.  Float terms, FP64 sum.
+__device__ __forceinline__ double fb_ln_ratio(const RepDev& R, const StepDesc& D, const float4& d, const float4& a,
                                               const float fn[6]) {
     const bool trn = D.move == MV_TRANSLATE;
     const float* g = trn ? fn : fn + 3;
-    const double c1 = trn ? (double)R.fb_c1t : (double)R.fb_c1r;
-    const double sg = trn ? (double)R.fb_sig_t : (double)R.fb_sig_r;
-    const double dd[3] = {(double)d.x, (double)d.y, (double)d.z};
-    const double zz[3] = {(double)z.x, (double)z.y, (double)z.z};
-    double fwd = 0.0, rev = 0.0;
-    for (int a = 0; a < 3; ++a) {
-        fwd = __dadd_rn(fwd, __dmul_rn(zz[a], zz[a]));
-        const double e = __ddiv_rn(__dsub_rn(-dd[a], __dmul_rn(c1, (double)g[a])), sg);
-        rev = __dadd_rn(rev, __dmul_rn(e, e));
+    const float lb = trn ? R.fb_at : R.fb_ar, h = trn ? R.fb_ht : R.fb_hr;
+    const float dd[3] = {d.x, d.y, d.z}, ao[3] = {a.x, a.y, a.z};
+    double s = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        const float an = fmul(lb, g[c]);
+        const double t = __dsub_rn(__dsub_rn((double)fb_lnorm(an, h), (double)fb_lnorm(ao[c], h)),
+                                   __dmul_rn(__dadd_rn((double)an, (double)ao[c]), (double)dd[c]));
+        s = __dadd_rn(s, t);
     }
-    return __dmul_rn(-0.5, __dsub_rn(rev, fwd));
+    return s;
 }
 
 // Load the pose of item (i, variant v) of step D into B.site; returns the

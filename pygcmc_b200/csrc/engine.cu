@@ -229,13 +229,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.rot_max = opt.rot_max;
     d.proposal = opt.proposal;
     d.fb = opt.proposal == 2 ? 1 : 0;
-    {
-        const double st = opt.fb_trn > 0.0f ? opt.fb_trn : 0.5, sr = opt.fb_rot > 0.0f ? opt.fb_rot : 10.0 * M_PI / 180.0;
-        d.fb_sig_t = (float)st;
-        d.fb_c1t = (float)(0.5 * (double)d.fb_sig_t * (double)d.fb_sig_t * kBeta);
-        d.fb_sig_r = (float)sr;
-        d.fb_c1r = (float)(0.5 * (double)d.fb_sig_r * (double)d.fb_sig_r * kBeta);
-    }
+    d.fb_ht = opt.fb_trn > 0.0f ? opt.fb_trn : 0.5f;
+    d.fb_hr = opt.fb_rot > 0.0f ? opt.fb_rot : (float)(10.0 * M_PI / 180.0);
+    d.fb_at = d.fb_ar = (float)((double)kFbLambda * kBeta);
     d.lncav = std::log((double)I->cavityFactor);
     d.nfixed = in.fragmentInfo[0].startRes;
     d.ntypes = I->fragTypeNum;

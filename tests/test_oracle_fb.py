@@ -1,5 +1,5 @@
-"""Host-side pieces of the force-biased proposal (no GPU): the own logarithm,
-the Box-Muller normals and a force-biased oracle run."""
+"""Host-side pieces of the force-biased proposal (no GPU): the own logarithm
+and exponential, and a force-biased oracle run."""
 import numpy as np
 
 
@@ -12,10 +12,13 @@ def test_det_log_accuracy(oracle_lib):
     assert np.all(np.abs(got - ref) <= 4e-7 * np.maximum(np.abs(ref), 1.0))
 
 
-def test_fb_normals_are_standard_normal(oracle_lib):
-    z = np.stack([oracle_lib.fb_normals(7, 0, s, i) for s in range(40) for i in range(100)]).ravel()
-    assert abs(z.mean()) < 0.05 and abs(z.std() - 1.0) < 0.03
-    assert abs((z ** 4).mean() - 3.0) < 0.3
+def test_det_exp_accuracy(oracle_lib):
+    L = oracle_lib.lib()
+    xs = np.concatenate([np.linspace(-86.9, 0.0, 4001, dtype=np.float32), np.float32([-1e-6, -0.3466, -0.3467])])
+    got = np.array([L.or_det_exp_neg(float(x)) for x in xs], dtype=np.float64)
+    ref = np.exp(xs.astype(np.float64))
+    assert np.all(np.abs(got - ref) <= 4e-7 * ref)
+    assert L.or_det_exp_neg(-90.0) == 0.0
 
 
 def test_force_biased_oracle_run(oracle_lib, protein_small):
