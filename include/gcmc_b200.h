@@ -283,6 +283,34 @@ int gcmc_synth_chain_sphere(int n, const float centre[3], float radius, float st
 int gcmc_synth_chain_slab(int n, float lo0, float hi0, float lo1, float hi1, float zc, float half,
                           float px, float py, float pore, float step, float excl, uint64_t seed,
                           float* out_xyz, int* n_breaks);
+/* ---- host-side system assembly (the reference's input builders, C++) ---- */
+/* get_grid (gcmc/python/dataset.py:21-139): box origin start[3] (centre of the
+ * atoms' bounding box minus cryst/2), the lower corners of the empty voxels of
+ * edge grid_dx in lexicographic (x, y, z) order (all voxels of a 1 A grid
+ * without cavity bias) and the cavity factor.  pts == NULL: count only
+ * (*npts); else pts[3 * cap].  GCMC_ERR_ARG when the factor is below 0.05,
+ * where the reference exits (dataset.py:95-97). */
+int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                     double* start, float* pts, int64_t cap, int64_t* npts, double* factor);
+/* set_fixCut (gcmc/python/dataset.py:175-188): group id per atom (a new group
+ * starts more than fix_cutoff from the current group's first atom); returns the
+ * number of groups. */
+int32_t gcmc_fix_groups(int32_t n, const double* xyz, double fix_cutoff, int32_t* group);
+/* Unweighted centres of groups [starts[g], starts[g] + counts[g]) with the
+ * reference's arithmetic (float32 running sums of float64 additions). */
+int gcmc_group_centres(int32_t ngroups, const double* xyz, const int64_t* starts, const int32_t* counts,
+                       float* out);
+/* update_data's residue and atom arrays (gcmc/python/dataset.py:190-373): fixed
+ * atoms grouped by fixed_group (contiguous runs), then per fragment type
+ * max_num slots of num_atoms atoms, the first n_initial holding the given
+ * copies (initial_xyz, concatenated by type) with the type's template charges
+ * and types (tpl_q / tpl_type concatenated by type); start_res[f] out. */
+int gcmc_fill_layout(int32_t nfix, const double* fixed_xyz, const double* fixed_q, const int32_t* fixed_type,
+                     const int32_t* fixed_group, int32_t nfrag, const int32_t* max_num, const int32_t* num_atoms,
+                     const float* tpl_q, const int32_t* tpl_type, const int32_t* n_initial,
+                     const double* initial_xyz, int32_t total_res, int64_t total_atoms, residue* res, Atom* atoms,
+                     int32_t* start_res);
+
 /* count random non-clashing copies (sites >= min_dist from all atoms) of a rigid
  * template in the periodic box [lo, lo+L); out_xyz[count*nsites*3]. */
 int gcmc_synth_place(int n_existing, const float* existing_xyz, const float lo[3], const float L[3],

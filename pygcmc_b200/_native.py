@@ -62,6 +62,12 @@ def lib():
         "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
         "gcmc_last_status": (c_int, []),
         "gcmc_release_cache": (c_int, []),
+        "gcmc_cavity_grid": (c_int, [c_int, c_void, c_void, ctypes.c_double, c_int, c_void, c_void, ctypes.c_int64,
+                                     P(ctypes.c_int64), P(ctypes.c_double)]),
+        "gcmc_fix_groups": (ctypes.c_int32, [c_int, c_void, ctypes.c_double, c_void]),
+        "gcmc_group_centres": (c_int, [c_int, c_void, c_void, c_void, c_void]),
+        "gcmc_fill_layout": (c_int, [c_int, c_void, c_void, c_void, c_void, c_int, c_void, c_void, c_void, c_void,
+                                     c_void, c_void, c_int, ctypes.c_int64, c_void, c_void, c_void]),
         "gcmc_get_forces": (c_int, [c_void, c_int, c_void, c_int, P(c_int)]),
         "gcmc_energy_total": (c_int, [c_void, c_int, P(ctypes.c_double)]),
         "gcmc_energy_grad": (c_int, [c_void, c_int] + [c_void] * 4 + [c_int, c_void, c_void, c_int] + [c_void] * 7),
@@ -86,7 +92,7 @@ def lib():
                                               c_int, c_void, c_void, c_void]),
         "gcmc_synth_chain_sphere": (c_int, [c_int, c_void, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_uint64, c_void, P(ctypes.c_int)]),
-        "gcmc_synth_chain_slab": (c_int, [c_int] + [ctypes.c_float] * 12 + [ctypes.c_uint64, c_void,
+        "gcmc_synth_chain_slab": (c_int, [c_int] + [ctypes.c_float] * 11 + [ctypes.c_uint64, c_void,
                                                                            P(ctypes.c_int)]),
         "gcmc_synth_place": (c_int, [c_int, c_void, c_void, c_void, c_void, c_int, c_int, ctypes.c_float,
                                      ctypes.c_uint64, c_void]),
@@ -124,6 +130,7 @@ def default_options(**kw):
 
 
 EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_get_forces",
+           "gcmc_cavity_grid", "gcmc_fix_groups", "gcmc_group_centres", "gcmc_fill_layout",
            "gcmc_energy_total", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",

@@ -1,0 +1,165 @@
+// Host-side system assembly: the reference's input builders in C++.
+//
+//   gcmc_cavity_grid   -- GCMCDataset.get_grid   (gcmc/python/dataset.py:21-139)
+//   gcmc_fix_groups    -- GCMCDataset.set_fixCut (gcmc/python/dataset.py:175-188)
+//   gcmc_group_centres -- the residue centres of update_data (gcmc/python/dataset.py:248-300)
+//   gcmc_fill_layout   -- update_data's residue / atom arrays (gcmc/python/dataset.py:190-373)
+//
+// The arithmetic follows the reference's Python/numpy (under its numpy<2
+// dependency) so that the outputs are identical: float64 geometry, centres as
+// float32 running sums of float64 additions divided in float64, voxel indices
+// by truncation and Python's non-negative modulo.  Differences are deliberate
+// and few: empty voxels come out in lexicographic (x, y, z) order instead of
+// Python set order, and unused slots are zero-filled.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gcmc_b200.h"
+
+namespace {
+
+inline int64_t pymod(int64_t a, int64_t n) {
+    const int64_t r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// float32 running sum of float64 additions, then a float64 division (numpy<2
+// semantics of `float32 += float64` followed by `/ n`).
+inline void centre_of(const double* xyz, int64_t start, int32_t count, float out[3]) {
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int32_t j = 0; j < count; ++j)
+        for (int c = 0; c < 3; ++c) acc[c] = (float)((double)acc[c] + xyz[(start + j) * 3 + c]);
+    const double n = count > 0 ? (double)count : 1.0;
+    for (int c = 0; c < 3; ++c) out[c] = (float)((double)acc[c] / n);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                     double* start, float* pts, int64_t cap, int64_t* npts, double* factor) {
+    if (n < 1 || !xyz || !cryst || !start || !npts || !factor) return GCMC_ERR_ARG;
+    double lo[3], hi[3];
+    for (int c = 0; c < 3; ++c) lo[c] = hi[c] = xyz[c];
+    for (int32_t a = 1; a < n; ++a)
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = std::fmin(lo[c], xyz[3 * a + c]);
+            hi[c] = std::fmax(hi[c], xyz[3 * a + c]);
+        }
+    double end[3];
+    int64_t nv[3];
+    const double dx = cavity_bias ? grid_dx : 1.0;
+    for (int c = 0; c < 3; ++c) {
+        const double centre = (lo[c] + hi[c]) / 2.0;
+        start[c] = centre - cryst[c] / 2.0;
+        end[c] = centre + cryst[c] / 2.0;
+        nv[c] = (int64_t)((end[c] - start[c]) / dx);
+        if (nv[c] < 1) return GCMC_ERR_ARG;
+    }
+    const int64_t total = nv[0] * nv[1] * nv[2];
+    std::vector<uint8_t> occ(cavity_bias ? (size_t)total : 0, 0);
+    if (cavity_bias)
+        for (int32_t a = 0; a < n; ++a) {
+            int64_t v[3];
+            for (int c = 0; c < 3; ++c) v[c] = pymod((int64_t)std::trunc((xyz[3 * a + c] - start[c]) / dx), nv[c]);
+            occ[(size_t)((v[0] * nv[1] + v[1]) * nv[2] + v[2])] = 1;
+        }
+    int64_t ne = 0;
+    for (int64_t i = 0; i < total; ++i) ne += cavity_bias ? !occ[(size_t)i] : 1;
+    *npts = ne;
+    *factor = cavity_bias ? (double)ne / (double)total : 1.0;
+    if (cavity_bias && *factor < 0.05) return GCMC_ERR_ARG;  // the reference exits here (dataset.py:95-97)
+    if (!pts) return GCMC_OK;
+    if (cap < ne) return GCMC_ERR_LIMIT;
+    int64_t k = 0;
+    for (int64_t x = 0; x < nv[0]; ++x)
+        for (int64_t y = 0; y < nv[1]; ++y)
+            for (int64_t z = 0; z < nv[2]; ++z) {
+                if (cavity_bias && occ[(size_t)((x * nv[1] + y) * nv[2] + z)]) continue;
+                pts[3 * k] = (float)((double)x * dx + start[0]);
+                pts[3 * k + 1] = (float)((double)y * dx + start[1]);
+                pts[3 * k + 2] = (float)((double)z * dx + start[2]);
+                ++k;
+            }
+    return GCMC_OK;
+}
+
+int32_t gcmc_fix_groups(int32_t n, const double* xyz, double fix_cutoff, int32_t* group) {
+    if (n < 0 || (n > 0 && (!xyz || !group))) return -1;
+    double x0 = INFINITY, y0 = INFINITY, z0 = INFINITY;
+    int32_t g = -1;
+    for (int32_t i = 0; i < n; ++i) {
+        const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        if (std::sqrt((x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0)) > fix_cutoff) {
+            ++g;
+            x0 = x; y0 = y; z0 = z;
+        }
+        group[i] = g;
+    }
+    return g + 1;
+}
+
+int gcmc_group_centres(int32_t ngroups, const double* xyz, const int64_t* starts, const int32_t* counts,
+                       float* out) {
+    if (ngroups < 0 || (ngroups > 0 && (!xyz || !starts || !counts || !out))) return GCMC_ERR_ARG;
+    for (int32_t g = 0; g < ngroups; ++g) centre_of(xyz, starts[g], counts[g], out + 3 * g);
+    return GCMC_OK;
+}
+
+int gcmc_fill_layout(int32_t nfix, const double* fixed_xyz, const double* fixed_q, const int32_t* fixed_type,
+                     const int32_t* fixed_group, int32_t nfrag, const int32_t* max_num, const int32_t* num_atoms,
+                     const float* tpl_q, const int32_t* tpl_type, const int32_t* n_initial,
+                     const double* initial_xyz, int32_t total_res, int64_t total_atoms, residue* res, Atom* atoms,
+                     int32_t* start_res) {
+    if (nfix < 0 || nfrag < 0 || !res || !atoms || !start_res) return GCMC_ERR_ARG;
+    std::memset(res, 0, sizeof(residue) * (size_t)total_res);
+    std::memset(atoms, 0, sizeof(Atom) * (size_t)total_atoms);
+    // fixed atoms and their groups (contiguous runs of equal group id)
+    int32_t seq = 0;
+    int64_t a = 0;
+    while (a < nfix) {
+        int64_t b = a;
+        while (b < nfix && fixed_group[b] == fixed_group[a]) ++b;
+        if (seq >= total_res) return GCMC_ERR_LIMIT;
+        res[seq].atomStart = (int32_t)a;
+        res[seq].atomNum = (int32_t)(b - a);
+        centre_of(fixed_xyz, a, (int32_t)(b - a), res[seq].position);
+        ++seq;
+        a = b;
+    }
+    if (nfix > total_atoms) return GCMC_ERR_LIMIT;
+    for (int64_t i = 0; i < nfix; ++i) {
+        for (int c = 0; c < 3; ++c) atoms[i].position[c] = (float)fixed_xyz[3 * i + c];
+        atoms[i].charge = (float)fixed_q[i];
+        atoms[i].type = fixed_type[i];
+    }
+    // fragment slots: maxNum per type, the first n_initial filled
+    int64_t next = nfix, tq = 0, ix = 0;
+    for (int32_t f = 0; f < nfrag; ++f) {
+        start_res[f] = seq;
+        const int32_t na = num_atoms[f];
+        for (int32_t j = 0; j < max_num[f]; ++j) {
+            if (seq >= total_res || next + na > total_atoms) return GCMC_ERR_LIMIT;
+            res[seq].atomNum = na;
+            res[seq].atomStart = (int32_t)next;
+            if (j < n_initial[f]) {
+                for (int32_t s = 0; s < na; ++s) {
+                    for (int c = 0; c < 3; ++c) atoms[next + s].position[c] = (float)initial_xyz[(ix + s) * 3 + c];
+                    atoms[next + s].charge = tpl_q[tq + s];
+                    atoms[next + s].type = tpl_type[tq + s];
+                }
+                centre_of(initial_xyz, ix, na, res[seq].position);
+                ix += na;
+            }
+            next += na;
+            ++seq;
+        }
+        tq += na;
+    }
+    return GCMC_OK;
+}
+
+}  // extern "C"

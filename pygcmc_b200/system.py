@@ -19,6 +19,7 @@ fragments, and batches of such systems of uneven size.
 """
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 import math
 import random
@@ -27,6 +28,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import values as V
+from ._native import check, lib, ptr
 
 
 # ---------------------------------------------------------------------------
@@ -64,33 +66,30 @@ class System:
 # reference input builders
 # ---------------------------------------------------------------------------
 def cavity_grid(xyz: np.ndarray, cryst: Sequence[float], grid_dx: float = 1.0, cavity_bias: bool = True):
-    """Box origin, insertion base points and cavity factor (dataset.py:21-139).
+    """Box origin, insertion base points and cavity factor (dataset.py:21-139), in C++
+    (``gcmc_cavity_grid``).
 
     The box is centred on the bounding box of all atoms; voxels of edge
     ``grid_dx`` that contain no atom are the insertion base points (their
     lower corners) and ``cavity_factor = empty / all``.  Without cavity bias
     every voxel of a 1 A grid is used and the factor is 1.
     """
-    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
-    cryst = [float(c) for c in cryst]
-    lo, hi = xyz.min(axis=0), xyz.max(axis=0)
-    centre = (lo + hi) / 2.0
-    start = [float(centre[i]) - cryst[i] / 2.0 for i in range(3)]
-    end = [float(centre[i]) + cryst[i] / 2.0 for i in range(3)]
-    dx = float(grid_dx) if cavity_bias else 1.0
-    n = [int((end[i] - start[i]) / dx) for i in range(3)]
-    occupied = np.zeros(n, dtype=bool)
-    if cavity_bias:
-        idx = [np.trunc((xyz[:, i] - start[i]) / dx).astype(np.int64) % n[i] for i in range(3)]
-        occupied[idx[0], idx[1], idx[2]] = True
-    empty = np.argwhere(~occupied)
-    factor = len(empty) / float(n[0] * n[1] * n[2]) if cavity_bias else 1.0
-    if cavity_bias and factor < 0.05:
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    cr = np.ascontiguousarray([float(c) for c in cryst], dtype=np.float64)
+    start = np.zeros(3, np.float64)
+    n = ctypes.c_int64(0)
+    factor = ctypes.c_double(0.0)
+    L = lib()
+    st = L.gcmc_cavity_grid(len(xyz), ptr(xyz), ptr(cr), float(grid_dx), int(bool(cavity_bias)), ptr(start), None, 0,
+                            ctypes.byref(n), ctypes.byref(factor))
+    if st == 2 and cavity_bias:
         raise ValueError("cavity_bias_factor is too small (< 0.05); decrease the grid spacing")
-    pts = np.empty((len(empty), 3), dtype=np.float32)
-    for i in range(3):
-        pts[:, i] = empty[:, i] * dx + start[i]
-    return start, pts.reshape(-1), factor, dx
+    check(st, "gcmc_cavity_grid")
+    pts = np.empty(3 * n.value, dtype=np.float32)
+    check(L.gcmc_cavity_grid(len(xyz), ptr(xyz), ptr(cr), float(grid_dx), int(bool(cavity_bias)), ptr(start),
+                             ptr(pts), n.value, ctypes.byref(n), ctypes.byref(factor)), "gcmc_cavity_grid")
+    dx = float(grid_dx) if cavity_bias else 1.0
+    return [float(v) for v in start], pts, factor.value, dx
 
 
 def move_array(nsteps: int, names: Sequence[str], mctime: Sequence[float],
@@ -121,18 +120,14 @@ def move_array_np(nsteps: int, names: Sequence[str], mctime: Sequence[float],
 
 
 def fix_groups(xyz: np.ndarray, fix_cutoff: float = 6.0) -> np.ndarray:
-    """Group id per fixed atom (dataset.py:175-188): a new group starts when an
-    atom lies more than ``fix_cutoff`` from the current group's first atom."""
-    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
-    out = np.empty(len(xyz), dtype=np.int64)
-    x0 = y0 = z0 = float("inf")
-    n = -1
-    for i, (x, y, z) in enumerate(xyz.tolist()):
-        if math.sqrt((x - x0) ** 2 + (y - y0) ** 2 + (z - z0) ** 2) > fix_cutoff:
-            n += 1
-            x0, y0, z0 = x, y, z
-        out[i] = n
-    return out
+    """Group id per fixed atom (dataset.py:175-188), in C++ (``gcmc_fix_groups``): a
+    new group starts when an atom lies more than ``fix_cutoff`` from the current
+    group's first atom."""
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    out = np.empty(len(xyz), dtype=np.int32)
+    if len(xyz) and lib().gcmc_fix_groups(len(xyz), ptr(xyz), float(fix_cutoff), ptr(out)) < 0:
+        raise ValueError("gcmc_fix_groups")
+    return out.astype(np.int64)
 
 
 def lj_pair_table(frag_types: Sequence[str], env_types: Sequence[str], nb: dict, nbfix: Optional[dict] = None):
@@ -172,17 +167,15 @@ def lj_pair_table(frag_types: Sequence[str], env_types: Sequence[str], nb: dict,
 
 def group_centres(xyz: np.ndarray, starts: np.ndarray, counts: np.ndarray) -> np.ndarray:
     """Unweighted group centres with the reference's arithmetic (dataset.py:248-300
-    under its numpy<2 dependency): each coordinate is added in float64 to a
-    float32 running sum that is rounded back to float32, then divided by the
-    count in float64 and stored as float32."""
-    xyz = np.asarray(xyz, dtype=np.float64)
-    starts = np.asarray(starts, dtype=np.int64)
-    counts = np.asarray(counts, dtype=np.int64)
-    acc = np.zeros((len(starts), 3), dtype=np.float32)
-    for j in range(int(counts.max()) if len(counts) else 0):
-        m = counts > j
-        acc[m] = (acc[m].astype(np.float64) + xyz[starts[m] + j]).astype(np.float32)
-    return (acc.astype(np.float64) / np.maximum(counts, 1)[:, None]).astype(np.float32)
+    under its numpy<2 dependency), in C++ (``gcmc_group_centres``): each coordinate
+    is added in float64 to a float32 running sum that is rounded back to float32,
+    then divided by the count in float64 and stored as float32."""
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    starts = np.ascontiguousarray(starts, dtype=np.int64)
+    counts = np.ascontiguousarray(counts, dtype=np.int32)
+    out = np.zeros((len(starts), 3), dtype=np.float32)
+    check(lib().gcmc_group_centres(len(starts), ptr(xyz), ptr(starts), ptr(counts), ptr(out)), "gcmc_group_centres")
+    return out
 
 
 def charmm_to_nb(eps_kcal: float, rmin_half: float):
@@ -223,37 +216,28 @@ def assemble(*, names: Sequence[str], templates: Sequence[dict], initial: Sequen
         frag[i]["atoms"]["charge"][: len(xyz)] = t["q"]
         frag[i]["atoms"]["type"][: len(xyz)] = t["type"]
     nfix = len(fixed_xyz)
-    ngroups_fixed = int(fixed_group[-1]) + 1 if nfix else 0
+    fixed_group = np.ascontiguousarray(fixed_group, dtype=np.int32)
+    ngroups_fixed = int(np.count_nonzero(np.diff(fixed_group))) + 1 if nfix else 0
     total_res = ngroups_fixed + int(frag["maxNum"].sum())
     total_atoms = nfix + int((frag["maxNum"].astype(np.int64) * frag["num_atoms"]).sum())
     res = np.zeros(total_res, dtype=V.Residue_dtype)
     atoms = np.zeros(total_atoms, dtype=V.Atom_dtype)
-    if nfix:
-        atoms["position"][:nfix] = fixed_xyz
-        atoms["charge"][:nfix] = fixed_q
-        atoms["type"][:nfix] = fixed_type
-        bounds = np.flatnonzero(np.diff(fixed_group)) + 1
-        starts = np.concatenate([[0], bounds])
-        ends = np.concatenate([bounds, [nfix]])
-        res["atomStart"][:len(starts)] = starts
-        res["atomNum"][:len(starts)] = ends - starts
-        res["position"][:len(starts)] = group_centres(fixed_xyz, starts, ends - starts)
-    seq = ngroups_fixed
-    next_atom = nfix
-    for i in range(nt):
-        frag[i]["startRes"] = seq
-        na = int(frag[i]["num_atoms"])
-        for j in range(int(frag[i]["maxNum"])):
-            res[seq]["atomNum"] = na
-            res[seq]["atomStart"] = next_atom
-            if j < len(initial[i]):
-                p = np.asarray(initial[i][j], dtype=np.float64)
-                atoms["position"][next_atom:next_atom + na] = p
-                atoms["charge"][next_atom:next_atom + na] = templates[i]["q"]
-                atoms["type"][next_atom:next_atom + na] = templates[i]["type"]
-                res[seq]["position"] = group_centres(p, [0], [na])[0]
-            next_atom += na
-            seq += 1
+    # residue / atom arrays in C++ (gcmc_fill_layout)
+    fx = np.ascontiguousarray(np.asarray(fixed_xyz, dtype=np.float64).reshape(-1, 3))
+    fq = np.ascontiguousarray(fixed_q, dtype=np.float64)
+    ft = np.ascontiguousarray(fixed_type, dtype=np.int32)
+    tq = np.ascontiguousarray(np.concatenate([np.asarray(t["q"], np.float32) for t in templates]), dtype=np.float32)
+    tt = np.ascontiguousarray(np.concatenate([np.asarray(t["type"], np.int32) for t in templates]), dtype=np.int32)
+    ninit = np.ascontiguousarray([len(c) for c in initial], dtype=np.int32)
+    parts = [np.asarray(p, dtype=np.float64).reshape(-1, 3) for c in initial for p in c]
+    ixyz = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((0, 3)), dtype=np.float64)
+    start_res = np.zeros(nt, dtype=np.int32)
+    check(lib().gcmc_fill_layout(nfix, ptr(fx), ptr(fq), ptr(ft), ptr(fixed_group), nt,
+                                 ptr(np.ascontiguousarray(frag["maxNum"], np.int32)),
+                                 ptr(np.ascontiguousarray(frag["num_atoms"], np.int32)), ptr(tq), ptr(tt), ptr(ninit),
+                                 ptr(ixyz), total_res, total_atoms, ptr(res), ptr(atoms), ptr(start_res)),
+          "gcmc_fill_layout")
+    frag["startRes"] = start_res
     info = np.zeros(1, dtype=V.Info_dtype)
     info[0]["ffXNum"] = n_frag_types_ff
     info[0]["ffYNum"] = n_types_ff
@@ -404,7 +388,6 @@ def protein_system(seed: int = 1, n_atoms: int = 6000, box: float = 64.0, radius
     muex ~ U[-5, -1] (+ muex_shift).  Each type starts with
     round(conc * V * 6.023e-4) copies placed without clashes (>= 2 A).
     """
-    from ._native import lib, ptr
     g = np.random.default_rng(seed)
     L = np.array([box, box, box], dtype=np.float64)
     centre = (L / 2).astype(np.float32)
@@ -488,3 +471,92 @@ def replica_batch(n_rep: int = 64, seed: int = 1, atoms_range=(2000, 40000), mcs
         out.append(protein_system(seed=seed * 1000 + i, n_atoms=n, box=box, radius=radius, mcsteps=mcsteps,
                                   conf_bias=conf_bias, muex_shift=shift))
     return out
+
+
+def slab_system(seed: int = 1, n_atoms: int = 200_000, box=(150.0, 150.0, 120.0), density: float = 0.09,
+                pore: float = 12.0, n_frag: int = 8, n_types: int = 24, water: bool = True, mcsteps: int = 100_000,
+                conf_bias: int = 1000, conc: float = 0.25, water_conc: float = 55.0, cutoff: float = 12.0,
+                grid_dx: float = 1.0, excl: float = 1.6, water_fill: float = 1.0) -> System:
+    """Large periodic system: a slab of random-walk chains with a cylindrical pore
+    along z, generic rigid fragments and (optionally) TIP3P water.
+
+    The slab holds ``n_atoms`` at ``density`` atoms/A^3, so its thickness is
+    n_atoms / (density * (Lx Ly - pi pore^2)); chains restart at a random free
+    point when a step cannot be placed.  LJ types, charges and fragment
+    templates are drawn as in :func:`protein_system`; water is the TIP3P model
+    (O -0.834, eps 0.1521, rmin/2 1.7682; H +0.417, eps 0.046, rmin/2 0.2245)
+    named ``SOL`` (equal move probabilities), with ``water_fill`` times its
+    bulk count (``water_conc`` mol/L over the volume outside the slab) placed
+    initially, >= 2.2 A from everything.
+    """
+    g = np.random.default_rng(seed)
+    L = np.asarray(box, dtype=np.float64)
+    area = L[0] * L[1] - math.pi * pore * pore
+    thick = n_atoms / (density * area)
+    if thick >= L[2]:
+        raise ValueError("slab thicker than the box")
+    xyz = np.empty((n_atoms, 3), dtype=np.float32)
+    nbreak = ctypes.c_int(0)
+    rc = lib().gcmc_synth_chain_slab(n_atoms, 0.0, float(L[0]), 0.0, float(L[1]), float(L[2] / 2), float(thick / 2),
+                                     float(L[0] / 2), float(L[1] / 2), float(pore), 1.5, excl, int(seed) * 7919 + 29,
+                                     ptr(xyz), ctypes.byref(nbreak))
+    if rc != 0:
+        raise RuntimeError("slab generation failed")
+    tnames = [f"T{i:02d}" for i in range(n_types)]
+    eps = g.uniform(0.02, 0.20, n_types)
+    rmin2 = g.uniform(1.0, 2.2, n_types)
+    nb = {tnames[i]: charmm_to_nb(eps[i], rmin2[i]) for i in range(n_types)}
+    nb["OT"] = charmm_to_nb(0.1521, 1.7682)
+    nb["HT"] = charmm_to_nb(0.046, 0.2245)
+    q = g.normal(0.0, 0.35, n_atoms)
+    q -= q.mean()
+    ptype = g.integers(n_types, size=n_atoms)
+    names, raw = [], []
+    for f in range(n_frag):
+        ns = int(g.integers(4, 13))
+        kind = "planar" if g.random() < 0.5 else "tetrahedral"
+        txyz = lattice_template(g, ns, kind)
+        tq = g.normal(0.0, 0.3, ns)
+        tq += (int(g.integers(-1, 2)) - tq.sum()) / ns
+        raw.append((txyz, tq, [tnames[t] for t in g.integers(n_types, size=ns)]))
+        names.append(f"FR{f:02d}")
+    if water:
+        raw.append((tip3p_template(), np.array([-0.834, 0.417, 0.417]), ["OT", "HT", "HT"]))
+        names.append("SOL")
+    t1, t2, ff = lj_pair_table([t for (_, _, tt) in raw for t in tt], [tnames[t] for t in ptype], nb)
+    col = {t: i for i, t in enumerate(t2)}
+    templates = [{"xyz": txyz, "q": tq, "type": np.array([col[t] for t in tt])} for (txyz, tq, tt) in raw]
+    fixed_type = np.array([col[tnames[t]] for t in ptype])
+    nt = len(names)
+    muex = g.uniform(-5.0, -1.0, n_frag).tolist() + ([-5.8] if water else [])
+    concs = [conc] * n_frag + ([water_conc] if water else [])
+    free = float(np.prod(L)) - thick * area
+    existing = np.ascontiguousarray(xyz, dtype=np.float32)
+    lo = np.zeros(3, np.float32)
+    Lf = L.astype(np.float32)
+    initial = []
+    for f in range(nt):
+        n0 = int(round(concs[f] * free * V.MOLES_TO_MOLECULES * (water_fill if names[f] == "SOL" else 1.0)))
+        tx = np.ascontiguousarray(templates[f]["xyz"] - templates[f]["xyz"].mean(axis=0), dtype=np.float32)
+        out = np.zeros((n0, len(tx), 3), np.float32)
+        if n0:
+            rc = lib().gcmc_synth_place(len(existing), ptr(existing), ptr(lo), ptr(Lf), ptr(tx), len(tx), n0,
+                                        2.2 if names[f] == "SOL" else 2.0, int(seed) * 104729 + 31 * f + 11, ptr(out))
+            if rc != 0:
+                raise RuntimeError("could not place the initial copies")
+            existing = np.ascontiguousarray(np.concatenate([existing, out.reshape(-1, 3)]))
+        initial.append([out[c].astype(np.float64) for c in range(n0)])
+    start, grid, cav, dx = cavity_grid(existing.astype(np.float64), L, grid_dx)
+    groups = fix_groups(xyz, 6.0)
+    moves = move_array_np(mcsteps, names, [1.0] * nt, seed=seed + 1)
+    s = assemble(names=names, templates=templates, initial=initial, fixed_xyz=xyz, fixed_q=q, fixed_type=fixed_type,
+                 fixed_group=groups, muex=muex, conc=concs, conf_bias=[conf_bias] * nt, mctime=[1.0] * nt, cryst=L,
+                 cutoff=cutoff, grid_dx=dx, start=start, grid=grid, cavity_factor=cav, ff=ff,
+                 n_frag_types_ff=len(t1), n_types_ff=len(t2), moves=moves, seed=seed)
+    s.meta.update({"chain_breaks": int(nbreak.value), "n_fixed": n_atoms, "box": tuple(L), "slab_thickness": thick,
+                   "lj_types": {"names": list(t2),
+                                "eps_kcal": np.array([(eps[tnames.index(n)] if n in tnames else
+                                                       {"OT": 0.1521, "HT": 0.046}[n]) for n in t2]),
+                                "rmin_half": np.array([(rmin2[tnames.index(n)] if n in tnames else
+                                                        {"OT": 1.7682, "HT": 0.2245}[n]) for n in t2])}})
+    return s
