@@ -96,6 +96,10 @@ typedef struct {
                             occupancy limit)                                        */
     float fb_trn;        /* proposal 2: translate half-width h_t, A (0 = 0.5)        */
     float fb_rot;        /* proposal 2: rotation half-width h_r, rad (0 = 10 degrees)*/
+    uint32_t step_offset; /* the RNG counts steps from this value: a context created
+                            from a checkpoint taken after s steps, with moveArray
+                            starting at step s and step_offset = s, continues the
+                            same chain (0 for a fresh run)                         */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
@@ -310,6 +314,15 @@ int gcmc_fill_layout(int32_t nfix, const double* fixed_xyz, const double* fixed_
                      const float* tpl_q, const int32_t* tpl_type, const int32_t* n_initial,
                      const double* initial_xyz, int32_t total_res, int64_t total_atoms, residue* res, Atom* atoms,
                      int32_t* start_res);
+
+/* get_data's fragment PDB records (gcmc/python/dataset.py:393-408): an ATOM line
+ * per atom of every occupied slot (type, then slot order), serials / residue
+ * numbers from serial0 / resnum0 wrapping at 99999 / 9999; atom_names holds 20
+ * names of 4 chars per type.  Returns the bytes written, or, when out is NULL
+ * or cap is short, the capacity to provide; -1 on bad input. */
+int64_t gcmc_pdb_fragment_lines(int32_t nfrag, const AtomArray* fragmentInfo, const residue* residueInfo,
+                                const Atom* atomInfo, const char* atom_names, int64_t serial0, int64_t resnum0,
+                                char* out, int64_t cap);
 
 /* count random non-clashing copies (sites >= min_dist from all atoms) of a rigid
  * template in the periodic box [lo, lo+L); out_xyz[count*nsites*3]. */

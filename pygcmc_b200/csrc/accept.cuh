@@ -131,13 +131,13 @@ __device__ void prepare_step(const RepDev& R, int step) {
                 D.k = n > 0 ? 1 : 0;
                 D.nvar = 1;
                 if (n > 0) {
-                    U4 r = rng(R.seed, R.replica, (uint32_t)step, 0u, RP_DELETE, 0);
+                    U4 r = rng(R.seed, R.replica, R.step_base + (uint32_t)step, 0u, RP_DELETE, 0);
                     D.del_slot = (int)(r.x % (uint32_t)n);
                 }
             } else {
                 D.k = min(F.confBias, n);
                 D.nvar = 2;
-                D.perm_key = rng(R.seed, R.replica, (uint32_t)step, 0u, RP_PERM, 0);
+                D.perm_key = rng(R.seed, R.replica, R.step_base + (uint32_t)step, 0u, RP_PERM, 0);
                 D.perm_h = perm_bits(n);
                 D.fb = R.fb;
             }
@@ -171,7 +171,7 @@ __device__ void prepare_step(const RepDev& R, int step) {
             R.pslot[i] = slot;
             float4 c = R.gcen[startRes + slot];
             if (D.move == MV_TRANSLATE && !D.fb) {  // force-biased: set by the old-pose launch
-                U4 r = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_MOVE, 0);
+                U4 r = rng(R.seed, R.replica, R.step_base + (uint32_t)step, (uint32_t)i, RP_MOVE, 0);
                 c.x = fadd(c.x, trn_shift(R, r.x, 0, c.x));
                 c.y = fadd(c.y, trn_shift(R, r.y, 1, c.y));
                 c.z = fadd(c.z, trn_shift(R, r.z, 2, c.z));
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             const double E = S.E[0];
             const int n = D.n;
             const double lnp = log((double)n) - F.B + kBeta * E;
-            const U4 r = rng(R.seed, R.replica, (uint32_t)D.step, 0u, RP_DELETE, 0);
+            const U4 r = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, 0u, RP_DELETE, 0);
             const double u = u53(r.y, r.z);
             const bool acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
             if (acc) {
@@ -315,9 +315,9 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             const double e = S.E[i];
             const bool fin = isfinite(e);
             S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
-            const U4 g = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
+            const U4 g = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
             S.key[i] = fin ? key_order(-kBeta * e - log(-log(u53_open(g.x, g.y)))) : 0ull;
-            const U4 ua = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
+            const U4 ua = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
             S.lnu[i] = log(u53(ua.x, ua.y));
             S.c[i] = R.pcen[i];
         }

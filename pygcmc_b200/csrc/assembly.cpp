@@ -13,12 +13,15 @@
 // Python set order, and unused slots are zero-filled.
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
 #include "../../include/gcmc_b200.h"
 
 namespace {
+
+constexpr int kMaxSitesAbi = 20;  // AtomArray.atoms[20]
 
 inline int64_t pymod(int64_t a, int64_t n) {
     const int64_t r = a % n;
@@ -160,6 +163,47 @@ int gcmc_fill_layout(int32_t nfix, const double* fixed_xyz, const double* fixed_
         tq += na;
     }
     return GCMC_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// get_data's fragment records (gcmc/python/dataset.py:393-408): one ATOM line
+// per atom of every occupied slot, in type and slot order, serials and residue
+// numbers continuing from serial0 / resnum0 and wrapping at 99999 / 9999.
+// atom_names: per type 20 names of 4 chars (not NUL-terminated).  Returns the
+// number of bytes written, or (out == NULL or cap too small) the number needed.
+int64_t gcmc_pdb_fragment_lines(int32_t nfrag, const AtomArray* fragmentInfo, const residue* residueInfo,
+                                const Atom* atomInfo, const char* atom_names, int64_t serial0, int64_t resnum0,
+                                char* out, int64_t cap) {
+    if (nfrag < 0 || !fragmentInfo || !residueInfo || !atomInfo || !atom_names) return -1;
+    int64_t need = 0;
+    for (int32_t i = 0; i < nfrag; ++i) need += (int64_t)fragmentInfo[i].totalNum * fragmentInfo[i].num_atoms;
+    // a record is 66 bytes while every coordinate fits %8.3f; 96 bounds any line
+    if (!out || cap < need * 96) return need * 96;
+    int64_t pos = 0, serial = serial0, resnum = resnum0;
+    char buf[160];
+    for (int32_t i = 0; i < nfrag; ++i) {
+        const AtomArray& F = fragmentInfo[i];
+        for (int32_t j = 0; j < F.totalNum; ++j) {
+            const residue& r = residueInfo[F.startRes + j];
+            for (int32_t k = 0; k < r.atomNum; ++k) {
+                const Atom& a = atomInfo[r.atomStart + k];
+                const char* nm = atom_names + ((size_t)i * kMaxSitesAbi + k) * 4;
+                const int len = std::snprintf(buf, sizeof(buf), "ATOM  %5lld  %-4.4s%-4.4s %4lld    %8.3f%8.3f%8.3f  1.00  0.00\n",
+                                              (long long)((serial - 1) % 99999 + 1), nm, F.name,
+                                              (long long)((resnum - 1) % 9999 + 1), (double)a.position[0],
+                                              (double)a.position[1], (double)a.position[2]);
+                if (len <= 0 || pos + len > cap) return -1;
+                std::memcpy(out + pos, buf, (size_t)len);
+                pos += len;
+                ++serial;
+            }
+            ++resnum;
+        }
+    }
+    return pos;
 }
 
 }  // extern "C"

@@ -363,6 +363,7 @@ struct RepDev {
     int nfixed, ntypes, ffY, G;
     int mcsteps;
     uint32_t seed, replica;
+    uint32_t step_base; // RNG step counter = step_base + local step (resume from a checkpoint)
     int run_end;        // steps below this index are executed
     int log_cap, log_kmax;
     // force-biased translate/rotate (proposal 2): each component of the
@@ -421,7 +422,7 @@ __device__ __forceinline__ int cell_of(const RepDev& R, float x, float y, float 
 // Centre of insertion pose i (gcmc/cpp/gcmc_energy.h:82-93): grid point + U(0,1]*dx.
 __device__ __forceinline__ void insert_centre(const RepDev& R, int step, int i, float& x, float& y,
                                               float& z) {
-    U4 r0 = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 0);
+    U4 r0 = rng(R.seed, R.replica, R.step_base + (uint32_t)step, (uint32_t)i, RP_INSERT, 0);
     int g = (int)(r0.x % (uint32_t)R.G);
     float4 gp = R.grid[g];
     x = fadd(fmul(u01_oc(r0.y), R.grid_dx), gp.x);
@@ -430,7 +431,7 @@ __device__ __forceinline__ void insert_centre(const RepDev& R, int step, int i, 
 }
 
 __device__ __forceinline__ Mat3 insert_rotation(const RepDev& R, int step, int i) {
-    U4 r1 = rng(R.seed, R.replica, (uint32_t)step, (uint32_t)i, RP_INSERT, 1);
+    U4 r1 = rng(R.seed, R.replica, R.step_base + (uint32_t)step, (uint32_t)i, RP_INSERT, 1);
     if (R.proposal == 0) {
         float sn, cs;
         det_sincos(fmul(u01_oc(r1.w), kTwoPiF), sn, cs);

@@ -329,7 +329,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // identical arithmetic to build_pose's moved variant.
 __device__ __forceinline__ void moved_site(const RepDev& R, const StepDesc& D, int i, const float4& gc,
                                            int ns, int lane, float& px, float& py, float& pz) {
-    U4 r = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_MOVE, 0);
+    U4 r = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_MOVE, 0);
     if (D.move == MV_TRANSLATE) {
         px = fadd(px, trn_shift(R, r.x, 0, gc.x));
         py = fadd(py, trn_shift(R, r.y, 1, gc.y));
@@ -386,7 +386,7 @@ __device__ __forceinline__ float fb_shift(const RepDev& R, float d, int axis, fl
 // prop[0] = (d, invalid), prop[1] = (a, 0); returns the new centre.
 __device__ __forceinline__ float4 fb_propose(const RepDev& R, const StepDesc& D, int i, const float f[6],
                                              float4 gc, float4* prop) {
-    const U4 r = rng(R.seed, R.replica, (uint32_t)D.step, (uint32_t)i, RP_FB, 0);
+    const U4 r = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_FB, 0);
     const float u[3] = {u01_co(r.x), u01_co(r.y), u01_co(r.z)};
     const bool trn = D.move == MV_TRANSLATE;
     const float* g = trn ? f : f + 3;

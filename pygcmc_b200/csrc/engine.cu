@@ -240,6 +240,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.mcsteps = I->mcsteps;
     d.seed = I->seed;
     d.replica = opt.replica + (uint32_t)r;
+    d.step_base = opt.step_offset;
     d.run_end = 0;
 
     // the per-group periodic image is exact when every pair of an included

@@ -87,6 +87,22 @@ class Engine:
               "gcmc_download")
         return s
 
+    def checkpoint(self, rep: int = 0):
+        """The replica's state after the steps run so far, as a System whose
+        move schedule is the remaining steps; ``meta["step_offset"]`` is the
+        absolute step to resume at (pass it as ``options.step_offset`` when
+        creating the Engine that continues the chain)."""
+        c = self.counters(rep)
+        done = int(c["steps"]) if c["steps"] >= 0 else 0
+        base = int(self.systems[rep].meta.get("step_offset", 0))
+        s = self.download(rep)
+        s.moveArray = np.ascontiguousarray(self.systems[rep].moveArray[done:])
+        s.SimInfo = s.SimInfo.copy()
+        s.SimInfo[0]["mcsteps"] = len(s.moveArray)
+        s.meta = dict(s.meta)
+        s.meta["step_offset"] = base + done
+        return s
+
     def logs(self, rep: int = 0):
         n = int(self.options.log_steps)
         logs = np.zeros(n, dtype=V.StepLog_dtype)

@@ -86,6 +86,21 @@ def main(ref):
     o.showInfo = 0
     o.PME = 0
     mods["dataset"].GCMCDataset.update_data(o)
+    # get_data (dataset.py:375-440): PDB of the fixed atoms' own lines plus the
+    # fragments, and the [ molecules ] counts of the topology
+    for k, a in enumerate(o.fix_atoms):
+        a.serial = k + 1
+        a.sequence = int(groups[k]) + 1
+        a.s = "ATOM  %5d  CA  GLY A%4d    %8.3f%8.3f%8.3f  1.00  0.00" % (k + 1, int(groups[k]) + 1, a.x, a.y, a.z)
+    frag_names = [["OW", "HW1", "HW2"], ["C1", "C2", "C3", "C4"]]
+    for i in range(2):
+        for k, a in enumerate(o.fragments[i]):
+            a.name = frag_names[i][k]
+    o.fragmentInfo[0]["totalNum"] = 2
+    o.topologyType = "top"
+    o.TOPString = "[ system ]\ntest\n\n[ molecules ]\nProtein 1\nWAT3 7\n"
+    mods["dataset"].GCMCDataset.get_data(o)
+    pdb, top = o.PDBString, o.TOPString
     np.savez_compressed(
         os.path.join(HERE, "builders.npz"),
         fix=fix, fix_q=fix_q, fix_t=fix_t, cryst=np.array(cryst),
@@ -93,7 +108,8 @@ def main(ref):
         copies0=np.array(copies[0]), ff=np.array(o.ff, np.float32),
         ref_startxyz=np.array(o.startxyz), ref_grid=o.grid, ref_cavity=np.array(o.cavity_bias_factor),
         ref_moves=o.moveArray, ref_groups=groups, ref_frag=o.fragmentInfo, ref_res=o.residueInfo,
-        ref_atoms=o.atomInfo, ref_info=o.SimInfo)
+        ref_atoms=o.atomInfo, ref_info=o.SimInfo, ref_pdb=np.array(pdb), ref_top=np.array(top),
+        frag_atom_names0=np.array(frag_names[0]), frag_atom_names1=np.array(frag_names[1]))
     print("wrote builders.npz")
 
 

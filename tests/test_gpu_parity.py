@@ -261,3 +261,30 @@ def test_autotune_picks_the_fastest_trial(protein_small, water_small):
         f = eng.download(1)
     solo = _solo_final(systems[1], 64, 1)
     assert (solo.fragmentInfo["totalNum"] == f.fragmentInfo["totalNum"]).all()
+
+
+@pytest.mark.parametrize("proposal", [0, 2])
+def test_checkpoint_resume_continues_the_chain(protein_small, proposal):
+    """A context created from a checkpoint (state + remaining moves, RNG step
+    offset) continues the same chain as an uninterrupted run, bit for bit."""
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    n, cut = 200, 120
+    with Engine(protein_small.copy(), default_options(proposal=proposal)) as e:
+        e.run(n)
+        e.sync()
+        full = e.download()
+    with Engine(protein_small.copy(), default_options(proposal=proposal)) as e:
+        e.run(cut)
+        e.sync()
+        ck = e.checkpoint()
+    assert ck.meta["step_offset"] == cut and len(ck.moveArray) == int(protein_small.SimInfo[0]["mcsteps"]) - cut
+    with Engine(ck, default_options(proposal=proposal, step_offset=ck.meta["step_offset"])) as e:
+        e.run(n - cut)
+        e.sync()
+        res = e.download()
+    assert (full.fragmentInfo["totalNum"] == res.fragmentInfo["totalNum"]).all()
+    a = occupied_atoms(full)
+    assert np.array_equal(full.atomInfo["position"][a], res.atomInfo["position"][a])
+    r = occupied_res(full)
+    assert np.array_equal(full.residueInfo["position"][r], res.residueInfo["position"][r])
