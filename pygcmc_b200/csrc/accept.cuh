@@ -45,35 +45,56 @@ struct AcceptSmem {
 };
 
 // ---- cell list maintenance (single thread) ----
-__device__ __forceinline__ void cell_add(const RepDev& R, int g, float x, float y, float z) {
-    int c = cell_of(R, x, y, z);
-    int pos = R.cell_count[c];
-    if (pos >= R.cap) {
+// Each cell keeps its group ids in increasing order, so a cell's content (and
+// with it the order in which the energy kernels visit groups and sum their
+// terms) depends only on the current state, not on the history of moves: a
+// context rebuilt from a checkpoint evaluates bit-identical energies.
+__device__ __forceinline__ void cell_insert(const RepDev& R, int c, int g) {
+    const int n = R.cell_count[c];
+    if (n >= R.cap) {
         atomicOr(R.err, ERR_CELL_OVERFLOW);
         R.gcell[g] = -1;
         return;
     }
-    R.cell_ent[c * R.cap + pos] = g;
-    R.cell_count[c] = pos + 1;
-    R.gcell[g] = c * R.cap + pos;
+    int* ent = R.cell_ent + (size_t)c * R.cap;
+    int p = n;
+    while (p > 0 && ent[p - 1] > g) {  // shift larger ids up by one
+        const int h = ent[p - 1];
+        ent[p] = h;
+        R.gcell[h] = c * R.cap + p;
+        --p;
+    }
+    ent[p] = g;
+    R.cell_count[c] = n + 1;
+    R.gcell[g] = c * R.cap + p;
+}
+__device__ __forceinline__ void cell_add(const RepDev& R, int g, float x, float y, float z) {
+    cell_insert(R, cell_of(R, x, y, z), g);
 }
 __device__ __forceinline__ void cell_remove(const RepDev& R, int g) {
-    int cp = R.gcell[g];
+    const int cp = R.gcell[g];
     if (cp < 0) return;
-    int c = cp / R.cap;
-    int last = R.cell_count[c] - 1;
-    int gl = R.cell_ent[c * R.cap + last];
-    R.cell_ent[cp] = gl;
-    R.gcell[gl] = cp;
-    R.cell_count[c] = last;
+    const int c = cp / R.cap;
+    const int n = R.cell_count[c];
+    int* ent = R.cell_ent + (size_t)c * R.cap;
+    for (int p = cp - c * R.cap; p + 1 < n; ++p) {  // shift the rest down by one
+        const int h = ent[p + 1];
+        ent[p] = h;
+        R.gcell[h] = c * R.cap + p;
+    }
+    R.cell_count[c] = n - 1;
     R.gcell[g] = -1;
 }
-// the cell entry of group `from` now stands for group `to`
+// the cell entry of group `from` now stands for group `to` (same cell)
 __device__ __forceinline__ void cell_rename(const RepDev& R, int from, int to) {
-    int cp = R.gcell[from];
-    R.gcell[from] = -1;
-    R.gcell[to] = cp;
-    if (cp >= 0) R.cell_ent[cp] = to;
+    const int cp = R.gcell[from];
+    if (cp < 0) {
+        R.gcell[to] = -1;
+        return;
+    }
+    const int c = cp / R.cap;
+    cell_remove(R, from);
+    cell_insert(R, c, to);
 }
 
 // Order-preserving map of a double to uint64 (larger key -> larger integer);
