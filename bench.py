@@ -139,7 +139,7 @@ def nominal_fp32_tflops(sm_max_mhz):
 
 
 def load_traffic():
-    p = os.path.join(ROOT, "profiles", "k_energy_cfg1.json")
+    p = os.path.join(ROOT, "profiles", "k_energy_protein6000.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
