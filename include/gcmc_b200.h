@@ -100,6 +100,15 @@ typedef struct {
                             from a checkpoint taken after s steps, with moveArray
                             starting at step s and step_offset = s, continues the
                             same chain (0 for a fresh run)                         */
+    int32_t pme;         /* Ewald electrostatics by smooth PME (no counterpart in the
+                            reference): 1 on, -1 off, 0 = InfoStruct.PME decides.
+                            Real-space Coulomb erfc(alpha r)/r in the group cutoff,
+                            the reciprocal potential of the state on an FP64 mesh
+                            rebuilt every step, order-4 B-splines; not with
+                            proposal 2                                           */
+    float pme_alpha;     /* Ewald splitting parameter, 1/A (0 = 0.32)              */
+    int32_t pme_grid[3]; /* mesh points per axis (0 = box edge / 1.2 A rounded up to
+                            a 2-3-5-7-smooth size)                                 */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
@@ -186,6 +195,10 @@ int gcmc_download(gcmc_ctx* ctx, int32_t rep, AtomArray* fragmentInfo, residue* 
  * (optional) receives log_kmax doubles per step. */
 int gcmc_get_logs(gcmc_ctx* ctx, int32_t rep, gcmc_step_log* logs, double* energies,
                   int32_t max_steps, int32_t* n_steps);
+/* Ewald runs: the reciprocal-space potential (kJ/mol/e) of replica rep's
+ * current state at n points (host arrays pts[3n], out[n]); rebuilds the mesh
+ * first.  Synchronous. */
+int gcmc_pme_potential(gcmc_ctx* ctx, int32_t rep, const double* pts, int32_t n, double* out);
 /* Force-biased runs with logs: per step, log_kmax x 12 floats -- the force and
  * torque at the old pose, then at the new pose, of each translate/rotate pose
  * (as used by the proposal and the acceptance). */

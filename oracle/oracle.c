@@ -22,6 +22,7 @@
 #define OR_KCAL_TO_KJ 4.184
 #define OR_COULOMB 1388.431112 /* gcmc/cpp/gcmc_energy.h:137 */
 #define OR_TWO_PI_F 6.28318530717958647692f
+#define OR_PI 3.14159265358979323846
 
 /* RNG purposes (third counter word, high half). */
 enum { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_PERM = 5, RP_GUMBEL = 6, RP_FB = 7 };
@@ -260,9 +261,9 @@ float or_dist_host(const float a[3], const float b[3], const float L[3]) {
 /* ------------------------------------------------------------------------- */
 /* Pose energy (gcmc/cpp/gcmc_energy.h:142-204).                              */
 /* ------------------------------------------------------------------------- */
-static double group_pairs64(const or_info* info, const or_atom* atoms, const float* ff, int a0,
-                            int na, const float (*sx)[3], const float* sq, const int32_t* st,
-                            int ns, double* l1) {
+static double group_pairs64a(const or_info* info, const or_atom* atoms, const float* ff, int a0,
+                             int na, const float (*sx)[3], const float* sq, const int32_t* st,
+                             int ns, double* l1, double alpha) {
     const double L[3] = {info->cryst[0], info->cryst[1], info->cryst[2]};
     double e = 0.0;
     for (int a = a0; a < a0 + na; ++a) {
@@ -280,11 +281,17 @@ static double group_pairs64(const or_info* info, const or_atom* atoms, const flo
             double s6 = s2 * s2 * s2;
             double lj = 4.0 * eps * (s6 * s6 - s6);
             double el = OR_COULOMB * (double)sq[s] * (double)A->charge / sqrt(d2);
+            if (alpha > 0.0) el *= erfc(alpha * sqrt(d2));  /* Ewald real-space kernel */
             e += lj + el;
             *l1 += fabs(lj) + fabs(el);
         }
     }
     return e;
+}
+
+static double group_pairs64(const or_info* info, const or_atom* atoms, const float* ff, int a0, int na,
+                            const float (*sx)[3], const float* sq, const int32_t* st, int ns, double* l1) {
+    return group_pairs64a(info, atoms, ff, a0, na, sx, sq, st, ns, l1, 0.0);
 }
 
 /* FP32 mirror of one reference thread's pair work on one group. */
@@ -314,6 +321,26 @@ double or_pose_energy(const or_info* info, const or_atomarray* frag, const or_re
                       int32_t self, int32_t mode, int32_t* n_groups, int64_t* pairs) {
     return or_pose_energy_l1(info, frag, res, atoms, ff, sx, sq, st, ns, centre, self, mode, n_groups, pairs,
                              NULL);
+}
+
+/* FP64 real-space pose energy with the Ewald real-space kernel erfc(alpha r)/r
+ * for Coulomb (alpha = 0: plain 1/r, calcEnergy's form). */
+static double pose_energy64a(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                             const or_atom* atoms, const float* ff, const float (*sx)[3], const float* sq,
+                             const int32_t* st, int32_t ns, const float centre[3], int32_t self, double alpha,
+                             double* l1_out) {
+    double e = 0.0, l1 = 0.0;
+    for (int t = -1; t < info->fragTypeNum; ++t) {
+        const int g0 = t < 0 ? 0 : frag[t].startRes;
+        const int g1 = t < 0 ? frag[0].startRes : g0 + frag[t].totalNum;
+        for (int g = g0; g < g1; ++g) {
+            if (g == self) continue;
+            if (or_dist_group(centre, res[g].position, info->cryst) <= info->cutoff)
+                e += group_pairs64a(info, atoms, ff, res[g].atomStart, res[g].atomNum, sx, sq, st, ns, &l1, alpha);
+        }
+    }
+    if (l1_out) *l1_out = l1;
+    return e;
 }
 
 double or_pose_energy_l1(const or_info* info, const or_atomarray* frag, const or_residue* res,
@@ -688,6 +715,201 @@ static void pose_grad64(const pose64* P, const float centre[3], int self, double
 }
 
 /* ------------------------------------------------------------------------- */
+/* Ewald electrostatics (not in the reference): exact reciprocal-space        */
+/* potential by a direct k-space sum, for checking the engine's smooth PME.   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int nk, n[3];
+    int* idx;       /* [nk*3] integer wave vector (half space)                 */
+    double* coef;   /* [nk] 2 K exp(-pi^2 m^2/alpha^2) / (pi V m^2)            */
+    double* sre;    /* [nk] Re S(m)                                             */
+    double* sim;    /* [nk] Im S(m)                                             */
+    double L[3];
+} ewald_t;
+
+static void ewald_free(ewald_t* E) {
+    free(E->idx); free(E->coef); free(E->sre); free(E->sim);
+    memset(E, 0, sizeof(*E));
+}
+
+static int ewald_init(ewald_t* E, const or_info* info, double alpha) {
+    memset(E, 0, sizeof(*E));
+    const double mmax = alpha * sqrt(-log(1e-13)) / OR_PI;
+    const double V = (double)info->cryst[0] * info->cryst[1] * info->cryst[2];
+    for (int d = 0; d < 3; ++d) {
+        E->L[d] = info->cryst[d];
+        E->n[d] = (int)ceil(mmax * E->L[d]);
+    }
+    const size_t cap = (size_t)(E->n[0] + 1) * (2 * E->n[1] + 1) * (2 * E->n[2] + 1);
+    E->idx = malloc(sizeof(int) * 3 * cap);
+    E->coef = malloc(sizeof(double) * cap);
+    if (!E->idx || !E->coef) return -1;
+    for (int a = 0; a <= E->n[0]; ++a)
+        for (int b = -E->n[1]; b <= E->n[1]; ++b)
+            for (int c = -E->n[2]; c <= E->n[2]; ++c) {
+                if (a == 0 && (b < 0 || (b == 0 && c <= 0))) continue; /* half space, m != 0 */
+                const double m[3] = {a / E->L[0], b / E->L[1], c / E->L[2]};
+                const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+                if (m2 > mmax * mmax) continue;
+                E->idx[3 * E->nk] = a; E->idx[3 * E->nk + 1] = b; E->idx[3 * E->nk + 2] = c;
+                E->coef[E->nk] = 2.0 * OR_COULOMB * exp(-OR_PI * OR_PI * m2 / (alpha * alpha)) / (OR_PI * V * m2);
+                E->nk++;
+            }
+    E->sre = calloc((size_t)E->nk, sizeof(double));
+    E->sim = calloc((size_t)E->nk, sizeof(double));
+    return (E->sre && E->sim) ? 0 : -1;
+}
+
+/* e^{2 pi i n x / L} for n = -N..N by repeated multiplication */
+static void ewald_powers(double x, double L, int N, double* re, double* im) {
+    const double th = 2.0 * OR_PI * x / L;
+    const double c = cos(th), s2 = sin(th);
+    re[N] = 1.0; im[N] = 0.0;
+    for (int k = 1; k <= N; ++k) {
+        re[N + k] = re[N + k - 1] * c - im[N + k - 1] * s2;
+        im[N + k] = re[N + k - 1] * s2 + im[N + k - 1] * c;
+        re[N - k] = re[N + k]; im[N - k] = -im[N + k];
+    }
+}
+
+static void ewald_term(const ewald_t* E, const double r[3], double* wre, double* wim, double* tmp) {
+    /* tmp: 6 * (2N+1) doubles; (wre, wim)[k] = e^{2 pi i m_k . r} */
+    const int N0 = E->n[0], N1 = E->n[1], N2 = E->n[2];
+    double *xr = tmp, *xi = xr + 2 * N0 + 1, *yr = xi + 2 * N0 + 1, *yi = yr + 2 * N1 + 1, *zr = yi + 2 * N1 + 1,
+           *zi = zr + 2 * N2 + 1;
+    ewald_powers(r[0], E->L[0], N0, xr, xi);
+    ewald_powers(r[1], E->L[1], N1, yr, yi);
+    ewald_powers(r[2], E->L[2], N2, zr, zi);
+    for (int k = 0; k < E->nk; ++k) {
+        const int a = E->idx[3 * k] + N0, b = E->idx[3 * k + 1] + N1, c = E->idx[3 * k + 2] + N2;
+        const double pr = xr[a] * yr[b] - xi[a] * yi[b], pi = xr[a] * yi[b] + xi[a] * yr[b];
+        wre[k] = pr * zr[c] - pi * zi[c];
+        wim[k] = pr * zi[c] + pi * zr[c];
+    }
+}
+
+static int ewald_tmp_size(const ewald_t* E) { return 2 * (2 * E->n[0] + 1 + 2 * E->n[1] + 1 + 2 * E->n[2] + 1); }
+
+/* S(m) of the fixed atoms and occupied slots */
+static void ewald_structure(ewald_t* E, const or_info* info, const or_atomarray* frag, const or_residue* res,
+                            const or_atom* atoms, int threads) {
+    memset(E->sre, 0, sizeof(double) * E->nk);
+    memset(E->sim, 0, sizeof(double) * E->nk);
+    const int nfix = frag[0].startRes;
+    /* atom list of the occupied groups */
+    int na = 0;
+    for (int t = -1; t < info->fragTypeNum; ++t) {
+        const int g0 = t < 0 ? 0 : frag[t].startRes, g1 = t < 0 ? nfix : g0 + frag[t].totalNum;
+        for (int g = g0; g < g1; ++g) na += res[g].atomNum;
+    }
+    int* list = malloc(sizeof(int) * (size_t)(na > 0 ? na : 1));
+    na = 0;
+    for (int t = -1; t < info->fragTypeNum; ++t) {
+        const int g0 = t < 0 ? 0 : frag[t].startRes, g1 = t < 0 ? nfix : g0 + frag[t].totalNum;
+        for (int g = g0; g < g1; ++g)
+            for (int a = 0; a < res[g].atomNum; ++a) list[na++] = res[g].atomStart + a;
+    }
+#pragma omp parallel num_threads(threads)
+    {
+        double* wre = malloc(sizeof(double) * E->nk);
+        double* wim = malloc(sizeof(double) * E->nk);
+        double* tmp = malloc(sizeof(double) * ewald_tmp_size(E));
+        double* are = calloc((size_t)E->nk, sizeof(double));
+        double* aim = calloc((size_t)E->nk, sizeof(double));
+#pragma omp for schedule(static)
+        for (int j = 0; j < na; ++j) {
+            const or_atom* A = &atoms[list[j]];
+            const double r[3] = {A->position[0], A->position[1], A->position[2]};
+            ewald_term(E, r, wre, wim, tmp);
+            for (int k = 0; k < E->nk; ++k) {
+                are[k] += A->charge * wre[k];
+                aim[k] += A->charge * wim[k];
+            }
+        }
+#pragma omp critical
+        for (int k = 0; k < E->nk; ++k) {
+            E->sre[k] += are[k];
+            E->sim[k] += aim[k];
+        }
+        free(wre); free(wim); free(tmp); free(are); free(aim);
+    }
+    free(list);
+}
+
+/* phi(r) = sum_half coef (Re S cos th + Im S sin th), th = 2 pi m.r; work: 2*nk + tmp */
+static double ewald_phi(const ewald_t* E, const double r[3], double* work) {
+    double* wre = work;
+    double* wim = work + E->nk;
+    ewald_term(E, r, wre, wim, work + 2 * E->nk);
+    double p = 0.0;
+    for (int k = 0; k < E->nk; ++k) p += E->coef[k] * (E->sre[k] * wre[k] + E->sim[k] * wim[k]);
+    return p;
+}
+
+void or_ewald_potential(const or_info* info, const or_atomarray* frag, const or_residue* res, const or_atom* atoms,
+                        double alpha, const double* pts, int32_t n, double* out, int32_t threads) {
+    if (threads <= 0) threads = 1;
+    ewald_t E;
+    if (ewald_init(&E, info, alpha) != 0) { ewald_free(&E); return; }
+    ewald_structure(&E, info, frag, res, atoms, threads);
+#pragma omp parallel num_threads(threads)
+    {
+        double* work = malloc(sizeof(double) * (2 * E.nk + ewald_tmp_size(&E)));
+#pragma omp for schedule(dynamic, 4)
+        for (int i = 0; i < n; ++i) out[i] = ewald_phi(&E, pts + 3 * i, work);
+        free(work);
+    }
+    ewald_free(&E);
+}
+
+/* g(r) = erf(alpha r) / r, g(0) = 2 alpha / sqrt(pi) */
+static inline double ewald_g(double r, double alpha) {
+    return r < 1e-10 ? 2.0 * alpha / sqrt(OR_PI) : erf(alpha * r) / r;
+}
+
+/* Reciprocal-space and molecular terms of a pose energy (see the engine's
+ * PME description): sum_s q_s phi(r_s), minus, when the pose replaces the
+ * occupied group `self`, K sum_{s,t} q_s q_t g(|r_s - x_t|) over that group's
+ * current atoms x_t (minimum image). */
+static double ewald_pose_terms(const ewald_t* E, const or_info* info, const or_residue* res, const or_atom* atoms,
+                               const float (*sx)[3], const float* sq, int ns, int self, double alpha, double* work) {
+    double e = 0.0;
+    for (int s2 = 0; s2 < ns; ++s2) {
+        const double r[3] = {sx[s2][0], sx[s2][1], sx[s2][2]};
+        e += (double)sq[s2] * ewald_phi(E, r, work);
+    }
+    if (self >= 0) {
+        const or_residue* R = &res[self];
+        double m = 0.0;
+        for (int s2 = 0; s2 < ns; ++s2)
+            for (int t = 0; t < R->atomNum; ++t) {
+                const or_atom* A = &atoms[R->atomStart + t];
+                double d2 = 0.0;
+                for (int c = 0; c < 3; ++c) {
+                    double d = (double)sx[s2][c] - (double)A->position[c];
+                    d -= fast_round_d(d / info->cryst[c]) * info->cryst[c];
+                    d2 += d * d;
+                }
+                m += (double)sq[s2] * (double)A->charge * ewald_g(sqrt(d2), alpha);
+            }
+        e -= OR_COULOMB * m;
+    }
+    return e;
+}
+
+/* Total charge of the fixed atoms and occupied slots. */
+static double total_charge(const or_info* info, const or_atomarray* frag, const or_residue* res,
+                           const or_atom* atoms) {
+    double Q = 0.0;
+    for (int t = -1; t < info->fragTypeNum; ++t) {
+        const int g0 = t < 0 ? 0 : frag[t].startRes, g1 = t < 0 ? frag[0].startRes : g0 + frag[t].totalNum;
+        for (int g = g0; g < g1; ++g)
+            for (int a = 0; a < res[g].atomNum; ++a) Q += atoms[res[g].atomStart + a].charge;
+    }
+    return Q;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Moves and the step loop.                                                   */
 /* ------------------------------------------------------------------------- */
 typedef struct {
@@ -703,7 +925,37 @@ typedef struct {
     double* forces;
     double* fscale;
     const float* replay_forces;
+    /* Ewald electrostatics (opt->pme): structure factors of the step's state */
+    ewald_t* ew;
 } sysref;
+
+/* A trial pose's energy: real space (erfc kernel under Ewald) plus, under
+ * Ewald, the reciprocal-space and molecular terms; *l1 = sum of |real-space
+ * pair terms| plus sum |q_s phi(r_s)| and |molecular terms|. */
+static double step_pose_energy(const sysref* S, const float (*sx)[3], const float* sq, const int32_t* st, int ns,
+                               const float centre[3], int self, double* l1) {
+    const or_info* info = S->info;
+    if (!S->opt->pme)
+        return or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, sx, sq, st, ns, centre, self, 0, NULL, NULL,
+                                 l1);
+    const double alpha = S->opt->pme_alpha;
+    double lr = 0.0;
+    double e = pose_energy64a(info, S->frag, S->res, S->atoms, S->ff, sx, sq, st, ns, centre, self, alpha, &lr);
+    double* work = malloc(sizeof(double) * (2 * S->ew->nk + ewald_tmp_size(S->ew)));
+    const double er = ewald_pose_terms(S->ew, info, S->res, S->atoms, sx, sq, ns, self, alpha, work);
+    free(work);
+    if (l1) *l1 = lr + fabs(er);
+    return e + er;
+}
+
+/* Change of the neutralising-background energy -K pi Q^2 / (2 V alpha^2) when the
+ * total charge goes from Q to Q + dq. */
+static double background_change(const sysref* S, double Q, double dq) {
+    const or_info* info = S->info;
+    const double V = (double)info->cryst[0] * info->cryst[1] * info->cryst[2];
+    const double a = S->opt->pme_alpha;
+    return -OR_COULOMB * OR_PI * ((Q + dq) * (Q + dq) - Q * Q) / (2.0 * V * a * a);
+}
 
 /* FP64 force and torque (about the site centroid) on a pose of float sites:
  * f = (F, tau) with F = -sum_s dE/dx_s, tau = -sum_s (x_s - m) x dE/dx_s;
@@ -800,8 +1052,13 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
 #pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
         for (int i = 0; i < k; ++i) {
             or_insert_pose(info, S->frag, S->grid, S->opt, f, step, i, xyz[i], cen[i]);
-            E[i] = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
-                                     sq, st, ns, cen[i], -1, 0, NULL, NULL, &l1[i]);
+            E[i] = step_pose_energy(S, (const float (*)[3])xyz[i], sq, st, ns, cen[i], -1, &l1[i]);
+        }
+        if (S->opt->pme) {  /* neutralising background: Q -> Q + q_fragment */
+            double qf = 0.0;
+            for (int s2 = 0; s2 < ns; ++s2) qf += sq[s2];
+            const double bg = background_change(S, total_charge(info, S->frag, S->res, S->atoms), qf);
+            for (int i = 0; i < k; ++i) E[i] += bg;
         }
         double esum = 0.0;
         for (int i = 0; i < k; ++i) {
@@ -845,8 +1102,12 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         for (int s = 0; s < ns; ++s)
             for (int j = 0; j < 3; ++j) xyz[s][j] = S->atoms[R->atomStart + s].position[j];
         double l1 = 0.0;
-        double E = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz, sq, st,
-                                     ns, R->position, F->startRes + slot, 0, NULL, NULL, &l1);
+        double E = step_pose_energy(S, (const float (*)[3])xyz, sq, st, ns, R->position, F->startRes + slot, &l1);
+        if (S->opt->pme) {  /* the removal changes Q by -q_fragment; E is minus the system's change */
+            double qf = 0.0;
+            for (int s2 = 0; s2 < ns; ++s2) qf += sq[s2];
+            E -= background_change(S, total_charge(info, S->frag, S->res, S->atoms), -qf);
+        }
         if (Eout) Eout[0] = E;
         if (Escale) Escale[0] = l1;
         double Ed = Ereplay ? Ereplay[0] : E;
@@ -870,6 +1131,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         }
     } else if (S->opt->proposal == 2) {
         /* force-biased translate/rotate with the Metropolis-Hastings correction */
+        if (S->opt->pme) return -4; /* force bias runs without Ewald */
         int n = F->totalNum;
         k = F->confBias < n ? F->confBias : n;
         if (k == 0) goto done;
@@ -1010,11 +1272,11 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
             for (int s = 0; s < ns; ++s)
                 for (int j = 0; j < 3; ++j) old[s][j] = S->atoms[R->atomStart + s].position[j];
             double lo = 0.0, ln = 0.0;
-            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
-                                          st, ns, R->position, F->startRes + slot, 0, NULL, NULL, &lo);
+            double Eo = step_pose_energy(S, (const float (*)[3])old, sq, st, ns, R->position, F->startRes + slot,
+                                         &lo);
             or_move_pose(info, S->frag, S->res, S->atoms, S->opt, f, m, step, i, slot, xyz[i], cen[i]);
-            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i],
-                                          sq, st, ns, cen[i], F->startRes + slot, 0, NULL, NULL, &ln);
+            double En = step_pose_energy(S, (const float (*)[3])xyz[i], sq, st, ns, cen[i], F->startRes + slot,
+                                         &ln);
             dE[i] = En - Eo;
             sc[i] = ln + lo;
         }
@@ -1060,17 +1322,25 @@ int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_
                    const double* replay, int32_t kmax, int32_t threads, double* e_total,
                    double* forces, double* fscale, const float* replay_forces) {
     if (threads <= 0) threads = 1;
-    for (int s = 0; s < nsteps; ++s) {
+    ewald_t ew;
+    memset(&ew, 0, sizeof(ew));
+    if (opt->pme && ewald_init(&ew, info, opt->pme_alpha) != 0) {
+        ewald_free(&ew);
+        return -5;
+    }
+    int rc = 0;
+    for (int s = 0; s < nsteps && rc == 0; ++s) {
         int step = step0 + s;
+        if (opt->pme) ewald_structure(&ew, info, frag, res, atoms, threads);
         sysref S = {info, frag, res, atoms, grid, ff, opt, e_total,
                     forces ? forces + (size_t)s * kmax * 12 : NULL, fscale ? fscale + (size_t)s * kmax * 4 : NULL,
-                    replay_forces ? replay_forces + (size_t)s * kmax * 12 : NULL};
-        int rc = do_step(&S, moves, step, log ? &log[s] : NULL, energies ? energies + (size_t)s * kmax : NULL,
-                         escale ? escale + (size_t)s * kmax : NULL, replay ? replay + (size_t)s * kmax : NULL,
-                         kmax, threads);
-        if (rc) return rc;
+                    replay_forces ? replay_forces + (size_t)s * kmax * 12 : NULL, opt->pme ? &ew : NULL};
+        rc = do_step(&S, moves, step, log ? &log[s] : NULL, energies ? energies + (size_t)s * kmax : NULL,
+                     escale ? escale + (size_t)s * kmax : NULL, replay ? replay + (size_t)s * kmax : NULL,
+                     kmax, threads);
     }
-    return 0;
+    ewald_free(&ew);
+    return rc;
 }
 
 int64_t or_energy_batch(const or_info* info, const or_atomarray* frag, const or_residue* res,

@@ -69,9 +69,11 @@ typedef struct {
     float trn_step;     /* symmetric translate: cube edge (A)                   */
     float rot_max;      /* symmetric rotate: max angle (rad)                    */
     uint32_t replica;   /* RNG stream id                                        */
-    float fb_trn;       /* proposal 2: translate step sigma_t (A)               */
-    float fb_rot;       /* proposal 2: rotation step sigma_r (rad)              */
-    int32_t reserved;
+    float fb_trn;       /* proposal 2: translate half-width (A)                 */
+    float fb_rot;       /* proposal 2: rotation half-width (rad)                */
+    int32_t pme;        /* 1: Ewald electrostatics (erfc real space, exact k-space
+                           potential of the environment, background term)       */
+    float pme_alpha;    /* Ewald splitting parameter (1/A)                      */
 } or_options;
 
 /* Per-step record; identical layout to gcmc_step_log in include/gcmc_b200.h. */
@@ -152,6 +154,13 @@ int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_
                    int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,
                    const double* replay_energies, int32_t kmax, int32_t threads, double* e_total,
                    double* forces, double* fscale, const float* replay_forces);
+
+/* Ewald reciprocal-space potential of the current state (fixed atoms and
+ * occupied slots) at n points: phi(r) = (K / (pi V)) sum_{m != 0}
+ * exp(-pi^2 m^2 / alpha^2) / m^2 Re[S(m) exp(-2 pi i m.r)], S(m) = sum_j q_j
+ * exp(2 pi i m.r_j), summed over all m with exp(-pi^2 m^2 / alpha^2) > 1e-13. */
+void or_ewald_potential(const or_info* info, const or_atomarray* frag, const or_residue* res, const or_atom* atoms,
+                        double alpha, const double* pts, int32_t n, double* out, int32_t threads);
 
 /* Own float log and exp(x <= 0), identical to the engine's (force-biased proposals). */
 float or_det_log(float x);

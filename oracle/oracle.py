@@ -17,7 +17,7 @@ c_void = ctypes.c_void_p
 class OrOptions(ctypes.Structure):
     _fields_ = [("proposal", ctypes.c_int32), ("muex_kcal", ctypes.c_int32), ("trn_step", ctypes.c_float),
                 ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("fb_trn", ctypes.c_float),
-                ("fb_rot", ctypes.c_float), ("reserved", ctypes.c_int32)]
+                ("fb_rot", ctypes.c_float), ("pme", ctypes.c_int32), ("pme_alpha", ctypes.c_float)]
 
 
 def build():
@@ -39,6 +39,8 @@ def lib():
                                                 ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void]
         L.or_det_log.restype = ctypes.c_float
         L.or_det_log.argtypes = [ctypes.c_float]
+        L.or_ewald_potential.argtypes = [c_void] * 4 + [ctypes.c_double, c_void, ctypes.c_int32, c_void,
+                                                        ctypes.c_int32]
         L.or_det_exp_neg.restype = ctypes.c_float
         L.or_det_exp_neg.argtypes = [ctypes.c_float]
         L.or_run.restype = ctypes.c_int32
@@ -74,8 +76,19 @@ def _p(a):
 
 
 def options(proposal=0, muex_kcal=0, trn_step=1.0, rot_max=np.radians(15.0), replica=0, fb_trn=0.5,
-            fb_rot=np.radians(10.0)):
-    return OrOptions(proposal, muex_kcal, trn_step, rot_max, replica, fb_trn, fb_rot, 0)
+            fb_rot=np.radians(10.0), pme=0, pme_alpha=0.32):
+    return OrOptions(proposal, muex_kcal, trn_step, rot_max, replica, fb_trn, fb_rot, pme, pme_alpha)
+
+
+def ewald_potential(system, alpha, pts, threads=None):
+    """Exact Ewald reciprocal-space potential (kJ/mol/e) of the state at points [n, 3]."""
+    threads = threads or os.cpu_count() or 1
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(len(pts))
+    s = system
+    lib().or_ewald_potential(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), float(alpha),
+                             _p(pts), len(pts), _p(out), threads)
+    return out
 
 
 def run_ext(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, replay_forces=None,

@@ -20,7 +20,8 @@ class Options(ctypes.Structure):
                 ("rot_max", ctypes.c_float), ("replica", ctypes.c_uint32), ("cells_per_cutoff", c_int),
                 ("log_steps", c_int), ("log_kmax", c_int), ("split_items", c_int), ("branches", c_int),
                 ("energy_blocks_per_sm", c_int), ("fb_trn", ctypes.c_float), ("fb_rot", ctypes.c_float),
-                ("step_offset", ctypes.c_uint32)]
+                ("step_offset", ctypes.c_uint32), ("pme", c_int), ("pme_alpha", ctypes.c_float),
+                ("pme_grid", c_int * 3)]
 
 
 class TuneTrial(ctypes.Structure):
@@ -63,6 +64,7 @@ def lib():
         "gcmc_run_gcmc": (c_int, [c_void] * 7 + [P(Options)]),
         "gcmc_last_status": (c_int, []),
         "gcmc_release_cache": (c_int, []),
+        "gcmc_pme_potential": (c_int, [c_void, c_int, c_void, c_int, c_void]),
         "gcmc_pdb_fragment_lines": (ctypes.c_int64, [c_int, c_void, c_void, c_void, c_void, ctypes.c_int64,
                                                      ctypes.c_int64, c_void, ctypes.c_int64]),
         "gcmc_cavity_grid": (c_int, [c_int, c_void, c_void, ctypes.c_double, c_int, c_void, c_void, ctypes.c_int64,
@@ -132,7 +134,7 @@ def default_options(**kw):
     return o
 
 
-EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_get_forces",
+EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_get_forces", "gcmc_pme_potential",
            "gcmc_cavity_grid", "gcmc_fix_groups", "gcmc_group_centres", "gcmc_fill_layout", "gcmc_pdb_fragment_lines",
            "gcmc_energy_total", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",

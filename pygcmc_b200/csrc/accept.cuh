@@ -259,6 +259,14 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
 
     // ---- phase 0: pose energies (sum of slab partials; dE for translate/rotate)
     const bool logging = R.log != nullptr && D.step < R.log_cap;
+    double bg = 0.0;  // Ewald: change of the neutralising-background energy -bgc Q^2
+    if (R.pme && (D.move == MV_INSERT || D.move == MV_DELETE)) {
+        double Q = R.pme_qfix;
+        for (int t = 0; t < R.ntypes; ++t) Q += (double)R.totalNum[t] * R.frag[t].qnet;
+        const double dq = D.move == MV_INSERT ? F.qnet : -F.qnet;
+        const double change = -R.pme_bgc * ((Q + dq) * (Q + dq) - Q * Q);
+        bg = D.move == MV_INSERT ? change : -change;  // a deletion's E is minus the system's change
+    }
     for (int i = tid; i < k; i += nt) {
         double e = 0.0;
         for (int z = 0; z < D.nslab; ++z) e += R.epart[(i * D.nvar) * D.nslab + z];
@@ -267,6 +275,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             for (int z = 0; z < D.nslab; ++z) eo += R.epart[(i * 2 + 1) * D.nslab + z];
             e = e - eo;
         }
+        e += bg;
         S.ephys[i] = e;
         if (D.fb) {  // Metropolis-Hastings: exp(-beta dE) q(new -> old) / q(old -> new)
             float fo[6], fn[6];

@@ -321,6 +321,7 @@ __host__ __device__ __forceinline__ int perm_bits(int n) {
 struct FragDev {
     int startRes, maxNum, confBias, nsites;
     double B;                  // beta*muex_eff + ln(V*conc*6.023e-4)
+    double qnet;               // sum of the site charges (Ewald background term)
     float4 site[kMaxSites];    // template x, y, z, charge
     int stype[kMaxSites];      // template type
 };
@@ -402,6 +403,15 @@ struct RepDev {
     float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (a0, a1, a2, 0) of the old pose
     int* fbcnt;         // [kMaxPoses] old-pose items finished (reset by the last one)
     float* logF;        // [log_cap * log_kmax * 12] F_old, tau_old, F_new, tau_new used
+    // Ewald electrostatics by smooth PME (pme = 1): real-space Coulomb erfc(alpha r)/r,
+    // the reciprocal-space potential phi of the current state on a mesh (FP64),
+    // interpolated at trial sites with order-4 B-splines
+    int pme;
+    float pme_alpha;
+    int pme_n[3];
+    const double* pme_phi;  // [n0 * n1 * n2] theta_rec * Q (kJ/mol/e)
+    double pme_bgc;         // K pi / (2 V alpha^2): background energy -bgc Q^2
+    double pme_qfix;        // total charge of the fixed atoms
 };
 
 __device__ __forceinline__ int wrapi(int c, int n) {

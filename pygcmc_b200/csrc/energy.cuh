@@ -17,6 +17,7 @@
 //      pose-pose "within cutoff" bit matrix (host distance form, bit-exact).
 #pragma once
 #include "common.cuh"
+#include "pme.cuh"
 
 namespace gcmc {
 
@@ -34,6 +35,7 @@ struct WarpBuf {
     int cand[kCCap];         // candidate group ids gathered from the cells
     float cs_hi[3][4];       // pose centre + image shift (code 0: 0, 1: +L, 2: -L), high part
     float cs_lo[3][4];       //   and its exact rounding error (TwoSum)
+    float4 site_abs[kMaxSites];  // absolute site position, raw charge (Ewald terms)
 };
 
 // Exact split of c + t into hi + lo (Knuth's TwoSum).
@@ -73,7 +75,7 @@ __device__ __forceinline__ float image_shift(uint32_t code2, float L) {
 // of an included group lies within half a box, checked at set-up); true:
 // per-pair minimum image as in gcmc_energy.h:115-122.  1/r is rsqrt refined by
 // one Newton step; each atom's site terms are summed in FP32, atoms in FP64.
-template <bool PairImage>
+template <bool PairImage, bool Ewald>
 __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
                                               double& acc) {
     for (int f = lane; f < na; f += 32) {
@@ -114,7 +116,8 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
             const float s2 = p.x * ir2;
             const float s6 = s2 * s2 * s2;
             e = fmaf(p.y, fmaf(s6, s6, -s6), e);
-            e = fmaf(sp.w * a.w, ir, e);
+            if (Ewald) e = fmaf(sp.w * a.w * erfcf(R.pme_alpha * (r2 * ir)), ir, e);
+            else e = fmaf(sp.w * a.w, ir, e);
         }
         acc += (double)e;
     }
@@ -122,8 +125,13 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
 
 __device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
                                             double& acc) {
-    if (R.pair_image) flush_atoms_t<true>(R, B, na, ns, lane, acc);
-    else flush_atoms_t<false>(R, B, na, ns, lane, acc);
+    if (R.pme) {
+        if (R.pair_image) flush_atoms_t<true, true>(R, B, na, ns, lane, acc);
+        else flush_atoms_t<false, true>(R, B, na, ns, lane, acc);
+    } else {
+        if (R.pair_image) flush_atoms_t<true, false>(R, B, na, ns, lane, acc);
+        else flush_atoms_t<false, false>(R, B, na, ns, lane, acc);
+    }
 }
 
 // What the cell walk does with each buffer of included atoms: the energy
@@ -476,6 +484,7 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
             const float sx = fadd(x, cx), sy = fadd(y, cy), sz = fadd(z, cz);
             B.site[lane] = make_float4((float)((double)sx - (double)cx), (float)((double)sy - (double)cy),
                                        (float)((double)sz - (double)cz), kCoulomb * t.w);
+            B.site_abs[lane] = make_float4(sx, sy, sz, t.w);
             B.srow[lane] = F.stype[lane] * R.ffY;
         }
         __syncwarp();
@@ -502,9 +511,11 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
         if (D.fb) fb_moved_site(R, D, i, gc, ns, lane, px, py, pz);
         else moved_site(R, D, i, gc, ns, lane, px, py, pz);
     }
-    if (lane < ns)
+    if (lane < ns) {
         B.site[lane] = make_float4((float)((double)px - (double)cx), (float)((double)py - (double)cy),
                                    (float)((double)pz - (double)cz), kCoulomb * F.site[lane].w);
+        B.site_abs[lane] = make_float4(px, py, pz, F.site[lane].w);
+    }
     __syncwarp();
 }
 
@@ -543,6 +554,10 @@ __global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy
         const int nwin = R.span[0] * R.span[1] * R.span[2];
         energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi * nwin / D.nslab,
                      (zi + 1) * nwin / D.nslab, lane, acc, ng, npair);
+        if (R.pme && zi == 0) {
+            const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
+            acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
+        }
         acc = warp_sum(acc);
         if (lane == 0) {
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
@@ -586,6 +601,7 @@ __global__ void __launch_bounds__(kWarpsE * 32)
             const double c0 = centres[3 * p], c1 = centres[3 * p + 1], c2 = centres[3 * p + 2];
             B.site[lane] = make_float4((float)((double)s[0] - c0), (float)((double)s[1] - c1),
                                        (float)((double)s[2] - c2), kCoulomb * q[lane]);
+            B.site_abs[lane] = make_float4(s[0], s[1], s[2], q[lane]);
             B.srow[lane] = type[lane] * R.ffY;
         }
         __syncwarp();
@@ -595,6 +611,10 @@ __global__ void __launch_bounds__(kWarpsE * 32)
         const int nwin = R.span[0] * R.span[1] * R.span[2];
         energy_cells(R, B, ns, centres[3 * p], centres[3 * p + 1], centres[3 * p + 2], self ? self[p] : -1,
                      z * nwin / nslab, (z + 1) * nwin / nslab, lane, acc, ng, npair);
+        if (R.pme && z == 0) {
+            const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
+            acc += pme_pose_lane(R, ns, lane, a.x, a.y, a.z, a.w, self ? self[p] : -1);
+        }
         acc = warp_sum(acc);
         if (lane == 0) {
             out[it] = acc;

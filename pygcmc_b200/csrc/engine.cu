@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <cufft.h>
+
 #include "accept.cuh"
 #include "grad.cuh"
 
@@ -58,6 +60,17 @@ struct RepHost {
     float4* fbprop = nullptr;
     int* fbcnt = nullptr;
     float* logF = nullptr;
+    // smooth PME (Ewald runs)
+    int pme = 0;
+    int pme_n[3] = {0, 0, 0};
+    int nfix_atoms = 0;
+    double* pme_qfix = nullptr;   // fixed atoms' spread charges
+    double* pme_q = nullptr;      // this step's spread charges
+    double* pme_phi = nullptr;    // potential on the mesh
+    double2* pme_spec = nullptr;  // half spectrum
+    double* pme_g = nullptr;      // influence function on the half spectrum
+    cufftHandle plan_f = 0, plan_b = 0;
+    bool plans = false;
 };
 
 }  // namespace
@@ -122,6 +135,12 @@ void free_rep(RepHost& h) {
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
     dfree(h.energy); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
+    dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
+    if (h.plans) {
+        cufftDestroy(h.plan_f);
+        cufftDestroy(h.plan_b);
+        h.plans = false;
+    }
     for (auto& c : h.capn) c = 0;
 }
 
@@ -188,6 +207,51 @@ int validate(const gcmc_replica_in& in) {
     }
     if (any_insert && (I->totalGridNum < 1 || !in.grid)) return GCMC_ERR_ARG;
     return GCMC_OK;
+}
+
+// smallest n' >= n whose prime factors are 2, 3, 5, 7 (fast FFT sizes)
+int smooth_size(int n) {
+    for (int m = std::max(n, 1);; ++m) {
+        int x = m;
+        for (int p : {2, 3, 5, 7})
+            while (x % p == 0) x /= p;
+        if (x == 1) return m;
+    }
+}
+
+// Smooth-PME influence function on the half spectrum (FP64):
+// G(m) = K exp(-pi^2 m^2 / alpha^2) / (pi V m^2) * prod_d |b_d(k_d)|^2, G(0) = 0,
+// |b(k)|^2 = 1 / |sum_{j=0}^{2} M4(j + 1) e^{2 pi i k j / n}|^2 (order-4 B-spline moduli).
+void pme_influence(const int n[3], const float cryst[3], double alpha, double* G) {
+    const double V = (double)cryst[0] * cryst[1] * cryst[2];
+    const double M4[3] = {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0};
+    std::vector<double> bm[3];
+    for (int a = 0; a < 3; ++a) {
+        bm[a].resize(n[a]);
+        for (int k = 0; k < n[a]; ++k) {
+            double re = 0.0, im = 0.0;
+            for (int j = 0; j < 3; ++j) {
+                const double th = 2.0 * M_PI * k * j / n[a];
+                re += M4[j] * std::cos(th);
+                im += M4[j] * std::sin(th);
+            }
+            bm[a][k] = 1.0 / (re * re + im * im);
+        }
+    }
+    const int nh = n[2] / 2 + 1;
+    for (int i = 0; i < n[0]; ++i)
+        for (int j = 0; j < n[1]; ++j)
+            for (int k = 0; k < nh; ++k) {
+                const double m0 = (i <= n[0] / 2 ? i : i - n[0]) / (double)cryst[0];
+                const double m1 = (j <= n[1] / 2 ? j : j - n[1]) / (double)cryst[1];
+                const double m2 = k / (double)cryst[2];
+                const double mm = m0 * m0 + m1 * m1 + m2 * m2;
+                double g = 0.0;
+                if (mm > 0.0)
+                    g = (double)kCoulomb * std::exp(-M_PI * M_PI * mm / (alpha * alpha)) / (M_PI * V * mm) *
+                        bm[0][i] * bm[1][j] * bm[2][k];
+                G[((size_t)i * n[1] + j) * nh + k] = g;
+            }
 }
 
 int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
@@ -331,6 +395,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
             F.site[s] = make_float4(f.atoms[s].position[0], f.atoms[s].position[1], f.atoms[s].position[2],
                                     f.atoms[s].charge);
             F.stype[s] = f.atoms[s].type;
+            F.qnet += (double)f.atoms[s].charge;
         }
         tot[t] = f.totalNum;
         h.startRes.push_back(f.startRes);
@@ -352,6 +417,46 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.counters, 16); AL(h.err, 1);
     AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
     AL(h.fbcnt, kMaxPoses);
+    // smooth PME: mesh, influence function, FFT plans
+    h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
+    if (h.pme && opt.proposal == 2) return GCMC_ERR_ARG;  // force bias runs without Ewald
+    d.pme = h.pme ? 1 : 0;
+    h.nfix_atoms = d.nfixed > 0 ? in.residueInfo[d.nfixed - 1].atomStart + in.residueInfo[d.nfixed - 1].atomNum : 0;
+    if (h.pme) {
+        const double alpha = opt.pme_alpha > 0.0f ? opt.pme_alpha : 0.32;
+        d.pme_alpha = (float)alpha;
+        int n[3];
+        for (int a = 0; a < 3; ++a) {
+            n[a] = opt.pme_grid[a] > 0 ? opt.pme_grid[a] : smooth_size((int)std::ceil(I->cryst[a] / 1.2));
+            if (n[a] < 8) return GCMC_ERR_ARG;
+            d.pme_n[a] = n[a];
+        }
+        const size_t nr = (size_t)n[0] * n[1] * n[2], nh = (size_t)n[0] * n[1] * (n[2] / 2 + 1);
+        AL(h.pme_qfix, nr); AL(h.pme_q, nr); AL(h.pme_phi, nr); AL(h.pme_spec, nh); AL(h.pme_g, nh);
+        std::vector<double> G(nh);
+        pme_influence(n, I->cryst, alpha, G.data());
+        CK(cudaMemcpyAsync(h.pme_g, G.data(), sizeof(double) * nh, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(h.pme_phi, 0, sizeof(double) * nr, ctx->stream));
+        if (!h.plans || n[0] != h.pme_n[0] || n[1] != h.pme_n[1] || n[2] != h.pme_n[2]) {
+            if (h.plans) {
+                cufftDestroy(h.plan_f);
+                cufftDestroy(h.plan_b);
+                h.plans = false;
+            }
+            if (cufftPlan3d(&h.plan_f, n[0], n[1], n[2], CUFFT_D2Z) != CUFFT_SUCCESS) return GCMC_ERR_CUDA;
+            if (cufftPlan3d(&h.plan_b, n[0], n[1], n[2], CUFFT_Z2D) != CUFFT_SUCCESS) {
+                cufftDestroy(h.plan_f);
+                return GCMC_ERR_CUDA;
+            }
+            h.plans = true;
+        }
+        for (int a = 0; a < 3; ++a) h.pme_n[a] = n[a];
+        d.pme_phi = h.pme_phi;
+        d.pme_bgc = (double)kCoulomb * M_PI / (2.0 * V * alpha * alpha);
+        double qf = 0.0;
+        for (int a = 0; a < h.nfix_atoms; ++a) qf += (double)in.atomInfo[a].charge;
+        d.pme_qfix = qf;
+    }
     h.log_cap = std::max(0, std::min(opt.log_steps, h.mcsteps));
     h.log_kmax = std::max(1, std::min(opt.log_kmax > 0 ? opt.log_kmax : 1, kMaxPoses));
     if (h.log_cap > 0) {
@@ -395,6 +500,40 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.counters = h.counters; d.err = h.err;
     d.energy = h.energy; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
     d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
+    return GCMC_OK;
+}
+
+// Rebuild replica r's PME mesh potential from its current state on stream s:
+// Q = Q_fixed + spread(occupied fragment atoms); phi = IFFT(G * FFT(Q)).
+int pme_update(gcmc_ctx* ctx, int r, cudaStream_t s) {
+    RepHost& h = ctx->reps[r];
+    if (!h.pme) return GCMC_OK;
+    const size_t nr = (size_t)h.pme_n[0] * h.pme_n[1] * h.pme_n[2];
+    const size_t nh = (size_t)h.pme_n[0] * h.pme_n[1] * (h.pme_n[2] / 2 + 1);
+    CK(cudaMemcpyAsync(h.pme_q, h.pme_qfix, sizeof(double) * nr, cudaMemcpyDeviceToDevice, s));
+    k_pme_spread_frag<<<148, 256, 0, s>>>(ctx->d_reps + r, h.pme_q);
+    if (cufftSetStream(h.plan_f, s) != CUFFT_SUCCESS ||
+        cufftExecD2Z(h.plan_f, h.pme_q, reinterpret_cast<cufftDoubleComplex*>(h.pme_spec)) != CUFFT_SUCCESS)
+        return GCMC_ERR_CUDA;
+    k_pme_scale<<<(int)std::min<size_t>((nh + 255) / 256, 4096), 256, 0, s>>>(h.pme_spec, h.pme_g, nh);
+    if (cufftSetStream(h.plan_b, s) != CUFFT_SUCCESS ||
+        cufftExecZ2D(h.plan_b, reinterpret_cast<cufftDoubleComplex*>(h.pme_spec), h.pme_phi) != CUFFT_SUCCESS)
+        return GCMC_ERR_CUDA;
+    CK(cudaGetLastError());
+    return GCMC_OK;
+}
+
+// The fixed atoms' spread charges (once per set-up; needs d_reps uploaded).
+int pme_init_fixed(gcmc_ctx* ctx) {
+    for (int r = 0; r < ctx->nrep; ++r) {
+        RepHost& h = ctx->reps[r];
+        if (!h.pme) continue;
+        const size_t nr = (size_t)h.pme_n[0] * h.pme_n[1] * h.pme_n[2];
+        CK(cudaMemsetAsync(h.pme_qfix, 0, sizeof(double) * nr, ctx->stream));
+        if (h.nfix_atoms > 0)
+            k_pme_spread_range<<<296, 256, 0, ctx->stream>>>(ctx->d_reps + r, h.pme_qfix, 0, h.nfix_atoms);
+        CK(cudaGetLastError());
+    }
     return GCMC_OK;
 }
 
@@ -462,7 +601,9 @@ int build_graph(gcmc_ctx* ctx) {
             for (int r = r0; r < r0 + cnt; ++r) part += (double)ctx->reps[r].natoms + 1.0;
             const int grid = nb == 1 ? ctx->gridE : std::max(1, (int)std::ceil(ctx->gridE * part / tot));
             const int gridf = nb == 1 ? ctx->gridF : std::max(1, (int)std::ceil(ctx->gridF * part / tot));
-            for (int s = 0; s < kGraphSteps; ++s) {
+            for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) {
+                for (int r = r0; r < r0 + cnt; ++r)
+                    if (pme_update(ctx, r, side[b]) != GCMC_OK) e = cudaErrorUnknown;
                 if (ctx->fb) {
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
@@ -555,6 +696,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
         k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
         if (cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
     }
+    if (st == GCMC_OK) st = pme_init_fixed(ctx);
     if (st == GCMC_OK) st = build_graph(ctx);
     if (st == GCMC_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) {
@@ -590,6 +732,8 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
                        ctx->stream));
     k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
     CK(cudaGetLastError());
+    st = pme_init_fixed(ctx);
+    if (st != GCMC_OK) return st;
     const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
     const int fb = opt.proposal == 2 ? 1 : 0;
     if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb) {
@@ -876,6 +1020,10 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
     std::vector<cudaEvent_t> ev(3 * (size_t)need);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int i = 0; i < need; ++i) {
+        for (int r = 0; r < ctx->nrep; ++r) {
+            const int st = pme_update(ctx, r, ctx->stream);
+            if (st != GCMC_OK) return st;
+        }
         CK(cudaEventRecord(ev[3 * i], ctx->stream));
         if (ctx->fb) {
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
@@ -994,6 +1142,31 @@ int gcmc_energy_total(gcmc_ctx* ctx, int32_t rep, double* e_total) {
     return GCMC_OK;
 }
 
+int gcmc_pme_potential(gcmc_ctx* ctx, int32_t rep, const double* pts, int32_t n, double* out) {
+    if (!ctx || rep < 0 || rep >= ctx->nrep || n < 0 || (n > 0 && (!pts || !out))) return GCMC_ERR_ARG;
+    if (!ctx->reps[rep].pme) return GCMC_ERR_ARG;
+    if (n == 0) return GCMC_OK;
+    int st = pme_update(ctx, rep, ctx->stream);
+    if (st != GCMC_OK) return st;
+    double *dp = nullptr, *dout = nullptr;
+    if ((st = dalloc(&dp, (size_t)3 * n)) || (st = dalloc(&dout, (size_t)n))) {
+        dfree(dp);
+        return st;
+    }
+    cudaStream_t s = ctx->stream;
+    if (cudaMemcpyAsync(dp, pts, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (st == GCMC_OK) {
+        k_pme_phi_points<<<(n + 127) / 128, 128, 0, s>>>(ctx->d_reps + rep, dp, n, dout);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            st = GCMC_ERR_CUDA;
+    }
+    dfree(dp);
+    dfree(dout);
+    return st;
+}
+
 int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, int64_t* pairs) {
     if (!ctx || rep < 0 || rep >= ctx->nrep) return GCMC_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1048,6 +1221,7 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
             st = GCMC_ERR_CUDA;
             break;
         }
+        if ((st = pme_update(ctx, rep, s)) != GCMC_OK) break;
         k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->repdev[rep], dxyz, dq, dt, nsites, dc, dself,
                                                               nposes, nslab, dout, dng);
         if (cudaGetLastError() != cudaSuccess ||
@@ -1087,6 +1261,7 @@ int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float
     if (d_gff && (!d_ff || !d_gout)) return GCMC_ERR_ARG;
     if (nposes <= 0) return GCMC_OK;
     RepHost& h = ctx->reps[rep];
+    if (h.pme) return GCMC_ERR_ARG;  // gradients are of the plain-cutoff energy
     for (int s = 0; s < nsites; ++s)
         if (site_type[s] < 0 || site_type[s] >= h.ffX) return GCMC_ERR_ARG;
     const int nslab = h.nslab;
@@ -1207,6 +1382,10 @@ int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, co
     double* part = reinterpret_cast<double*>(scratch);
     int* ngpart = reinterpret_cast<int*>(part + kNoAllocMaxParts);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    {
+        const int pst = pme_update(ctx, rep, s);
+        if (pst != GCMC_OK) return pst;
+    }
     k_energy_explicit<<<ctx->gridE, kWarpsE * 32, 0, s>>>(ctx->repdev[rep], d_xyz, d_site_q, d_site_type, nsites,
                                                           d_centres, d_self, nposes, nslab, part, ngpart);
     k_sum_parts<<<(nposes + 255) / 256, 256, 0, s>>>(part, ngpart, nposes, nslab, d_out, d_ngroups);

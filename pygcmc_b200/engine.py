@@ -121,6 +121,13 @@ class Engine:
         check(lib().gcmc_get_forces(self._h, rep, ptr(out), n, ctypes.byref(got)), "gcmc_get_forces")
         return out[: got.value]
 
+    def pme_potential(self, pts, rep: int = 0):
+        """Ewald runs: reciprocal-space potential (kJ/mol/e) of the current state at points [n, 3]."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(len(pts))
+        check(lib().gcmc_pme_potential(self._h, rep, ptr(pts), len(pts), ptr(out)), "gcmc_pme_potential")
+        return out
+
     def energy_total(self, rep: int = 0) -> float:
         """Running sum of the accepted energy changes since creation (kJ/mol)."""
         e = ctypes.c_double(0.0)
