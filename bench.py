@@ -571,6 +571,86 @@ def run_ours_forcebias(args, ws, rank, local):
     return out
 
 
+LARGE_WORKLOAD = ("large periodic slab with Ewald electrostatics: 150 x 150 x 120 A box, 200000 fixed atoms "
+                  "(random-walk chains, 0.09 atoms/A^3, 12 A pore along z), 8 fragment types + TIP3P water "
+                  "(15827 waters, 178915 slots), smooth PME 128 x 128 x 96, order 4, alpha 0.32, FP64 mesh, "
+                  "cutoff 12 A, reference move semantics; REPLICAS replicas of the system (own RNG streams) "
+                  "in one context")
+
+
+def run_ours_large(args, ws, rank, local):
+    import torch
+    from pygcmc_b200 import system as S
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    from pygcmc_b200.gpu import runGCMC_batch
+    torch.cuda.set_device(local)
+    chunk = args.chunk
+    nrep = args.replicas
+    total = (args.warmup + args.steps) * chunk + 64 + 16
+    t0 = time.perf_counter()
+    base = S.slab_system(seed=args.seed + rank, mcsteps=total)
+    t_gen = time.perf_counter() - t0
+    opt = default_options(pme=1, pme_alpha=0.32, branches=min(4, nrep))
+    for a, n in enumerate((128, 128, 96)):
+        opt.pme_grid[a] = n
+    eng = Engine([base.copy() for _ in range(nrep)], opt)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    barrier(ws)
+    clocks = ClockSampler(local)
+    ms = max_over_ranks(time_engine(eng, stream, flush, chunk, args.warmup, args.steps), ws)
+    clk = clocks.stop()
+    c1 = [eng.counters(r) for r in range(nrep)]
+    te, ta, _ = eng.run_profiled(16)
+    c2 = [eng.counters(r) for r in range(nrep)]
+    eng.close()
+    # end to end: the batched drop-in with host arrays (all replicas per call)
+    state = [base.copy() for _ in range(nrep)]
+    for r, st in enumerate(state):
+        st.SimInfo[0]["mcsteps"] = chunk
+    h2d = sum(sum(a.nbytes for a in s_.arrays()[:6]) + 4 * chunk for s_ in state)
+    d2h = sum(s_.fragmentInfo.nbytes + s_.residueInfo.nbytes + s_.atomInfo.nbytes for s_ in state)
+    times = []
+    for k in range(args.warmup + min(args.steps, 3)):
+        for r, st in enumerate(state):
+            st.SimInfo[0]["seed"] = (args.seed * 7 + 131 * r + k) & 0xFFFFFFFF
+            st.moveArray = np.ascontiguousarray(base.moveArray[k * chunk:(k + 1) * chunk])
+        barrier(ws)
+        t0 = time.perf_counter()
+        runGCMC_batch(state, opt)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(times) * 1e3, ws) / 1e3
+    pairs = sum(b["pairs"] - a["pairs"] for a, b in zip(c1, c2))
+    e_ms, a_ms = float(te.sum()), float(ta.sum())
+    sm_max = (clk or {}).get("sm_max_mhz") or 1965.0
+    peak, sms = nominal_fp32_tflops(sm_max)
+    achieved = pairs * FLOPS_PER_PAIR / (e_ms / 1e3) / 1e12
+    return {
+        "metric": METRIC, "value": round(args.steps * chunk * nrep * ws / (ms / 1e3), 1), "unit": "moves/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair terms, fp64 sums/acceptance, fp64 PME mesh",
+        "data": "synthetic (seeded generator; no public dataset)",
+        "config": {"workload": LARGE_WORKLOAD.replace("REPLICAS", str(nrep)), "replicas_per_gpu": nrep,
+                   "mc_steps_per_bench_step": chunk, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (state + meshes of all replicas)", "generate_s": round(t_gen, 2),
+                   "proposals": "reference (force-biased moves run without Ewald)"},
+        "e2e": {"value": round(min(args.steps, 3) * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
+                "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+        "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies incl. erfc and PME interpolation)",
+                     "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 5), "flops_per_pair": FLOPS_PER_PAIR,
+                     "peak_source": f"nominal FP32: {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz",
+                     "avg_step_us_pme_and_energy": e_ms / 16 * 1e3, "avg_accept_us": a_ms / 16 * 1e3,
+                     "traffic": None},
+        "gpu_launches": args.steps * (2 + 32 * ((chunk + 31) // 32) * (2 * nrep + 2 * opt.branches)),
+        "clocks": clk,
+    }
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
@@ -654,10 +734,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["protein", "batched", "forcebias"], default="protein",
+    ap.add_argument("--workload", choices=["protein", "batched", "forcebias", "large"], default="protein",
                     help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU; "
-                         "forcebias: force-biased vs plain translate/rotate on the protein system")
-    ap.add_argument("--replicas", type=int, default=64)
+                         "forcebias: force-biased vs plain translate/rotate on the protein system; "
+                         "large: 200000-atom slab with PME, --replicas replicas")
+    ap.add_argument("--replicas", type=int, default=0, help="default 64 (batched), 16 (large)")
     ap.add_argument("--chunk", type=int, default=0, help="MC steps per bench step (default 2048; batched 256)")
     ap.add_argument("--ref-chunk", type=int, default=0,
                     help="MC steps per bench step for the reference arm (default: --chunk, same step range)")
@@ -667,7 +748,9 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.chunk <= 0:
-        args.chunk = {"batched": 256, "forcebias": 8192}.get(args.workload, 2048)
+        args.chunk = {"batched": 256, "forcebias": 8192, "large": 64}.get(args.workload, 2048)
+    if args.replicas <= 0:
+        args.replicas = 16 if args.workload == "large" else 64
     if args.ref_chunk <= 0:
         args.ref_chunk = 16 if args.workload == "batched" else args.chunk
     ws, rank, local = dist_env()
@@ -684,6 +767,8 @@ def main():
             out = run_ours_batched(args, ws, rank, local)
         elif args.workload == "forcebias":
             out = run_ours_forcebias(args, ws, rank, local)
+        elif args.workload == "large":
+            out = run_ours_large(args, ws, rank, local)
         else:
             out = run_ours(args, ws, rank, local)
         if rank == 0 and out is not None:
