@@ -161,7 +161,6 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
             cnt = sp.y;
             code = ge >> 26;
         }
-        npair += (long long)cnt * ns;
         int incl = cnt;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
@@ -169,6 +168,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
             if (lane >= off) incl += v;
         }
         const int total = __shfl_sync(kFull, incl, 31);
+        npair += (long long)total * ns;  // warp-uniform: atom x site pairs of this batch's groups
         const int maxcnt = __reduce_max_sync(kFull, (unsigned)cnt);
         if (maxcnt <= kACap / 2) {
             if (na + total > kACap) {

@@ -288,3 +288,34 @@ def test_checkpoint_resume_continues_the_chain(protein_small, proposal):
     assert np.array_equal(full.atomInfo["position"][a], res.atomInfo["position"][a])
     r = occupied_res(full)
     assert np.array_equal(full.residueInfo["position"][r], res.residueInfo["position"][r])
+
+
+def test_pair_counter_equals_oracle_pairs(oracle_lib, protein_small):
+    """The engine's pair counter is the number of atom x site pairs of the
+    included groups -- the oracle's count for the same insertion poses."""
+    from pygcmc_b200.engine import Engine
+    s = protein_small
+    checked = 0
+    with Engine(s.copy()) as e:
+        for step in range(60):
+            before = e.download()
+            c0 = e.counters()["pairs"]
+            e.run(1)
+            e.sync()
+            dp = e.counters()["pairs"] - c0
+            f, m = divmod(int(s.moveArray[step]), 4)
+            fr = before.fragmentInfo[f]
+            if m != 0 or fr["totalNum"] >= fr["maxNum"]:
+                continue
+            k = int(fr["confBias"])
+            ns = int(fr["num_atoms"])
+            poses = [oracle_lib.insert_pose(before, f, step, i) for i in range(k)]
+            xyz = np.stack([p[0] for p in poses])
+            cen = np.stack([p[1] for p in poses])
+            _, _, pairs = oracle_lib.energy_batch(before, xyz, fr["atoms"]["charge"][:ns],
+                                                  fr["atoms"]["type"][:ns].astype(np.int32), cen, mode=0)
+            assert dp == pairs, (step, dp, pairs)
+            checked += 1
+            if checked == 3:
+                break
+    assert checked >= 1
