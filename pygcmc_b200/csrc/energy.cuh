@@ -36,6 +36,8 @@ struct WarpBuf {
     float cs_hi[3][4];       // pose centre + image shift (code 0: 0, 1: +L, 2: -L), high part
     float cs_lo[3][4];       //   and its exact rounding error (TwoSum)
     float4 site_abs[kMaxSites];  // absolute site position, raw charge (Ewald terms)
+    int cbase[32];           // cell gather: entry base of each of the batch's cells
+    int cexcl[32];           //   and the exclusive prefix of their entry counts
 };
 
 // Exact split of c + t into hi + lo (Knuth's TwoSum).
@@ -295,8 +297,19 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
         }
         const int total = __shfl_sync(kFull, incl, 31);
         if (total <= kCCap) {
-            const int* ent = R.cell_ent + (size_t)cell * R.cap;
-            for (int e = 0, o = incl - cnt; e < cnt; ++e) B.cand[o + e] = ent[e];
+            // gather the batch's entries with independent loads: entry t belongs to the
+            // last cell whose exclusive prefix is <= t (found by binary search)
+            B.cbase[lane] = cell * R.cap;
+            B.cexcl[lane] = incl - cnt;
+            __syncwarp();
+            for (int t = lane; t < total; t += 32) {
+                int lo = 0, hi = 31;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (B.cexcl[mid] <= t) lo = mid; else hi = mid - 1;
+                }
+                B.cand[t] = __ldg(R.cell_ent + B.cbase[lo] + (t - B.cexcl[lo]));
+            }
             __syncwarp();
             test_candidates(R, B, total, self, cx, cy, cz, lane, ng, ngroups, ns, sink, npair);
             __syncwarp();
