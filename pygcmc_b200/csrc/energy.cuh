@@ -532,6 +532,31 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
     __syncwarp();
 }
 
+// Words [zi nw / nslab, (zi + 1) nw / nslab) of pose i's row of the pose-pose
+// "within cutoff" bit matrix (host distance form, bit-exact): the other poses'
+// centres are loaded four words ahead so the loads overlap.
+__device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int i, int zi, int lane) {
+    const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
+    const float4 ci = R.pcen[i];
+    for (int wb = w0; wb < w1; wb += 4) {
+        float4 cj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = 32 * (wb + u) + lane;
+            cj[u] = (wb + u < w1 && j < D.k) ? R.pcen[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (wb + u >= w1) break;  // warp-uniform
+            const int j = 32 * (wb + u) + lane;
+            const bool b = j < D.k && within_cutoff<true>(ci.x, ci.y, ci.z, cj[u].x, cj[u].y, cj[u].z, R.L, R.invL,
+                                                          R.cutoff, R.cut2_lo, R.cut2_hi, R.fast_incl);
+            const unsigned m = __ballot_sync(kFull, b);
+            if (lane == 0) R.nbr[i * D.nw + wb + u] = m;
+        }
+    }
+}
+
 // One launch per MC step: every replica's (pose, variant, slab) items.
 #ifndef GCMC_ENERGY_MIN_BLOCKS
 #define GCMC_ENERGY_MIN_BLOCKS 3
@@ -576,21 +601,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
-        if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
-            const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
-            const float4 ci = R.pcen[i];
-            for (int w = w0; w < w1; ++w) {
-                int j = 32 * w + lane;
-                bool b = false;
-                if (j < D.k) {
-                    float4 cj = R.pcen[j];
-                    b = within_cutoff<true>(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
-                                            R.cut2_hi, R.fast_incl);
-                }
-                unsigned m = __ballot_sync(kFull, b);
-                if (lane == 0) R.nbr[i * D.nw + w] = m;
-            }
-        }
+        if (v == 0 && D.nw > 0) nbr_rows(R, D, i, zi, lane);  // this slab's share of pose i's row
         __syncwarp();
     }
 }

@@ -290,19 +290,7 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
                 R.pcen[i] = fb_propose(R, D, i, fo, gc, R.fbprop + 2 * i);
             }
         } else if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
-            const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
-            const float4 ci = R.pcen[i];
-            for (int w = w0; w < w1; ++w) {
-                const int j = 32 * w + lane;
-                bool b = false;
-                if (j < D.k) {
-                    const float4 cj = R.pcen[j];
-                    b = within_cutoff<true>(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
-                                            R.cut2_hi, R.fast_incl);
-                }
-                const unsigned m = __ballot_sync(kFull, b);
-                if (lane == 0) R.nbr[i * D.nw + w] = m;
-            }
+            nbr_rows(R, D, i, zi, lane);
         }
         __syncwarp();
     }
