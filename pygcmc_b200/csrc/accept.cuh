@@ -29,6 +29,7 @@ struct AcceptSmem {
     double w[kMaxPoses];
     unsigned long long key[kMaxPoses];  // order-preserving encoding of the Gumbel key
     double lnu[kMaxPoses];              // ln of the acceptance draw of the cluster seeded by pose i
+    double lnn[kMaxPoses + 1];          // insertion: ln(n + 1) for n = D.n .. D.n + k
     float4 c[kMaxPoses];
     uint32_t nb[kMaxPoses * kMaxWords];
     int acc_list[kMaxPoses];
@@ -345,14 +346,14 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             const double e = S.E[i];
             const bool fin = isfinite(e);
             S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
-            const U4 g = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
-            S.key[i] = fin ? key_order(-kBeta * e - log(-log(u53_open(g.x, g.y)))) : 0ull;
-            const U4 ua = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
-            S.lnu[i] = log(u53(ua.x, ua.y));
+            S.key[i] = fin ? key_order(-kBeta * e + R.pgum[i]) : 0ull;  // Gumbel-max key
+            S.lnu[i] = R.plnu[i];
             S.c[i] = R.pcen[i];
         }
         const int nw = D.nw;
         for (int x = tid; x < k * nw; x += nt) S.nb[x] = R.nbr[x];
+        if (D.move == MV_INSERT)  // ln(n + 1) for every count the walk can reach
+            for (int j = tid; j <= k && D.n + j <= F.maxNum; j += nt) S.lnn[j] = log((double)(D.n + j) + 1.0);
         __syncthreads();
         PHASE(1);
 
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         }
         int wn = D.n, wna = 0, wnc = 0, wfa = -1;
         const double K0 = ins ? (R.lncav + F.B) : 0.0;
-        double K = ins ? K0 - log((double)wn + 1.0) : 0.0;
+        double K = ins ? K0 - S.lnn[0] : 0.0;
         int nrounds = 0;
         int depth = 32;  // speculation depth: halves after a round cut short, doubles after a full one
         for (int round = 0; round <= k; ++round) {
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                             if (wn < F.maxNum) {
                                 slot = wn;
                                 ++wn;
-                                K = K0 - log((double)wn + 1.0);
+                                K = K0 - S.lnn[wn - D.n];
                             } else {
                                 slot = -1;
                             }

@@ -398,6 +398,8 @@ struct RepDev {
     unsigned long long* counters;  // steps, poses, pairs, then 8 accept-kernel phase cycle sums
     int* err;
     double* energy;     // running sum of the accepted moves' energy changes (FP64)
+    double* pgum;       // [kMaxPoses] -ln(-ln u) Gumbel draw of pose i (clustering moves)
+    double* plnu;       // [kMaxPoses] ln u of the acceptance draw of the cluster seeded by pose i
     // force-biased moves
     float* fpart;       // [kMaxPoses * 2 * nslab_max * 6] per-item force and torque partials
     float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (a0, a1, a2, 0) of the old pose

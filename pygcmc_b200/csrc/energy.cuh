@@ -557,6 +557,16 @@ __device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int
     }
 }
 
+// The draws of pose i that do not depend on energies, made once per pose by
+// the pose-energy kernels (off the single-CTA accept kernel's critical path):
+// the Gumbel perturbation -ln(-ln u) and ln u of the cluster acceptance draw.
+__device__ __forceinline__ void pose_draws(const RepDev& R, const StepDesc& D, int i) {
+    const U4 g = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_GUMBEL, 0);
+    R.pgum[i] = -log(-log(u53_open(g.x, g.y)));
+    const U4 ua = rng(R.seed, R.replica, R.step_base + (uint32_t)D.step, (uint32_t)i, RP_CLUSTER, 0);
+    R.plnu[i] = log(u53(ua.x, ua.y));
+}
+
 // One launch per MC step: every replica's (pose, variant, slab) items.
 #ifndef GCMC_ENERGY_MIN_BLOCKS
 #define GCMC_ENERGY_MIN_BLOCKS 3
@@ -602,6 +612,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
         if (v == 0 && D.nw > 0) nbr_rows(R, D, i, zi, lane);  // this slab's share of pose i's row
+        if (v == 0 && zi == 0 && D.nw > 0 && lane == 0) pose_draws(R, D, i);
         __syncwarp();
     }
 }
