@@ -455,13 +455,23 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             }
             __syncthreads();
             if (warp == 0) {  // in-order commit
+                // lane j holds speculative cluster j's scalars (broadcast by shuffles), and the
+                // next cluster's mask word is loaded one cluster ahead
+                const int my_seed = lane < nb ? S.spec_seed[lane] : 0;
+                const int my_chosen = lane < nb ? S.spec_chosen[lane] : -1;
+                const double my_lnq = lane < nb ? S.spec_lnq[lane] : 0.0;
+                const double my_lnu = lane < nb ? S.lnu[my_seed] : 0.0;
+                uint32_t mnext = S.spec_mask[0][lane];
                 int j = 0;
                 for (; j < nb; ++j) {
-                    const uint32_t m = S.spec_mask[j][lane];
+                    const uint32_t m = mnext;
+                    if (j + 1 < nb) mnext = S.spec_mask[j + 1][lane];
                     if (__ballot_sync(kFull, (m & ~u) != 0u)) break;  // speculation no longer exact
-                    const int sd = S.spec_seed[j];
-                    int chosen = S.spec_chosen[j];
-                    const bool acc = chosen >= 0 && S.lnu[sd] < S.spec_lnq[j] + K;
+                    const int sd = __shfl_sync(kFull, my_seed, j);
+                    int chosen = __shfl_sync(kFull, my_chosen, j);
+                    const double lnq = __shfl_sync(kFull, my_lnq, j);
+                    const double lnu_s = __shfl_sync(kFull, my_lnu, j);
+                    const bool acc = chosen >= 0 && lnu_s < lnq + K;
                     if (chosen < 0) chosen = sd;
                     u &= ~m;
                     if (acc) {
