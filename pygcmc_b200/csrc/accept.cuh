@@ -98,6 +98,38 @@ __device__ __forceinline__ void cell_rename(const RepDev& R, int from, int to) {
     cell_insert(R, c, to);
 }
 
+// Cell-list moves of up to 32 groups by one warp: lane l (active) takes group
+// g out of its current cell (rem) and/or inserts it into cell `cnew` (cnew < 0:
+// no insertion).  All removals run before all insertions; lanes touching the
+// same cell take turns (lowest lane first), different cells are independent,
+// and since cells are kept sorted their content does not depend on the order.
+__device__ __forceinline__ void warp_cell_moves(const RepDev& R, int lane, bool active, int g, bool rem,
+                                                int cnew) {
+    int cold = -1;
+    if (active && rem) {
+        const int cp = R.gcell[g];
+        cold = cp >= 0 ? cp / R.cap : -1;
+    }
+    bool pend = active && cold >= 0;
+    while (__any_sync(kFull, pend)) {
+        const unsigned grp = __match_any_sync(kFull, pend ? cold : -2 - lane);
+        if (pend && __ffs(grp) - 1 == lane) {
+            cell_remove(R, g);
+            pend = false;
+        }
+        __syncwarp();
+    }
+    pend = active && cnew >= 0;
+    while (__any_sync(kFull, pend)) {
+        const unsigned grp = __match_any_sync(kFull, pend ? cnew : -2 - lane);
+        if (pend && __ffs(grp) - 1 == lane) {
+            cell_insert(R, cnew, g);
+            pend = false;
+        }
+        __syncwarp();
+    }
+}
+
 // Order-preserving map of a double to uint64 (larger key -> larger integer);
 // 0 is reserved for "no candidate".
 __device__ __forceinline__ bool normal_positive(double a) { return a >= 2.2250738585072014e-308 && a <= 1.7976931348623157e308; }
@@ -524,14 +556,19 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 if (lane == 0) R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
             }
             __syncthreads();
-            if (tid == 0) {
-                for (int a = 0; a < na; ++a) {
-                    const int slot = S.acc_slot[a];
-                    if (slot < 0) continue;
-                    const float4 c = S.c[S.acc_list[a]];
-                    cell_add(R, F.startRes + slot, c.x, c.y, c.z);
+            if (warp == 0) {
+                for (int a0 = 0; a0 < na; a0 += 32) {
+                    const int a = a0 + lane;
+                    const bool act = a < na && S.acc_slot[a] >= 0;
+                    int g = 0, cn = -1;
+                    if (act) {
+                        const float4 c = S.c[S.acc_list[a]];
+                        g = F.startRes + S.acc_slot[a];
+                        cn = cell_of(R, c.x, c.y, c.z);
+                    }
+                    warp_cell_moves(R, lane, act, g, false, cn);
                 }
-                R.totalNum[D.ftype] = S.misc[3];
+                if (lane == 0) R.totalNum[D.ftype] = S.misc[3];
             }
         } else {
             for (int a = warp; a < na; a += nwarps) {
@@ -549,17 +586,21 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 if (lane < ns) R.xyzq[sp.x + lane] = make_float4(px, py, pz, qw);
             }
             __syncthreads();
-            if (tid == 0 && D.move == MV_TRANSLATE) {
-                for (int a = 0; a < na; ++a) {
-                    const int i = S.acc_list[a];
-                    const int res = F.startRes + R.pslot[i];
-                    const float4 c = S.c[i];
-                    R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
-                    const int cp = R.gcell[res];
-                    if (cp < 0 || cp / R.cap != cell_of(R, c.x, c.y, c.z)) {
-                        cell_remove(R, res);
-                        cell_add(R, res, c.x, c.y, c.z);
+            if (warp == 0 && D.move == MV_TRANSLATE) {
+                for (int a0 = 0; a0 < na; a0 += 32) {
+                    const int a = a0 + lane;
+                    bool act = a < na;
+                    int res = 0, cn = -1;
+                    if (act) {
+                        const int i = S.acc_list[a];
+                        res = F.startRes + R.pslot[i];
+                        const float4 c = S.c[i];
+                        R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
+                        cn = cell_of(R, c.x, c.y, c.z);
+                        const int cp = R.gcell[res];
+                        act = cp < 0 || cp / R.cap != cn;  // only groups that change cell
                     }
+                    warp_cell_moves(R, lane, act, res, true, cn);
                 }
             }
         }
