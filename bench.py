@@ -43,10 +43,13 @@ WORKLOAD = ("synthetic protein: 6000-atom random-walk chain in a 24 A sphere, 64
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from pygcmc_b200 import replicas
+    return replicas.env()
+
+
+def replicas_seed(base, rank, stride=1):
+    from pygcmc_b200 import replicas
+    return replicas.replica_seed(base, rank, stride)
 
 
 def make_system(seed, mcsteps):
@@ -153,7 +156,7 @@ def run_ours(args, ws, rank, local):
     from pygcmc_b200.gpu import runGCMC
     torch.cuda.set_device(local)
     chunk = args.chunk
-    seed = args.seed + rank
+    seed = replicas_seed(args.seed, rank)
     prof_steps = 256
     total = (args.warmup + args.steps) * chunk + prof_steps + 64
     sysm = make_system(seed, total)
@@ -270,7 +273,7 @@ def run_ours_batched(args, ws, rank, local):
     from pygcmc_b200.gpu import runGCMC_batch
     torch.cuda.set_device(local)
     chunk = args.chunk
-    seed = args.seed + 1000 * rank
+    seed = replicas_seed(args.seed, rank, 1000)
     prof_steps = 64
     total = (args.warmup + args.steps) * chunk + prof_steps + 256
     t0 = time.perf_counter()
@@ -497,7 +500,7 @@ def run_ours_forcebias(args, ws, rank, local):
     from pygcmc_b200.gpu import runGCMC
     torch.cuda.set_device(local)
     chunk = args.chunk
-    seed = args.seed + rank
+    seed = replicas_seed(args.seed, rank)
     total = (args.warmup + args.steps) * chunk + 256
     sysm = make_system(seed, total)
     # translate/rotate-only schedule: fixed N, so the comparison isolates the proposals
@@ -713,19 +716,13 @@ def run_reference(args, ws, rank, local):
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from pygcmc_b200 import replicas
+    replicas.barrier(ws)
 
 
 def max_over_ranks(x, ws):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from pygcmc_b200 import replicas
+    return replicas.max_over_ranks(x, ws)
 
 
 def main():
@@ -755,11 +752,10 @@ def main():
         args.ref_chunk = 16 if args.workload == "batched" else args.chunk
     ws, rank, local = dist_env()
     if ws > 1:
-        import datetime
         import torch
-        import torch.distributed as dist
+        from pygcmc_b200 import replicas
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        replicas.init("nccl", timeout_s=300)
     try:
         if args.impl == "reference":
             out = run_reference(args, ws, rank, local)
@@ -775,8 +771,8 @@ def main():
             print(json.dumps(out), flush=True)
     finally:
         if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+            from pygcmc_b200 import replicas
+            replicas.finalize()
 
 
 if __name__ == "__main__":
