@@ -344,7 +344,8 @@ def run_ours_batched(args, ws, rank, local):
                    "autotuned": {"cells_per_cutoff": best.cells_per_cutoff, "split_items": best.split_items,
                                  "branches": best.branches, "energy_blocks_per_sm": best.energy_blocks_per_sm,
                                  "trials": len(trials), "tune_s": round(t_tune, 2),
-                                 "trial_ms_per_step": [[*t[:4], round(t[4], 4)] for t in trials]},
+                                 "energy_variant": best.energy_variant,
+                                 "trial_ms_per_step": [[*t[:5], round(t[5], 4)] for t in trials]},
                    "generate_s": round(t_gen, 2)},
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,

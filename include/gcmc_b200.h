@@ -109,11 +109,13 @@ typedef struct {
     float pme_alpha;     /* Ewald splitting parameter, 1/A (0 = 0.32)              */
     int32_t pme_grid[3]; /* mesh points per axis (0 = box edge / 1.2 A rounded up to
                             a 2-3-5-7-smooth size)                                 */
+    int32_t energy_variant; /* pose-energy kernel register budget: 0 = 3 CTAs per SM,
+                            1 = 4 CTAs per SM (autotuned)                           */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
 typedef struct {
-    int32_t cells_per_cutoff, split_items, branches, energy_blocks_per_sm;
+    int32_t cells_per_cutoff, split_items, branches, energy_blocks_per_sm, energy_variant;
     float ms_per_step;   /* device time per MC step (all replicas)                  */
 } gcmc_tune_trial;
 
@@ -223,7 +225,8 @@ int gcmc_destroy(gcmc_ctx* ctx);
  * replicas, times trial_steps MC steps (after 8 warm-up steps) on temporary
  * contexts for a coordinate-descent sequence of candidates -- cell-grid
  * resolution (cells_per_cutoff 1..3), pose-energy work split (split_items
- * 512..8192), graph branches (1, 2, 4) and pose-energy CTAs per SM -- and
+ * 512..8192), graph branches (1, 2, 4), the pose-energy kernel's register
+ * budget (energy_variant) and pose-energy CTAs per SM -- and
  * writes the base options with the fastest shape into *best.  trials
  * (optional, max_trials entries) receives each trial; *ntrials their number.
  * The inputs are not modified; the trajectories of a context created with

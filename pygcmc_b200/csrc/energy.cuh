@@ -532,31 +532,6 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
     __syncwarp();
 }
 
-// Words [zi nw / nslab, (zi + 1) nw / nslab) of pose i's row of the pose-pose
-// "within cutoff" bit matrix (host distance form, bit-exact): the other poses'
-// centres are loaded four words ahead so the loads overlap.
-__device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int i, int zi, int lane) {
-    const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
-    const float4 ci = R.pcen[i];
-    for (int wb = w0; wb < w1; wb += 4) {
-        float4 cj[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int j = 32 * (wb + u) + lane;
-            cj[u] = (wb + u < w1 && j < D.k) ? R.pcen[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (wb + u >= w1) break;  // warp-uniform
-            const int j = 32 * (wb + u) + lane;
-            const bool b = j < D.k && within_cutoff<true>(ci.x, ci.y, ci.z, cj[u].x, cj[u].y, cj[u].z, R.L, R.invL,
-                                                          R.cutoff, R.cut2_lo, R.cut2_hi, R.fast_incl);
-            const unsigned m = __ballot_sync(kFull, b);
-            if (lane == 0) R.nbr[i * D.nw + wb + u] = m;
-        }
-    }
-}
-
 // The draws of pose i that do not depend on energies, made once per pose by
 // the pose-energy kernels (off the single-CTA accept kernel's critical path):
 // the Gumbel perturbation -ln(-ln u) and ln u of the cluster acceptance draw.
@@ -567,11 +542,34 @@ __device__ __forceinline__ void pose_draws(const RepDev& R, const StepDesc& D, i
     R.plnu[i] = log(u53(ua.x, ua.y));
 }
 
+// Words [zi nw / nslab, (zi + 1) nw / nslab) of pose i's row of the pose-pose
+// "within cutoff" bit matrix (host distance form, bit-exact).  The row of pose
+// 32 w also makes the energy-independent draws of the 32 poses of word w, one
+// per lane.
+__device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int i, int zi, int lane) {
+    const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
+    const float4 ci = R.pcen[i];
+    for (int w = w0; w < w1; ++w) {
+        const int j = 32 * w + lane;
+        if (i == 32 * w && j < D.k) pose_draws(R, D, j);
+        bool b = false;
+        if (j < D.k) {
+            const float4 cj = R.pcen[j];
+            b = within_cutoff<true>(ci.x, ci.y, ci.z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                    R.cut2_hi, R.fast_incl);
+        }
+        const unsigned m = __ballot_sync(kFull, b);
+        if (lane == 0) R.nbr[i * D.nw + w] = m;
+    }
+}
+
 // One launch per MC step: every replica's (pose, variant, slab) items.
-#ifndef GCMC_ENERGY_MIN_BLOCKS
-#define GCMC_ENERGY_MIN_BLOCKS 3
-#endif
-__global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy(const RepDev* __restrict__ reps, int nrep) {
+// Two register budgets of the same kernel, picked per context (gcmc_options.
+// energy_variant, autotuned): MinBlocks = 3 CTAs per SM (up to 85 registers,
+// fewer spills; best for a single replica whose step is latency-bound) or 4
+// (64 registers, more warps in flight; best for large batches).
+template <int MinBlocks>
+__global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -612,10 +610,12 @@ __global__ void __launch_bounds__(kWarpsE * 32, GCMC_ENERGY_MIN_BLOCKS) k_energy
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
         if (v == 0 && D.nw > 0) nbr_rows(R, D, i, zi, lane);  // this slab's share of pose i's row
-        if (v == 0 && zi == 0 && D.nw > 0 && lane == 0) pose_draws(R, D, i);
         __syncwarp();
     }
 }
+
+template __global__ void k_energy_t<3>(const RepDev* __restrict__, int);
+template __global__ void k_energy_t<4>(const RepDev* __restrict__, int);
 
 // Energies of caller-supplied poses (gcmc_energy_poses): item = (pose, slab).
 // The replica descriptor is passed by value so that callers can substitute

@@ -89,6 +89,7 @@ struct gcmc_ctx {
     int gridE = 0;       // pose-energy CTAs for all replicas
     int branches = 1;    // independent chains in the captured step loop
     int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
+    int evar = 0;        // pose-energy kernel variant: 0 = 3 CTAs per SM, 1 = 4 CTAs per SM
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
     int gridF = 0;       // k_energy_fb CTAs
     std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
@@ -505,6 +506,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     return GCMC_OK;
 }
 
+using EnergyKernel = void (*)(const RepDev*, int);
+EnergyKernel energy_kernel(int variant) { return variant == 1 ? k_energy_t<4> : k_energy_t<3>; }
+
 // Rebuild replica r's PME mesh potential from its current state on stream s:
 // Q = Q_fixed + spread(occupied fragment atoms); phi = IFFT(G * FFT(Q)).
 int pme_update(gcmc_ctx* ctx, int r, cudaStream_t s) {
@@ -543,7 +547,7 @@ int pme_init_fixed(gcmc_ctx* ctx) {
 int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     int sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy, kWarpsE * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, energy_kernel(ctx->evar), kWarpsE * 32, 0));
     per_sm = std::max(1, per_sm);
     if (ebps > 0) per_sm = std::min(per_sm, ebps);
     ctx->ebps = ebps;
@@ -610,7 +614,7 @@ int build_graph(gcmc_ctx* ctx) {
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
                 } else {
-                    k_energy<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
+                    energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
                 }
                 k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt);
             }
@@ -692,6 +696,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
             st = GCMC_ERR_CUDA;
     }
     ctx->fb = opt.proposal == 2 ? 1 : 0;
+    ctx->evar = opt.energy_variant == 1 ? 1 : 0;
     if (st == GCMC_OK) st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
     if (st == GCMC_OK) {
         split_branches(ctx, opt.branches > 0 ? opt.branches : 1);
@@ -738,8 +743,10 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     if (st != GCMC_OK) return st;
     const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
     const int fb = opt.proposal == 2 ? 1 : 0;
-    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb) {
+    const int evar = opt.energy_variant == 1 ? 1 : 0;
+    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb || evar != ctx->evar) {
         ctx->fb = fb;
+        ctx->evar = evar;
         st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
         if (st != GCMC_OK) return st;
         split_branches(ctx, nb);
@@ -943,7 +950,8 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         int st = trial(o, &ms);
         if (st != GCMC_OK) return st;
         if (trials && n < max_trials)
-            trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items, o.branches, o.energy_blocks_per_sm, ms};
+            trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items, o.branches, o.energy_blocks_per_sm,
+                                        o.energy_variant, ms};
         ++n;
         if (ms < best_ms) {
             best_ms = ms;
@@ -970,6 +978,11 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         if (nb == base_br || nb > nrep) continue;
         gcmc_options o = cur;
         o.branches = nb;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    {
+        gcmc_options o = cur;
+        o.energy_variant = cur.energy_variant == 1 ? 0 : 1;
         if (st == GCMC_OK) st = consider(o);
     }
     const int base_e = cur.energy_blocks_per_sm;
@@ -1031,7 +1044,7 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
         } else {
-            k_energy<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+            energy_kernel(ctx->evar)<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
         }
         CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
         k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);

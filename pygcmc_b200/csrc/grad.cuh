@@ -291,7 +291,6 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
             }
         } else if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
             nbr_rows(R, D, i, zi, lane);
-            if (zi == 0 && lane == 0) pose_draws(R, D, i);
         }
         __syncwarp();
     }

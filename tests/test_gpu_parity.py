@@ -247,10 +247,11 @@ def test_autotune_picks_the_fastest_trial(protein_small, water_small):
     before = [s.copy() for s in systems]
     best, trials = autotune(systems, default_options(), trial_steps=32)
     assert len(trials) >= 8
-    ms = [t[4] for t in trials]
+    ms = [t[5] for t in trials]
     assert all(np.isfinite(ms)) and min(ms) > 0
     k = int(np.argmin(ms))
-    assert (best.cells_per_cutoff, best.split_items, best.branches, best.energy_blocks_per_sm) == trials[k][:4]
+    assert (best.cells_per_cutoff, best.split_items, best.branches, best.energy_blocks_per_sm,
+            best.energy_variant) == trials[k][:5]
     for s, b in zip(systems, before):  # inputs untouched
         assert np.array_equal(s.atomInfo, b.atomInfo)
         assert (s.fragmentInfo["totalNum"] == b.fragmentInfo["totalNum"]).all()
