@@ -9,7 +9,9 @@ fragments of 4-12 sites starting at their bulk-concentration counts, confBias
 1000, cutoff 12 A, the reference's move schedule and acceptance semantics.
 A bench step is CHUNK MC steps (moveArray entries); `value` is MC steps/s with
 the state resident on the GPU, `e2e` the same through the runGCMC drop-in
-with host arrays (upload, run, download inside the timed region).
+with host arrays (upload, run, download inside the timed region).  The launch
+shape comes from the autotuner, run before the timed region (--cells N fixes
+the cell-grid resolution instead).
 
 --workload batched: 64 replicas of uneven size (2000-40000 atoms, a muex scan)
 advanced together in one context, with the launch shape from the autotuner;
@@ -160,7 +162,14 @@ def run_ours(args, ws, rank, local):
     prof_steps = 256
     total = (args.warmup + args.steps) * chunk + prof_steps + 64
     sysm = make_system(seed, total)
-    eng = Engine(sysm.copy(), default_options(cells_per_cutoff=args.cells))
+    if args.cells > 0:
+        opts, t_tune = default_options(cells_per_cutoff=args.cells), 0.0
+    else:  # launch shape from the autotuner (untimed set-up)
+        from pygcmc_b200.engine import autotune
+        t0 = time.perf_counter()
+        opts, _ = autotune(sysm, default_options(), trial_steps=128)
+        t_tune = time.perf_counter() - t0
+    eng = Engine(sysm.copy(), opts)
     stream = torch.cuda.ExternalStream(eng.stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     for _ in range(args.warmup):
@@ -204,7 +213,7 @@ def run_ours(args, ws, rank, local):
         barrier(ws)
         t0 = time.perf_counter()
         runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
-                e2e_state.ff, mv)
+                e2e_state.ff, mv, options=opts)
         if k >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(e2e_times) * 1e3, ws) / 1e3
@@ -226,7 +235,11 @@ def run_ours(args, ws, rank, local):
         "data": "synthetic (seeded generator; no public dataset)",
         "config": {"workload": WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
                    "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
-                   "cells_per_cutoff": args.cells},
+                   "launch_shape": {"cells_per_cutoff": opts.cells_per_cutoff, "split_items": opts.split_items,
+                                    "branches": opts.branches, "energy_blocks_per_sm": opts.energy_blocks_per_sm,
+                                    "energy_variant": opts.energy_variant,
+                                    "source": "--cells" if args.cells > 0 else
+                                    f"autotuned before timing ({t_tune:.1f} s, untimed)"}},
         "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
                 "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
@@ -740,7 +753,7 @@ def main():
     ap.add_argument("--chunk", type=int, default=0, help="MC steps per bench step (default 2048; batched 256)")
     ap.add_argument("--ref-chunk", type=int, default=0,
                     help="MC steps per bench step for the reference arm (default: --chunk, same step range)")
-    ap.add_argument("--cells", type=int, default=2)
+    ap.add_argument("--cells", type=int, default=0, help="cells per cutoff (0: autotune the launch shape)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
