@@ -28,10 +28,11 @@ struct AcceptSmem {
     double ephys[kMaxPoses];  // the pose's energy (insert/delete) or energy change (translate/rotate)
     double w[kMaxPoses];
     unsigned long long key[kMaxPoses];  // order-preserving encoding of the Gumbel key
-    double lnu[kMaxPoses];              // ln of the acceptance draw of the cluster seeded by pose i
+    alignas(16) double lnu[kMaxPoses];  // ln of the acceptance draw of the cluster seeded by pose i
+    alignas(16) double gum[kMaxPoses];  // Gumbel draw -ln(-ln u) of pose i
     double lnn[kMaxPoses + 1];          // insertion: ln(n + 1) for n = D.n .. D.n + k
-    float4 c[kMaxPoses];
-    uint32_t nb[kMaxPoses * kMaxWords];
+    alignas(16) float4 c[kMaxPoses];
+    alignas(16) uint32_t nb[kMaxPoses * kMaxWords];
     int acc_list[kMaxPoses];
     int acc_slot[kMaxPoses];
     double red[32];
@@ -44,6 +45,15 @@ struct AcceptSmem {
     double spec_lnq[32];  // ln(W) - ln(cnt), W = sum over members of exp(-beta E)
     int spec_n;
 };
+
+// ---- asynchronous 16-byte global -> shared copies (cp.async) ----
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(__cvta_generic_to_global(gmem))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---- cell list maintenance (single thread) ----
 // Each cell keeps its group ids in increasing order, so a cell's content (and
@@ -280,6 +290,22 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     const FragDev& F = R.frag[D.ftype];
     const int k = D.k, ns = F.nsites;
     long long t_start = clock64(), t_mark = t_start;
+    // Clustering moves: the per-pose inputs of the walk (centres, Gumbel and
+    // acceptance draws, neighbour bit rows; written by the pose-energy launch)
+    // are copied into shared memory asynchronously, issued first so that they
+    // arrive while the energies are summed.  Sizes are rounded up to whole
+    // 16-byte chunks; the sources hold kMaxPoses entries (kMaxPoses x kMaxWords
+    // words), so the rounding stays inside them.
+    if (D.move != MV_DELETE && k > 0) {
+        const int nb16 = (k * D.nw + 3) >> 2, d16 = (k + 1) >> 1;
+        for (int x = tid; x < nb16; x += nt) cp_async16(&S.nb[4 * x], R.nbr + 4 * x);
+        for (int x = tid; x < k; x += nt) cp_async16(&S.c[x], R.pcen + x);
+        for (int x = tid; x < d16; x += nt) {
+            cp_async16(&S.gum[2 * x], R.pgum + 2 * x);
+            cp_async16(&S.lnu[2 * x], R.plnu + 2 * x);
+        }
+        cp_async_commit();
+    }
     // phase cycle sums (thread 0): 0 energies, 1 per-pose precompute, 2 cluster walk, 3 apply, 4 prepare
 #define PHASE(i)                                                                  \
     do {                                                                          \
@@ -373,17 +399,15 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         double emin_loc = INFINITY;
         for (int i = tid; i < k; i += nt)
             if (isfinite(S.E[i])) emin_loc = fmin(emin_loc, S.E[i]);
+        cp_async_wait_all();  // this thread's staged copies; block_min's barriers publish them
         const double Eref = block_min(emin_loc, S.red);
         for (int i = tid; i < k; i += nt) {
             const double e = S.E[i];
             const bool fin = isfinite(e);
             S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
-            S.key[i] = fin ? key_order(-kBeta * e + R.pgum[i]) : 0ull;  // Gumbel-max key
-            S.lnu[i] = R.plnu[i];
-            S.c[i] = R.pcen[i];
+            S.key[i] = fin ? key_order(-kBeta * e + S.gum[i]) : 0ull;  // Gumbel-max key
         }
         const int nw = D.nw;
-        for (int x = tid; x < k * nw; x += nt) S.nb[x] = R.nbr[x];
         if (D.move == MV_INSERT)  // ln(n + 1) for every count the walk can reach
             for (int j = tid; j <= k && D.n + j <= F.maxNum; j += nt) S.lnn[j] = log((double)(D.n + j) + 1.0);
         __syncthreads();
@@ -420,13 +444,13 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 uint32_t us = u;
                 int nb = 0;
                 while (nb < depth) {
-                    const unsigned nz = __ballot_sync(kFull, us != 0u);
-                    if (nz == 0u) break;
-                    const int L = __ffs(nz) - 1;
-                    const uint32_t uw = __shfl_sync(kFull, us, L);
-                    const int sd = 32 * L + __ffs(uw) - 1;
+                    // lowest unused pose: minimum over the lanes' lowest set bits
+                    const unsigned low = us ? (unsigned)(32 * lane + __ffs(us) - 1) : 0xffffffffu;
+                    const unsigned sdu = __reduce_min_sync(kFull, low);
+                    if (sdu == 0xffffffffu) break;
+                    const int sd = (int)sdu;
                     uint32_t m = (lane < nw) ? (us & S.nb[sd * nw + lane]) : 0u;
-                    if (lane == L) m |= 1u << (sd & 31);
+                    if (lane == (sd >> 5)) m |= 1u << (sd & 31);
                     us &= ~m;
                     S.spec_mask[nb][lane] = m;
                     if (lane == 0) S.spec_seed[nb] = sd;
@@ -487,46 +511,68 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             }
             __syncthreads();
             if (warp == 0) {  // in-order commit
-                // lane j holds speculative cluster j's scalars (broadcast by shuffles), and the
-                // next cluster's mask word is loaded one cluster ahead
+                // Lane j holds speculative cluster j's scalars.  The decision of a
+                // cluster depends only on its own scalars and on K, which changes only
+                // at an acceptance, so the decisions of all clusters after the last
+                // acceptance are made at once and the clusters before the first
+                // accepting one are committed together (u loses the union of their
+                // members).  A cluster is exact while none of its poses has left u;
+                // only an acceptance (its chosen pose's neighbours) can break that
+                // within a round, so the check runs after one.
                 const int my_seed = lane < nb ? S.spec_seed[lane] : 0;
                 const int my_chosen = lane < nb ? S.spec_chosen[lane] : -1;
                 const double my_lnq = lane < nb ? S.spec_lnq[lane] : 0.0;
                 const double my_lnu = lane < nb ? S.lnu[my_seed] : 0.0;
-                uint32_t mnext = S.spec_mask[0][lane];
                 int j = 0;
-                for (; j < nb; ++j) {
-                    const uint32_t m = mnext;
-                    if (j + 1 < nb) mnext = S.spec_mask[j + 1][lane];
-                    if (__ballot_sync(kFull, (m & ~u) != 0u)) break;  // speculation no longer exact
-                    const int sd = __shfl_sync(kFull, my_seed, j);
-                    int chosen = __shfl_sync(kFull, my_chosen, j);
-                    const double lnq = __shfl_sync(kFull, my_lnq, j);
-                    const double lnu_s = __shfl_sync(kFull, my_lnu, j);
-                    const bool acc = chosen >= 0 && lnu_s < lnq + K;
-                    if (chosen < 0) chosen = sd;
-                    u &= ~m;
-                    if (acc) {
-                        if (lane < nw) u &= ~S.nb[chosen * nw + lane];
-                        int slot = 0;
-                        if (ins) {
-                            if (wn < F.maxNum) {
-                                slot = wn;
-                                ++wn;
-                                K = K0 - S.lnn[wn - D.n];
-                            } else {
-                                slot = -1;
-                            }
+                bool dirty = false;  // an acceptance of this round has removed poses from u
+                while (j < nb) {
+                    const unsigned am =
+                        __ballot_sync(kFull, lane >= j && lane < nb && my_chosen >= 0 && my_lnu < my_lnq + K);
+                    const int ja = am ? __ffs(am) - 1 : nb;  // first accepting cluster (nb: none)
+                    int jstop = ja;                          // clusters [j, jstop) are rejected
+                    bool cut = false;
+                    if (dirty) {  // first cluster in [j, min(ja, nb - 1)] that lost a pose
+                        const int jend = min(ja, nb - 1);
+                        unsigned bad = 0u;
+                        for (int c = j; c <= jend; ++c)
+                            if (S.spec_mask[c][lane] & ~u) bad |= 1u << c;
+                        bad = __reduce_or_sync(kFull, bad);
+                        if (bad) {
+                            jstop = __ffs(bad) - 1;
+                            cut = true;
                         }
-                        if (lane == 0) { S.acc_list[wna] = chosen; S.acc_slot[wna] = slot; }
-                        ++wna;
-                        if (wfa < 0) wfa = chosen;
                     }
+                    uint32_t gone = 0u;
+                    for (int c = j; c < jstop; ++c) gone |= S.spec_mask[c][lane];
+                    u &= ~gone;
+                    wnc += jstop - j;
+                    j = jstop;
+                    if (cut || j >= nb) break;
+                    // cluster j accepts its chosen pose
+                    const int chosen = __shfl_sync(kFull, my_chosen, j);
+                    u &= ~S.spec_mask[j][lane];
+                    if (lane < nw) u &= ~S.nb[chosen * nw + lane];
+                    int slot = 0;
+                    if (ins) {
+                        if (wn < F.maxNum) {
+                            slot = wn;
+                            ++wn;
+                            K = K0 - S.lnn[wn - D.n];
+                        } else {
+                            slot = -1;
+                        }
+                    }
+                    if (lane == 0) { S.acc_list[wna] = chosen; S.acc_slot[wna] = slot; }
+                    ++wna;
+                    if (wfa < 0) wfa = chosen;
                     ++wnc;
+                    ++j;
+                    dirty = true;
                 }
                 depth = (j < nb) ? max(1, min(depth, 2 * j) / 2 + 1) : min(32, 2 * depth);
             }
-            __syncthreads();
+            // no barrier here: warp 0 seeds the next round next, and the other warps
+            // read its results only after the barrier that follows the seeding
         }
         if (tid == 0) {
             S.misc[0] = wna; S.misc[1] = wnc; S.misc[2] = wfa; S.misc[3] = wn;

@@ -27,9 +27,16 @@ constexpr int kACap = 512;
 constexpr int kCCap = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Sites 2p and 2p+1 of a pose, component-interleaved for the packed (f32x2)
+// pair loop: negated centre-relative coordinates and Coulomb constant * charge.
+struct SitePair {
+    float2 nx, ny, nz, kq;
+};
+
 struct WarpBuf {
     float4 site[kMaxSites];  // x, y, z relative to the pose centre, Coulomb constant * charge
     int srow[kMaxSites];     // template type * ffY
+    SitePair spair[kMaxSites / 2];
     uint32_t glist[kGCap];   // group id | image code << 26
     uint32_t alist[kACap];   // atom id  | image code << 26
     int cand[kCCap];         // candidate group ids gathered from the cells
@@ -63,6 +70,17 @@ __device__ __forceinline__ void set_centre(const RepDev& R, WarpBuf& B, float cx
     __syncwarp();
 }
 
+// Site s of the pose (centre-relative x, y, z and K q) into B.site and its
+// slot of the interleaved pair layout.
+__device__ __forceinline__ void put_site(WarpBuf& B, int s, float x, float y, float z, float kq) {
+    B.site[s] = make_float4(x, y, z, kq);
+    float* p = reinterpret_cast<float*>(&B.spair[s >> 1]) + (s & 1);
+    p[0] = -x;
+    p[2] = -y;
+    p[4] = -z;
+    p[6] = kq;
+}
+
 __device__ __forceinline__ float image_shift(uint32_t code2, float L) {
     return code2 == 1u ? L : (code2 == 2u ? -L : 0.0f);
 }
@@ -77,6 +95,90 @@ __device__ __forceinline__ float image_shift(uint32_t code2, float L) {
 // of an included group lies within half a box, checked at set-up); true:
 // per-pair minimum image as in gcmc_energy.h:115-122.  1/r is rsqrt refined by
 // one Newton step; each atom's site terms are summed in FP32, atoms in FP64.
+template <bool PairImage, bool Ewald>
+__device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
+                                              double& acc);
+
+// Plain Coulomb: two sites per step with Blackwell's packed FP32 operations
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn: one instruction for both lanes of a
+// float2, each lane correctly rounded as its scalar counterpart).  The per-pair
+// arithmetic is the scalar form's; only the order of the per-atom FP32 site sum
+// differs (even and odd sites in two partial sums, then added, then a last odd
+// site).
+template <bool PairImage>
+__device__ __forceinline__ void flush_atoms_packed(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
+                                                   double& acc) {
+    const int np = ns >> 1;
+    const float2 mhalf = make_float2(-0.5f, -0.5f), three_half = make_float2(1.5f, 1.5f);
+    for (int f = lane; f < na; f += 32) {
+        const uint32_t u = B.alist[f];
+        const int idx = (int)(u & 0x3FFFFFFu);
+        const float4 a = __ldg(&R.xyzq[idx]);
+        const int ta = __ldg(&R.atype[idx]);
+        uint32_t c0, c1, c2;
+        if (PairImage) {
+            const float kx = rintf((a.x - B.cs_hi[0][0]) * R.invL[0]);
+            const float ky = rintf((a.y - B.cs_hi[1][0]) * R.invL[1]);
+            const float kz = rintf((a.z - B.cs_hi[2][0]) * R.invL[2]);
+            c0 = kx > 0.0f ? 1u : (kx < 0.0f ? 2u : 0u);
+            c1 = ky > 0.0f ? 1u : (ky < 0.0f ? 2u : 0u);
+            c2 = kz > 0.0f ? 1u : (kz < 0.0f ? 2u : 0u);
+        } else {
+            const uint32_t code = u >> 26;
+            c0 = code & 3u; c1 = (code >> 2) & 3u; c2 = (code >> 4) & 3u;
+        }
+        const float ax = (a.x - B.cs_hi[0][c0]) - B.cs_lo[0][c0];
+        const float ay = (a.y - B.cs_hi[1][c1]) - B.cs_lo[1][c1];
+        const float az = (a.z - B.cs_hi[2][c2]) - B.cs_lo[2][c2];
+        const float2 Ax = make_float2(ax, ax), Ay = make_float2(ay, ay), Az = make_float2(az, az);
+        const float2 Aq = make_float2(a.w, a.w);
+        float2 e2 = make_float2(0.0f, 0.0f);
+#pragma unroll 2
+        for (int p = 0; p < np; ++p) {
+            const SitePair sp = B.spair[p];
+            float2 dx = __fadd2_rn(Ax, sp.nx), dy = __fadd2_rn(Ay, sp.ny), dz = __fadd2_rn(Az, sp.nz);
+            if (PairImage) {
+                dx.x = fmaf(-rintf(dx.x * R.invL[0]), R.L[0], dx.x);
+                dx.y = fmaf(-rintf(dx.y * R.invL[0]), R.L[0], dx.y);
+                dy.x = fmaf(-rintf(dy.x * R.invL[1]), R.L[1], dy.x);
+                dy.y = fmaf(-rintf(dy.y * R.invL[1]), R.L[1], dy.y);
+                dz.x = fmaf(-rintf(dz.x * R.invL[2]), R.L[2], dz.x);
+                dz.y = fmaf(-rintf(dz.y * R.invL[2]), R.L[2], dz.y);
+            }
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            float2 ir = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            ir = __fmul2_rn(ir, __ffma2_rn(__fmul2_rn(__fmul2_rn(mhalf, r2), ir), ir, three_half));
+            const float2 ir2 = __fmul2_rn(ir, ir);
+            const float2 p0 = __ldg(&R.lj[B.srow[2 * p] + ta]);
+            const float2 p1 = __ldg(&R.lj[B.srow[2 * p + 1] + ta]);
+            const float2 s2 = __fmul2_rn(make_float2(p0.x, p1.x), ir2);
+            const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+            e2 = __ffma2_rn(make_float2(p0.y, p1.y), __ffma2_rn(s6, s6, make_float2(-s6.x, -s6.y)), e2);
+            e2 = __ffma2_rn(__fmul2_rn(sp.kq, Aq), ir, e2);
+        }
+        float e = e2.x + e2.y;
+        if (ns & 1) {  // last site of an odd count
+            const float4 sp = B.site[ns - 1];
+            float dx = ax - sp.x, dy = ay - sp.y, dz = az - sp.z;
+            if (PairImage) {
+                dx = fmaf(-rintf(dx * R.invL[0]), R.L[0], dx);
+                dy = fmaf(-rintf(dy * R.invL[1]), R.L[1], dy);
+                dz = fmaf(-rintf(dz * R.invL[2]), R.L[2], dz);
+            }
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            float ir = rsqrtf(r2);
+            ir = ir * fmaf(-0.5f * r2 * ir, ir, 1.5f);
+            const float ir2 = ir * ir;
+            const float2 pp = __ldg(&R.lj[B.srow[ns - 1] + ta]);
+            const float s2 = pp.x * ir2;
+            const float s6 = s2 * s2 * s2;
+            e = fmaf(pp.y, fmaf(s6, s6, -s6), e);
+            e = fmaf(sp.w * a.w, ir, e);
+        }
+        acc += (double)e;
+    }
+}
+
 template <bool PairImage, bool Ewald>
 __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
                                               double& acc) {
@@ -125,15 +227,19 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
     }
 }
 
-__device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
-                                            double& acc) {
+// This lane's FP64 sum of the pair energies of the buffered atoms.  (Inlined:
+// an out-of-line copy shared by the call sites measured slower, as the call
+// makes the kernels spill around it.)
+__device__ __forceinline__ double flush_atoms(const RepDev& R, const WarpBuf& B, int na, int ns, int lane) {
+    double acc = 0.0;
     if (R.pme) {
         if (R.pair_image) flush_atoms_t<true, true>(R, B, na, ns, lane, acc);
         else flush_atoms_t<false, true>(R, B, na, ns, lane, acc);
     } else {
-        if (R.pair_image) flush_atoms_t<true, false>(R, B, na, ns, lane, acc);
-        else flush_atoms_t<false, false>(R, B, na, ns, lane, acc);
+        if (R.pair_image) flush_atoms_packed<true>(R, B, na, ns, lane, acc);
+        else flush_atoms_packed<false>(R, B, na, ns, lane, acc);
     }
+    return acc;
 }
 
 // What the cell walk does with each buffer of included atoms: the energy
@@ -141,7 +247,7 @@ __device__ __forceinline__ void flush_atoms(const RepDev& R, const WarpBuf& B, i
 struct EnergySink {
     double acc = 0.0;
     __device__ __forceinline__ void flush(const RepDev& R, WarpBuf& B, int na, int ns, int lane) {
-        flush_atoms(R, B, na, ns, lane, acc);
+        acc += flush_atoms(R, B, na, ns, lane);
     }
 };
 
@@ -495,8 +601,8 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
             rotate(Rm, t.x, t.y, t.z, x, y, z);
             // absolute site (bit-exact, as written to the slot on acceptance), stored centre-relative
             const float sx = fadd(x, cx), sy = fadd(y, cy), sz = fadd(z, cz);
-            B.site[lane] = make_float4((float)((double)sx - (double)cx), (float)((double)sy - (double)cy),
-                                       (float)((double)sz - (double)cz), kCoulomb * t.w);
+            put_site(B, lane, (float)((double)sx - (double)cx), (float)((double)sy - (double)cy),
+                     (float)((double)sz - (double)cz), kCoulomb * t.w);
             B.site_abs[lane] = make_float4(sx, sy, sz, t.w);
             B.srow[lane] = F.stype[lane] * R.ffY;
         }
@@ -525,8 +631,8 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
         else moved_site(R, D, i, gc, ns, lane, px, py, pz);
     }
     if (lane < ns) {
-        B.site[lane] = make_float4((float)((double)px - (double)cx), (float)((double)py - (double)cy),
-                                   (float)((double)pz - (double)cz), kCoulomb * F.site[lane].w);
+        put_site(B, lane, (float)((double)px - (double)cx), (float)((double)py - (double)cy),
+                 (float)((double)pz - (double)cz), kCoulomb * F.site[lane].w);
         B.site_abs[lane] = make_float4(px, py, pz, F.site[lane].w);
     }
     __syncwarp();
@@ -563,6 +669,38 @@ __device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int
     }
 }
 
+// pre[r] = work items of the replicas before r, pre[nrep] = all of them,
+// computed by the whole block (one replica per thread, warp scans, then the
+// warp totals) so that no thread walks the replica list alone.
+template <class Items>
+__device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Items items) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < nrep; base += blockDim.x) {
+        const int r = base + tid;
+        const int v = r < nrep ? items(r) : 0;
+        int inc = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int t = __shfl_up_sync(kFull, inc, off);
+            if (lane >= off) inc += t;
+        }
+        if (lane == 31) wtot[warp] = inc;
+        __syncthreads();
+        int before = 0, tot = 0;
+        for (int w = 0; w < nwarp; ++w) {
+            const int t = wtot[w];
+            if (w < warp) before += t;
+            tot += t;
+        }
+        if (r < nrep) pre[r] = carry + before + inc - v;
+        carry += tot;
+        __syncthreads();
+    }
+    if (tid == 0) pre[nrep] = carry;
+    __syncthreads();
+}
+
 // One launch per MC step: every replica's (pose, variant, slab) items.
 // Two register budgets of the same kernel, picked per context (gcmc_options.
 // energy_variant, autotuned): MinBlocks = 3 CTAs per SM (up to 85 registers,
@@ -572,13 +710,9 @@ template <int MinBlocks>
 __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
+    __shared__ int wtot[kWarpsE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int r = 0; r < nrep; ++r) { pre[r] = acc; acc += reps[r].desc->items; }
-        pre[nrep] = acc;
-    }
-    __syncthreads();
+    items_prefix(nrep, pre, wtot, [&](int r) { return reps[r].desc->items; });
     const int total = pre[nrep];
     WarpBuf& B = bufs[warp];
     for (int it = blockIdx.x * kWarpsE + warp; it < total; it += gridDim.x * kWarpsE) {
@@ -621,7 +755,7 @@ template __global__ void k_energy_t<4>(const RepDev* __restrict__, int);
 // The replica descriptor is passed by value so that callers can substitute
 // the pair table (R.lj).
 __global__ void __launch_bounds__(kWarpsE * 32)
-    k_energy_explicit(const RepDev R, const float* __restrict__ xyz,
+    k_energy_explicit(__grid_constant__ const RepDev R, const float* __restrict__ xyz,
                       const float* __restrict__ q, const int* __restrict__ type, int ns,
                       const float* __restrict__ centres, const int* __restrict__ self, int nposes,
                       int nslab, double* __restrict__ out, int* __restrict__ ngout) {
@@ -634,8 +768,8 @@ __global__ void __launch_bounds__(kWarpsE * 32)
         if (lane < ns) {
             const float* s = xyz + ((size_t)p * ns + lane) * 3;
             const double c0 = centres[3 * p], c1 = centres[3 * p + 1], c2 = centres[3 * p + 2];
-            B.site[lane] = make_float4((float)((double)s[0] - c0), (float)((double)s[1] - c1),
-                                       (float)((double)s[2] - c2), kCoulomb * q[lane]);
+            put_site(B, lane, (float)((double)s[0] - c0), (float)((double)s[1] - c1), (float)((double)s[2] - c2),
+                     kCoulomb * q[lane]);
             B.site_abs[lane] = make_float4(s[0], s[1], s[2], q[lane]);
             B.srow[lane] = type[lane] * R.ffY;
         }

@@ -618,7 +618,7 @@ int build_graph(gcmc_ctx* ctx) {
                 }
                 k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt);
             }
-            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaGetLastError();
         }
         for (int b = 1; b < nb && e == cudaSuccess; ++b) {
             e = cudaEventRecord(ev[b], side[b]);

@@ -194,17 +194,12 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
     __shared__ WarpBuf bufs[kWarpsG];
     __shared__ GradStage stages[kWarpsG];
     __shared__ int pre[257];
+    __shared__ int wtot[kWarpsG];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int r = 0; r < nrep; ++r) {
-            pre[r] = acc;
-            const StepDesc* d = reps[r].desc;
-            acc += phase == 1 ? d->items_pre : d->items;
-        }
-        pre[nrep] = acc;
-    }
-    __syncthreads();
+    items_prefix(nrep, pre, wtot, [&](int r) {
+        const StepDesc* d = reps[r].desc;
+        return phase == 1 ? d->items_pre : d->items;
+    });
     const int total = pre[nrep];
     WarpBuf& B = bufs[warp];
     for (int it = blockIdx.x * kWarpsG + warp; it < total; it += gridDim.x * kWarpsG) {
