@@ -56,10 +56,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---- cell list maintenance (single thread) ----
-// Each cell keeps its group ids in increasing order, so a cell's content (and
+// Each cell keeps its entries in increasing group id, so a cell's content (and
 // with it the order in which the energy kernels visit groups and sum their
 // terms) depends only on the current state, not on the history of moves: a
-// context rebuilt from a checkpoint evaluates bit-identical energies.
+// context rebuilt from a checkpoint evaluates bit-identical energies.  An
+// entry carries the group's centre and atom range (from R.gcen / R.gspan at
+// insertion; translated groups that stay in their cell are refreshed in place).
+__device__ __forceinline__ int ent_id(const CellEnt& e) { return __float_as_int(e.c.w); }
+__device__ __forceinline__ CellEnt make_ent(const RepDev& R, int g) {
+    const float4 c = R.gcen[g];
+    CellEnt e;
+    e.c = make_float4(c.x, c.y, c.z, __int_as_float(g));
+    e.span = R.gspan[g];
+    e.pad = make_int2(0, 0);
+    return e;
+}
 __device__ __forceinline__ void cell_insert(const RepDev& R, int c, int g) {
     const int n = R.cell_count[c];
     if (n >= R.cap) {
@@ -67,15 +78,15 @@ __device__ __forceinline__ void cell_insert(const RepDev& R, int c, int g) {
         R.gcell[g] = -1;
         return;
     }
-    int* ent = R.cell_ent + (size_t)c * R.cap;
+    CellEnt* ent = R.cell_ent + (size_t)c * R.cap;
     int p = n;
-    while (p > 0 && ent[p - 1] > g) {  // shift larger ids up by one
-        const int h = ent[p - 1];
+    while (p > 0 && ent_id(ent[p - 1]) > g) {  // shift larger ids up by one
+        const CellEnt h = ent[p - 1];
         ent[p] = h;
-        R.gcell[h] = c * R.cap + p;
+        R.gcell[ent_id(h)] = c * R.cap + p;
         --p;
     }
-    ent[p] = g;
+    ent[p] = make_ent(R, g);
     R.cell_count[c] = n + 1;
     R.gcell[g] = c * R.cap + p;
 }
@@ -87,16 +98,16 @@ __device__ __forceinline__ void cell_remove(const RepDev& R, int g) {
     if (cp < 0) return;
     const int c = cp / R.cap;
     const int n = R.cell_count[c];
-    int* ent = R.cell_ent + (size_t)c * R.cap;
+    CellEnt* ent = R.cell_ent + (size_t)c * R.cap;
     for (int p = cp - c * R.cap; p + 1 < n; ++p) {  // shift the rest down by one
-        const int h = ent[p + 1];
+        const CellEnt h = ent[p + 1];
         ent[p] = h;
-        R.gcell[h] = c * R.cap + p;
+        R.gcell[ent_id(h)] = c * R.cap + p;
     }
     R.cell_count[c] = n - 1;
     R.gcell[g] = -1;
 }
-// the cell entry of group `from` now stands for group `to` (same cell)
+// the cell entry of group `from` now stands for group `to` (same cell; R.gcen[to] already set)
 __device__ __forceinline__ void cell_rename(const RepDev& R, int from, int to) {
     const int cp = R.gcell[from];
     if (cp < 0) {
@@ -637,16 +648,24 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     const int a = a0 + lane;
                     bool act = a < na;
                     int res = 0, cn = -1;
+                    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (act) {
                         const int i = S.acc_list[a];
                         res = F.startRes + R.pslot[i];
-                        const float4 c = S.c[i];
+                        c = S.c[i];
                         R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
                         cn = cell_of(R, c.x, c.y, c.z);
                         const int cp = R.gcell[res];
                         act = cp < 0 || cp / R.cap != cn;  // only groups that change cell
                     }
                     warp_cell_moves(R, lane, act, res, true, cn);
+                    // groups that stay in their cell: new centre in their entry (wherever
+                    // the moves above have shifted it)
+                    if (a < na && !act) {
+                        const int cp = R.gcell[res];
+                        if (cp >= 0) R.cell_ent[cp].c = make_float4(c.x, c.y, c.z, __int_as_float(res));
+                    }
+                    __syncwarp();
                 }
             }
         }

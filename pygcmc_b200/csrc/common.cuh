@@ -344,6 +344,15 @@ struct StepDesc {
     U4 perm_key;
 };
 
+// One cell-list entry: the group's centre, id and atom range, so that the
+// cell walk tests a candidate group and expands it into atoms from this one
+// record (no further loads of the group's centre or atom range).
+struct __align__(16) CellEnt {
+    float4 c;   // group centre x, y, z; w: the group id (int bits)
+    int2 span;  // atomStart, atomNum
+    int2 pad;
+};
+
 struct RepDev {
     // geometry and physics
     float L[3], start[3];
@@ -379,7 +388,7 @@ struct RepDev {
     float4* gcen;       // group centre
     int2* gspan;        // (atomStart, atomNum)
     int* cell_count;
-    int* cell_ent;      // [ncell * cap] group ids
+    CellEnt* cell_ent;  // [ncell * cap] entries of each cell, in increasing group id
     int* gcell;         // [ngroups] cell*cap + position, or -1
     float4* grid;       // insertion base points
     float2* lj;         // [ffX * ffY] (100*sigma^2 [nm^2 -> A^2], 4*eps)

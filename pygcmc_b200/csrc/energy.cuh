@@ -24,7 +24,6 @@ namespace gcmc {
 constexpr int kWarpsE = 8;
 constexpr int kGCap = 128;
 constexpr int kACap = 512;
-constexpr int kCCap = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
 // Sites 2p and 2p+1 of a pose, component-interleaved for the packed (f32x2)
@@ -37,9 +36,8 @@ struct WarpBuf {
     float4 site[kMaxSites];  // x, y, z relative to the pose centre, Coulomb constant * charge
     int srow[kMaxSites];     // template type * ffY
     SitePair spair[kMaxSites / 2];
-    uint32_t glist[kGCap];   // group id | image code << 26
+    uint2 glist[kGCap];      // included group: (atomStart | image code << 26, atomNum)
     uint32_t alist[kACap];   // atom id  | image code << 26
-    int cand[kCCap];         // candidate group ids gathered from the cells
     float cs_hi[3][4];       // pose centre + image shift (code 0: 0, 1: +L, 2: -L), high part
     float cs_lo[3][4];       //   and its exact rounding error (TwoSum)
     float4 site_abs[kMaxSites];  // absolute site position, raw charge (Ewald terms)
@@ -263,11 +261,10 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
         int start = 0, cnt = 0;
         uint32_t code = 0;
         if (gi < ng) {
-            const uint32_t ge = B.glist[gi];
-            const int2 sp = __ldg(&R.gspan[(int)(ge & 0x3FFFFFFu)]);
-            start = sp.x;
-            cnt = sp.y;
-            code = ge >> 26;
+            const uint2 ge = B.glist[gi];
+            start = (int)(ge.x & 0x3FFFFFFu);
+            cnt = (int)ge.y;
+            code = ge.x >> 26;
         }
         int incl = cnt;
 #pragma unroll
@@ -318,70 +315,27 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
 }
 
 // Energy of the pose in B.site against the groups whose cells lie in the
-// z-layers [z0, z1) of the +-R window around the pose centre; returns this
-// lane's FP64 partial.  ngroups (warp-uniform) counts the included groups.
-// Cells are visited 32 at a time; their entries are first copied into a warp
-// candidate list, then every lane tests one candidate at a time.
+// window cells [c0, c1) around the pose centre (flattened as
+// ((z * span1) + y) * span0 + x), handed to the sink in buffers of atoms;
+// ngroups (warp-uniform) counts the included groups.  Cells are visited 32 at
+// a time: a warp scan of their entry counts numbers the batch's candidates,
+// and lane t of each round of 32 finds its candidate's cell by binary search
+// over the exclusive prefix, loads the entry (centre, id, atom range; one
+// record) and tests it with the bit-exact inclusion distance.
 __device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
     return c < 0 ? c + n : (c >= n ? c - n : c);
 }
 template <class Sink>
-__device__ __forceinline__ void test_candidates(const RepDev& R, WarpBuf& B, int nc, int self, float cx, float cy,
-                                                float cz, int lane, int& ng, int& ngroups, int ns, Sink& sink,
-                                                long long& npair) {
-    const unsigned lt = (1u << lane) - 1u;
-    for (int base = 0; base < nc; base += 32) {
-        const int t = base + lane;
-        bool inc = false;
-        uint32_t packed = 0;
-        if (t < nc) {
-            const int g = B.cand[t];
-            if (g != self) {
-                const float4 gc = R.gcen[g];
-                inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
-                                           R.cut2_hi, R.fast_incl);
-                if (inc) {
-                    packed = (uint32_t)g;
-                    if (!R.pair_image) {  // the group's periodic image relative to the pose centre
-                        const float rx = rintf((gc.x - cx) * R.invL[0]);
-                        const float ry = rintf((gc.y - cy) * R.invL[1]);
-                        const float rz = rintf((gc.z - cz) * R.invL[2]);
-                        if (fabsf(rx) > 1.0f || fabsf(ry) > 1.0f || fabsf(rz) > 1.0f) {
-                            atomicOr(R.err, ERR_IMAGE);
-                            inc = false;
-                        } else {
-                            const uint32_t code = (rx > 0.0f ? 1u : (rx < 0.0f ? 2u : 0u)) |
-                                                  ((ry > 0.0f ? 1u : (ry < 0.0f ? 2u : 0u)) << 2) |
-                                                  ((rz > 0.0f ? 1u : (rz < 0.0f ? 2u : 0u)) << 4);
-                            packed |= code << 26;
-                        }
-                    }
-                }
-            }
-        }
-        const unsigned m = __ballot_sync(kFull, inc);
-        if (inc) B.glist[ng + __popc(m & lt)] = packed;
-        ng += __popc(m);
-        ngroups += __popc(m);
-        if (ng > kGCap - 32) {
-            __syncwarp();
-            process_groups(R, B, ng, ns, lane, sink, npair);
-            ng = 0;
-        }
-    }
-}
-
-template <class Sink>
 __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                            int self, int c0, int c1, int lane, Sink& sink, int& ngroups,
                                            long long& npair) {
-    // cells [c0, c1) of the window, flattened as ((z * span1) + y) * span0 + x
     set_centre(R, B, cx, cy, cz, lane);
     const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
     const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
     const int pcz = cell_coord(cz, R.start[2], R.invLc[2], R.nc[2]);
     const int sxy = R.span[0] * R.span[1];
     const float inv_s0 = 1.0f / (float)R.span[0], inv_sxy = 1.0f / (float)sxy;
+    const unsigned lt = (1u << lane) - 1u;
     int ng = 0;
     for (int base = c0; base < c1; base += 32) {
         const int j = base + lane;
@@ -402,36 +356,55 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
             if (lane >= off) incl += v;
         }
         const int total = __shfl_sync(kFull, incl, 31);
-        if (total <= kCCap) {
-            // gather the batch's entries with independent loads: entry t belongs to the
-            // last cell whose exclusive prefix is <= t (found by binary search)
-            B.cbase[lane] = cell * R.cap;
-            B.cexcl[lane] = incl - cnt;
-            __syncwarp();
-            for (int t = lane; t < total; t += 32) {
-                int lo = 0, hi = 31;
+        B.cbase[lane] = cell * R.cap;
+        B.cexcl[lane] = incl - cnt;
+        __syncwarp();
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            bool inc = false;
+            uint2 packed = make_uint2(0u, 0u);
+            if (t < total) {
+                int lo = 0, hi = 31;  // the last cell whose exclusive prefix is <= t
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
                     if (B.cexcl[mid] <= t) lo = mid; else hi = mid - 1;
                 }
-                B.cand[t] = __ldg(R.cell_ent + B.cbase[lo] + (t - B.cexcl[lo]));
-            }
-            __syncwarp();
-            test_candidates(R, B, total, self, cx, cy, cz, lane, ng, ngroups, ns, sink, npair);
-            __syncwarp();
-        } else {  // more candidates than the buffer holds: one cell at a time
-            for (int l = 0; l < 32; ++l) {
-                const int cl = __shfl_sync(kFull, cell, l), cn = __shfl_sync(kFull, cnt, l);
-                const int* ent = R.cell_ent + (size_t)cl * R.cap;
-                for (int e0 = 0; e0 < cn; e0 += kCCap) {
-                    const int m = min(kCCap, cn - e0);
-                    for (int e = lane; e < m; e += 32) B.cand[e] = ent[e0 + e];
-                    __syncwarp();
-                    test_candidates(R, B, m, self, cx, cy, cz, lane, ng, ngroups, ns, sink, npair);
-                    __syncwarp();
+                const CellEnt* e = R.cell_ent + B.cbase[lo] + (t - B.cexcl[lo]);
+                const float4 gc = __ldg(&e->c);
+                const int2 sp = __ldg(&e->span);
+                if (__float_as_int(gc.w) != self) {
+                    inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                               R.cut2_hi, R.fast_incl);
+                    if (inc) {
+                        packed = make_uint2((uint32_t)sp.x, (uint32_t)sp.y);
+                        if (!R.pair_image) {  // the group's periodic image relative to the pose centre
+                            const float rx = rintf((gc.x - cx) * R.invL[0]);
+                            const float ry = rintf((gc.y - cy) * R.invL[1]);
+                            const float rz = rintf((gc.z - cz) * R.invL[2]);
+                            if (fabsf(rx) > 1.0f || fabsf(ry) > 1.0f || fabsf(rz) > 1.0f) {
+                                atomicOr(R.err, ERR_IMAGE);
+                                inc = false;
+                            } else {
+                                const uint32_t code = (rx > 0.0f ? 1u : (rx < 0.0f ? 2u : 0u)) |
+                                                      ((ry > 0.0f ? 1u : (ry < 0.0f ? 2u : 0u)) << 2) |
+                                                      ((rz > 0.0f ? 1u : (rz < 0.0f ? 2u : 0u)) << 4);
+                                packed.x |= code << 26;
+                            }
+                        }
+                    }
                 }
             }
+            const unsigned m = __ballot_sync(kFull, inc);
+            if (inc) B.glist[ng + __popc(m & lt)] = packed;
+            ng += __popc(m);
+            ngroups += __popc(m);
+            if (ng > kGCap - 32) {
+                __syncwarp();
+                process_groups(R, B, ng, ns, lane, sink, npair);
+                ng = 0;
+            }
         }
+        __syncwarp();  // cbase / cexcl are rewritten by the next batch
     }
     __syncwarp();
     process_groups(R, B, ng, ns, lane, sink, npair);

@@ -39,7 +39,7 @@ struct RepHost {
     float4* gcen = nullptr;
     int2* gspan = nullptr;
     int* cell_count = nullptr;
-    int* cell_ent = nullptr;
+    CellEnt* cell_ent = nullptr;
     int* gcell = nullptr;
     float4* grid = nullptr;
     float2* lj = nullptr;
