@@ -5,15 +5,16 @@
 //
 // One CTA per replica.  For clustering moves the CTA
 //   1. sums each pose's slab partials (FP64) and precomputes per pose the
-//      Boltzmann weight relative to the step's lowest energy, the Gumbel key
-//      -beta*E + G (Gumbel-max picks pose i with probability w_i / sum w, the
-//      law of the reference's roulette selection) and ln u of the acceptance
-//      draw; it stages the pose-pose bit matrix in shared memory;
-//   2. warp 0 walks the clusters in pose-index order: seed = lowest unused
+//      log-weight -beta*E and the Gumbel key -beta*E + G (Gumbel-max picks
+//      pose i with probability w_i / sum w, the law of the reference's
+//      roulette selection); the per-pose draws and the pose-pose bit matrix
+//      are staged in shared memory;
+//   2. the clusters are walked in pose-index order: seed = lowest unused
 //      pose, members = unused poses within the cutoff of the seed (one 32-bit
-//      word per lane), W and the argmax key by butterfly reductions, the
-//      Rosenbluth / Metropolis acceptance in FP64; an accepted cluster also
-//      removes the unused poses within the cutoff of its chosen pose;
+//      word per lane), the argmax key and the Rosenbluth / Metropolis
+//      acceptance in FP64 (decided from bounds on ln W where they settle it);
+//      an accepted cluster also removes the unused poses within the cutoff of
+//      its chosen pose;
 //   3. all warps write the accepted poses into their slots, then one thread
 //      applies the cell-list and count updates in acceptance order.
 #pragma once
@@ -26,7 +27,7 @@ constexpr int kAcceptThreads = 1024;
 struct AcceptSmem {
     double E[kMaxPoses];      // energy entering the acceptance (force-biased: dE - ln(q ratio) / beta)
     double ephys[kMaxPoses];  // the pose's energy (insert/delete) or energy change (translate/rotate)
-    double w[kMaxPoses];
+    double a[kMaxPoses];      // log-weight -beta E of pose i (-inf if E is not finite)
     unsigned long long key[kMaxPoses];  // order-preserving encoding of the Gumbel key
     alignas(16) double lnu[kMaxPoses];  // ln of the acceptance draw of the cluster seeded by pose i
     alignas(16) double gum[kMaxPoses];  // Gumbel draw -ln(-ln u) of pose i
@@ -42,7 +43,9 @@ struct AcceptSmem {
     int spec_seed[32];
     int spec_cnt[32];
     int spec_chosen[32];  // Gumbel argmax, -1 if no member has a finite energy
-    double spec_lnq[32];  // ln(W) - ln(cnt), W = sum over members of exp(-beta E)
+    double spec_lnq[32];  // exact ln(W) - ln(cnt) (W = sum over members of exp(-beta E)) when spec_dec = 0
+    int spec_dec[32];     // +1 / -1: accepted / rejected for every K the round can reach; 0: compare with lnq
+    double kr[2];         // K range of the round: the lowest K the step can reach, K at the round's start
     int spec_n;
 };
 
@@ -161,16 +164,6 @@ __device__ __forceinline__ unsigned long long key_order(double d) {
 }
 
 // ---- block reductions ----
-__device__ __forceinline__ double block_min(double v, double* red) {
-    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, off));
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : INFINITY;
-    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, off));
-    return v;
-}
 __device__ __forceinline__ double block_sum(double v, double* red) {
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,6 +284,74 @@ __global__ void k_build_cells(const RepDev* __restrict__ reps, int nrep) {
     }
 }
 
+__device__ __forceinline__ double key_value(unsigned long long k) {  // inverse of key_order
+    return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
+}
+
+// Evaluation of the cluster with member words m (lane = word) and seed draw
+// ln u, warp-collective.  Results: member count, the Gumbel argmax (-1 if no
+// member has a finite energy) and the decision of "ln u < lnq + K" with
+//   lnq = ln(W') + M - ln(cnt),  W' = sum over members of exp(a_i - M),
+// a_i = -beta E_i, M = max a_i, for every K of the round's range [Klo, Khi]:
+// dec = +1 (accepted for all of them), -1 (rejected for all), or 0 with lnq
+// computed (then the commit compares with its K).  The max term of W' is
+// exactly 1 and the others lie in [0, 1], so ln W' lies in [0, ln cnt] and
+// lnq in [M - ln cnt, M]; dec is decided from that range (ln cnt bounded above
+// by ln 2 * ceil(log2 cnt), a margin above the rounding of the exact form),
+// and exp / log are evaluated only when ln u falls inside it.
+__device__ __forceinline__ void eval_cluster(const AcceptSmem& S, uint32_t m, int lane, double lnu, double Klo,
+                                             double Khi, int& cnt_out, int& chosen_out, int& dec_out,
+                                             double& lnq_out) {
+    const int cnt = __reduce_add_sync(kFull, (unsigned)__popc(m));
+    unsigned long long best = 0ull, amax = 0ull;
+    int bi = -1;
+    for (uint32_t mm = m; mm; mm &= mm - 1u) {
+        const int i = 32 * lane + __ffs(mm) - 1;
+        const unsigned long long kk = S.key[i];
+        if (kk > best) { best = kk; bi = i; }
+        const double ai = S.a[i];
+        if (ai > -INFINITY) {
+            const unsigned long long ak = key_order(ai);
+            if (ak > amax) amax = ak;
+        }
+    }
+    // Gumbel argmax (keys are distinct integers; ties cannot occur between members)
+    const unsigned hi = (unsigned)(best >> 32);
+    const unsigned mhi = __reduce_max_sync(kFull, hi);
+    const unsigned lo = (hi == mhi) ? (unsigned)best : 0u;
+    const unsigned mlo = __reduce_max_sync(kFull, lo);
+    const unsigned win = __ballot_sync(kFull, best != 0ull && hi == mhi && (unsigned)best == mlo);
+    const int chosen = win ? __shfl_sync(kFull, bi, __ffs(win) - 1) : -1;
+    // M = max a_i over the members with a finite energy
+    const unsigned ahi = (unsigned)(amax >> 32);
+    const unsigned mahi = __reduce_max_sync(kFull, ahi);
+    const unsigned alo = (ahi == mahi) ? (unsigned)amax : 0u;
+    const unsigned malo = __reduce_max_sync(kFull, alo);
+    int dec = -1;
+    double lnq = -INFINITY;
+    if (chosen >= 0) {
+        const double M = key_value(((unsigned long long)mahi << 32) | malo);
+        const double lnc_hi = 0.6931471805599453 * (double)(32 - __clz(cnt - 1));  // >= ln(cnt)
+        const double eps = 1e-9 * (1.0 + fabs(M) + fabs(Klo) + fabs(Khi) + fabs(lnu));
+        if (lnu < (M - lnc_hi) + Klo - eps) {
+            dec = 1;
+        } else if (lnu > M + Khi + eps) {
+            dec = -1;
+        } else {
+            double w = 0.0;
+            for (uint32_t mm = m; mm; mm &= mm - 1u) w += exp(S.a[32 * lane + __ffs(mm) - 1] - M);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) w += __shfl_xor_sync(kFull, w, off);
+            lnq = (log(w) + M) - log((double)cnt);
+            dec = 0;
+        }
+    }
+    cnt_out = cnt;
+    chosen_out = chosen;
+    dec_out = dec;
+    lnq_out = lnq;
+}
+
 __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     AcceptSmem& S = *reinterpret_cast<AcceptSmem*>(smem_raw);
@@ -407,15 +468,12 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         }
     } else if (k > 0) {
         // ---- phase 1: per-pose weights, Gumbel keys, acceptance draws, bit rows
-        double emin_loc = INFINITY;
-        for (int i = tid; i < k; i += nt)
-            if (isfinite(S.E[i])) emin_loc = fmin(emin_loc, S.E[i]);
-        cp_async_wait_all();  // this thread's staged copies; block_min's barriers publish them
-        const double Eref = block_min(emin_loc, S.red);
+        cp_async_wait_all();  // this thread's staged copies
+        __syncthreads();      // everyone's
         for (int i = tid; i < k; i += nt) {
             const double e = S.E[i];
             const bool fin = isfinite(e);
-            S.w[i] = fin ? exp(-kBeta * (e - Eref)) : 0.0;
+            S.a[i] = fin ? -kBeta * e : -INFINITY;
             S.key[i] = fin ? key_order(-kBeta * e + S.gum[i]) : 0ull;  // Gumbel-max key
         }
         const int nw = D.nw;
@@ -430,8 +488,8 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         // acceptance the unused poses within the cutoff of the chosen pose) leave
         // the unused set.  Each round, warp 0 seeds up to 32 clusters ahead
         // assuming no acceptance; all warps evaluate them in parallel (member
-        // count, Gumbel argmax and ln(W) - ln(cnt) with W = sum of exp(-beta E));
-        // warp 0 then commits them in order.  A speculative cluster is exactly
+        // count, Gumbel argmax and the decision for the round's range of K, see
+        // eval_cluster); warp 0 then commits them in order.  A speculative cluster is exactly
         // the sequential one while its seed and all its members are still unused
         // (removing other poses can neither lower the seed nor change the member
         // set); at the first cluster that fails this test the round ends and the
@@ -447,6 +505,8 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         int wn = D.n, wna = 0, wnc = 0, wfa = -1;
         const double K0 = ins ? (R.lncav + F.B) : 0.0;
         double K = ins ? K0 - S.lnn[0] : 0.0;
+        // K only decreases (one ln(n+1) step per accepted insertion), down to Klo
+        const double Klo = ins ? K0 - S.lnn[min(k, F.maxNum - D.n)] : 0.0;
         int nrounds = 0;
         int depth = 32;  // speculation depth: halves after a round cut short, doubles after a full one
         for (int round = 0; round <= k; ++round) {
@@ -467,57 +527,25 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     if (lane == 0) S.spec_seed[nb] = sd;
                     ++nb;
                 }
-                if (lane == 0) S.spec_n = nb;
+                if (lane == 0) {
+                    S.spec_n = nb;
+                    S.kr[0] = Klo;
+                    S.kr[1] = K;
+                }
             }
             __syncthreads();
             const int nb = S.spec_n;
             if (nb == 0) break;
             if (warp < nb) {  // evaluation, one warp per speculative cluster
-                const uint32_t m = S.spec_mask[warp][lane];
-                const int cnt = __reduce_add_sync(kFull, (unsigned)__popc(m));
-                double wsum = 0.0;
-                unsigned long long best = 0ull;
-                int bi = -1;
-                for (uint32_t mm = m; mm; mm &= mm - 1u) {
-                    const int i = 32 * lane + __ffs(mm) - 1;
-                    wsum += S.w[i];
-                    const unsigned long long kk = S.key[i];
-                    if (kk > best) { best = kk; bi = i; }
-                }
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) wsum += __shfl_xor_sync(kFull, wsum, off);
-                const unsigned hi = (unsigned)(best >> 32);
-                const unsigned mhi = __reduce_max_sync(kFull, hi);
-                const unsigned lo = (hi == mhi) ? (unsigned)best : 0u;
-                const unsigned mlo = __reduce_max_sync(kFull, lo);
-                const unsigned win = __ballot_sync(kFull, best != 0ull && hi == mhi && (unsigned)best == mlo);
-                const int chosen = win ? __shfl_sync(kFull, bi, __ffs(win) - 1) : -1;
-                double lnq = -INFINITY;
-                if (chosen >= 0) {
-                    double lnW;
-                    if (wsum > 1e-300) {
-                        lnW = log(wsum) - kBeta * Eref;
-                    } else {  // every member far above Eref: weights relative to the cluster minimum
-                        double em = INFINITY;
-                        for (uint32_t mm = m; mm; mm &= mm - 1u) {
-                            const double e = S.E[32 * lane + __ffs(mm) - 1];
-                            if (isfinite(e)) em = fmin(em, e);
-                        }
-                        for (int off = 16; off > 0; off >>= 1) em = fmin(em, __shfl_xor_sync(kFull, em, off));
-                        double w2 = 0.0;
-                        for (uint32_t mm = m; mm; mm &= mm - 1u) {
-                            const double e = S.E[32 * lane + __ffs(mm) - 1];
-                            if (isfinite(e)) w2 += exp(-kBeta * (e - em));
-                        }
-                        for (int off = 16; off > 0; off >>= 1) w2 += __shfl_xor_sync(kFull, w2, off);
-                        lnW = log(w2) - kBeta * em;
-                    }
-                    lnq = lnW - log((double)cnt);
-                }
+                const int sd = S.spec_seed[warp];
+                int cnt, chosen, dec;
+                double lnq;
+                eval_cluster(S, S.spec_mask[warp][lane], lane, S.lnu[sd], S.kr[0], S.kr[1], cnt, chosen, dec, lnq);
                 if (lane == 0) {
                     S.spec_cnt[warp] = cnt;
                     S.spec_lnq[warp] = lnq;
                     S.spec_chosen[warp] = chosen;
+                    S.spec_dec[warp] = dec;
                 }
             }
             __syncthreads();
@@ -532,13 +560,15 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 // within a round, so the check runs after one.
                 const int my_seed = lane < nb ? S.spec_seed[lane] : 0;
                 const int my_chosen = lane < nb ? S.spec_chosen[lane] : -1;
+                const int my_dec = lane < nb ? S.spec_dec[lane] : -1;
                 const double my_lnq = lane < nb ? S.spec_lnq[lane] : 0.0;
                 const double my_lnu = lane < nb ? S.lnu[my_seed] : 0.0;
                 int j = 0;
                 bool dirty = false;  // an acceptance of this round has removed poses from u
                 while (j < nb) {
-                    const unsigned am =
-                        __ballot_sync(kFull, lane >= j && lane < nb && my_chosen >= 0 && my_lnu < my_lnq + K);
+                    const unsigned am = __ballot_sync(
+                        kFull, lane >= j && lane < nb && my_chosen >= 0 &&
+                                   (my_dec > 0 || (my_dec == 0 && my_lnu < my_lnq + K)));
                     const int ja = am ? __ffs(am) - 1 : nb;  // first accepting cluster (nb: none)
                     int jstop = ja;                          // clusters [j, jstop) are rejected
                     bool cut = false;
