@@ -23,6 +23,7 @@
 namespace gcmc {
 
 constexpr int kAcceptThreads = 1024;
+constexpr int kNbHalf = kMaxPoses * kMaxWords / 2;  // words
 
 struct AcceptSmem {
     double E[kMaxPoses];      // energy entering the acceptance (force-biased: dE - ln(q ratio) / beta)
@@ -368,8 +369,16 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     // arrive while the energies are summed.  Sizes are rounded up to whole
     // 16-byte chunks; the sources hold kMaxPoses entries (kMaxPoses x kMaxWords
     // words), so the rounding stays inside them.
+    // The slab partials of the pose energies follow when they fit in the upper
+    // half of the bit-matrix array beside the step's rows (translate/rotate
+    // steps: few poses, many slabs each).
+    double* const Ep = reinterpret_cast<double*>(&S.nb[kNbHalf]);
+    const int npart = k * D.nvar * D.nslab;
+    const bool stage_e = D.move != MV_DELETE && k > 0 && ((k * D.nw + 3) & ~3) <= kNbHalf && npart <= kNbHalf / 2;
     if (D.move != MV_DELETE && k > 0) {
         const int nb16 = (k * D.nw + 3) >> 2, d16 = (k + 1) >> 1;
+        if (stage_e)  // the source holds kMaxPoses * 2 * (max slabs) partials: an even count
+            for (int x = tid; x < (npart + 1) >> 1; x += nt) cp_async16(&Ep[2 * x], R.epart + 2 * x);
         for (int x = tid; x < nb16; x += nt) cp_async16(&S.nb[4 * x], R.nbr + 4 * x);
         for (int x = tid; x < k; x += nt) cp_async16(&S.c[x], R.pcen + x);
         for (int x = tid; x < d16; x += nt) {
@@ -398,12 +407,17 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
         const double change = -R.pme_bgc * ((Q + dq) * (Q + dq) - Q * Q);
         bg = D.move == MV_INSERT ? change : -change;  // a deletion's E is minus the system's change
     }
+    if (stage_e) {
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    const double* ep = stage_e ? Ep : R.epart;
     for (int i = tid; i < k; i += nt) {
         double e = 0.0;
-        for (int z = 0; z < D.nslab; ++z) e += R.epart[(i * D.nvar) * D.nslab + z];
+        for (int z = 0; z < D.nslab; ++z) e += ep[(i * D.nvar) * D.nslab + z];
         if (D.nvar == 2) {
             double eo = 0.0;
-            for (int z = 0; z < D.nslab; ++z) eo += R.epart[(i * 2 + 1) * D.nslab + z];
+            for (int z = 0; z < D.nslab; ++z) eo += ep[(i * 2 + 1) * D.nslab + z];
             e = e - eo;
         }
         e += bg;
@@ -632,12 +646,8 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 const int res = F.startRes + slot;
                 const int2 sp = R.gspan[res];
                 const float4 c = S.c[i];
-                const Mat3 Rm = insert_rotation(R, D.step, i);
-                if (lane < ns) {
-                    const float4 t = F.site[lane];
-                    float x, y, z;
-                    rotate(Rm, t.x, t.y, t.z, x, y, z);
-                    R.xyzq[sp.x + lane] = make_float4(fadd(x, c.x), fadd(y, c.y), fadd(z, c.z), t.w);
+                if (lane < ns) {  // the pose's sites as built by the pose-energy kernel
+                    R.xyzq[sp.x + lane] = R.psite[i * kMaxSites + lane];
                     R.atype[sp.x + lane] = F.stype[lane];
                 }
                 if (lane == 0) R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
@@ -662,15 +672,13 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 const int i = S.acc_list[a];
                 const int res = F.startRes + R.pslot[i];
                 const int2 sp = R.gspan[res];
-                const float4 gc = R.gcen[res];
-                float px = 0.f, py = 0.f, pz = 0.f, qw = 0.f;
-                if (lane < ns) {
-                    const float4 at = R.xyzq[sp.x + lane];
-                    px = at.x; py = at.y; pz = at.z; qw = at.w;
+                if (lane < ns) {  // moved sites as built by the pose-energy kernel; the charge stays
+                    const float4 p = R.psite[i * kMaxSites + lane];
+                    float* dst = reinterpret_cast<float*>(R.xyzq + sp.x + lane);
+                    dst[0] = p.x;
+                    dst[1] = p.y;
+                    dst[2] = p.z;
                 }
-                if (D.fb) fb_moved_site(R, D, i, gc, ns, lane, px, py, pz);
-                else moved_site(R, D, i, gc, ns, lane, px, py, pz);
-                if (lane < ns) R.xyzq[sp.x + lane] = make_float4(px, py, pz, qw);
             }
             __syncthreads();
             if (warp == 0 && D.move == MV_TRANSLATE) {

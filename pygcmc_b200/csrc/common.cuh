@@ -407,6 +407,7 @@ struct RepDev {
     unsigned long long* counters;  // steps, poses, pairs, then 8 accept-kernel phase cycle sums
     int* err;
     double* energy;     // running sum of the accepted moves' energy changes (FP64)
+    float4* psite;      // [kMaxPoses * kMaxSites] trial sites (x, y, z, charge) of pose i, new variant
     double* pgum;       // [kMaxPoses] -ln(-ln u) Gumbel draw of pose i (clustering moves)
     double* plnu;       // [kMaxPoses] ln u of the acceptance draw of the cluster seeded by pose i
     // force-biased moves

@@ -611,6 +611,15 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
     __syncwarp();
 }
 
+// The first item of pose i's new variant keeps its trial sites (absolute
+// position, charge) for the accept kernel, which writes an accepted pose from
+// them instead of rebuilding it.
+__device__ __forceinline__ void keep_sites(const RepDev& R, const StepDesc& D, const WarpBuf& B, int i, int v, int zi,
+                                           int lane) {
+    if (v == 0 && zi == 0 && D.move != MV_DELETE && lane < R.frag[D.ftype].nsites)
+        R.psite[i * kMaxSites + lane] = B.site_abs[lane];
+}
+
 // The draws of pose i that do not depend on energies, made once per pose by
 // the pose-energy kernels (off the single-CTA accept kernel's critical path):
 // the Gumbel perturbation -ln(-ln u) and ln u of the cluster acceptance draw.
@@ -701,6 +710,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
+        keep_sites(R, D, B, i, v, zi, lane);
         double acc = 0.0;
         int ng = 0;
         long long npair = 0;

@@ -32,7 +32,7 @@ struct RepHost {
     int nslab = 0, log_cap = 0, log_kmax = 0;
     int host_end = 0;
     std::vector<int> startRes, maxNum, moves_host;
-    size_t capn[32] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
+    size_t capn[48] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
     // device allocations (owned)
     float4* xyzq = nullptr;
     int* atype = nullptr;
@@ -56,6 +56,7 @@ struct RepHost {
     unsigned long long* counters = nullptr;
     int* err = nullptr;
     double* energy = nullptr;
+    float4* psite = nullptr;
     double* pgum = nullptr;
     double* plnu = nullptr;
     float* fpart = nullptr;
@@ -137,7 +138,7 @@ void free_rep(RepHost& h) {
     dfree(h.gcell); dfree(h.grid); dfree(h.lj); dfree(h.moves); dfree(h.frag); dfree(h.totalNum);
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
-    dfree(h.energy); dfree(h.pgum); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
+    dfree(h.energy); dfree(h.pgum); dfree(h.psite); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
     if (h.plans) {
         cufftDestroy(h.plan_f);
@@ -420,6 +421,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.counters, 16); AL(h.err, 1);
     AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
+    AL(h.psite, (size_t)kMaxPoses * kMaxSites);
     // smooth PME: mesh, influence function, FFT plans
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
     if (h.pme && opt.proposal == 2) return GCMC_ERR_ARG;  // force bias runs without Ewald
@@ -501,7 +503,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.desc = h.desc; d.pcen = h.pcen; d.pslot = h.pslot; d.epart = h.epart; d.nbr = h.nbr;
     d.log = h.log; d.logE = h.logE; d.log_cap = h.log_cap; d.log_kmax = h.log_kmax;
     d.counters = h.counters; d.err = h.err;
-    d.energy = h.energy; d.pgum = h.pgum; d.plnu = h.plnu; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
+    d.energy = h.energy; d.pgum = h.pgum; d.psite = h.psite; d.plnu = h.plnu; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
     d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
     return GCMC_OK;
 }

@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
+        if (phase != 1) keep_sites(R, D, B, i, v, zi, lane);
         const int ns = R.frag[D.ftype].nsites;
         const int nwin = R.span[0] * R.span[1] * R.span[2];
         const int c0 = zi * nwin / D.nslab, c1 = (zi + 1) * nwin / D.nslab;
