@@ -651,6 +651,72 @@ __device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int
     }
 }
 
+// Transpose of a 32 x 32 bit block held one row per lane (bit c of lane r =
+// entry (r, c)): afterwards lane c holds column c (bit r = entry (r, c)).
+// Five rounds of exchanging the off-diagonal s x s sub-blocks between lanes
+// l and l ^ s (s = 16, 8, 4, 2, 1).
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+    const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const int sft = 16 >> t;
+        const uint32_t M = masks[t];
+        const uint32_t y = __shfl_xor_sync(kFull, x, sft);
+        x = (lane & sft) ? ((x & ~M) | ((y >> sft) & M)) : ((x & M) | ((y & M) << sft));
+    }
+    return x;
+}
+
+// Block task p (upper triangle in row order) of the pose-pose "within cutoff"
+// bit matrix, whose 32 x 32 blocks (I, J), I <= J, cover all of it: the matrix
+// is symmetric bit for bit (both distance forms are odd in the difference and
+// round symmetrically), so lane c tests pose 32 J + c against the block's 32
+// row poses (centres broadcast by shuffles), the row words of (I, J) come from
+// ballots and those of the mirror block (J, I) from their transpose.  A
+// diagonal block also makes the energy-independent draws of its 32 poses.
+__device__ __forceinline__ void nbr_block(const RepDev& R, const StepDesc& D, int p, int lane) {
+    const int k = D.k, nw = D.nw;
+    int I = 0, rem = p;
+    while (rem >= nw - I) {
+        rem -= nw - I;
+        ++I;
+    }
+    const int J = I + rem;
+    const int jc = 32 * J + lane, ir = 32 * I + lane;
+    if (I == J && jc < k) pose_draws(R, D, jc);
+    float4 cj = make_float4(0.f, 0.f, 0.f, 0.f), cr = cj;
+    if (jc < k) cj = R.pcen[jc];
+    if (ir < k) cr = R.pcen[ir];
+    const int nrow = min(32, k - 32 * I);
+    uint32_t mine = 0u;  // lane r: word J of row 32 I + r
+    for (int r = 0; r < nrow; ++r) {
+        const float x = __shfl_sync(kFull, cr.x, r), y = __shfl_sync(kFull, cr.y, r), z = __shfl_sync(kFull, cr.z, r);
+        const bool b = jc < k && within_cutoff<true>(x, y, z, cj.x, cj.y, cj.z, R.L, R.invL, R.cutoff, R.cut2_lo,
+                                                     R.cut2_hi, R.fast_incl);
+        const unsigned m = __ballot_sync(kFull, b);
+        if (lane == r) mine = m;
+    }
+    if (ir < k) R.nbr[ir * nw + J] = mine;
+    if (I != J) {
+        const uint32_t t = transpose32(mine, lane);  // lane c: word I of row 32 J + c
+        if (jc < k) R.nbr[jc * nw + I] = t;
+    }
+}
+
+// New-variant item (i, zi)'s share of the bit matrix.  A launch with more
+// items than resident warps is throughput-bound: there the first
+// nw (nw + 1) / 2 items compute a block each (half the distance tests);
+// otherwise every item computes its slab's share of pose i's row, which keeps
+// each item's latency short.  Both give the same matrix.
+__device__ __forceinline__ void nbr_share(const RepDev& R, const StepDesc& D, int i, int zi, int lane, bool sym) {
+    if (sym) {
+        const int p = i * D.nslab + zi;
+        if (p < D.nw * (D.nw + 1) / 2) nbr_block(R, D, p, lane);
+    } else {
+        nbr_rows(R, D, i, zi, lane);
+    }
+}
+
 // pre[r] = work items of the replicas before r, pre[nrep] = all of them,
 // computed by the whole block (one replica per thread, warp scans, then the
 // warp totals) so that no thread walks the replica list alone.
@@ -696,6 +762,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     items_prefix(nrep, pre, wtot, [&](int r) { return reps[r].desc->items; });
     const int total = pre[nrep];
+    const bool sym = total > (int)(gridDim.x * kWarpsE);  // more items than warps: throughput-bound
     WarpBuf& B = bufs[warp];
     for (int it = blockIdx.x * kWarpsE + warp; it < total; it += gridDim.x * kWarpsE) {
         int lo = 0, hi = nrep;  // find r with pre[r] <= it < pre[r+1]
@@ -726,7 +793,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
-        if (v == 0 && D.nw > 0) nbr_rows(R, D, i, zi, lane);  // this slab's share of pose i's row
+        if (v == 0 && D.nw > 0) nbr_share(R, D, i, zi, lane, sym);
         __syncwarp();
     }
 }

@@ -190,7 +190,9 @@ __global__ void __launch_bounds__(kWarpsG * 32)
 //          are (pose i, slab) of the NEW poses (variant 0) with forces.
 // Non-force-biased steps have no phase-1 items and run the energy path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __restrict__ reps, int nrep, int phase) {
+// (Five CTAs per SM: at most 102 registers a thread, the budget that keeps
+// 20 warps per SM resident.)
+__global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __restrict__ reps, int nrep, int phase) {
     __shared__ WarpBuf bufs[kWarpsG];
     __shared__ GradStage stages[kWarpsG];
     __shared__ int pre[257];
@@ -201,6 +203,7 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
         return phase == 1 ? d->items_pre : d->items;
     });
     const int total = pre[nrep];
+    const bool sym = total > (int)(gridDim.x * kWarpsG);
     WarpBuf& B = bufs[warp];
     for (int it = blockIdx.x * kWarpsG + warp; it < total; it += gridDim.x * kWarpsG) {
         int lo = 0, hi = nrep;
@@ -285,8 +288,8 @@ __global__ void __launch_bounds__(kWarpsG * 32) k_energy_fb(const RepDev* __rest
                 const float4 gc = R.gcen[R.frag[D.ftype].startRes + R.pslot[i]];
                 R.pcen[i] = fb_propose(R, D, i, fo, gc, R.fbprop + 2 * i);
             }
-        } else if (v == 0 && D.nw > 0) {  // this slab's share of the neighbour row of pose i
-            nbr_rows(R, D, i, zi, lane);
+        } else if (v == 0 && D.nw > 0) {  // this item's share of the neighbour bit matrix
+            nbr_share(R, D, i, zi, lane, sym);
         }
         __syncwarp();
     }
