@@ -41,6 +41,7 @@ struct AcceptSmem {
     int misc[8];
     // one round of speculative clusters (seeded in order assuming no acceptance)
     uint32_t spec_mask[32][kMaxWords];
+    uint32_t spec_us[33][kMaxWords];  // unused words after the round's first c seeds (c = 0..32)
     int spec_seed[32];
     int spec_cnt[32];
     int spec_chosen[32];  // Gumbel argmax, -1 if no member has a finite energy
@@ -528,6 +529,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             if (warp == 0) {  // speculative seeding
                 uint32_t us = u;
                 int nb = 0;
+                S.spec_us[0][lane] = us;
                 while (nb < depth) {
                     // lowest unused pose: minimum over the lanes' lowest set bits
                     const unsigned low = us ? (unsigned)(32 * lane + __ffs(us) - 1) : 0xffffffffu;
@@ -538,6 +540,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     if (lane == (sd >> 5)) m |= 1u << (sd & 31);
                     us &= ~m;
                     S.spec_mask[nb][lane] = m;
+                    S.spec_us[nb + 1][lane] = us;
                     if (lane == 0) S.spec_seed[nb] = sd;
                     ++nb;
                 }
@@ -568,45 +571,49 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                 // cluster depends only on its own scalars and on K, which changes only
                 // at an acceptance, so the decisions of all clusters after the last
                 // acceptance are made at once and the clusters before the first
-                // accepting one are committed together (u loses the union of their
-                // members).  A cluster is exact while none of its poses has left u;
-                // only an acceptance (its chosen pose's neighbours) can break that
-                // within a round, so the check runs after one.
+                // accepting one are committed together: u keeps only the unused
+                // words after their seeding (spec_us).  A cluster is exact while none
+                // of its poses has left u, and only an acceptance (the unused poses
+                // within the cutoff of its chosen pose) removes poses of later
+                // clusters.  A removed pose's cluster is the first c whose seeding
+                // took it out of spec_us (binary search over c), and the earliest
+                // such cluster is where the round ends.
                 const int my_seed = lane < nb ? S.spec_seed[lane] : 0;
                 const int my_chosen = lane < nb ? S.spec_chosen[lane] : -1;
                 const int my_dec = lane < nb ? S.spec_dec[lane] : -1;
                 const double my_lnq = lane < nb ? S.spec_lnq[lane] : 0.0;
                 const double my_lnu = lane < nb ? S.lnu[my_seed] : 0.0;
                 int j = 0;
-                bool dirty = false;  // an acceptance of this round has removed poses from u
+                int cut = nb + 1;  // first cluster that lost a pose to an acceptance (nb + 1: none)
                 while (j < nb) {
                     const unsigned am = __ballot_sync(
                         kFull, lane >= j && lane < nb && my_chosen >= 0 &&
                                    (my_dec > 0 || (my_dec == 0 && my_lnu < my_lnq + K)));
                     const int ja = am ? __ffs(am) - 1 : nb;  // first accepting cluster (nb: none)
-                    int jstop = ja;                          // clusters [j, jstop) are rejected
-                    bool cut = false;
-                    if (dirty) {  // first cluster in [j, min(ja, nb - 1)] that lost a pose
-                        const int jend = min(ja, nb - 1);
-                        unsigned bad = 0u;
-                        for (int c = j; c <= jend; ++c)
-                            if (S.spec_mask[c][lane] & ~u) bad |= 1u << c;
-                        bad = __reduce_or_sync(kFull, bad);
-                        if (bad) {
-                            jstop = __ffs(bad) - 1;
-                            cut = true;
-                        }
-                    }
-                    uint32_t gone = 0u;
-                    for (int c = j; c < jstop; ++c) gone |= S.spec_mask[c][lane];
-                    u &= ~gone;
+                    const int jstop = min(ja, cut);          // clusters [j, jstop) are rejected
+                    u &= S.spec_us[jstop][lane];
                     wnc += jstop - j;
                     j = jstop;
-                    if (cut || j >= nb) break;
+                    if (j >= nb || j == cut) break;
                     // cluster j accepts its chosen pose
                     const int chosen = __shfl_sync(kFull, my_chosen, j);
-                    u &= ~S.spec_mask[j][lane];
-                    if (lane < nw) u &= ~S.nb[chosen * nw + lane];
+                    u &= S.spec_us[j + 1][lane];
+                    const uint32_t row = lane < nw ? S.nb[chosen * nw + lane] : 0u;
+                    const uint32_t lost = u & row;
+                    u &= ~row;
+                    unsigned first = 0xffffffffu;
+                    for (uint32_t mm = lost; mm; mm &= mm - 1u) {
+                        const int b = __ffs(mm) - 1;
+                        if ((S.spec_us[nb][lane] >> b) & 1u) continue;  // in no cluster of this round
+                        int lo = j + 2, hi = nb;  // first t with the bit cleared in spec_us[t]: cluster t - 1
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if ((S.spec_us[mid][lane] >> b) & 1u) lo = mid + 1; else hi = mid;
+                        }
+                        first = min(first, (unsigned)(lo - 1));
+                    }
+                    first = __reduce_min_sync(kFull, first);
+                    if (first != 0xffffffffu) cut = min(cut, (int)first);
                     int slot = 0;
                     if (ins) {
                         if (wn < F.maxNum) {
@@ -622,7 +629,6 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
                     if (wfa < 0) wfa = chosen;
                     ++wnc;
                     ++j;
-                    dirty = true;
                 }
                 depth = (j < nb) ? max(1, min(depth, 2 * j) / 2 + 1) : min(32, 2 * depth);
             }
