@@ -200,9 +200,9 @@ def run_ours(args, ws, rank, local):
     eng.close()
     # end to end through the drop-in API with host arrays, over the same step range:
     # warm-up calls advance the host state through the first `warmup` chunks
-    e2e_state = sysm.copy()
+    e2e_state = sysm.pinned()  # host arrays in page-locked memory
     h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * chunk
-    d2h = e2e_state.fragmentInfo.nbytes + e2e_state.residueInfo.nbytes + e2e_state.atomInfo.nbytes
+    d2h = e2e_state.moved_bytes()
     info = e2e_state.SimInfo
     info[0]["mcsteps"] = chunk
     moves = e2e_state.moveArray
@@ -242,7 +242,7 @@ def run_ours(args, ws, rank, local):
                                     f"autotuned before timing ({t_tune:.1f} s, untimed)"}},
         "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 5),
@@ -323,10 +323,10 @@ def run_ours_batched(args, ws, rank, local):
     c2 = [eng.counters(r) for r in range(nrep)]
     eng.close()
     # end to end: the batched drop-in with host arrays (upload, run, download per call)
-    state = [x.copy() for x in systems]
+    state = [x.pinned() for x in systems]  # host arrays in page-locked memory
     h2d = sum(sum(a.nbytes for a in s.arrays()[:6]) + 4 * chunk for s in state)
-    d2h = sum(s.fragmentInfo.nbytes + s.residueInfo.nbytes + s.atomInfo.nbytes for s in state)
-    full_moves = [s.moveArray for s in systems]
+    d2h = sum(s.moved_bytes() for s in state)
+    full_moves = [s.moveArray for s in state]  # page-locked; each call takes a slice of it
     e2e_times = []
     for k in range(args.warmup + args.steps):
         for r, s in enumerate(state):
@@ -362,7 +362,7 @@ def run_ours_batched(args, ws, rank, local):
                    "generate_s": round(t_gen, 2)},
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies, all replicas)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 5),
@@ -547,16 +547,16 @@ def run_ours_forcebias(args, ws, rank, local):
         eng.close()
         res[name] = summ
     # end to end: the runGCMC drop-in with force-biased options, host arrays per call
-    e2e_state = sysm.copy()
+    e2e_state = sysm.pinned()  # host arrays in page-locked memory
     info = e2e_state.SimInfo
     info[0]["mcsteps"] = chunk
     h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * chunk
-    d2h = e2e_state.fragmentInfo.nbytes + e2e_state.residueInfo.nbytes + e2e_state.atomInfo.nbytes
+    d2h = e2e_state.moved_bytes()
     fbopt = default_options(proposal=2, fb_trn=0.5, fb_rot=float(np.radians(10.0)))
     times = []
     for k in range(args.warmup + args.steps):
         info[0]["seed"] = (seed * 7 + k) & 0xFFFFFFFF
-        mv = np.ascontiguousarray(sysm.moveArray[k * chunk:(k + 1) * chunk])
+        mv = np.ascontiguousarray(e2e_state.moveArray[k * chunk:(k + 1) * chunk])  # a page-locked slice
         barrier(ws)
         t0 = time.perf_counter()
         runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
@@ -575,7 +575,7 @@ def run_ours_forcebias(args, ws, rank, local):
                    "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks"},
         "e2e": {"value": round(args.steps * chunk * ws / e2e_s, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "api": "pygcmc_b200.gpu.runGCMC(..., options=proposal 2)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC(..., options=proposal 2)"},
         "forcebias": {"plain": pl, "force_biased": fb,
                       "decorrelated_samples_per_s_ratio": round(fb["decorrelated_samples_per_s"]
                                                                 / max(pl["decorrelated_samples_per_s"], 1e-30), 3),
@@ -623,16 +623,17 @@ def run_ours_large(args, ws, rank, local):
     c2 = [eng.counters(r) for r in range(nrep)]
     eng.close()
     # end to end: the batched drop-in with host arrays (all replicas per call)
-    state = [base.copy() for _ in range(nrep)]
+    state = [base.pinned() for _ in range(nrep)]  # host arrays in page-locked memory
+    full_moves = [st.moveArray for st in state]
     for r, st in enumerate(state):
         st.SimInfo[0]["mcsteps"] = chunk
     h2d = sum(sum(a.nbytes for a in s_.arrays()[:6]) + 4 * chunk for s_ in state)
-    d2h = sum(s_.fragmentInfo.nbytes + s_.residueInfo.nbytes + s_.atomInfo.nbytes for s_ in state)
+    d2h = sum(s_.moved_bytes() for s_ in state)
     times = []
     for k in range(args.warmup + min(args.steps, 3)):
         for r, st in enumerate(state):
             st.SimInfo[0]["seed"] = (args.seed * 7 + 131 * r + k) & 0xFFFFFFFF
-            st.moveArray = np.ascontiguousarray(base.moveArray[k * chunk:(k + 1) * chunk])
+            st.moveArray = np.ascontiguousarray(full_moves[r][k * chunk:(k + 1) * chunk])
         barrier(ws)
         t0 = time.perf_counter()
         runGCMC_batch(state, opt)
@@ -656,7 +657,7 @@ def run_ours_large(args, ws, rank, local):
                    "proposals": "reference (force-biased moves run without Ewald)"},
         "e2e": {"value": round(min(args.steps, 3) * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies incl. erfc and PME interpolation)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 5), "flops_per_pair": FLOPS_PER_PAIR,

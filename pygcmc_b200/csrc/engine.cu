@@ -40,6 +40,9 @@ struct RepHost {
     int2* gspan = nullptr;
     int* cell_count = nullptr;
     CellEnt* cell_ent = nullptr;
+    Atom* raw_atoms = nullptr;      // the caller's arrays as uploaded, unpacked on the device
+    residue* raw_groups = nullptr;
+    float* raw_grid = nullptr;
     int* gcell = nullptr;
     float4* grid = nullptr;
     float2* lj = nullptr;
@@ -138,7 +141,8 @@ void free_rep(RepHost& h) {
     dfree(h.gcell); dfree(h.grid); dfree(h.lj); dfree(h.moves); dfree(h.frag); dfree(h.totalNum);
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
-    dfree(h.energy); dfree(h.pgum); dfree(h.psite); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
+    dfree(h.energy); dfree(h.pgum); dfree(h.psite);
+    dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
     if (h.plans) {
         cufftDestroy(h.plan_f);
@@ -258,6 +262,31 @@ void pme_influence(const int n[3], const float cryst[3], double alpha, double* G
             }
 }
 
+// The caller's arrays (uploaded unchanged) into the engine's layout: atoms ->
+// (x, y, z, charge) + type, residues -> centre + (atomStart, atomNum), cavity
+// grid points -> float4.
+__global__ void k_unpack_atoms(const Atom* __restrict__ in, float4* __restrict__ xyzq, int* __restrict__ atype,
+                               int n) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        const Atom A = in[a];
+        xyzq[a] = make_float4(A.position[0], A.position[1], A.position[2], A.charge);
+        atype[a] = A.type;
+    }
+}
+__global__ void k_unpack_groups(const residue* __restrict__ in, float4* __restrict__ gcen, int2* __restrict__ gspan,
+                                int n) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const residue R = in[g];
+        gcen[g] = make_float4(R.position[0], R.position[1], R.position[2], 0.0f);
+        gspan[g] = make_int2(R.atomStart, R.atomNum);
+    }
+}
+__global__ void k_unpack_grid(const float* __restrict__ in, float4* __restrict__ grid, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        grid[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
+}
+int unpack_blocks(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
+
 int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
     const InfoStruct* I = in.info;
     RepHost& h = ctx->reps[r];
@@ -360,23 +389,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     if (cap > 4096) return GCMC_ERR_LIMIT;
     h.cap = d.cap = cap;
 
-    // host-side SoA conversion
-    std::vector<float4> xyzq(std::max(1, h.natoms));
-    std::vector<int> atype(std::max(1, h.natoms));
-    for (int a = 0; a < h.natoms; ++a) {
-        const Atom& A = in.atomInfo[a];
-        xyzq[a] = make_float4(A.position[0], A.position[1], A.position[2], A.charge);
-        atype[a] = A.type;
-    }
-    std::vector<float4> gcen(std::max(1, h.ngroups));
-    std::vector<int2> gspan(std::max(1, h.ngroups));
-    for (int g = 0; g < h.ngroups; ++g) {
-        const residue& rs = in.residueInfo[g];
-        gcen[g] = make_float4(rs.position[0], rs.position[1], rs.position[2], 0.0f);
-        gspan[g] = make_int2(rs.atomStart, rs.atomNum);
-    }
-    std::vector<float4> grid(std::max(1, h.G));
-    for (int i = 0; i < h.G; ++i) grid[i] = make_float4(in.grid[3 * i], in.grid[3 * i + 1], in.grid[3 * i + 2], 0.0f);
+    // atoms, groups and cavity grid points are uploaded as the caller holds them
+    // and unpacked on the device (k_unpack_*): no host-side copies of the
+    // large arrays
     std::vector<float2> lj((size_t)h.ffX * h.ffY);
     for (size_t x = 0; x < lj.size(); ++x) {
         float sigma = in.ff[2 * x], eps = in.ff[2 * x + 1];
@@ -422,6 +437,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
+    AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
     // smooth PME: mesh, influence function, FFT plans
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
     if (h.pme && opt.proposal == 2) return GCMC_ERR_ARG;  // force bias runs without Ewald
@@ -471,13 +487,23 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     }
 #undef AL
     cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(h.xyzq, xyzq.data(), sizeof(float4) * h.natoms, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(h.atype, atype.data(), sizeof(int) * h.natoms, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(h.gcen, gcen.data(), sizeof(float4) * h.ngroups, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(h.gspan, gspan.data(), sizeof(int2) * h.ngroups, cudaMemcpyHostToDevice, s));
+    if (h.natoms > 0) {
+        CK(cudaMemcpyAsync(h.raw_atoms, in.atomInfo, sizeof(Atom) * h.natoms, cudaMemcpyHostToDevice, s));
+        k_unpack_atoms<<<unpack_blocks(h.natoms), 256, 0, s>>>(h.raw_atoms, h.xyzq, h.atype, h.natoms);
+    }
+    if (h.ngroups > 0) {
+        CK(cudaMemcpyAsync(h.raw_groups, in.residueInfo, sizeof(residue) * h.ngroups, cudaMemcpyHostToDevice, s));
+        k_unpack_groups<<<unpack_blocks(h.ngroups), 256, 0, s>>>(h.raw_groups, h.gcen, h.gspan, h.ngroups);
+    }
     CK(cudaMemsetAsync(h.cell_count, 0, sizeof(int) * h.ncell, s));
     CK(cudaMemsetAsync(h.gcell, 0xff, sizeof(int) * std::max(1, h.ngroups), s));
-    CK(cudaMemcpyAsync(h.grid, grid.data(), sizeof(float4) * std::max(1, h.G), cudaMemcpyHostToDevice, s));
+    if (h.G > 0) {
+        CK(cudaMemcpyAsync(h.raw_grid, in.grid, sizeof(float) * 3 * (size_t)h.G, cudaMemcpyHostToDevice, s));
+        k_unpack_grid<<<unpack_blocks(h.G), 256, 0, s>>>(h.raw_grid, h.grid, h.G);
+    } else {
+        CK(cudaMemsetAsync(h.grid, 0, sizeof(float4), s));
+    }
+    CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h.lj, lj.data(), sizeof(float2) * lj.size(), cudaMemcpyHostToDevice, s));
     if (h.mcsteps > 0) {
         CK(cudaMemcpyAsync(h.moves, in.moveArray, sizeof(int) * h.mcsteps, cudaMemcpyHostToDevice, s));
@@ -767,6 +793,47 @@ std::mutex g_cache_mutex;
 gcmc_ctx* g_cache = nullptr;
 gcmc_ctx* g_batch = nullptr;
 
+// What a run can change in the caller's arrays, written back in place: the
+// fragment types' counts, the fragment residues' centres and the atoms of the
+// fragment slots (fixed groups and atoms never move, so their entries already
+// hold the device's values).
+int download_moved(gcmc_ctx* ctx, int r, const gcmc_replica_in& in) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    RepHost& h = ctx->reps[r];
+    AtomArray* frag = const_cast<AtomArray*>(in.fragmentInfo);
+    residue* res = const_cast<residue*>(in.residueInfo);
+    Atom* atoms = const_cast<Atom*>(in.atomInfo);
+    std::vector<int> tot(h.ntypes);
+    CK(cudaMemcpy(tot.data(), h.totalNum, sizeof(int) * h.ntypes, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < h.ntypes; ++t) frag[t].totalNum = tot[t];
+    const int g0 = frag[0].startRes, g1 = h.ngroups;
+    if (g1 <= g0) return GCMC_OK;
+    std::vector<float4> gcen(g1 - g0);
+    CK(cudaMemcpy(gcen.data(), h.gcen + g0, sizeof(float4) * (g1 - g0), cudaMemcpyDeviceToHost));
+    int lo = h.natoms, hi = 0;
+    for (int g = g0; g < g1; ++g) {
+        res[g].position[0] = gcen[g - g0].x;
+        res[g].position[1] = gcen[g - g0].y;
+        res[g].position[2] = gcen[g - g0].z;
+        lo = std::min(lo, res[g].atomStart);
+        hi = std::max(hi, res[g].atomStart + res[g].atomNum);
+    }
+    if (hi <= lo) return GCMC_OK;
+    std::vector<float4> xyzq(hi - lo);
+    std::vector<int> atype(hi - lo);
+    CK(cudaMemcpy(xyzq.data(), h.xyzq + lo, sizeof(float4) * (hi - lo), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(atype.data(), h.atype + lo, sizeof(int) * (hi - lo), cudaMemcpyDeviceToHost));
+    for (int a = lo; a < hi; ++a) {
+        const float4 p = xyzq[a - lo];
+        atoms[a].position[0] = p.x;
+        atoms[a].position[1] = p.y;
+        atoms[a].position[2] = p.z;
+        atoms[a].charge = p.w;
+        atoms[a].type = atype[a - lo];
+    }
+    return GCMC_OK;
+}
+
 // Refill *slot (or create it) for these inputs, run every replica's mcsteps
 // steps and download the results in place.  Called under g_cache_mutex.
 int cached_run(gcmc_ctx** slot, int nrep, const gcmc_replica_in* ins, const gcmc_options* opt) {
@@ -798,9 +865,7 @@ int cached_run(gcmc_ctx** slot, int nrep, const gcmc_replica_in* ins, const gcmc
     for (int r = 0; r < nrep; ++r) most = std::max(most, (int)ins[r].info->mcsteps);
     st = gcmc_run(*slot, most);
     if (st == GCMC_OK) st = gcmc_sync(*slot);
-    for (int r = 0; r < nrep && st == GCMC_OK; ++r)
-        st = gcmc_download(*slot, r, const_cast<AtomArray*>(ins[r].fragmentInfo),
-                           const_cast<residue*>(ins[r].residueInfo), const_cast<Atom*>(ins[r].atomInfo));
+    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = download_moved(*slot, r, ins[r]);
     if (st != GCMC_OK) {
         destroy_impl(*slot);
         *slot = nullptr;

@@ -53,6 +53,34 @@ class System:
     def copy(self) -> "System":
         return System(*(a.copy() for a in self.arrays()), meta=dict(self.meta))
 
+    def pinned(self) -> "System":
+        """A copy whose arrays live in page-locked host memory (needs torch with
+        CUDA).  The drop-in calls copy page-locked arrays to and from the GPU
+        directly instead of through the driver's staging buffers."""
+        import torch
+        keep, arrs = [], []
+        for a in self.arrays():
+            buf = torch.empty(max(1, a.nbytes), dtype=torch.uint8, pin_memory=True)
+            v = buf.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+            v[...] = a
+            keep.append(buf)
+            arrs.append(v)
+        out = System(*arrs, meta=dict(self.meta))
+        out._page_locked = keep  # the buffers the arrays view
+        return out
+
+    def moved_bytes(self) -> int:
+        """Bytes a drop-in call copies back to the host: the fragment types'
+        counts, the fragment residues' centres and the fragment slots' atoms
+        (position + charge, type)."""
+        g0 = int(self.fragmentInfo[0]["startRes"])
+        res = self.residueInfo[g0:]
+        if len(res) == 0:
+            return 4 * len(self.fragmentInfo)
+        lo = int(res["atomStart"].min())
+        hi = int((res["atomStart"] + res["atomNum"]).max())
+        return 4 * len(self.fragmentInfo) + 16 * len(res) + 20 * max(0, hi - lo)
+
     @property
     def info(self):
         return self.SimInfo[0]

@@ -135,6 +135,21 @@ def test_runGCMC_dropin_matches_engine(protein_small):
     assert np.array_equal(s.atomInfo["position"][a], final.atomInfo["position"][a])
 
 
+def test_runGCMC_writes_back_what_a_full_download_holds(protein_small):
+    """The drop-in copies back only what a run can change (the counts, the
+    fragment residues' centres, the fragment slots' atoms); the caller's arrays
+    then equal the engine's full download field for field, for ordinary and
+    for page-locked host arrays."""
+    from pygcmc_b200.gpu import runGCMC
+    n = int(protein_small.SimInfo[0]["mcsteps"])
+    _, _, final, _ = engine_trajectory(protein_small, n)
+    for s in (protein_small.copy(), protein_small.pinned()):
+        runGCMC(*s.arrays())
+        assert np.array_equal(s.fragmentInfo, final.fragmentInfo)
+        assert np.array_equal(s.residueInfo, final.residueInfo)
+        assert np.array_equal(s.atomInfo, final.atomInfo)
+
+
 def test_replicas_in_one_context_match_single(protein_small, water_small):
     """Several replicas advanced together give each replica's solo result."""
     from pygcmc_b200._native import default_options
