@@ -269,20 +269,54 @@ __global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
     }
 }
 
-// Initial cell lists: fixed groups, then each type's occupied slots, in index order.
-__global__ void k_build_cells(const RepDev* __restrict__ reps, int nrep) {
-    const RepDev& R = reps[blockIdx.x];
-    if (threadIdx.x != 0) return;
-    for (int g = 0; g < R.nfixed; ++g) {
-        float4 c = R.gcen[g];
-        cell_add(R, g, c.x, c.y, c.z);
-    }
-    for (int t = 0; t < R.ntypes; ++t) {
-        const int s0 = R.frag[t].startRes, n = R.totalNum[t];
-        for (int s = 0; s < n; ++s) {
-            float4 c = R.gcen[s0 + s];
-            cell_add(R, s0 + s, c.x, c.y, c.z);
+// Initial cell lists in two parallel passes (grid.y = replica): every present
+// group (fixed, or an occupied fragment slot) appends its record to its cell
+// at a slot from an atomic counter, then each cell is ordered by group id and
+// the groups' record slots are noted -- the same lists as inserting the groups
+// one by one.  A cell that overflows keeps cap records and raises the error
+// flag; the groups left out keep gcell = -1.
+__global__ void k_fill_cells(const RepDev* __restrict__ reps) {
+    const RepDev& R = reps[blockIdx.y];
+    const FragDev& Fl = R.frag[R.ntypes - 1];
+    const int ng = Fl.startRes + Fl.maxNum;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        bool present = g < R.nfixed;
+        for (int t = 0; !present && t < R.ntypes; ++t) {
+            const int s = g - R.frag[t].startRes;
+            if (s >= 0 && s < R.frag[t].maxNum) {
+                present = s < R.totalNum[t];
+                break;
+            }
         }
+        if (!present) continue;
+        const float4 c = R.gcen[g];
+        const int cell = cell_of(R, c.x, c.y, c.z);
+        const int p = atomicAdd(&R.cell_count[cell], 1);
+        if (p < R.cap) R.cell_ent[(size_t)cell * R.cap + p] = make_ent(R, g);
+        else atomicOr(R.err, ERR_CELL_OVERFLOW);
+    }
+}
+
+__global__ void k_sort_cells(const RepDev* __restrict__ reps) {
+    const RepDev& R = reps[blockIdx.y];
+    const int ncell = R.nc[0] * R.nc[1] * R.nc[2];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        int n = R.cell_count[c];
+        if (n > R.cap) {
+            n = R.cap;
+            R.cell_count[c] = n;
+        }
+        CellEnt* ent = R.cell_ent + (size_t)c * R.cap;
+        for (int i = 1; i < n; ++i) {  // insertion sort by group id
+            const CellEnt e = ent[i];
+            int j = i;
+            while (j > 0 && ent_id(ent[j - 1]) > ent_id(e)) {
+                ent[j] = ent[j - 1];
+                --j;
+            }
+            ent[j] = e;
+        }
+        for (int i = 0; i < n; ++i) R.gcell[ent_id(ent[i])] = c * R.cap + i;
     }
 }
 

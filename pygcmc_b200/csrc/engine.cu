@@ -586,6 +586,20 @@ int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     return GCMC_OK;
 }
 
+// Cell lists of every replica from its current centres and counts (cell_count
+// zeroed and gcell = -1 beforehand).
+void build_cells(gcmc_ctx* ctx) {
+    int ng = 1, nc = 1;
+    for (const auto& h : ctx->reps) {
+        ng = std::max(ng, h.ngroups);
+        nc = std::max(nc, h.ncell);
+    }
+    const dim3 gf((unsigned)std::min((ng + 255) / 256, 148 * 4), (unsigned)ctx->nrep);
+    const dim3 gs((unsigned)std::min((nc + 255) / 256, 148 * 4), (unsigned)ctx->nrep);
+    k_fill_cells<<<gf, 256, 0, ctx->stream>>>(ctx->d_reps);
+    k_sort_cells<<<gs, 256, 0, ctx->stream>>>(ctx->d_reps);
+}
+
 // Split the replicas into `nb` contiguous groups of about equal atom count.
 void split_branches(gcmc_ctx* ctx, int nb) {
     nb = std::max(1, std::min(nb, ctx->nrep));
@@ -728,7 +742,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     if (st == GCMC_OK) st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
     if (st == GCMC_OK) {
         split_branches(ctx, opt.branches > 0 ? opt.branches : 1);
-        k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
+        build_cells(ctx);
         if (cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
     }
     if (st == GCMC_OK) st = pme_init_fixed(ctx);
@@ -765,7 +779,7 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     if (st != GCMC_OK) return st;
     CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice,
                        ctx->stream));
-    k_build_cells<<<nrep, 32, 0, ctx->stream>>>(ctx->d_reps, nrep);
+    build_cells(ctx);
     CK(cudaGetLastError());
     st = pme_init_fixed(ctx);
     if (st != GCMC_OK) return st;
