@@ -77,6 +77,8 @@ struct RepHost {
     double* pme_g = nullptr;      // influence function on the half spectrum
     cufftHandle plan_f = 0, plan_b = 0;
     bool plans = false;
+    double pme_key[7] = {0, 0, 0, 0, 0, 0, 0};  // mesh, box and alpha the influence function in pme_g is for
+    const double* pme_g_for = nullptr;          // the buffer it was written to
 };
 
 }  // namespace
@@ -454,9 +456,16 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         }
         const size_t nr = (size_t)n[0] * n[1] * n[2], nh = (size_t)n[0] * n[1] * (n[2] / 2 + 1);
         AL(h.pme_qfix, nr); AL(h.pme_q, nr); AL(h.pme_phi, nr); AL(h.pme_spec, nh); AL(h.pme_g, nh);
-        std::vector<double> G(nh);
-        pme_influence(n, I->cryst, alpha, G.data());
-        CK(cudaMemcpyAsync(h.pme_g, G.data(), sizeof(double) * nh, cudaMemcpyHostToDevice, ctx->stream));
+        // the influence function depends only on the mesh, the box and alpha: kept between refills
+        const double key[7] = {(double)n[0], (double)n[1], (double)n[2], (double)I->cryst[0], (double)I->cryst[1],
+                               (double)I->cryst[2], alpha};
+        if (h.pme_g_for != h.pme_g || std::memcmp(key, h.pme_key, sizeof(key)) != 0) {
+            std::vector<double> G(nh);
+            pme_influence(n, I->cryst, alpha, G.data());
+            CK(cudaMemcpyAsync(h.pme_g, G.data(), sizeof(double) * nh, cudaMemcpyHostToDevice, ctx->stream));
+            std::memcpy(h.pme_key, key, sizeof(key));
+            h.pme_g_for = h.pme_g;
+        }
         CK(cudaMemsetAsync(h.pme_phi, 0, sizeof(double) * nr, ctx->stream));
         if (!h.plans || n[0] != h.pme_n[0] || n[1] != h.pme_n[1] || n[2] != h.pme_n[2]) {
             if (h.plans) {
