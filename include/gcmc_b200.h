@@ -86,8 +86,10 @@ typedef struct {
     int32_t cells_per_cutoff; /* cell-grid resolution R (cells of >= cutoff/R); 0 = 2 */
     int32_t log_steps;   /* record per-step logs for this many steps (0 = off)      */
     int32_t log_kmax;    /* per-step pose energies recorded (<= 1024)               */
-    int32_t split_items; /* target pose-energy work items per step: each pose's cell
-                            window is split into ~split_items/poses ranges; 0 = 2048 */
+    int32_t split_items; /* pose-energy work items per step at most: each pose's cell
+                            window is split into floor(split_items / poses) ranges (1 to
+                            window cells / 8); 0 = one wave of the pose-energy grid (its
+                            resident warps) */
     int32_t branches;    /* independent chains of the captured step loop: the
                             replicas are split into this many contiguous groups
                             (balanced by atom count) whose kernels run

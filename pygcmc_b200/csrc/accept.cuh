@@ -216,9 +216,10 @@ __device__ void prepare_step(const RepDev& R, int step) {
                 D.k = 0;
             }
             D.nw = (D.move == MV_DELETE) ? 0 : (D.k + 31) >> 5;
-            // split each pose's cell window so a step has about split_items work items
+            // split each pose's cell window so a step has at most split_items work items
+            // (at least one range per pose, at most max_split)
             const int kv = max(1, D.k * D.nvar);
-            D.nslab = max(1, min(R.max_split, (R.split_items + kv - 1) / kv));
+            D.nslab = max(1, min(R.max_split, R.split_items / kv));
             D.items = D.fb ? D.k * D.nslab : D.k * D.nvar * D.nslab;
             D.items_pre = D.fb ? D.k * D.nslab : 0;
         }

@@ -289,6 +289,8 @@ __global__ void k_unpack_grid(const float* __restrict__ in, float4* __restrict__
 }
 int unpack_blocks(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
 
+int energy_warps(int device, int evar, int ebps);
+
 int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
     const InfoStruct* I = in.info;
     RepHost& h = ctx->reps[r];
@@ -319,7 +321,11 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     }
     d.range = Rc;
     d.max_split = std::max(1, d.span[0] * d.span[1] * d.span[2] / 8);
-    d.split_items = opt.split_items > 0 ? opt.split_items : 2048;
+    // default: one wave of the pose-energy grid (its resident warps), the most items a
+    // step can have without a second round of warps
+    d.split_items = opt.split_items > 0 ? opt.split_items
+                                        : energy_warps(ctx->device, opt.energy_variant == 1 ? 1 : 0,
+                                                       opt.energy_blocks_per_sm);
     h.nslab = std::max(d.span[2], d.max_split);
     h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
     d.cutoff = I->cutoff;
@@ -545,6 +551,20 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
 
 using EnergyKernel = void (*)(const RepDev*, int);
 EnergyKernel energy_kernel(int variant) { return variant == 1 ? k_energy_t<4> : k_energy_t<3>; }
+
+// Resident warps of the pose-energy grid for this register variant and CTA cap.
+int energy_warps(int device, int evar, int ebps) {
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, energy_kernel(evar), kWarpsE * 32, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 2048;
+    }
+    per_sm = std::max(1, per_sm);
+    if (ebps > 0) per_sm = std::min(per_sm, ebps);
+    return std::max(1, sms) * per_sm * kWarpsE;
+}
+
 
 // Rebuild replica r's PME mesh potential from its current state on stream s:
 // Q = Q_fixed + spread(occupied fragment atoms); phi = IFFT(G * FFT(Q)).
@@ -964,7 +984,7 @@ void gcmc_default_options(gcmc_options* opt) {
     opt->cells_per_cutoff = 2;
     opt->log_steps = 0;
     opt->log_kmax = 1;
-    opt->split_items = 2048;
+    opt->split_items = 0;
     opt->branches = 1;
     opt->energy_blocks_per_sm = 0;
     opt->fb_trn = 0.5f;
@@ -1005,7 +1025,6 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
     gcmc_options opt;
     if (base) opt = *base; else gcmc_default_options(&opt);
     if (opt.cells_per_cutoff <= 0) opt.cells_per_cutoff = 2;
-    if (opt.split_items <= 0) opt.split_items = 2048;
     if (opt.branches <= 0) opt.branches = 1;
     opt.log_steps = 0;
     int n = 0;
