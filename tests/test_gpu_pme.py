@@ -93,3 +93,25 @@ def test_pme_replicas_match_single(protein_small, water_small):
         a = occupied_atoms(f1)
         assert (f1.fragmentInfo["totalNum"] == finals[k].fragmentInfo["totalNum"]).all()
         assert np.array_equal(f1.atomInfo["position"][a], finals[k].atomInfo["position"][a])
+
+
+def test_pme_dropin_repeated_calls_match_engine(water_small):
+    """Drop-in calls with Ewald electrostatics: the second call refills the
+    context kept from the first (its mesh, FFT plans and influence function are
+    reused); both give the result of a fresh engine run of the same steps."""
+    from pygcmc_b200.engine import Engine
+    from pygcmc_b200.gpu import runGCMC
+    n = 40
+    base = water_small.copy()
+    base.SimInfo[0]["mcsteps"] = n
+    base.moveArray = np.ascontiguousarray(base.moveArray[:n])
+    with Engine(base.copy(), pme_options(32)) as e:
+        e.run(n)
+        e.sync()
+        final = e.download()
+    for _ in range(2):
+        s = base.copy()
+        runGCMC(*s.arrays(), options=pme_options(32))
+        assert (s.fragmentInfo["totalNum"] == final.fragmentInfo["totalNum"]).all()
+        a = occupied_atoms(s)
+        assert np.array_equal(s.atomInfo["position"][a], final.atomInfo["position"][a])
