@@ -770,10 +770,11 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         const RepDev& R = reps[lo];
         const StepDesc D = *R.desc;
         const int local = it - pre[lo];
-        const int per_pose = D.nvar * D.nslab;
-        const int i = local / per_pose;
-        const int rem = local - i * per_pose;
-        const int v = rem / D.nslab, zi = rem - v * D.nslab;
+        // pose fastest: the ranges of one pose go to different CTAs (and SMs), so the
+        // items of a heavy pose do not share one SM's issue slots
+        const int q = local / max(1, D.k);
+        const int i = local - q * D.k;
+        const int v = q / D.nslab, zi = q - v * D.nslab;
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
