@@ -212,11 +212,10 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
         const StepDesc D = *R.desc;
         const int local = it - pre[lo];
         const bool fbitem = phase == 1 || D.fb;
-        const int per_pose = fbitem ? D.nslab : D.nvar * D.nslab;
-        const int i = local / per_pose;
-        const int rem = local - i * per_pose;
-        const int v = fbitem ? (phase == 1 ? 1 : 0) : rem / D.nslab;
-        const int zi = fbitem ? rem : rem - v * D.nslab;
+        const int q = local / max(1, D.k);  // pose fastest, as in k_energy_t
+        const int i = local - q * D.k;
+        const int v = fbitem ? (phase == 1 ? 1 : 0) : q / D.nslab;
+        const int zi = fbitem ? q : q - v * D.nslab;
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
