@@ -171,6 +171,29 @@ def test_replicas_in_one_context_match_single(protein_small, water_small):
         assert np.array_equal(f1.atomInfo["position"][a], finals[r].atomInfo["position"][a])
 
 
+def test_neighbour_matrix_blocks_equal_rows(protein_small):
+    """Eight replicas in one context give a pose-energy launch with more items
+    than resident warps, which fills the pose-pose bit matrix from mirrored
+    32 x 32 blocks; each replica alone fills it row by row.  With the same
+    options (the same ranges per pose) every replica's chain must be
+    bit-identical to its solo run."""
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    n, nrep = 60, 8
+    with Engine([protein_small.copy() for _ in range(nrep)], default_options()) as eng:
+        eng.run(n)
+        eng.sync()
+        finals = [eng.download(r) for r in range(nrep)]
+    for r in (0, 5):
+        with Engine(protein_small.copy(), default_options(replica=r)) as solo:
+            solo.run(n)
+            solo.sync()
+            f1 = solo.download()
+        assert (f1.fragmentInfo["totalNum"] == finals[r].fragmentInfo["totalNum"]).all()
+        a = occupied_atoms(f1)
+        assert np.array_equal(f1.atomInfo["position"][a], finals[r].atomInfo["position"][a])
+
+
 def test_run_in_chunks_equals_one_run(protein_small):
     from pygcmc_b200.engine import Engine
     with Engine(protein_small.copy()) as e1:
