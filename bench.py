@@ -176,6 +176,7 @@ def run_ours(args, ws, rank, local):
         eng.run(chunk)
     eng.sync()
     c0 = eng.counters()
+    kept0 = int(eng.phase_cycles()[6])
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(ws)
     torch.cuda.synchronize()
@@ -193,6 +194,7 @@ def run_ours(args, ws, rank, local):
     ms = max_over_ranks(ms, ws)
     barrier(ws)
     c1 = eng.counters()
+    kept = int(eng.phase_cycles()[6]) - kept0
     # live per-kernel durations on the same trajectory (kernels launched one by one)
     te, ta, mv = eng.run_profiled(prof_steps)
     c2 = eng.counters()
@@ -227,7 +229,11 @@ def run_ours(args, ws, rank, local):
     peak, sms = nominal_fp32_tflops(sm_max)
     achieved = pairs_prof * FLOPS_PER_PAIR / (e_ms / 1e3) / 1e12
     traffic = load_traffic()
-    launches = args.steps * (2 + 2 * 32 * ((chunk + 31) // 32))
+    # per MC step: pose energies + accept, or (speculating, the default for one
+    # replica) re-prepare + completion + accept + speculative prepare + speculative
+    # energies; per run call: run-end update + start-step set-up
+    speculating = opts.speculate >= 0 and opts.branches <= 1
+    launches = args.steps * (2 + (5 if speculating else 2) * 32 * ((chunk + 31) // 32))
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -251,11 +257,14 @@ def run_ours(args, ws, rank, local):
                      "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_prof / prof_steps,
                      "avg_launch_us": e_ms / prof_steps * 1e3,
                      "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3)},
+                     "share_of_step_time": round(e_ms / (e_ms + a_ms), 3),
+                     "timing": "launch by launch, steps in sequence (run_profiled)"},
         "roofline_accept": {"kernel": "k_accept (cluster walk, accept/update; 1 CTA per replica)",
                             "bound": "latency (sequential greedy clustering on one SM)",
                             "avg_launch_us": a_ms / prof_steps * 1e3,
                             "share_of_step_time": round(a_ms / (e_ms + a_ms), 3)},
+        "speculation": {"on": speculating, "steps_whose_energies_were_kept": kept,
+                        "of_steps": args.steps * chunk},
         "pose_energies_per_s": round((c1["poses"] - c0["poses"]) / (ms / 1e3), 1),
         "pairs_per_s": round((c1["pairs"] - c0["pairs"]) / (ms / 1e3), 1),
         "gpu_launches": launches,

@@ -113,6 +113,12 @@ typedef struct {
                             a 2-3-5-7-smooth size)                                 */
     int32_t energy_variant; /* pose-energy kernel register budget: 0 = 3 CTAs per SM,
                             1 = 4 CTAs per SM (autotuned)                           */
+    int32_t speculate;   /* one-replica contexts with one branch, no PME and proposal
+                            0 or 1: each step's successor is prepared and its pose
+                            energies evaluated while the step's accept kernel runs,
+                            and kept when the step accepts nothing (the state is then
+                            unchanged, so the results are those of the sequential
+                            order); 0 = on, -1 = off                               */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
@@ -214,7 +220,9 @@ int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, in
 /* SM cycles spent by replica `rep`'s accept kernel in its phases, summed over
  * steps: [0] pose energies, [1] per-pose weights and bit rows, [2] cluster
  * walk, [3] state update, [4] next-step preparation; [5] number of
- * speculative cluster rounds; [6..7] reserved. */
+ * speculative cluster rounds; [6] steps whose pose energies were evaluated
+ * beside the previous step's accept kernel and kept (gcmc_options.speculate);
+ * [7] reserved. */
 int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8);
 /* Device error word (bit 0 cell overflow, bit 1 periodic image > 1 box,
  * bit 2 slot overflow, bit 3 pose limit). */

@@ -21,7 +21,7 @@ class Options(ctypes.Structure):
                 ("log_steps", c_int), ("log_kmax", c_int), ("split_items", c_int), ("branches", c_int),
                 ("energy_blocks_per_sm", c_int), ("fb_trn", ctypes.c_float), ("fb_rot", ctypes.c_float),
                 ("step_offset", ctypes.c_uint32), ("pme", c_int), ("pme_alpha", ctypes.c_float),
-                ("pme_grid", c_int * 3), ("energy_variant", c_int)]
+                ("pme_grid", c_int * 3), ("energy_variant", c_int), ("speculate", c_int)]
 
 
 class TuneTrial(ctypes.Structure):

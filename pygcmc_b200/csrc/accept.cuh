@@ -262,12 +262,51 @@ __global__ void __launch_bounds__(kAcceptThreads) k_prepare(const RepDev* __rest
     if (D.move == MV_NONE) prepare_step(R, D.step);
 }
 
+// Prepare step `step` in one descriptor (a run's first step, whichever copy holds it).
+__global__ void __launch_bounds__(kAcceptThreads) k_prepare_at(const RepDev* __restrict__ rep, int step) {
+    prepare_step(*rep, step);
+}
+
 __global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nrep) {
         long long e = (long long)reps[r].run_end + nsteps;
         reps[r].run_end = (int)(e < reps[r].mcsteps ? e : reps[r].mcsteps);
+        if (reps[r].other != &reps[r]) {  // the speculating copy: same run end, no standing speculation
+            RepDev* o = const_cast<RepDev*>(reps[r].other);
+            o->run_end = reps[r].run_end;
+            *reps[r].valid = 0;
+            *o->valid = 0;
+            *reps[r].abort = -1;
+            *o->abort = -1;
+        }
     }
+}
+
+// Speculative step preparation (one CTA, nrep = 1).  mode 0: prepare in this
+// copy the step after the other copy's, from the state after the step before
+// that (as if the other copy's step accepts nothing); mode 1: prepare this
+// copy's step again from the current state unless its speculation stands.
+__global__ void __launch_bounds__(kAcceptThreads) k_prep_spec(const RepDev* __restrict__ reps, int mode) {
+    const RepDev& R = reps[0];
+    if (mode == 0) {
+        const int step = *R.other->spec_step + 1;
+        if (threadIdx.x == 0) {
+            *R.pairs_pending = 0ull;
+            *R.spec_step = step;
+        }
+        prepare_step(R, step);
+    } else {
+        const int valid = *R.valid;
+        const int step = *R.spec_step;
+        __syncthreads();
+        if (!valid) prepare_step(R, step);
+    }
+}
+
+// The step a speculating run starts at, in the copy that holds it.
+__global__ void k_spec_start(const RepDev* __restrict__ rep, int step) {
+    if (threadIdx.x == 0) *rep->spec_step = step;
 }
 
 // Initial cell lists in two parallel passes (grid.y = replica): every present
@@ -389,13 +428,28 @@ __device__ __forceinline__ void eval_cluster(const AcceptSmem& S, uint32_t m, in
     lnq_out = lnq;
 }
 
-__global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep) {
+// Void the speculative evaluation of step `step` (the other descriptor copy's):
+// its walks stop at their next batch of candidate groups.
+__device__ __forceinline__ void void_next(const RepDev& R, int step) {
+    *reinterpret_cast<volatile int*>(R.other->abort) = step;
+    __threadfence();
+}
+
+// spec (one replica, speculating): the step's pose energies may come from the
+// speculative launch (booked here); as soon as a move is accepted the
+// speculative evaluation of the next step is voided, and at the end the next
+// step is marked as standing when nothing was accepted.
+__global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep, int spec) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     AcceptSmem& S = *reinterpret_cast<AcceptSmem*>(smem_raw);
     const RepDev& R = reps[blockIdx.x];
     const StepDesc D = *R.desc;
     if (D.move == MV_NONE) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, nwarps = nt >> 5;
+    if (spec && tid == 0 && *R.valid) {  // energies evaluated beside the previous step's accept kernel
+        R.counters[2] += *R.pairs_pending;
+        R.counters[13] += 1ull;
+    }
     const FragDev& F = R.frag[D.ftype];
     const int k = D.k, ns = F.nsites;
     long long t_start = clock64(), t_mark = t_start;
@@ -495,6 +549,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             const double u = u53(r.y, r.z);
             const bool acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
             if (acc) {
+                if (spec) void_next(R, D.step + 1);
                 const int slot = D.del_slot, last = n - 1;
                 const int gs = F.startRes + slot, gl = F.startRes + last;
                 cell_remove(R, gs);
@@ -671,6 +726,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
             // read its results only after the barrier that follows the seeding
         }
         if (tid == 0) {
+            if (spec && wna > 0) void_next(R, D.step + 1);
             S.misc[0] = wna; S.misc[1] = wnc; S.misc[2] = wfa; S.misc[3] = wn;
             atomicAdd(&R.counters[12], (unsigned long long)nrounds);
         }
@@ -779,7 +835,11 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     }
     __syncthreads();
     PHASE(3);
-    prepare_step(R, D.step + 1);
+    if (spec) {  // the next step's speculation stands iff this step accepted nothing
+        if (tid == 0) *R.other->valid = S.misc[0] == 0 ? 1 : 0;
+    } else {
+        prepare_step(R, D.step + 1);
+    }
     PHASE(4);
 #undef PHASE
 }

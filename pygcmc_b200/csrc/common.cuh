@@ -395,7 +395,16 @@ struct RepDev {
     const int* moves;
     FragDev* frag;
     int* totalNum;      // [ntypes]
-    // per-step scratch
+    // per-step scratch.  A replica advanced speculatively has two descriptors
+    // whose scratch alternates by step parity (other: the second one); otherwise
+    // other is the descriptor itself.
+    const RepDev* other;
+    int* valid;                         // speculating: this copy's step was prepared and evaluated
+                                        // while the previous step accepted nothing
+    unsigned long long* pairs_pending;  // speculating: pair count of that evaluation
+    int* abort;                         // speculating: the step whose evaluation is void (the
+                                        // step before it accepted a move); set while it runs
+    int* spec_step;                     // speculating: the step this copy holds
     StepDesc* desc;
     float4* pcen;       // [kMaxPoses] pose centres (w unused)
     int* pslot;         // [kMaxPoses]

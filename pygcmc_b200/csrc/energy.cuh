@@ -328,7 +328,7 @@ __device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
 template <class Sink>
 __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                            int self, int c0, int c1, int lane, Sink& sink, int& ngroups,
-                                           long long& npair) {
+                                           long long& npair, const int* stop = nullptr, int stop_at = 0) {
     set_centre(R, B, cx, cy, cz, lane);
     const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
     const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
@@ -360,6 +360,11 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
         B.cexcl[lane] = incl - cnt;
         __syncwarp();
         for (int t0 = 0; t0 < total; t0 += 32) {
+            if (stop) {  // a speculative evaluation that has become void ends early
+                int v = 0;
+                if (lane == 0) v = *reinterpret_cast<const volatile int*>(stop);
+                if (__shfl_sync(kFull, v, 0) == stop_at) { c1 = base; ng = -1; break; }
+            }
             const int t = t0 + lane;
             bool inc = false;
             uint2 packed = make_uint2(0u, 0u);
@@ -407,15 +412,15 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
         __syncwarp();  // cbase / cexcl are rewritten by the next batch
     }
     __syncwarp();
-    process_groups(R, B, ng, ns, lane, sink, npair);
+    if (ng >= 0) process_groups(R, B, ng, ns, lane, sink, npair);  // ng < 0: stopped
 }
 
 __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                              int self, int c0, int c1, int lane, double& acc, int& ngroups,
-                                             long long& npair) {
+                                             long long& npair, const int* stop = nullptr, int stop_at = 0) {
     EnergySink sink;
     sink.acc = acc;
-    walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair);
+    walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair, stop, stop_at);
     acc = sink.acc;
 }
 
@@ -754,12 +759,20 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // energy_variant, autotuned): MinBlocks = 3 CTAs per SM (up to 85 registers,
 // fewer spills; best for a single replica whose step is latency-bound) or 4
 // (64 registers, more warps in flight; best for large batches).
+//
+// mode 0: every item; mode 1 (speculative, nrep = 1): pair count into
+// pairs_pending, and the walks end early once the step has been voided (the
+// accept kernel of the step before accepted a move); mode 2 (completion,
+// nrep = 1): nothing if the speculative evaluation of this step stands (the
+// accept kernel books its pair count), else mode 0.
 template <int MinBlocks>
-__global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep) {
+__global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep,
+                                                                      int mode) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     __shared__ int wtot[kWarpsE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (mode == 2 && *reps[0].valid) return;
     items_prefix(nrep, pre, wtot, [&](int r) { return reps[r].desc->items; });
     const int total = pre[nrep];
     const bool sym = total > (int)(gridDim.x * kWarpsE);  // more items than warps: throughput-bound
@@ -784,7 +797,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         long long npair = 0;
         const int nwin = R.span[0] * R.span[1] * R.span[2];
         energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi * nwin / D.nslab,
-                     (zi + 1) * nwin / D.nslab, lane, acc, ng, npair);
+                     (zi + 1) * nwin / D.nslab, lane, acc, ng, npair, mode == 1 ? R.abort : nullptr, D.step);
         if (R.pme && zi == 0) {
             const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
             acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
@@ -792,15 +805,19 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         acc = warp_sum(acc);
         if (lane == 0) {
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
-            atomicAdd(&R.counters[2], (unsigned long long)npair);
+            atomicAdd(mode == 1 ? R.pairs_pending : &R.counters[2], (unsigned long long)npair);
         }
-        if (v == 0 && D.nw > 0) nbr_share(R, D, i, zi, lane, sym);
+        if (v == 0 && D.nw > 0) {
+            int stop = 0;
+            if (mode == 1 && lane == 0) stop = *reinterpret_cast<const volatile int*>(R.abort) == D.step;
+            if (!__shfl_sync(kFull, stop, 0)) nbr_share(R, D, i, zi, lane, sym);
+        }
         __syncwarp();
     }
 }
 
-template __global__ void k_energy_t<3>(const RepDev* __restrict__, int);
-template __global__ void k_energy_t<4>(const RepDev* __restrict__, int);
+template __global__ void k_energy_t<3>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4>(const RepDev* __restrict__, int, int);
 
 // Energies of caller-supplied poses (gcmc_energy_poses): item = (pose, slab).
 // The replica descriptor is passed by value so that callers can substitute

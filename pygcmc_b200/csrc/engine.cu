@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -24,6 +25,7 @@ using namespace gcmc;
 namespace {
 
 constexpr int kGraphSteps = 32;
+static_assert(kGraphSteps % 2 == 0, "a speculating graph ends on its start parity");
 constexpr int kMaxRep = 256;
 thread_local int g_last_status = GCMC_OK;
 
@@ -32,7 +34,9 @@ struct RepHost {
     int nslab = 0, log_cap = 0, log_kmax = 0;
     int host_end = 0;
     std::vector<int> startRes, maxNum, moves_host;
-    size_t capn[48] = {0};  // allocated element count per buffer (grown on demand, reused on refill)
+    // allocated element count of each device buffer, keyed by the offset of its
+    // pointer member (grown on demand, reused on refill)
+    std::map<size_t, size_t> capn;
     // device allocations (owned)
     float4* xyzq = nullptr;
     int* atype = nullptr;
@@ -60,6 +64,19 @@ struct RepHost {
     int* err = nullptr;
     double* energy = nullptr;
     float4* psite = nullptr;
+    // per-step scratch of the speculating copy (single-replica contexts)
+    StepDesc* desc2 = nullptr;
+    float4* pcen2 = nullptr;
+    int* pslot2 = nullptr;
+    double* epart2 = nullptr;
+    uint32_t* nbr2 = nullptr;
+    double* pgum2 = nullptr;
+    double* plnu2 = nullptr;
+    float4* psite2 = nullptr;
+    int* valid2 = nullptr;                  // [2] per copy
+    int* abort2 = nullptr;                  // [2] per copy
+    int* sstep2 = nullptr;                  // [2] per copy
+    unsigned long long* pending2 = nullptr; // [2] per copy
     double* pgum = nullptr;
     double* plnu = nullptr;
     float* fpart = nullptr;
@@ -92,6 +109,14 @@ struct gcmc_ctx {
     std::vector<RepDev> repdev;
     RepDev* d_reps = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    // speculation (one replica, one branch, no PME, no force bias): the next step's pose
+    // energies run beside the accept kernel; a second descriptor copy holds every other
+    // step's scratch, and the step loop has one graph per parity of its first step
+    bool spec = false;
+    RepDev repdev_b{};
+    RepDev* d_reps_b = nullptr;
+    cudaGraphExec_t gexec_spec[2] = {nullptr, nullptr};
+    int per_sm_e = 1;      // pose-energy CTAs per SM
     int gridE = 0;       // pose-energy CTAs for all replicas
     int branches = 1;    // independent chains in the captured step loop
     int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
@@ -144,14 +169,16 @@ void free_rep(RepHost& h) {
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
     dfree(h.energy); dfree(h.pgum); dfree(h.psite);
-    dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
+    dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid);
+    dfree(h.desc2); dfree(h.pcen2); dfree(h.pslot2); dfree(h.epart2); dfree(h.nbr2); dfree(h.pgum2); dfree(h.plnu2);
+    dfree(h.psite2); dfree(h.valid2); dfree(h.abort2); dfree(h.sstep2); dfree(h.pending2); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
     if (h.plans) {
         cufftDestroy(h.plan_f);
         cufftDestroy(h.plan_b);
         h.plans = false;
     }
-    for (auto& c : h.capn) c = 0;
+    h.capn.clear();
 }
 
 // Host copy of the device cell index function (floor((x - start) * invLc) mod nc),
@@ -289,7 +316,13 @@ __global__ void k_unpack_grid(const float* __restrict__ in, float4* __restrict__
 }
 int unpack_blocks(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
 
-int energy_warps(int device, int evar, int ebps);
+int energy_warps(int device, int evar, int ebps, int spare_sms);
+
+// Speculation applies to one replica on one branch, without PME or force bias.
+bool spec_eligible(int nrep, const gcmc_replica_in* ins, const gcmc_options& opt) {
+    const bool pme = opt.pme > 0 || (opt.pme == 0 && ins[0].info->PME != 0);
+    return nrep == 1 && opt.speculate >= 0 && opt.proposal != 2 && opt.branches <= 1 && !pme;
+}
 
 int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
     const InfoStruct* I = in.info;
@@ -322,10 +355,11 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.range = Rc;
     d.max_split = std::max(1, d.span[0] * d.span[1] * d.span[2] / 8);
     // default: one wave of the pose-energy grid (its resident warps), the most items a
-    // step can have without a second round of warps
+    // step can have without a second round of warps (speculating: without the SM that
+    // the accept kernel holds meanwhile)
     d.split_items = opt.split_items > 0 ? opt.split_items
                                         : energy_warps(ctx->device, opt.energy_variant == 1 ? 1 : 0,
-                                                       opt.energy_blocks_per_sm);
+                                                       opt.energy_blocks_per_sm, ctx->spec ? 1 : 0);
     h.nslab = std::max(d.span[2], d.max_split);
     h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
     d.cutoff = I->cutoff;
@@ -430,11 +464,10 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     }
 
     int st;
-    int bi = 0;
 #define AL(ptr, n)                                                                          \
     do {                                                                                    \
-        if (bi >= (int)(sizeof(h.capn) / sizeof(h.capn[0]))) return GCMC_ERR_LIMIT;          \
-        if ((st = ensure(&(ptr), &h.capn[bi++], (size_t)(n))) != GCMC_OK) return st;        \
+        const size_t key_ = (size_t)((const char*)&(ptr) - (const char*)&h);                \
+        if ((st = ensure(&(ptr), &h.capn[key_], (size_t)(n))) != GCMC_OK) return st;        \
     } while (0)
     AL(h.xyzq, h.natoms); AL(h.atype, h.natoms); AL(h.gcen, h.ngroups); AL(h.gspan, h.ngroups);
     AL(h.cell_count, h.ncell); AL(h.cell_ent, (size_t)h.ncell * cap); AL(h.gcell, h.ngroups);
@@ -446,6 +479,12 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
     AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
+    if (ctx->spec) {
+        AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.nslab);
+        AL(h.nbr2, (size_t)kMaxPoses * kMaxWords); AL(h.pgum2, kMaxPoses); AL(h.plnu2, kMaxPoses);
+        AL(h.psite2, (size_t)kMaxPoses * kMaxSites); AL(h.valid2, 2); AL(h.abort2, 2); AL(h.sstep2, 2);
+        AL(h.pending2, 2);
+    }
     // smooth PME: mesh, influence function, FFT plans
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
     if (h.pme && opt.proposal == 2) return GCMC_ERR_ARG;  // force bias runs without Ewald
@@ -537,6 +576,17 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     CK(cudaMemsetAsync(h.fpart, 0, sizeof(float) * kMaxPoses * 2 * h.nslab * 6, s));
     CK(cudaMemsetAsync(h.fbprop, 0, sizeof(float4) * kMaxPoses * 2, s));
     CK(cudaMemsetAsync(h.fbcnt, 0, sizeof(int) * kMaxPoses, s));
+    if (ctx->spec) {
+        // a speculative evaluation may read a cell while the accept kernel edits it:
+        // every record slot then holds a span of real atoms (or none)
+        CK(cudaMemsetAsync(h.cell_ent, 0, sizeof(CellEnt) * (size_t)h.ncell * cap, s));
+        CK(cudaMemcpyAsync(h.desc2, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(h.epart2, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
+        CK(cudaMemsetAsync(h.valid2, 0, sizeof(int) * 2, s));
+        CK(cudaMemsetAsync(h.abort2, 0xff, sizeof(int) * 2, s));  // -1: no step voided
+        CK(cudaMemsetAsync(h.sstep2, 0, sizeof(int) * 2, s));
+        CK(cudaMemsetAsync(h.pending2, 0, sizeof(unsigned long long) * 2, s));
+    }
 
     d.xyzq = h.xyzq; d.atype = h.atype; d.gcen = h.gcen; d.gspan = h.gspan;
     d.cell_count = h.cell_count; d.cell_ent = h.cell_ent; d.gcell = h.gcell;
@@ -546,14 +596,36 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.counters = h.counters; d.err = h.err;
     d.energy = h.energy; d.pgum = h.pgum; d.psite = h.psite; d.plnu = h.plnu; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
     d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
+    if (ctx->spec) {
+        RepDev& b = ctx->repdev_b;
+        b = d;
+        b.desc = h.desc2; b.pcen = h.pcen2; b.pslot = h.pslot2; b.epart = h.epart2; b.nbr = h.nbr2;
+        b.pgum = h.pgum2; b.plnu = h.plnu2; b.psite = h.psite2;
+        d.valid = h.valid2; d.pairs_pending = h.pending2; d.abort = h.abort2; d.spec_step = h.sstep2;
+        b.valid = h.valid2 + 1; b.pairs_pending = h.pending2 + 1; b.abort = h.abort2 + 1; b.spec_step = h.sstep2 + 1;
+    }
     return GCMC_OK;
 }
 
-using EnergyKernel = void (*)(const RepDev*, int);
+// Link each descriptor to its partner (itself unless speculating) and upload.
+int upload_reps(gcmc_ctx* ctx) {
+    if (ctx->spec && !ctx->d_reps_b) CK(cudaMalloc(&ctx->d_reps_b, sizeof(RepDev)));
+    for (int r = 0; r < ctx->nrep; ++r) ctx->repdev[r].other = ctx->d_reps + r;
+    if (ctx->spec) {
+        ctx->repdev[0].other = ctx->d_reps_b;
+        ctx->repdev_b.other = ctx->d_reps;
+        CK(cudaMemcpyAsync(ctx->d_reps_b, &ctx->repdev_b, sizeof(RepDev), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return GCMC_OK;
+}
+
+using EnergyKernel = void (*)(const RepDev*, int, int);
 EnergyKernel energy_kernel(int variant) { return variant == 1 ? k_energy_t<4> : k_energy_t<3>; }
 
 // Resident warps of the pose-energy grid for this register variant and CTA cap.
-int energy_warps(int device, int evar, int ebps) {
+int energy_warps(int device, int evar, int ebps, int spare_sms) {
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, energy_kernel(evar), kWarpsE * 32, 0) != cudaSuccess) {
@@ -562,7 +634,7 @@ int energy_warps(int device, int evar, int ebps) {
     }
     per_sm = std::max(1, per_sm);
     if (ebps > 0) per_sm = std::min(per_sm, ebps);
-    return std::max(1, sms) * per_sm * kWarpsE;
+    return std::max(1, sms - spare_sms) * per_sm * kWarpsE;
 }
 
 
@@ -608,6 +680,7 @@ int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     per_sm = std::max(1, per_sm);
     if (ebps > 0) per_sm = std::min(per_sm, ebps);
     ctx->ebps = ebps;
+    ctx->per_sm_e = per_sm;
     ctx->gridE = std::max(1, sms) * per_sm;
     int per_sm_f = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_energy_fb, kWarpsG * 32, 0));
@@ -650,10 +723,85 @@ void split_branches(gcmc_ctx* ctx, int nb) {
 // to the context's stream, so one branch's accept kernel (a CTA per replica)
 // overlaps another's pose energies; each branch gets a share of the
 // pose-energy grid in proportion to its atoms.
+// Speculating (one replica): step j (descriptor copy j & 1) is, on the
+// context's stream, F_p (prepare it again unless its speculation stands), F_e
+// (its pose energies unless they stand) and A (accept).  On a second stream P
+// prepares step j + 1 in the other copy as soon as A of step j - 1 is done (as
+// if step j accepts nothing), and on a third S evaluates its pose energies
+// once P and F_e are done, on the SMs that A leaves free, stopping early when
+// A accepts a move.  F_p of step j + 1 waits for A and S.  One graph per
+// parity of the run's first step (kGraphSteps is even).
+int build_spec_graph(gcmc_ctx* ctx, int parity) {
+    cudaStream_t sp = nullptr, ss = nullptr;
+    cudaEvent_t ev[4 * kGraphSteps + 1] = {};
+    int st = GCMC_OK;
+    if (cudaStreamCreateWithFlags(&sp, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking) != cudaSuccess)
+        st = GCMC_ERR_CUDA;
+    for (auto& e : ev)
+        if (st == GCMC_OK && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) st = GCMC_ERR_CUDA;
+    cudaGraph_t graph = nullptr;
+    if (st == GCMC_OK && cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        st = GCMC_ERR_CUDA;
+    if (st == GCMC_OK) {
+        const EnergyKernel ek = energy_kernel(ctx->evar);
+        const int grid_s = std::max(1, ctx->gridE - ctx->per_sm_e);
+        cudaEvent_t* evF = ev;                    // F_e of step j done
+        cudaEvent_t* evA = ev + kGraphSteps;      // A of step j done
+        cudaEvent_t* evP = ev + 2 * kGraphSteps;  // P of step j + 1 done
+        cudaEvent_t* evS = ev + 3 * kGraphSteps;  // S of step j + 1 done
+        cudaError_t e = cudaEventRecord(ev[4 * kGraphSteps], ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sp, ev[4 * kGraphSteps], 0);
+        for (int i = 0; i < kGraphSteps && e == cudaSuccess; ++i) {
+            const RepDev* cur = ((parity + i) & 1) ? ctx->d_reps_b : ctx->d_reps;
+            const RepDev* nxt = ((parity + i) & 1) ? ctx->d_reps : ctx->d_reps_b;
+            if (i > 0) e = cudaStreamWaitEvent(ctx->stream, evS[i - 1], 0);
+            k_prep_spec<<<1, kAcceptThreads, 0, ctx->stream>>>(cur, 1);
+            ek<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(cur, 1, 2);
+            if (e == cudaSuccess) e = cudaEventRecord(evF[i], ctx->stream);
+            k_accept<<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);
+            if (e == cudaSuccess) e = cudaEventRecord(evA[i], ctx->stream);
+            if (i > 0 && e == cudaSuccess) e = cudaStreamWaitEvent(sp, evA[i - 1], 0);
+            k_prep_spec<<<1, kAcceptThreads, 0, sp>>>(nxt, 0);
+            if (e == cudaSuccess) e = cudaEventRecord(evP[i], sp);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, evP[i], 0);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, evF[i], 0);
+            ek<<<grid_s, kWarpsE * 32, 0, ss>>>(nxt, 1, 1);
+            if (e == cudaSuccess) e = cudaEventRecord(evS[i], ss);
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, evS[kGraphSteps - 1], 0);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            std::fprintf(stderr, "gcmc_b200: graph capture failed: %s\n",
+                         cudaGetErrorString(e != cudaSuccess ? e : e2));
+            st = GCMC_ERR_CUDA;
+        }
+    }
+    if (st == GCMC_OK && cudaGraphInstantiate(&ctx->gexec_spec[parity], graph, 0) != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+    if (sp) cudaStreamDestroy(sp);
+    if (ss) cudaStreamDestroy(ss);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (st != GCMC_OK) cudaGetLastError();
+    return st;
+}
+
 int build_graph(gcmc_ctx* ctx) {
     if (ctx->gexec) {
         cudaGraphExecDestroy(ctx->gexec);
         ctx->gexec = nullptr;
+    }
+    for (auto& g : ctx->gexec_spec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    if (ctx->spec) {
+        int st = build_spec_graph(ctx, 0);
+        if (st == GCMC_OK) st = build_spec_graph(ctx, 1);
+        return st;
     }
     const int nb = ctx->branches;
     std::vector<cudaStream_t> side(nb, nullptr);
@@ -685,9 +833,9 @@ int build_graph(gcmc_ctx* ctx) {
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
                 } else {
-                    energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt);
+                    energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 0);
                 }
-                k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt);
+                k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt, 0);
             }
             if (e == cudaSuccess) e = cudaGetLastError();
         }
@@ -716,8 +864,11 @@ int destroy_impl(gcmc_ctx* ctx) {
     if (!ctx) return GCMC_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    for (auto g : ctx->gexec_spec)
+        if (g) cudaGraphExecDestroy(g);
     for (auto& h : ctx->reps) free_rep(h);
     if (ctx->d_reps) cudaFree(ctx->d_reps);
+    if (ctx->d_reps_b) cudaFree(ctx->d_reps_b);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GCMC_OK;
@@ -754,13 +905,10 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     }
     ctx->reps.resize(nrep);
     ctx->repdev.resize(nrep);
+    ctx->spec = spec_eligible(nrep, ins, opt);
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
-    if (st == GCMC_OK) {
-        if (cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess ||
-            cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice,
-                            ctx->stream) != cudaSuccess)
-            st = GCMC_ERR_CUDA;
-    }
+    if (st == GCMC_OK && cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess) st = GCMC_ERR_CUDA;
+    if (st == GCMC_OK) st = upload_reps(ctx);
     if (st == GCMC_OK) {
         if (cudaFuncSetAttribute(k_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(AcceptSmem)) != cudaSuccess)
@@ -804,10 +952,13 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = validate(ins[r]);
     if (st != GCMC_OK) return st;
     CK(cudaStreamSynchronize(ctx->stream));
+    const bool spec = spec_eligible(nrep, ins, opt);
+    const bool spec_changed = spec != ctx->spec;
+    ctx->spec = spec;
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
     if (st != GCMC_OK) return st;
-    CK(cudaMemcpyAsync(ctx->d_reps, ctx->repdev.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice,
-                       ctx->stream));
+    st = upload_reps(ctx);
+    if (st != GCMC_OK) return st;
     build_cells(ctx);
     CK(cudaGetLastError());
     st = pme_init_fixed(ctx);
@@ -815,7 +966,8 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
     const int fb = opt.proposal == 2 ? 1 : 0;
     const int evar = opt.energy_variant == 1 ? 1 : 0;
-    if (nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb || evar != ctx->evar) {
+    if (spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb ||
+        evar != ctx->evar) {
         ctx->fb = fb;
         ctx->evar = evar;
         st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
@@ -1113,6 +1265,7 @@ void* gcmc_stream(gcmc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 int gcmc_run(gcmc_ctx* ctx, int32_t nsteps) {
     if (!ctx) return GCMC_ERR_ARG;
     if (nsteps <= 0) return GCMC_OK;
+    const int first = ctx->reps[0].host_end;
     int need = 0;
     for (auto& h : ctx->reps) {
         long long e = std::min<long long>((long long)h.host_end + nsteps, h.mcsteps);
@@ -1121,6 +1274,13 @@ int gcmc_run(gcmc_ctx* ctx, int32_t nsteps) {
     }
     if (need == 0) return GCMC_OK;
     k_set_run_end<<<(ctx->nrep + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, nsteps);
+    if (ctx->spec) {  // step `first` lives in descriptor copy first & 1
+        k_spec_start<<<1, 32, 0, ctx->stream>>>((first & 1) ? ctx->d_reps_b : ctx->d_reps, first);
+        CK(cudaGetLastError());
+        for (int done = 0; done < need; done += kGraphSteps)
+            CK(cudaGraphLaunch(ctx->gexec_spec[first & 1], ctx->stream));
+        return GCMC_OK;
+    }
     k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
     CK(cudaGetLastError());
     for (int done = 0; done < need; done += kGraphSteps) CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
@@ -1139,7 +1299,10 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
     }
     if (need == 0) return GCMC_OK;
     k_set_run_end<<<(ctx->nrep + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, nsteps);
-    k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+    if (ctx->spec)  // timed one step after another: the first descriptor copy only
+        k_prepare_at<<<1, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, first);
+    else
+        k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
     CK(cudaGetLastError());
     std::vector<cudaEvent_t> ev(3 * (size_t)need);
     for (auto& e : ev) CK(cudaEventCreate(&e));
@@ -1153,10 +1316,10 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
         } else {
-            energy_kernel(ctx->evar)<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+            energy_kernel(ctx->evar)<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);
         }
         CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
-        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);
         CK(cudaEventRecord(ev[3 * i + 2], ctx->stream));
     }
     CK(cudaGetLastError());
@@ -1309,7 +1472,8 @@ int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8) {
     CK(cudaMemcpy(c, ctx->reps[rep].counters, sizeof(c), cudaMemcpyDeviceToHost));
     for (int i = 0; i < 5; ++i) out8[i] = (int64_t)c[4 + i];
     out8[5] = (int64_t)c[12];  // speculative cluster rounds
-    out8[6] = out8[7] = 0;
+    out8[6] = (int64_t)c[13];  // steps whose pose energies were evaluated in advance and kept
+    out8[7] = 0;
     return GCMC_OK;
 }
 

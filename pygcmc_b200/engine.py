@@ -141,10 +141,12 @@ class Engine:
 
     def phase_cycles(self, rep: int = 0):
         """Accept-kernel SM cycles per phase (energies, precompute, cluster walk,
-        update, prepare) and the number of speculative cluster rounds."""
+        update, prepare), the number of speculative cluster rounds and the
+        number of steps whose pose energies were evaluated beside the previous
+        step's accept kernel and kept."""
         out = np.zeros(8, np.int64)
         check(lib().gcmc_phase_cycles(self._h, rep, ptr(out)), "gcmc_phase_cycles")
-        return out[:6]
+        return out[:7]
 
     def device_error(self) -> int:
         e = ctypes.c_int32(0)

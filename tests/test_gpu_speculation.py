@@ -1,0 +1,78 @@
+"""Speculative next-step evaluation (gcmc_options.speculate) against the
+sequential step order (needs a B200).
+
+A one-replica context prepares step j + 1 and evaluates its pose energies
+while step j's accept kernel runs, and keeps them when step j accepted
+nothing.  Every logged field, every logged pose energy, the final state and
+the pair counter must then be bit-identical to the sequential order's, on
+systems whose steps accept often (water) and rarely (protein).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LOG_KMAX = 1024
+
+
+def _run(system, nsteps, speculate, chunks=None):
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, speculate=speculate)
+    with Engine(system.copy(), opts) as eng:
+        if chunks is None:
+            eng.run(nsteps)
+        else:
+            for kind, n in chunks:
+                if kind == "graph":
+                    eng.run(n)
+                else:
+                    eng.run_profiled(n)
+        eng.sync()
+        assert eng.device_error() == 0
+        logs, E = eng.logs()
+        return logs, E, eng.download(), eng.counters(), eng.phase_cycles()
+
+
+def _same(a, b):
+    logs_a, E_a, fin_a, cnt_a, _ = a
+    logs_b, E_b, fin_b, cnt_b, _ = b
+    assert len(logs_a) == len(logs_b)
+    for f in logs_a.dtype.names:
+        bad = np.flatnonzero(logs_a[f] != logs_b[f])
+        assert bad.size == 0, (f, bad[:5])
+    assert np.array_equal(E_a.view(np.uint64), E_b.view(np.uint64))
+    assert cnt_a == cnt_b
+    assert np.array_equal(fin_a.fragmentInfo["totalNum"], fin_b.fragmentInfo["totalNum"])
+    assert np.array_equal(fin_a.atomInfo["position"], fin_b.atomInfo["position"])
+    assert np.array_equal(fin_a.residueInfo["position"], fin_b.residueInfo["position"])
+
+
+@pytest.mark.parametrize("which", ["protein_small", "water_small"])
+def test_speculation_equals_sequential_order(request, which):
+    s = request.getfixturevalue(which)
+    n = int(s.SimInfo[0]["mcsteps"])
+    on = _run(s, n, 0)
+    off = _run(s, n, -1)
+    _same(on, off)
+    kept = int(on[4][6])
+    accepted_steps = int((on[0]["n_accept"] > 0).sum())
+    # a step's speculation is kept iff the step before it accepted nothing
+    assert 0 < kept <= n - accepted_steps
+    assert int(off[4][6]) == 0
+
+
+def test_speculation_on_the_benchmark_protein():
+    """6000 atoms, 1000 insertion poses: the one-wave split and the mirrored
+    neighbour blocks of the benchmark workload."""
+    from pygcmc_b200 import system as S
+    s = S.protein_system(seed=1, mcsteps=300)
+    _same(_run(s, 300, 0), _run(s, 300, -1))
+
+
+def test_speculation_mixed_with_timed_steps(protein_small):
+    """Graph runs (speculating) interleaved with step-by-step timed runs
+    (sequential, first descriptor copy) continue one chain."""
+    chunks = [("graph", 37), ("timed", 5), ("graph", 60), ("timed", 3), ("graph", 21), ("graph", 1)]
+    n = sum(c[1] for c in chunks)
+    _same(_run(protein_small, n, 0, chunks), _run(protein_small, n, -1))
