@@ -333,7 +333,7 @@ struct StepDesc {
     int k;         // poses
     int n;         // totalNum at the start of the step
     int nvar;      // 1, or 2 for translate/rotate (new, old)
-    int nslab;     // work items per pose variant (each covers a contiguous range of window cells)
+    int nslab;     // work items per pose variant (item z takes window cells z, z + nslab, ...)
     int nw;        // neighbour-row words (0 = no clustering)
     int items;     // k * nvar * nslab (force-biased steps: k * nslab, the new poses)
     int del_slot;

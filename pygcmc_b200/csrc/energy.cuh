@@ -315,7 +315,7 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
 }
 
 // Energy of the pose in B.site against the groups whose cells lie in the
-// window cells [c0, c1) around the pose centre (flattened as
+// window cells c0, c0 + stride, ... below c1 around the pose centre (flattened as
 // ((z * span1) + y) * span0 + x), handed to the sink in buffers of atoms;
 // ngroups (warp-uniform) counts the included groups.  Cells are visited 32 at
 // a time: a warp scan of their entry counts numbers the batch's candidates,
@@ -328,7 +328,8 @@ __device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
 template <class Sink>
 __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                            int self, int c0, int c1, int lane, Sink& sink, int& ngroups,
-                                           long long& npair, const int* stop = nullptr, int stop_at = 0) {
+                                           long long& npair, const int* stop = nullptr, int stop_at = 0,
+                                           int stride = 1) {
     set_centre(R, B, cx, cy, cz, lane);
     const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
     const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
@@ -337,8 +338,8 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
     const float inv_s0 = 1.0f / (float)R.span[0], inv_sxy = 1.0f / (float)sxy;
     const unsigned lt = (1u << lane) - 1u;
     int ng = 0;
-    for (int base = c0; base < c1; base += 32) {
-        const int j = base + lane;
+    for (int base = c0; base < c1; base += 32 * stride) {  // window cells c0, c0 + stride, ... < c1
+        const int j = base + lane * stride;
         int cell = 0, cnt = 0;
         if (j < c1) {
             const int jz = (int)(((float)j + 0.5f) * inv_sxy), jxy = j - jz * sxy;
@@ -417,10 +418,11 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
 
 __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                              int self, int c0, int c1, int lane, double& acc, int& ngroups,
-                                             long long& npair, const int* stop = nullptr, int stop_at = 0) {
+                                             long long& npair, const int* stop = nullptr, int stop_at = 0,
+                                             int stride = 1) {
     EnergySink sink;
     sink.acc = acc;
-    walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair, stop, stop_at);
+    walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair, stop, stop_at, stride);
     acc = sink.acc;
 }
 
@@ -796,8 +798,10 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         int ng = 0;
         long long npair = 0;
         const int nwin = R.span[0] * R.span[1] * R.span[2];
-        energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi * nwin / D.nslab,
-                     (zi + 1) * nwin / D.nslab, lane, acc, ng, npair, mode == 1 ? R.abort : nullptr, D.step);
+        // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
+        // range samples the whole cutoff sphere and the ranges of a pose take equal time)
+        energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
+                     mode == 1 ? R.abort : nullptr, D.step, D.nslab);
         if (R.pme && zi == 0) {
             const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
             acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);

@@ -222,13 +222,14 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
         if (phase != 1) keep_sites(R, D, B, i, v, zi, lane);
         const int ns = R.frag[D.ftype].nsites;
         const int nwin = R.span[0] * R.span[1] * R.span[2];
-        const int c0 = zi * nwin / D.nslab, c1 = (zi + 1) * nwin / D.nslab;
+        const int c0 = zi, c1 = nwin;  // interleaved range: cells zi, zi + nslab, ...
+        const int stride = D.nslab;
         int ng = 0;
         long long npair = 0;
         double acc = 0.0;
         if (!fbitem) {
             EnergySink sink;
-            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair);
+            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair, nullptr, 0, stride);
             acc = warp_sum(sink.acc);
         } else {
             GradSinkT<true> sink;
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
             sink.gtab = nullptr;
             sink.w = 1.0f;
             sink.ffY = R.ffY;
-            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair);
+            walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair, nullptr, 0, stride);
             acc = warp_sum((double)sink.e);
             // per-site gradient (lanes < ns after summing the atom subsets), then
             // force -sum g_s and torque -sum (x_s - m) x g_s about the site centroid
