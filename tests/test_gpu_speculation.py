@@ -76,3 +76,29 @@ def test_speculation_mixed_with_timed_steps(protein_small):
     chunks = [("graph", 37), ("timed", 5), ("graph", 60), ("timed", 3), ("graph", 21), ("graph", 1)]
     n = sum(c[1] for c in chunks)
     _same(_run(protein_small, n, 0, chunks), _run(protein_small, n, -1))
+
+
+def _occupied_atoms(s):
+    idx = []
+    for f in s.fragmentInfo:
+        for j in range(int(f["totalNum"])):
+            r = s.residueInfo[int(f["startRes"]) + j]
+            idx.extend(range(int(r["atomStart"]), int(r["atomStart"]) + int(r["atomNum"])))
+    return np.array(idx, dtype=np.int64)
+
+
+def test_dropin_refills_switching_speculation(protein_small, water_small):
+    """The drop-in's kept context is refilled with speculation switched off and
+    on again (per-step buffers and captured graphs change); every call equals
+    a fresh engine with the same options."""
+    from pygcmc_b200._native import default_options, lib
+    from pygcmc_b200.gpu import runGCMC
+    for sysm, spec in ((water_small, 0), (protein_small, -1), (water_small, -1), (protein_small, 0)):
+        s = sysm.copy()
+        n = int(s.SimInfo[0]["mcsteps"])
+        runGCMC(*s.arrays(), options=default_options(speculate=spec))
+        _, _, fin, _, _ = _run(sysm, n, spec)
+        assert np.array_equal(s.fragmentInfo["totalNum"], fin.fragmentInfo["totalNum"])
+        a = _occupied_atoms(s)
+        assert np.array_equal(s.atomInfo["position"][a], fin.atomInfo["position"][a])
+    assert lib().gcmc_release_cache() == 0
