@@ -5,7 +5,9 @@
 // centres) and a CUDA graph of `kGraphSteps` MC steps; each step is one
 // k_energy launch (every replica's pose items) and one k_accept launch (one
 // CTA per replica) that also prepares the next step, so the whole step loop
-// runs without host round trips.
+// runs without host round trips.  A one-replica context speculates instead
+// (build_spec_graph): the next step is prepared and its pose energies
+// evaluated beside the accept kernel, and kept when the step accepts nothing.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
