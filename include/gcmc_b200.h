@@ -174,7 +174,8 @@ int gcmc_release_cache(void);
 /* Batched drop-in (no counterpart in the reference, which runs one system per
  * runGCMC_cuda call): runs each replica's info->mcsteps steps in ONE device
  * context -- all replicas advance together, one pose-energy launch and one
- * accept launch per MC step -- and writes every replica's totalNum,
+ * accept launch per MC step (a single replica speculates instead, see
+ * gcmc_options.speculate) -- and writes every replica's totalNum,
  * residueInfo and atomInfo back in place (the arrays behind reps[r] are
  * written although the struct holds const pointers).  The context is kept
  * between calls with the same replica count, like gcmc_run_gcmc's. */

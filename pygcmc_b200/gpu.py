@@ -101,7 +101,8 @@ def runGCMC_batch(replicas, options=None):
     """Batched form of :func:`runGCMC` (no counterpart in the reference): every
     replica -- a :class:`pygcmc_b200.system.System` or a 7-tuple of the
     runGCMC arrays -- runs its ``mcsteps`` steps in one device context (one
-    pose-energy launch and one accept launch per MC step for all of them), and
+    pose-energy launch and one accept launch per MC step for all of them; a
+    single replica speculates instead, see ``Options.speculate``), and
     each replica's fragmentInfo/residueInfo/atomInfo are updated in place."""
     import ctypes
     from ._native import ReplicaIn
