@@ -39,7 +39,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MC trial moves/sec on 1 B200: batched/force-bias vs plain, ΔE rel err ≤1e-5"
-FLOPS_PER_PAIR = 19  # fixed algorithmic count per atom-site pair
+# fixed algorithmic count per atom-site pair: dx, dy, dz 3; r^2 5; 1/r^2 1; sigma^2/r^2 1; s^6 2;
+# 4 eps s^6 (s^6 - 1) 3; k q_i q_j / r 1; accumulate 2 (plus one rsqrt)
+FLOPS_PER_PAIR = 19
 WORKLOAD = ("synthetic protein: 6000-atom random-walk chain in a 24 A sphere, 64 A periodic box, "
             "8 rigid fragments (4-12 sites) at bulk counts, confBias 1000, cutoff 12 A, reference semantics")
 
@@ -239,13 +241,12 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair terms, fp64 sums/acceptance",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
-                   "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
-                   "launch_shape": {"cells_per_cutoff": opts.cells_per_cutoff, "split_items": opts.split_items,
-                                    "branches": opts.branches, "energy_blocks_per_sm": opts.energy_blocks_per_sm,
-                                    "energy_variant": opts.energy_variant,
-                                    "source": "--cells" if args.cells > 0 else
-                                    f"autotuned before timing ({t_tune:.1f} s, untimed)"}},
+        "config": ref_config(WORKLOAD, chunk, 1, ws),
+        "launch_shape": {"cells_per_cutoff": opts.cells_per_cutoff, "split_items": opts.split_items,
+                         "branches": opts.branches, "energy_blocks_per_sm": opts.energy_blocks_per_sm,
+                         "energy_variant": opts.energy_variant,
+                         "source": "--cells" if args.cells > 0 else
+                         f"autotuned before timing ({t_tune:.1f} s, untimed)"},
         "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
                 "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC (drop-in for gcmc.gpu.runGCMC)"},
@@ -360,15 +361,14 @@ def run_ours_batched(args, ws, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 pair terms, fp64 sums/acceptance", "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": BATCH_WORKLOAD, "replicas_per_gpu": nrep, "mc_steps_per_bench_step": chunk,
-                   "atoms_per_replica": [int(s.info["totalAtomNum"]) for s in systems][:nrep],
-                   "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks",
-                   "autotuned": {"cells_per_cutoff": best.cells_per_cutoff, "split_items": best.split_items,
-                                 "branches": best.branches, "energy_blocks_per_sm": best.energy_blocks_per_sm,
-                                 "trials": len(trials), "tune_s": round(t_tune, 2),
-                                 "energy_variant": best.energy_variant,
-                                 "trial_ms_per_step": [[*t[:5], round(t[5], 4)] for t in trials]},
-                   "generate_s": round(t_gen, 2)},
+        "config": ref_config(BATCH_WORKLOAD, chunk * nrep, nrep, ws,
+                             [int(s.info["totalAtomNum"]) for s in systems][:nrep]),
+        "autotuned": {"cells_per_cutoff": best.cells_per_cutoff, "split_items": best.split_items,
+                      "branches": best.branches, "energy_blocks_per_sm": best.energy_blocks_per_sm,
+                      "trials": len(trials), "tune_s": round(t_tune, 2),
+                      "energy_variant": best.energy_variant,
+                      "trial_ms_per_step": [[*t[:5], round(t[5], 4)] for t in trials]},
+        "generate_s": round(t_gen, 2),
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
                 "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
@@ -411,7 +411,7 @@ class RefRunner:
 
     def run_range(self, a, b):
         """Steps [a, b) in slices; a delete on an empty fragment type (where the
-        reference divides by zero, gcmc_move_del.h:316) is skipped.  Returns the
+        reference divides by zero, gcmc_move_del.h:113) is skipped.  Returns the
         number of calls made."""
         s, moves = self.s, self.s.moveArray
         calls = 0
@@ -678,26 +678,52 @@ def run_ours_large(args, ws, rank, local):
     }
 
 
+ARRAY_NAMES = ("SimInfo", "fragmentInfo", "residueInfo", "atomInfo", "grid", "ff", "moveArray")
+
+
+def write_inputs(path, workload, seed, mcsteps, replicas):
+    """Build the workload's input arrays and save them to `path` (.npz).  The
+    reference arm runs this in a child process, so that the process it times
+    loads no code of this repository's library (the generators are in it)."""
+    if workload == "batched":
+        systems = make_batch(seed, mcsteps, replicas)
+    else:
+        systems = [make_system(seed, mcsteps)]
+    arrs = {f"{r}_{name}": a for r, s in enumerate(systems) for name, a in zip(ARRAY_NAMES, s.arrays())}
+    np.savez(path, n=len(systems), **arrs)
+
+
+def read_inputs(path):
+    import types
+    z = np.load(path)
+    return [types.SimpleNamespace(**{name: np.ascontiguousarray(z[f"{r}_{name}"]) for name in ARRAY_NAMES})
+            for r in range(int(z["n"]))]
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
     lib_path = os.path.join(ROOT, "oracle", "_ref", "libgcmc_ref.so")
     if not os.path.exists(lib_path):
         return {"impl": "reference", "unavailable": "oracle/_ref/libgcmc_ref.so not built (make -C oracle ref)"}
+    chunk = args.ref_chunk
+    seed = args.seed
+    batched = args.workload == "batched"
+    mcsteps = (args.warmup + args.steps + 2) * chunk + 16
+    with tempfile.TemporaryDirectory() as tmp:  # inputs from a child process (untimed)
+        path = os.path.join(tmp, "inputs.npz")
+        subprocess.check_call([sys.executable, os.path.abspath(__file__), "--write-inputs", path, "--workload",
+                               args.workload, "--seed", str(seed), "--replicas", str(args.replicas),
+                               "--mcsteps", str(mcsteps)])
+        systems = read_inputs(path)
     import torch
     torch.cuda.set_device(local)
     L = ctypes.CDLL(lib_path)
     L.runGCMC_cuda.restype = None
     L.runGCMC_cuda.argtypes = [ctypes.c_void_p] * 7
-    chunk = args.ref_chunk
-    seed = args.seed
-    batched = args.workload == "batched"
-    if batched:
-        systems = make_batch(seed, (args.warmup + args.steps + 2) * chunk + 16, args.replicas)
-    else:
-        systems = [make_system(seed, (args.warmup + args.steps + 2) * chunk + 16)]
     runners = [RefRunner(L, s, seed + 7 * r) for r, s in enumerate(systems)]
     fixed = runners[0].fixed_cost()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     pos = 0
     for _ in range(args.warmup):
         for rr in runners:
@@ -707,6 +733,8 @@ def run_reference(args, ws, rank, local):
     clocks = ClockSampler(local)
     t_raw, t_adj, n = 0.0, 0.0, 0
     for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         calls = 0
         for rr in runners:
@@ -727,8 +755,9 @@ def run_reference(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(t_adj / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (reference kernels)", "impl": "reference",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": workload, "mc_steps_per_bench_step": chunk * len(runners),
-                   "replicas_per_gpu": len(runners), "parallelism": "replicas x1", "schedule": how},
+        "config": ref_config(workload, chunk * len(runners) if batched else chunk, len(runners), 1,
+                             [int(r.s.SimInfo[0]["totalAtomNum"]) for r in runners] if batched else None),
+        "schedule": how,
         "cpu_baseline": {"value": round(value, 1), "unit": "moves/s", "cores": 1, "kind": "reference",
                          "sample": f"reference runGCMC_cuda (unmodified pyGCMC gcmc.cu, sm_100a) on the B200, "
                                    f"{n} MC steps ({how}); the reference has no CPU implementation of this "
@@ -737,6 +766,42 @@ def run_reference(args, ws, rank, local):
         "skipped_deletes_on_empty_types": sum(rr.skipped for rr in runners),
         "clocks": clk,
     }
+
+
+def ref_config(workload, steps_per_bench_step, replicas, ws, atoms=None):
+    """The `config` both arms print for a workload (the same keys and values)."""
+    c = {"workload": workload, "mc_steps_per_bench_step": steps_per_bench_step, "replicas_per_gpu": replicas,
+         "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks"}
+    if atoms is not None:
+        c["atoms_per_replica"] = atoms
+    return c
+
+
+def run_probe(args):
+    """A small fixed run for kernel profiling (ncu) and per-kernel timing: the
+    workload's system advanced --probe-warm steps through the graph-captured
+    step loop, then --probe-steps steps launched kernel by kernel with CUDA
+    events around each launch; prints the per-step kernel times.  Under ncu the
+    pose-energy and accept launches after the warm-up are the individually
+    launched ones."""
+    from pygcmc_b200 import system as S
+    from pygcmc_b200._native import default_options
+    from pygcmc_b200.engine import Engine
+    total = args.probe_warm + args.probe_steps + 64
+    if args.workload == "batched":
+        s = S.replica_batch(n_rep=args.replicas, seed=args.seed, mcsteps=total)
+    elif args.workload == "water":
+        s = S.water_box(seed=args.seed, mcsteps=total)
+    else:
+        s = make_system(args.seed, total)
+    opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 2)
+    with Engine(s, opt) as eng:
+        eng.run(args.probe_warm)
+        eng.sync()
+        te, ta, mv = eng.run_profiled(args.probe_steps)
+        print(json.dumps({"move": (mv % 4).tolist(), "energy_us": [round(float(x) * 1e3, 2) for x in te],
+                          "accept_us": [round(float(x) * 1e3, 2) for x in ta], "counters": eng.counters(),
+                          "accept_phase_cycles": eng.phase_cycles().tolist()}))
 
 
 def barrier(ws):
@@ -755,7 +820,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["protein", "batched", "forcebias", "large"], default="protein",
+    ap.add_argument("--workload", choices=["protein", "batched", "forcebias", "large", "water"], default="protein",
                     help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU; "
                          "forcebias: force-biased vs plain translate/rotate on the protein system; "
                          "large: 200000-atom slab with PME, --replicas replicas")
@@ -766,7 +831,23 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="cells per cutoff (0: autotune the launch shape)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--probe", action="store_true",
+                    help="a small fixed run for kernel profiling: --probe-warm graph steps, then --probe-steps "
+                         "steps launched kernel by kernel (per-kernel times printed; no bench line)")
+    ap.add_argument("--probe-warm", type=int, default=64)
+    ap.add_argument("--probe-steps", type=int, default=24)
+    ap.add_argument("--write-inputs", default="", help=argparse.SUPPRESS)  # reference arm's child process
+    ap.add_argument("--mcsteps", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.probe:
+        if args.replicas <= 0:
+            args.replicas = 64
+        run_probe(args)
+        return
+    if args.write_inputs:
+        write_inputs(args.write_inputs, args.workload, args.seed, args.mcsteps,
+                     args.replicas if args.replicas > 0 else 64)
+        return
     args.warmup = max(args.warmup, 3)
     if args.chunk <= 0:
         args.chunk = {"batched": 256, "forcebias": 8192, "large": 64}.get(args.workload, 2048)

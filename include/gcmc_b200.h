@@ -226,7 +226,9 @@ int gcmc_counters(gcmc_ctx* ctx, int32_t rep, int64_t* steps, int64_t* poses, in
  * [7] reserved. */
 int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8);
 /* Device error word (bit 0 cell overflow, bit 1 periodic image > 1 box,
- * bit 2 slot overflow, bit 3 pose limit). */
+ * bit 2 slot overflow, bit 3 pose limit, bit 4 an explicit pose's site type
+ * outside the pair table -- gcmc_energy_poses_noalloc, whose device inputs the
+ * host does not read; such a pose's energy is NaN). */
 int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);
 /* The cudaStream_t the context launches on. */
 void* gcmc_stream(gcmc_ctx* ctx);
@@ -258,7 +260,10 @@ int gcmc_energy_poses(gcmc_ctx* ctx, int32_t rep, const float* xyz, const float*
  * calcEnergy, gcmc/cpp/gcmc_energy.h:142-204, has no derivative).  All arrays
  * are DEVICE pointers except site_type, a host copy of d_site_type used for
  * validation; launches on `stream` (NULL = the context's stream) and returns
- * without waiting (scratch comes from the stream-ordered allocator).
+ * without waiting (scratch comes from the stream-ordered allocator).  A
+ * caller's stream first waits for the work queued on the context's stream, and
+ * the context's stream then waits for the call's launches, so the call never
+ * overlaps a gcmc_run of the same context.
  *   d_xyz[p*nsites*3], d_centres[p*3], d_self[p] (optional), d_site_q /
  *   d_site_type[nsites]: as gcmc_energy_poses;
  *   d_ff: pair table in the reference's layout (sigma [nm], eps [kJ/mol] per
@@ -289,7 +294,14 @@ int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float
  * device.  This entry point takes DEVICE pointers the caller already owns
  * (inputs as in gcmc_energy_poses; out[nposes] doubles; ngroups[nposes] ints,
  * optional; self optional = none skipped), launches on `stream` (NULL = the
- * context's stream), returns without waiting, and calls no allocator.
+ * context's stream), returns without waiting, and calls no allocator.  The
+ * site types are device data the host does not read: a type outside the pair
+ * table's rows gives that pose a NaN energy and sets bit 4 of the device error
+ * word, which the next gcmc_sync reports as GCMC_ERR_DEVICE.  A caller's
+ * stream first waits (an event wait) for the work queued on the context's
+ * stream, and the context's stream then waits for the call's launches, so the
+ * call never overlaps a gcmc_run of the same context; with Ewald the call
+ * rebuilds the context's mesh on the caller's stream in that order.
  *
  * Its intermediate per-(pose, split) sums live in a fixed 2 MiB device array
  * inside the library, reserved on every GPU that loads the library until the

@@ -408,7 +408,7 @@ double or_pose_energy_l1(const or_info* info, const or_atomarray* frag, const or
 
 /* ------------------------------------------------------------------------- */
 /* Proposals (gcmc/cpp/gcmc_energy.h:75-107, gcmc_move_trn.h:54-75,           */
-/* gcmc_move_rot.h:313-355).                                                  */
+/* gcmc_move_rot.h:62-101).                                                  */
 /* ------------------------------------------------------------------------- */
 void or_insert_pose(const or_info* info, const or_atomarray* frag, const float* grid,
                     const or_options* opt, int32_t ftype, int32_t step, int32_t i,
@@ -524,6 +524,38 @@ int32_t or_perm_slot(const or_options* opt, uint32_t seed, int32_t step, int32_t
 /* Cluster / Rosenbluth / acceptance pass (gcmc_move_add.h:107-191,           */
 /* gcmc_move_trn.h:160-244).                                                  */
 /* ------------------------------------------------------------------------- */
+/* Decision margins (test statistics): for every acceptance decision, the
+ * distance |ln u - ln p| / beta of the draw from the threshold in energy units,
+ * against the largest per-trial tolerance max(1e-5 |E|, 1e-4 kcal/mol) of the
+ * energies the decision depends on (ln p moves by at most beta times the
+ * largest error of those energies: ln W is a log-sum-exp).  A decision inside
+ * that band may legitimately differ between two evaluations of the energies
+ * that both meet the per-trial criterion. */
+static long long g_dec_total = 0, g_dec_band = 0;
+static double g_dec_min_ratio = INFINITY;
+
+static void note_decision(double lnp, double u, double tol) {
+    if (isnan(lnp) || !(tol > 0.0)) return;
+    g_dec_total++;
+    /* accepted for sure when lnp >= 0: its margin is lnp itself */
+    const double m = (lnp >= 0.0 ? lnp : fabs(log(u) - lnp)) / OR_BETA;
+    if (m <= tol) g_dec_band++;
+    if (m / tol < g_dec_min_ratio) g_dec_min_ratio = m / tol;
+}
+
+static double trial_tol(double e) { return fmax(1e-5 * fabs(e), 1e-4 * 4.184); }
+
+void or_decision_stats(int32_t reset, int64_t* total, int64_t* band, double* min_ratio) {
+    if (total) *total = g_dec_total;
+    if (band) *band = g_dec_band;
+    if (min_ratio) *min_ratio = g_dec_min_ratio;
+    if (reset) {
+        g_dec_total = 0;
+        g_dec_band = 0;
+        g_dec_min_ratio = INFINITY;
+    }
+}
+
 typedef struct {
     int kind;        /* 0 insert, 1 translate/rotate */
     double lncav;    /* insert: ln(cavityFactor)     */
@@ -570,6 +602,10 @@ static int cluster_pass(const or_info* info, const or_options* opt, int step, in
             rng(info->seed, opt->replica, (uint32_t)step, (uint32_t)s, RP_CLUSTER, 0, ua);
             double u = u53(ua[0], ua[1]);
             acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+            double tol = 0.0;
+            for (int m = 0; m < nm; ++m)
+                if (isfinite(E[mem[m]])) tol = fmax(tol, trial_tol(E[mem[m]]));
+            note_decision(lnp, u, tol);
         }
         for (int m = 0; m < nm; ++m) U[mem[m]] = 0;
         if (acc) {
@@ -1115,6 +1151,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         double lnp = log((double)n) - (beta_muex(S->opt, F) + ln_nbar(info, F)) + OR_BETA * Ed;
         double u = u53(r[1], r[2]);
         int acc = !isnan(lnp) && (lnp >= 0.0 || u < exp(lnp));
+        if (isfinite(Ed)) note_decision(lnp, u, trial_tol(Ed));
         if (acc) {
             int last = n - 1;
             or_residue* RL = &S->res[F->startRes + last];

@@ -149,6 +149,11 @@ int32_t or_run(const or_info* info, or_atomarray* frag, or_residue* res, or_atom
  * l1 scales (sum of |pair terms| of the force, and of |r| times them for the
  * torque); replay_forces ([s*kmax + i][12], optional): forces to use instead
  * of the oracle's own (as float, the values another engine used). */
+/* Counts of the acceptance decisions made since the last reset and of those
+ * whose draw lies within the per-trial energy tolerance of the threshold, and
+ * the smallest margin / tolerance seen. */
+void or_decision_stats(int32_t reset, int64_t* total, int64_t* band, double* min_ratio);
+
 int32_t or_run_ext(const or_info* info, or_atomarray* frag, or_residue* res, or_atom* atoms,
                    const float* grid, const float* ff, const int32_t* moves, const or_options* opt,
                    int32_t step0, int32_t nsteps, or_step_log* log, double* energies, double* escale,

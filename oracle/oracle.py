@@ -37,6 +37,8 @@ def lib():
         L.or_run_ext.restype = ctypes.c_int32
         L.or_run_ext.argtypes = [c_void] * 8 + [ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void,
                                                 ctypes.c_int32, ctypes.c_int32, c_void, c_void, c_void, c_void]
+        L.or_decision_stats.restype = None
+        L.or_decision_stats.argtypes = [ctypes.c_int32, c_void, c_void, c_void]
         L.or_det_log.restype = ctypes.c_float
         L.or_det_log.argtypes = [ctypes.c_float]
         L.or_ewald_potential.argtypes = [c_void] * 4 + [ctypes.c_double, c_void, ctypes.c_int32, c_void,
@@ -89,6 +91,14 @@ def ewald_potential(system, alpha, pts, threads=None):
     lib().or_ewald_potential(_p(s.SimInfo), _p(s.fragmentInfo), _p(s.residueInfo), _p(s.atomInfo), float(alpha),
                              _p(pts), len(pts), _p(out), threads)
     return out
+
+
+def decision_stats(reset=True):
+    """(decisions, decisions within the per-trial tolerance band of their
+    threshold, smallest margin / tolerance) since the last reset."""
+    t, b, m = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+    lib().or_decision_stats(1 if reset else 0, ctypes.byref(t), ctypes.byref(b), ctypes.byref(m))
+    return t.value, b.value, m.value
 
 
 def run_ext(system, nsteps, step0=0, opts=None, kmax=1024, threads=None, replay=None, replay_forces=None,

@@ -1,6 +1,6 @@
 // Accept/update kernel: the host halves of move_add / move_del / move_trn /
-// move_rot (gcmc/cpp/gcmc_move_add.h:103-198, gcmc_move_del.h:334-389,
-// gcmc_move_trn.h:159-250, gcmc_move_rot.h:437-527) moved onto the device,
+// move_rot (gcmc/cpp/gcmc_move_add.h:103-198, gcmc_move_del.h:97-187,
+// gcmc_move_trn.h:159-250, gcmc_move_rot.h:151-275) moved onto the device,
 // plus the preparation of the next step's proposals.
 //
 // One CTA per replica.  For clustering moves the CTA

@@ -27,7 +27,7 @@ enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_
 // force-bias tilt lambda (Pangali, Rao and Berne): density ~ exp(lambda beta f . d) in the step cube
 constexpr float kFbLambda = 0.5f;
 enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
-enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8 };
+enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8, ERR_SITE_TYPE = 16 };
 
 // ---------------------------------------------------------------------------
 // exact-rounding float helpers
@@ -370,7 +370,7 @@ struct RepDev {
     int fast_incl;      // 1: multiply-based prefilter decides away from the cutoff (cutoff < L/2)
     float invL[3];
     float cut2_lo, cut2_hi;  // (cutoff*(1-1e-4))^2, (cutoff*(1+1e-4))^2
-    int nfixed, ntypes, ffY, G;
+    int nfixed, ntypes, ffX, ffY, G;
     int mcsteps;
     uint32_t seed, replica;
     uint32_t step_base; // RNG step counter = step_base + local step (resume from a checkpoint)

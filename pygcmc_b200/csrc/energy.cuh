@@ -837,6 +837,18 @@ __global__ void __launch_bounds__(kWarpsE * 32)
     const int total = nposes * nslab;
     for (int it = blockIdx.x * kWarpsE + warp; it < total; it += gridDim.x * kWarpsE) {
         const int p = it / nslab, z = it - p * nslab;
+        // a site type outside the pair table's rows would index past it: flag the
+        // input error (reported by the next gcmc_sync) and give the pose NaN
+        const bool bad_type = lane < ns && (unsigned)type[lane] >= (unsigned)R.ffX;
+        if (__any_sync(kFull, bad_type)) {
+            if (lane == 0) {
+                atomicOr(R.err, ERR_SITE_TYPE);
+                out[it] = __longlong_as_double(0x7ff8000000000000ll);
+                ngout[it] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
         if (lane < ns) {
             const float* s = xyz + ((size_t)p * ns + lane) * 3;
             const double c0 = centres[3 * p], c1 = centres[3 * p + 1], c2 = centres[3 * p + 2];

@@ -126,6 +126,10 @@ struct gcmc_ctx {
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
     int gridF = 0;       // k_energy_fb CTAs
     std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
+    // ordering of calls that launch on a caller's stream against the context's
+    // stream (created once, so such calls allocate nothing): ev_ctx marks the
+    // context's work so far, ev_call the caller's launches
+    cudaEvent_t ev_ctx = nullptr, ev_call = nullptr;
 };
 
 namespace {
@@ -376,6 +380,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.lncav = std::log((double)I->cavityFactor);
     d.nfixed = in.fragmentInfo[0].startRes;
     d.ntypes = I->fragTypeNum;
+    d.ffX = I->ffXNum;
     d.ffY = I->ffYNum;
     d.G = I->totalGridNum;
     d.mcsteps = I->mcsteps;
@@ -871,6 +876,8 @@ int destroy_impl(gcmc_ctx* ctx) {
     for (auto& h : ctx->reps) free_rep(h);
     if (ctx->d_reps) cudaFree(ctx->d_reps);
     if (ctx->d_reps_b) cudaFree(ctx->d_reps_b);
+    if (ctx->ev_ctx) cudaEventDestroy(ctx->ev_ctx);
+    if (ctx->ev_call) cudaEventDestroy(ctx->ev_call);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GCMC_OK;
@@ -904,6 +911,12 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
             return GCMC_ERR_CUDA;
         }
         ctx->own_stream = true;
+    }
+    if (cudaEventCreateWithFlags(&ctx->ev_ctx, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_call, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        destroy_impl(ctx);
+        return GCMC_ERR_CUDA;
     }
     ctx->reps.resize(nrep);
     ctx->repdev.resize(nrep);
@@ -1121,6 +1134,24 @@ __global__ void k_sum_parts(const double* __restrict__ part, const int* __restri
     }
     out[p] = e;
     if (ngroups) ngroups[p] = ng;
+}
+
+// A call that launches on a caller's stream s reads the context's state (cell
+// lists, positions) and, with Ewald, rewrites its mesh buffers: it must not
+// overlap a run on the context's stream.  Before its launches s waits for the
+// context's work so far; after them the context's stream waits for s.  Both
+// are event records and waits on events the context created once.
+int order_before(gcmc_ctx* ctx, cudaStream_t s) {
+    if (s == ctx->stream) return GCMC_OK;
+    CK(cudaEventRecord(ctx->ev_ctx, ctx->stream));
+    CK(cudaStreamWaitEvent(s, ctx->ev_ctx, 0));
+    return GCMC_OK;
+}
+int order_after(gcmc_ctx* ctx, cudaStream_t s) {
+    if (s == ctx->stream) return GCMC_OK;
+    CK(cudaEventRecord(ctx->ev_call, s));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_call, 0));
+    return GCMC_OK;
 }
 
 }  // namespace
@@ -1559,6 +1590,10 @@ int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float
     const size_t tab_smem = d_gff ? (size_t)nsites * h.ffY * 2 * sizeof(float) : 0;
     if (tab_smem > 160 * 1024) return GCMC_ERR_LIMIT;
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    {
+        const int ost = order_before(ctx, s);
+        if (ost != GCMC_OK) return ost;
+    }
     RepDev R = ctx->repdev[rep];
     float2* lj = nullptr;
     double *epart = nullptr, *glj = nullptr;
@@ -1611,6 +1646,7 @@ int gcmc_energy_grad(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, const float
     if (ngpart) cudaFreeAsync(ngpart, s);
     if (gpart) cudaFreeAsync(gpart, s);
     if (glj) cudaFreeAsync(glj, s);
+    if (st == GCMC_OK) st = order_after(ctx, s);
     return st;
 }
 
@@ -1672,6 +1708,7 @@ int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, co
     double* part = reinterpret_cast<double*>(scratch);
     int* ngpart = reinterpret_cast<int*>(part + kNoAllocMaxParts);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    if ((st = order_before(ctx, s)) != GCMC_OK) return st;
     {
         const int pst = pme_update(ctx, rep, s);
         if (pst != GCMC_OK) return pst;
@@ -1680,7 +1717,7 @@ int gcmc_energy_poses_noalloc(gcmc_ctx* ctx, int32_t rep, const float* d_xyz, co
                                                           d_centres, d_self, nposes, nslab, part, ngpart);
     k_sum_parts<<<(nposes + 255) / 256, 256, 0, s>>>(part, ngpart, nposes, nslab, d_out, d_ngroups);
     CK(cudaGetLastError());
-    return GCMC_OK;
+    return order_after(ctx, s);
 }
 
 }  // extern "C"

@@ -6,7 +6,7 @@ The builders restate pyGCMC's input assembly for the hot path:
 * :func:`move_array`       -- ``GCMCDataset.get_move``   (gcmc/python/dataset.py:141-171)
 * :func:`fix_groups`       -- ``GCMCDataset.set_fixCut`` (gcmc/python/dataset.py:175-188)
 * :func:`lj_pair_table`    -- ``GCMCSimulation.get_simulation`` type/LJ tables
-  (gcmc/python/simulation.py:166-214)
+  (gcmc/python/simulation.py:56-75)
 * :func:`assemble`         -- ``GCMCDataset.update_data`` (gcmc/python/dataset.py:190-373)
 
 Differences from the reference are deliberate and few: the cavity-grid voxels
@@ -159,7 +159,7 @@ def fix_groups(xyz: np.ndarray, fix_cutoff: float = 6.0) -> np.ndarray:
 
 
 def lj_pair_table(frag_types: Sequence[str], env_types: Sequence[str], nb: dict, nbfix: Optional[dict] = None):
-    """Type tables and the LJ pair table (simulation.py:166-214).
+    """Type tables and the LJ pair table (simulation.py:56-75).
 
     ``nb[type] = (sigma_nm, eps_kJ)``.  Rows are the fragment types in order of
     appearance, columns all types (fragment types first); pair parameters come

@@ -114,4 +114,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYGCMC_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: {os.path.basename(__file__)} /path/to/pyGCMC (or set PYGCMC_REFERENCE)")
+    main(ref)

@@ -79,3 +79,19 @@ def test_create_rejects_inconsistent_input_without_gpu(water_small):
     with pytest.raises(GcmcError) as e:
         Engine(s)
     assert e.value.status == 3
+
+
+def test_reference_binding_links_to_this_library():
+    """The reference's CPython binding (gcmc/cpp/gcmc.cpp, unmodified) built
+    against libgcmc_b200.so loads and exposes runGCMC (calling it needs a GPU)."""
+    import glob
+    import importlib.util
+    paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", "binding", "gpu*.so"))
+    if not paths:
+        pytest.skip("the reference's binding was not built (make -C oracle ref needs the pyGCMC sources)")
+    out = subprocess.check_output(["ldd", paths[0]]).decode()
+    assert "libgcmc_b200.so" in out and "not found" not in out
+    spec = importlib.util.spec_from_file_location("gpu", paths[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert callable(mod.runGCMC)

@@ -74,7 +74,7 @@ def test_update_data_matches_reference(gold):
 
 
 def test_lj_pair_table_combining_rules():
-    """Lorentz-Berthelot unless an NBFIX pair exists (simulation.py:183-202)."""
+    """Lorentz-Berthelot unless an NBFIX pair exists (simulation.py:56-75)."""
     from pygcmc_b200.system import lj_pair_table
     nb = {"A": (0.3, 0.5), "B": (0.2, 0.8), "C": (0.35, 0.2)}
     t1, t2, ff = lj_pair_table(["A", "B", "A"], ["C", "A"], nb, nbfix={("C", "B"): (0.11, 0.22)})
@@ -83,3 +83,24 @@ def test_lj_pair_table_combining_rules():
     np.testing.assert_allclose(tab[0, 1], [(0.3 + 0.2) / 2, np.sqrt(0.5 * 0.8)], rtol=1e-6)
     np.testing.assert_allclose(tab[1, 2], [0.11, 0.22], rtol=1e-6)
     np.testing.assert_allclose(tab[0, 0], [0.3, 0.5], rtol=1e-6)
+
+
+def test_lj_pair_table_matches_reference_get_simulation():
+    """Type tables and pair table equal the output of pyGCMC's own get_simulation
+    loop (simulation.py:37-86) on the golden case (tests/golden/make_lj_golden.py):
+    row and column type order, NBFIX looked up in both orders, Lorentz-Berthelot
+    otherwise, each atom's column index, and the float32 table bit for bit."""
+    import json
+    from pygcmc_b200.system import lj_pair_table
+    with open(os.path.join(ROOT, "tests", "golden", "lj_table.json")) as f:
+        G = json.load(f)
+    nb = {k: tuple(v) for k, v in G["nb"].items()}
+    nbfix = {(a, b): (s, e) for a, b, s, e in G["nbfix"]}
+    frag_flat = [t for ft in G["frag_types"] for t in ft]
+    t1, t2, ff = lj_pair_table(frag_flat, G["env_types"], nb, nbfix)
+    assert t1 == G["ref_atomtypes1"] and t2 == G["ref_atomtypes2"]
+    ref_ff = np.array(G["ref_ff_pairs"], dtype=np.float32).ravel()
+    assert np.array_equal(ff, ref_ff)
+    col = {t: i for i, t in enumerate(t2)}
+    assert [col[t] for t in G["env_types"]] == G["ref_env_typenum"]
+    assert [[col[t] for t in ft] for ft in G["frag_types"]] == G["ref_frag_typenum"]
