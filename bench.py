@@ -61,6 +61,21 @@ def make_system(seed, mcsteps):
     return S.protein_system(seed=seed, mcsteps=mcsteps)
 
 
+WATER_WORKLOAD = ("water box: 800 rigid TIP3P waters in a 30 A periodic box, no fixed atoms, muex -5.8 kcal/mol, "
+                  "55 M, confBias 1000, cutoff 12 A, equal move probabilities, translate in a 1 A cube, rotate "
+                  "<= 15 degrees about a uniform axis")
+
+
+def make_water(seed, mcsteps):
+    from pygcmc_b200 import system as S
+    return S.water_box(n_water=800, box=30.0, seed=seed, mcsteps=mcsteps)
+
+
+def water_options(**kw):
+    from pygcmc_b200._native import default_options
+    return default_options(proposal=1, muex_kcal=1, trn_step=1.0, rot_max=float(np.radians(15.0)), **kw)
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle sampling during the timed region."""
 
@@ -153,7 +168,8 @@ def load_traffic():
     return None
 
 
-def run_ours(args, ws, rank, local):
+def run_ours(args, ws, rank, local, kind="protein"):
+    """One replica per GPU: the protein workload (the headline), or the water box."""
     import torch
     from pygcmc_b200._native import default_options
     from pygcmc_b200.engine import Engine
@@ -163,13 +179,16 @@ def run_ours(args, ws, rank, local):
     seed = replicas_seed(args.seed, rank)
     prof_steps = 256
     total = (args.warmup + args.steps) * chunk + prof_steps + 64
-    sysm = make_system(seed, total)
+    water = kind == "water"
+    sysm = make_water(seed, total) if water else make_system(seed, total)
+    base = water_options() if water else default_options()
     if args.cells > 0:
-        opts, t_tune = default_options(cells_per_cutoff=args.cells), 0.0
+        base.cells_per_cutoff = args.cells
+        opts, t_tune = base, 0.0
     else:  # launch shape from the autotuner (untimed set-up)
         from pygcmc_b200.engine import autotune
         t0 = time.perf_counter()
-        opts, _ = autotune(sysm, default_options(), trial_steps=128)
+        opts, _ = autotune(sysm, base, trial_steps=128)
         t_tune = time.perf_counter() - t0
     eng = Engine(sysm.copy(), opts)
     stream = torch.cuda.ExternalStream(eng.stream)
@@ -241,10 +260,11 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair terms, fp64 sums/acceptance",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": ref_config(WORKLOAD, chunk, 1, ws),
+        "config": ref_config(WATER_WORKLOAD if water else WORKLOAD, chunk, 1, ws),
         "launch_shape": {"cells_per_cutoff": opts.cells_per_cutoff, "split_items": opts.split_items,
                          "branches": opts.branches, "energy_blocks_per_sm": opts.energy_blocks_per_sm,
-                         "energy_variant": opts.energy_variant,
+                         "energy_variant": opts.energy_variant, "energy_kernel": opts.energy_kernel,
+                         "tile_cells": opts.tile_cells,
                          "source": "--cells" if args.cells > 0 else
                          f"autotuned before timing ({t_tune:.1f} s, untimed)"},
         "e2e": {"value": round(e2e_val, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
@@ -271,9 +291,17 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu and not water:
         out["cpu_baseline"] = cpu_baseline(seed)
     return out
+
+
+def summary(out):
+    """The figures of a workload's bench line that the default run reports beside its headline."""
+    keys = ("value", "unit", "ms_per_step", "steps", "warmup", "config", "e2e", "roofline", "roofline_accept",
+            "launch_shape", "autotuned", "speculation", "forcebias", "gradient", "clocks", "gpu_launches",
+            "pairs_per_s")
+    return {k: out[k] for k in keys if k in out}
 
 
 BATCH_WORKLOAD = ("64 replicas of uneven size in one context: synthetic proteins of 2000-40000 atoms "
@@ -367,7 +395,8 @@ def run_ours_batched(args, ws, rank, local):
                       "branches": best.branches, "energy_blocks_per_sm": best.energy_blocks_per_sm,
                       "trials": len(trials), "tune_s": round(t_tune, 2),
                       "energy_variant": best.energy_variant,
-                      "trial_ms_per_step": [[*t[:5], round(t[5], 4)] for t in trials]},
+                      "energy_kernel": best.energy_kernel, "tile_cells": best.tile_cells,
+                      "trial_ms_per_step": [[*t[:5], *t[6:], round(t[5], 4)] for t in trials]},
         "generate_s": round(t_gen, 2),
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
@@ -820,10 +849,13 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["protein", "batched", "forcebias", "large", "water"], default="protein",
-                    help="protein: one 6000-atom replica per GPU; batched: --replicas uneven replicas per GPU; "
-                         "forcebias: force-biased vs plain translate/rotate on the protein system; "
-                         "large: 200000-atom slab with PME, --replicas replicas")
+    ap.add_argument("--workload", choices=["all", "protein", "batched", "forcebias", "large", "water"],
+                    default="all",
+                    help="all (default): the protein headline and, on one GPU, the batched, water and "
+                         "force-bias workloads as sub-results of the same line; protein: one 6000-atom "
+                         "replica per GPU; batched: --replicas uneven replicas per GPU; forcebias: force-biased "
+                         "vs plain translate/rotate on the protein system; water: the 800-water box; large: "
+                         "200000-atom slab with PME, --replicas replicas")
     ap.add_argument("--replicas", type=int, default=0, help="default 64 (batched), 16 (large)")
     ap.add_argument("--chunk", type=int, default=0, help="MC steps per bench step (default 2048; batched 256)")
     ap.add_argument("--ref-chunk", type=int, default=0,
@@ -870,8 +902,18 @@ def main():
             out = run_ours_forcebias(args, ws, rank, local)
         elif args.workload == "large":
             out = run_ours_large(args, ws, rank, local)
+        elif args.workload == "water":
+            out = run_ours(args, ws, rank, local, kind="water")
         else:
             out = run_ours(args, ws, rank, local)
+            if args.workload == "all" and ws == 1:
+                import copy
+                for name, fn, chunk, kw in (("batched", run_ours_batched, 256, {}),
+                                            ("water", run_ours, 2048, {"kind": "water"}),
+                                            ("forcebias", run_ours_forcebias, 8192, {})):
+                    sub = copy.copy(args)
+                    sub.chunk, sub.no_cpu = chunk, True
+                    out[name] = summary(fn(sub, ws, rank, local, **kw))
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

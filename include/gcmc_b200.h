@@ -119,12 +119,19 @@ typedef struct {
                             and kept when the step accepts nothing (the state is then
                             unchanged, so the results are those of the sequential
                             order); 0 = on, -1 = off                               */
+    int32_t energy_kernel; /* 0: tiled pose energies where the context allows them
+                            (no PME, proposal 0 or 1): the step's poses are binned
+                            into blocks of tile_cells^3 cells and each block's window
+                            of groups and atoms is staged in shared memory once for
+                            all its poses; -1: one warp per pose and cell range     */
+    int32_t tile_cells;  /* tiled kernel: pose-block edge in cells (0 = cells_per_cutoff) */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
 typedef struct {
     int32_t cells_per_cutoff, split_items, branches, energy_blocks_per_sm, energy_variant;
     float ms_per_step;   /* device time per MC step (all replicas)                  */
+    int32_t energy_kernel, tile_cells;
 } gcmc_tune_trial;
 
 /* One per-step record (56 bytes). */

@@ -18,7 +18,7 @@
 //   3. all warps write the accepted poses into their slots, then one thread
 //      applies the cell-list and count updates in acceptance order.
 #pragma once
-#include "energy.cuh"
+#include "tiles.cuh"
 
 namespace gcmc {
 
@@ -178,8 +178,10 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 
 // ---- next-step preparation (whole CTA) ----
-__device__ void prepare_step(const RepDev& R, int step) {
+// scratch: kBinScratchBytes of shared memory for the tiled contexts' pose binning.
+__device__ void prepare_step(const RepDev& R, int step, int* scratch) {
     __shared__ StepDesc Dsh;
+    __shared__ int wtot_sh[32];
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) {
         StepDesc D{};
@@ -219,8 +221,9 @@ __device__ void prepare_step(const RepDev& R, int step) {
             // split each pose's cell window so a step has at most split_items work items
             // (at least one range per pose, at most max_split)
             const int kv = max(1, D.k * D.nvar);
-            D.nslab = max(1, min(R.max_split, R.split_items / kv));
-            D.items = D.fb ? D.k * D.nslab : D.k * D.nvar * D.nslab;
+            // tiled contexts: one energy per pose variant, items = tiles (set below)
+            D.nslab = R.tiled ? 1 : max(1, min(R.max_split, R.split_items / kv));
+            D.items = R.tiled ? 0 : (D.fb ? D.k * D.nslab : D.k * D.nvar * D.nslab);
             D.items_pre = D.fb ? D.k * D.nslab : 0;
         }
         Dsh = D;
@@ -251,20 +254,33 @@ __device__ void prepare_step(const RepDev& R, int step) {
             R.pcen[i] = c;
         }
     }
-    if (tid == 0) *R.desc = D;
+    if (R.tiled && D.move != MV_NONE && D.k > 0) {
+        __syncthreads();  // centres and slots written above
+        const int ntiles = bin_entries(R, D, scratch, wtot_sh);
+        if (tid == 0) Dsh.items = ntiles;
+    }
+    if (tid == 0) {
+        StepDesc Dw = D;
+        Dw.items = Dsh.items;
+        *R.desc = Dw;
+    }
     __syncthreads();
 }
 
+// The preparation kernels take kBinScratchBytes of dynamic shared memory when
+// the context is tiled (the pose binning's scratch).
 __global__ void __launch_bounds__(kAcceptThreads) k_prepare(const RepDev* __restrict__ reps, int nrep) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const RepDev& R = reps[blockIdx.x];
     const StepDesc D = *R.desc;
     __syncthreads();
-    if (D.move == MV_NONE) prepare_step(R, D.step);
+    if (D.move == MV_NONE) prepare_step(R, D.step, reinterpret_cast<int*>(smem_raw));
 }
 
 // Prepare step `step` in one descriptor (a run's first step, whichever copy holds it).
 __global__ void __launch_bounds__(kAcceptThreads) k_prepare_at(const RepDev* __restrict__ rep, int step) {
-    prepare_step(*rep, step);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    prepare_step(*rep, step, reinterpret_cast<int*>(smem_raw));
 }
 
 __global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
@@ -288,6 +304,8 @@ __global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
 // that (as if the other copy's step accepts nothing); mode 1: prepare this
 // copy's step again from the current state unless its speculation stands.
 __global__ void __launch_bounds__(kAcceptThreads) k_prep_spec(const RepDev* __restrict__ reps, int mode) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int* scratch = reinterpret_cast<int*>(smem_raw);
     const RepDev& R = reps[0];
     if (mode == 0) {
         const int step = *R.other->spec_step + 1;
@@ -295,12 +313,12 @@ __global__ void __launch_bounds__(kAcceptThreads) k_prep_spec(const RepDev* __re
             *R.pairs_pending = 0ull;
             *R.spec_step = step;
         }
-        prepare_step(R, step);
+        prepare_step(R, step, scratch);
     } else {
         const int valid = *R.valid;
         const int step = *R.spec_step;
         __syncthreads();
-        if (!valid) prepare_step(R, step);
+        if (!valid) prepare_step(R, step, scratch);
     }
 }
 
@@ -838,7 +856,7 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     if (spec) {  // the next step's speculation stands iff this step accepted nothing
         if (tid == 0) *R.other->valid = S.misc[0] == 0 ? 1 : 0;
     } else {
-        prepare_step(R, D.step + 1);
+        prepare_step(R, D.step + 1, reinterpret_cast<int*>(S.nb));  // the bit matrix is dead here
     }
     PHASE(4);
 #undef PHASE

@@ -427,6 +427,16 @@ struct RepDev {
     // Ewald electrostatics by smooth PME (pme = 1): real-space Coulomb erfc(alpha r)/r,
     // the reciprocal-space potential phi of the current state on a mesh (FP64),
     // interpolated at trial sites with order-4 B-splines
+    // tiled pose energies (k_energy_tiles): pose blocks of tblk^3 cells, nbk blocks
+    // per axis, windows of tspan cells per axis (min(tblk + 2 range, nc)); per step
+    // the preparation bins the pose entries by block (pbin) and cuts the blocks
+    // into tiles (block, first entry in pbin, entry count, 0)
+    int tiled;
+    int tblk;
+    int nbk[3];
+    int tspan[3];
+    int* pbin;          // [2 * kMaxPoses]
+    int4* tiles;        // [2 * kMaxPoses]
     int pme;
     float pme_alpha;
     int pme_n[3];

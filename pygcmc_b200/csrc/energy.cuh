@@ -55,7 +55,8 @@ __device__ __forceinline__ void two_sum(float a, float b, float& hi, float& lo) 
 // Per item: the pose centre plus each periodic image shift as an exact
 // (hi, lo) pair, so an atom's centre-relative offset (a - hi) - lo carries a
 // single rounding of the offset itself.
-__device__ __forceinline__ void set_centre(const RepDev& R, WarpBuf& B, float cx, float cy, float cz, int lane) {
+template <class Buf>
+__device__ __forceinline__ void set_centre(const RepDev& R, Buf& B, float cx, float cy, float cz, int lane) {
     if (lane < 9) {
         const int ax = lane / 3, code = lane - 3 * (lane / 3);
         const float c = ax == 0 ? cx : (ax == 1 ? cy : cz);
@@ -70,7 +71,8 @@ __device__ __forceinline__ void set_centre(const RepDev& R, WarpBuf& B, float cx
 
 // Site s of the pose (centre-relative x, y, z and K q) into B.site and its
 // slot of the interleaved pair layout.
-__device__ __forceinline__ void put_site(WarpBuf& B, int s, float x, float y, float z, float kq) {
+template <class Buf>
+__device__ __forceinline__ void put_site(Buf& B, int s, float x, float y, float z, float kq) {
     B.site[s] = make_float4(x, y, z, kq);
     float* p = reinterpret_cast<float*>(&B.spair[s >> 1]) + (s & 1);
     p[0] = -x;
@@ -566,7 +568,8 @@ __device__ __forceinline__ double fb_ln_ratio(const RepDev& R, const StepDesc& D
 
 // Load the pose of item (i, variant v) of step D into B.site; returns the
 // pose centre and the residue to skip.
-__device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, int i, int v, WarpBuf& B,
+template <class Buf>
+__device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, int i, int v, Buf& B,
                                            int lane, float& cx, float& cy, float& cz, int& self) {
     const FragDev& F = R.frag[D.ftype];
     const int ns = F.nsites;
@@ -621,7 +624,8 @@ __device__ __forceinline__ void build_pose(const RepDev& R, const StepDesc& D, i
 // The first item of pose i's new variant keeps its trial sites (absolute
 // position, charge) for the accept kernel, which writes an accepted pose from
 // them instead of rebuilding it.
-__device__ __forceinline__ void keep_sites(const RepDev& R, const StepDesc& D, const WarpBuf& B, int i, int v, int zi,
+template <class Buf>
+__device__ __forceinline__ void keep_sites(const RepDev& R, const StepDesc& D, const Buf& B, int i, int v, int zi,
                                            int lane) {
     if (v == 0 && zi == 0 && D.move != MV_DELETE && lane < R.frag[D.ftype].nsites)
         R.psite[i * kMaxSites + lane] = B.site_abs[lane];

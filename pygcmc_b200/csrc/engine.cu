@@ -81,6 +81,10 @@ struct RepHost {
     unsigned long long* pending2 = nullptr; // [2] per copy
     double* pgum = nullptr;
     double* plnu = nullptr;
+    int* pbin = nullptr;       // tiled contexts: the step's pose entries by block
+    int4* tiles = nullptr;     //   and its tiles
+    int* pbin2 = nullptr;      //   (the speculating copy's)
+    int4* tiles2 = nullptr;
     float* fpart = nullptr;
     float4* fbprop = nullptr;
     int* fbcnt = nullptr;
@@ -124,6 +128,8 @@ struct gcmc_ctx {
     int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
     int evar = 0;        // pose-energy kernel variant: 0 = 3 CTAs per SM, 1 = 4 CTAs per SM
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
+    bool tiled = false;  // pose energies by k_energy_tiles (every replica allows it)
+    bool pme_any = false; // some replica runs Ewald electrostatics
     int gridF = 0;       // k_energy_fb CTAs
     std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
     // ordering of calls that launch on a caller's stream against the context's
@@ -179,6 +185,7 @@ void free_rep(RepHost& h) {
     dfree(h.desc2); dfree(h.pcen2); dfree(h.pslot2); dfree(h.epart2); dfree(h.nbr2); dfree(h.pgum2); dfree(h.plnu2);
     dfree(h.psite2); dfree(h.valid2); dfree(h.abort2); dfree(h.sstep2); dfree(h.pending2); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
+    dfree(h.pbin); dfree(h.tiles); dfree(h.pbin2); dfree(h.tiles2);
     if (h.plans) {
         cufftDestroy(h.plan_f);
         cufftDestroy(h.plan_b);
@@ -368,6 +375,24 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
                                                        opt.energy_blocks_per_sm, ctx->spec ? 1 : 0);
     h.nslab = std::max(d.span[2], d.max_split);
     h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
+    // tiled pose energies: blocks of B^3 cells, windows of B + 2R cells per axis
+    {
+        const int B = std::max(1, opt.tile_cells > 0 ? opt.tile_cells : Rc);
+        d.tblk = B;
+        long long nblk = 1, nwin = 1;
+        for (int a = 0; a < 3; ++a) {
+            d.nbk[a] = (d.nc[a] + B - 1) / B;
+            d.tspan[a] = std::min(B + 2 * Rc, d.nc[a]);
+            nblk *= d.nbk[a];
+            nwin *= d.tspan[a];
+        }
+        int maxga = 0;
+        for (int g = 0; g < in.fragmentInfo[0].startRes; ++g) maxga = std::max(maxga, in.residueInfo[g].atomNum);
+        for (int t = 0; t < I->fragTypeNum; ++t) maxga = std::max(maxga, in.fragmentInfo[t].num_atoms);
+        const bool pme_on = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
+        d.tiled = (opt.energy_kernel >= 0 && !pme_on && opt.proposal != 2 && nblk <= kMaxBlocks &&
+                   nwin <= kTileCells && maxga <= kTileMaxGroupAtoms) ? 1 : 0;
+    }
     d.cutoff = I->cutoff;
     d.grid_dx = I->grid_dx;
     d.trn_step = opt.trn_step;
@@ -485,12 +510,13 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
+    AL(h.pbin, 2 * kMaxPoses); AL(h.tiles, 2 * kMaxPoses);
     AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
     if (ctx->spec) {
         AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.nslab);
         AL(h.nbr2, (size_t)kMaxPoses * kMaxWords); AL(h.pgum2, kMaxPoses); AL(h.plnu2, kMaxPoses);
         AL(h.psite2, (size_t)kMaxPoses * kMaxSites); AL(h.valid2, 2); AL(h.abort2, 2); AL(h.sstep2, 2);
-        AL(h.pending2, 2);
+        AL(h.pending2, 2); AL(h.pbin2, 2 * kMaxPoses); AL(h.tiles2, 2 * kMaxPoses);
     }
     // smooth PME: mesh, influence function, FFT plans
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
@@ -603,11 +629,12 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.counters = h.counters; d.err = h.err;
     d.energy = h.energy; d.pgum = h.pgum; d.psite = h.psite; d.plnu = h.plnu; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
     d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
+    d.pbin = h.pbin; d.tiles = h.tiles;
     if (ctx->spec) {
         RepDev& b = ctx->repdev_b;
         b = d;
         b.desc = h.desc2; b.pcen = h.pcen2; b.pslot = h.pslot2; b.epart = h.epart2; b.nbr = h.nbr2;
-        b.pgum = h.pgum2; b.plnu = h.plnu2; b.psite = h.psite2;
+        b.pgum = h.pgum2; b.plnu = h.plnu2; b.psite = h.psite2; b.pbin = h.pbin2; b.tiles = h.tiles2;
         d.valid = h.valid2; d.pairs_pending = h.pending2; d.abort = h.abort2; d.spec_step = h.sstep2;
         b.valid = h.valid2 + 1; b.pairs_pending = h.pending2 + 1; b.abort = h.abort2 + 1; b.spec_step = h.sstep2 + 1;
     }
@@ -630,6 +657,30 @@ int upload_reps(gcmc_ctx* ctx) {
 
 using EnergyKernel = void (*)(const RepDev*, int, int);
 EnergyKernel energy_kernel(int variant) { return variant == 1 ? k_energy_t<4> : k_energy_t<3>; }
+
+// One pose-energy launch over replicas reps[0, n) in `mode` on `grid` CTAs:
+// the tiled kernel when the context is tiled, else the per-pose-warp kernel.
+void launch_energy(const gcmc_ctx* ctx, const RepDev* reps, int n, int mode, int grid, cudaStream_t s) {
+    if (ctx->tiled)
+        k_energy_tiles<<<grid, kWarpsT * 32, sizeof(TileSmem), s>>>(reps, n, mode);
+    else
+        energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+}
+
+// Dynamic shared memory of the preparation kernels (the pose binning's scratch).
+size_t prep_smem(const gcmc_ctx* ctx) { return ctx->tiled ? (size_t)kBinScratchBytes : 0; }
+
+// The context is tiled when every replica allows it; otherwise no replica is.
+void finalize_tiling(gcmc_ctx* ctx) {
+    bool all = true;
+    for (const auto& d : ctx->repdev) all = all && d.tiled;
+    ctx->tiled = all;
+    for (auto& d : ctx->repdev) d.tiled = all ? 1 : 0;
+    ctx->repdev_b.tiled = all ? 1 : 0;
+    bool pme = false;
+    for (const auto& h : ctx->reps) pme = pme || h.pme;
+    ctx->pme_any = pme;
+}
 
 // Resident warps of the pose-energy grid for this register variant and CTA cap.
 int energy_warps(int device, int evar, int ebps, int spare_sms) {
@@ -683,7 +734,12 @@ int pme_init_fixed(gcmc_ctx* ctx) {
 int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     int sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, energy_kernel(ctx->evar), kWarpsE * 32, 0));
+    if (ctx->tiled) {
+        CK(cudaFuncSetAttribute(k_energy_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_energy_tiles, kWarpsT * 32, sizeof(TileSmem)));
+    } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, energy_kernel(ctx->evar), kWarpsE * 32, 0));
+    }
     per_sm = std::max(1, per_sm);
     if (ebps > 0) per_sm = std::min(per_sm, ebps);
     ctx->ebps = ebps;
@@ -751,7 +807,6 @@ int build_spec_graph(gcmc_ctx* ctx, int parity) {
     if (st == GCMC_OK && cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) {
-        const EnergyKernel ek = energy_kernel(ctx->evar);
         const int grid_s = std::max(1, ctx->gridE - ctx->per_sm_e);
         cudaEvent_t* evF = ev;                    // F_e of step j done
         cudaEvent_t* evA = ev + kGraphSteps;      // A of step j done
@@ -763,17 +818,17 @@ int build_spec_graph(gcmc_ctx* ctx, int parity) {
             const RepDev* cur = ((parity + i) & 1) ? ctx->d_reps_b : ctx->d_reps;
             const RepDev* nxt = ((parity + i) & 1) ? ctx->d_reps : ctx->d_reps_b;
             if (i > 0) e = cudaStreamWaitEvent(ctx->stream, evS[i - 1], 0);
-            k_prep_spec<<<1, kAcceptThreads, 0, ctx->stream>>>(cur, 1);
-            ek<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(cur, 1, 2);
+            k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(cur, 1);
+            launch_energy(ctx, cur, 1, 2, ctx->gridE, ctx->stream);
             if (e == cudaSuccess) e = cudaEventRecord(evF[i], ctx->stream);
             k_accept<<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);
             if (e == cudaSuccess) e = cudaEventRecord(evA[i], ctx->stream);
             if (i > 0 && e == cudaSuccess) e = cudaStreamWaitEvent(sp, evA[i - 1], 0);
-            k_prep_spec<<<1, kAcceptThreads, 0, sp>>>(nxt, 0);
+            k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), sp>>>(nxt, 0);
             if (e == cudaSuccess) e = cudaEventRecord(evP[i], sp);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, evP[i], 0);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, evF[i], 0);
-            ek<<<grid_s, kWarpsE * 32, 0, ss>>>(nxt, 1, 1);
+            launch_energy(ctx, nxt, 1, 1, grid_s, ss);
             if (e == cudaSuccess) e = cudaEventRecord(evS[i], ss);
         }
         if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, evS[kGraphSteps - 1], 0);
@@ -840,7 +895,7 @@ int build_graph(gcmc_ctx* ctx) {
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
                     k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
                 } else {
-                    energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 0);
+                    launch_energy(ctx, ctx->d_reps + r0, cnt, 0, grid, side[b]);
                 }
                 k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt, 0);
             }
@@ -922,6 +977,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     ctx->repdev.resize(nrep);
     ctx->spec = spec_eligible(nrep, ins, opt);
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
+    if (st == GCMC_OK) finalize_tiling(ctx);
     if (st == GCMC_OK && cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) st = upload_reps(ctx);
     if (st == GCMC_OK) {
@@ -970,8 +1026,10 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const bool spec = spec_eligible(nrep, ins, opt);
     const bool spec_changed = spec != ctx->spec;
     ctx->spec = spec;
+    const bool tiled_before = ctx->tiled, pme_before = ctx->pme_any;
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
     if (st != GCMC_OK) return st;
+    finalize_tiling(ctx);
     st = upload_reps(ctx);
     if (st != GCMC_OK) return st;
     build_cells(ctx);
@@ -982,7 +1040,7 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const int fb = opt.proposal == 2 ? 1 : 0;
     const int evar = opt.energy_variant == 1 ? 1 : 0;
     if (spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb ||
-        evar != ctx->evar) {
+        evar != ctx->evar || ctx->tiled != tiled_before || ctx->pme_any != pme_before) {
         ctx->fb = fb;
         ctx->evar = evar;
         st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
@@ -1244,8 +1302,8 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         int st = trial(o, &ms);
         if (st != GCMC_OK) return st;
         if (trials && n < max_trials)
-            trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items, o.branches, o.energy_blocks_per_sm,
-                                        o.energy_variant, ms};
+            trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items,   o.branches,     o.energy_blocks_per_sm,
+                                        o.energy_variant,   ms,              o.energy_kernel, o.tile_cells};
         ++n;
         if (ms < best_ms) {
             best_ms = ms;
@@ -1254,36 +1312,52 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         return GCMC_OK;
     };
     int st = GCMC_OK;
-    // coordinate descent: cell grid, then work split, then branches, then energy CTAs per SM
+    // coordinate descent: cell grid; the tiled kernel's pose-block edge; the
+    // per-pose-warp kernel (and, if it wins, its work split, register budget and
+    // CTAs per SM); then graph branches
     for (int R : {1, 2, 3}) {
         gcmc_options o = cur;
         o.cells_per_cutoff = R;
         if (st == GCMC_OK) st = consider(o);
     }
-    const int base_split = cur.split_items;
-    for (int sp : {512, 1024, 2048, 4096, 8192}) {
-        if (sp == base_split) continue;
+    if (cur.energy_kernel >= 0) {
+        const int base_b = cur.tile_cells > 0 ? cur.tile_cells : cur.cells_per_cutoff;
+        for (int B : {1, 2, 3}) {
+            if (B == base_b) continue;
+            gcmc_options o = cur;
+            o.tile_cells = B;
+            if (st == GCMC_OK) st = consider(o);
+        }
         gcmc_options o = cur;
-        o.split_items = sp;
+        o.energy_kernel = -1;
         if (st == GCMC_OK) st = consider(o);
+    }
+    if (cur.energy_kernel < 0) {
+        const int base_split = cur.split_items;
+        for (int sp : {512, 1024, 2048, 4096, 8192}) {
+            if (sp == base_split) continue;
+            gcmc_options o = cur;
+            o.split_items = sp;
+            if (st == GCMC_OK) st = consider(o);
+        }
+        {
+            gcmc_options o = cur;
+            o.energy_variant = cur.energy_variant == 1 ? 0 : 1;
+            if (st == GCMC_OK) st = consider(o);
+        }
+        const int base_e = cur.energy_blocks_per_sm;
+        for (int e : {0, 2, 1}) {
+            if (e == base_e) continue;
+            gcmc_options o = cur;
+            o.energy_blocks_per_sm = e;
+            if (st == GCMC_OK) st = consider(o);
+        }
     }
     const int base_br = cur.branches;
     for (int nb : {1, 2, 4}) {
         if (nb == base_br || nb > nrep) continue;
         gcmc_options o = cur;
         o.branches = nb;
-        if (st == GCMC_OK) st = consider(o);
-    }
-    {
-        gcmc_options o = cur;
-        o.energy_variant = cur.energy_variant == 1 ? 0 : 1;
-        if (st == GCMC_OK) st = consider(o);
-    }
-    const int base_e = cur.energy_blocks_per_sm;
-    for (int e : {0, 2, 1}) {
-        if (e == base_e) continue;
-        gcmc_options o = cur;
-        o.energy_blocks_per_sm = e;
         if (st == GCMC_OK) st = consider(o);
     }
     if (ntrials) *ntrials = n;
@@ -1314,7 +1388,7 @@ int gcmc_run(gcmc_ctx* ctx, int32_t nsteps) {
             CK(cudaGraphLaunch(ctx->gexec_spec[first & 1], ctx->stream));
         return GCMC_OK;
     }
-    k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+    k_prepare<<<ctx->nrep, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(ctx->d_reps, ctx->nrep);
     CK(cudaGetLastError());
     for (int done = 0; done < need; done += kGraphSteps) CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     return GCMC_OK;
@@ -1333,9 +1407,9 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
     if (need == 0) return GCMC_OK;
     k_set_run_end<<<(ctx->nrep + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, nsteps);
     if (ctx->spec)  // timed one step after another: the first descriptor copy only
-        k_prepare_at<<<1, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, first);
+        k_prepare_at<<<1, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(ctx->d_reps, first);
     else
-        k_prepare<<<ctx->nrep, kAcceptThreads, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep);
+        k_prepare<<<ctx->nrep, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(ctx->d_reps, ctx->nrep);
     CK(cudaGetLastError());
     std::vector<cudaEvent_t> ev(3 * (size_t)need);
     for (auto& e : ev) CK(cudaEventCreate(&e));
@@ -1349,7 +1423,7 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
             k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
         } else {
-            energy_kernel(ctx->evar)<<<ctx->gridE, kWarpsE * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);
+            launch_energy(ctx, ctx->d_reps, ctx->nrep, 0, ctx->gridE, ctx->stream);
         }
         CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
         k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);

@@ -48,8 +48,9 @@ def occupied_res(s):
                            for f in s.fragmentInfo])
 
 
-def check_trajectory(oracle, system, nsteps, proposal=0, muex_kcal=0):
-    logs_g, E_g, final_g, counters = engine_trajectory(system, nsteps, proposal=proposal, muex_kcal=muex_kcal)
+def check_trajectory(oracle, system, nsteps, proposal=0, muex_kcal=0, **engine_opts):
+    logs_g, E_g, final_g, counters = engine_trajectory(system, nsteps, proposal=proposal, muex_kcal=muex_kcal,
+                                                       **engine_opts)
     assert len(logs_g) == nsteps
     s_o = system.copy()
     opts = oracle.options(proposal=proposal, muex_kcal=muex_kcal)
@@ -358,3 +359,18 @@ def test_pair_counter_equals_oracle_pairs(oracle_lib, protein_small):
             if checked == 3:
                 break
     assert checked >= 1
+
+
+@pytest.mark.parametrize("kernel,tile_cells,cells", [(-1, 0, 2), (0, 1, 2), (0, 3, 2), (0, 0, 1), (0, 0, 3)])
+def test_trajectory_pose_energy_kernels(oracle_lib, protein_small, kernel, tile_cells, cells):
+    """Every pose-energy kernel and launch shape replays on the oracle: the
+    per-pose-warp kernel (energy_kernel -1) and the tiled kernel with pose
+    blocks of 1 and 3 cells and cell grids of 1 and 3 cells per cutoff."""
+    check_trajectory(oracle_lib, protein_small, 96, energy_kernel=kernel, tile_cells=tile_cells,
+                     cells_per_cutoff=cells)
+
+
+def test_trajectory_water_tiled_pair_image(oracle_lib, water_small):
+    """The small water box takes the per-pair minimum image; the tiled kernel
+    with one-cell pose blocks (more tiles than the default for a small box)."""
+    check_trajectory(oracle_lib, water_small, 96, tile_cells=1)
