@@ -396,6 +396,9 @@ def run_ours_batched(args, ws, rank, local):
                       "trials": len(trials), "tune_s": round(t_tune, 2),
                       "energy_variant": best.energy_variant,
                       "energy_kernel": best.energy_kernel, "tile_cells": best.tile_cells,
+                      "persistent": best.persistent,
+                      "trial_fields": ["cells_per_cutoff", "split_items", "branches", "energy_blocks_per_sm",
+                                       "energy_variant", "energy_kernel", "tile_cells", "persistent", "ms_per_step"],
                       "trial_ms_per_step": [[*t[:5], *t[6:], round(t[5], 4)] for t in trials]},
         "generate_s": round(t_gen, 2),
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",

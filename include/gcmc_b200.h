@@ -119,19 +119,39 @@ typedef struct {
                             and kept when the step accepts nothing (the state is then
                             unchanged, so the results are those of the sequential
                             order); 0 = on, -1 = off                               */
-    int32_t energy_kernel; /* 0: tiled pose energies where the context allows them
+    int32_t energy_kernel; /* 0: one warp per pose (variant) and cell range;
+                            1: tiled pose energies where the context allows them
                             (no PME, proposal 0 or 1): the step's poses are binned
                             into blocks of tile_cells^3 cells and each block's window
                             of groups and atoms is staged in shared memory once for
-                            all its poses; -1: one warp per pose and cell range     */
+                            all its poses (autotuned)                               */
     int32_t tile_cells;  /* tiled kernel: pose-block edge in cells (0 = cells_per_cutoff) */
+    int32_t pair_delta;  /* 0: a translate / rotate step's energy changes in the
+                            pairwise-difference form where the context allows it
+                            (no PME, proposal 0 or 1): one evaluation per pose over
+                            the groups within the cutoff of either centre, each
+                            atom-site pair contributing its own change (the Coulomb
+                            change from r_o^2 - r_n^2 = delta.(d_o + d_n)), so the
+                            change carries the rounding of itself rather than of the
+                            two pose energies; -1: E_new - E_old from two
+                            evaluations                                         */
+    int32_t persistent;  /* 1: run the step loop of a context without speculation,
+                            PME or force bias, with the per-pose-warp pose-energy
+                            kernel, as one cooperative launch (one CTA per SM: per
+                            step all CTAs evaluate every replica's pose energies,
+                            a grid barrier, CTA r accepts replica r's moves and
+                            prepares its next step, a grid barrier) instead of a
+                            captured graph of per-step launches; 0 = the graph   */
+    int32_t persist_spin_cap; /* polls a CTA waits at the persistent loop's grid
+                            barrier before it gives up, raises device error bit 5
+                            and ends the launch (0 = 2^24, over a second)        */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */
 typedef struct {
     int32_t cells_per_cutoff, split_items, branches, energy_blocks_per_sm, energy_variant;
     float ms_per_step;   /* device time per MC step (all replicas)                  */
-    int32_t energy_kernel, tile_cells;
+    int32_t energy_kernel, tile_cells, persistent;
 } gcmc_tune_trial;
 
 /* One per-step record (56 bytes). */
@@ -235,7 +255,9 @@ int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8);
 /* Device error word (bit 0 cell overflow, bit 1 periodic image > 1 box,
  * bit 2 slot overflow, bit 3 pose limit, bit 4 an explicit pose's site type
  * outside the pair table -- gcmc_energy_poses_noalloc, whose device inputs the
- * host does not read; such a pose's energy is NaN). */
+ * host does not read; such a pose's energy is NaN; bit 5 the persistent step
+ * loop's grid barrier waited longer than gcmc_options.persist_spin_cap, in
+ * replica 0's word). */
 int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);
 /* The cudaStream_t the context launches on. */
 void* gcmc_stream(gcmc_ctx* ctx);
@@ -243,11 +265,12 @@ int gcmc_destroy(gcmc_ctx* ctx);
 
 /* Launch-shape autotuner (no counterpart in the reference).  For the given
  * replicas, times trial_steps MC steps (after 8 warm-up steps) on temporary
- * contexts for a coordinate-descent sequence of candidates -- cell-grid
- * resolution (cells_per_cutoff 1..3), pose-energy work split (split_items
- * 512..8192), graph branches (1, 2, 4), the pose-energy kernel's register
- * budget (energy_variant) and pose-energy CTAs per SM -- and
- * writes the base options with the fastest shape into *best.  trials
+ * contexts for a coordinate-descent sequence of candidates -- pose-energy
+ * kernel (energy_kernel 0 / 1) x cell-grid resolution (cells_per_cutoff 1..3);
+ * then the tiled kernel's pose-block edge, or the per-pose-warp kernel's work
+ * split (split_items 512..8192), register budget (energy_variant) and CTAs per
+ * SM; graph branches (1, 2, 4); for several replicas the persistent step loop
+ * -- and writes the base options with the fastest shape into *best.  trials
  * (optional, max_trials entries) receives each trial; *ntrials their number.
  * The inputs are not modified; the trajectories of a context created with
  * *best are the same MC chain up to FP32 summation order. */

@@ -22,14 +22,15 @@ class Options(ctypes.Structure):
                 ("energy_blocks_per_sm", c_int), ("fb_trn", ctypes.c_float), ("fb_rot", ctypes.c_float),
                 ("step_offset", ctypes.c_uint32), ("pme", c_int), ("pme_alpha", ctypes.c_float),
                 ("pme_grid", c_int * 3), ("energy_variant", c_int), ("speculate", c_int),
-                ("energy_kernel", c_int), ("tile_cells", c_int)]
+                ("energy_kernel", c_int), ("tile_cells", c_int), ("pair_delta", c_int),
+                ("persistent", c_int), ("persist_spin_cap", c_int)]
 
 
 class TuneTrial(ctypes.Structure):
     """gcmc_tune_trial: one autotuner trial."""
     _fields_ = [("cells_per_cutoff", c_int), ("split_items", c_int), ("branches", c_int),
                 ("energy_blocks_per_sm", c_int), ("energy_variant", c_int), ("ms_per_step", ctypes.c_float),
-                ("energy_kernel", c_int), ("tile_cells", c_int)]
+                ("energy_kernel", c_int), ("tile_cells", c_int), ("persistent", c_int)]
 
 
 class ReplicaIn(ctypes.Structure):

@@ -218,12 +218,17 @@ __device__ void prepare_step(const RepDev& R, int step, int* scratch) {
                 D.k = 0;
             }
             D.nw = (D.move == MV_DELETE) ? 0 : (D.k + 31) >> 5;
+            // translate / rotate in the pairwise-difference form: one item per pose (and slab)
+            D.dual = (R.dual && !D.fb && (D.move == MV_TRANSLATE || D.move == MV_ROTATE)) ? 1 : 0;
+            D.margin = (D.dual && D.move == MV_TRANSLATE) ? R.dmargin : 0;
             // split each pose's cell window so a step has at most split_items work items
             // (at least one range per pose, at most max_split)
-            const int kv = max(1, D.k * D.nvar);
-            // tiled contexts: one energy per pose variant, items = tiles (set below)
-            D.nslab = R.tiled ? 1 : max(1, min(R.max_split, R.split_items / kv));
-            D.items = R.tiled ? 0 : (D.fb ? D.k * D.nslab : D.k * D.nvar * D.nslab);
+            const int kv = max(1, D.k * (D.dual ? 1 : D.nvar));
+            // tiled contexts: one energy per pose variant (per pose when dual), items = tiles
+            // (set below)
+            // (a dual item carries both poses' pairs: up to twice as many ranges per pose)
+            D.nslab = R.tiled ? 1 : max(1, min(R.max_split * (D.dual ? 2 : 1), R.split_items / kv));
+            D.items = R.tiled ? 0 : ((D.fb || D.dual) ? D.k * D.nslab : D.k * D.nvar * D.nslab);
             D.items_pre = D.fb ? D.k * D.nslab : 0;
         }
         Dsh = D;
@@ -457,10 +462,10 @@ __device__ __forceinline__ void void_next(const RepDev& R, int step) {
 // speculative launch (booked here); as soon as a move is accepted the
 // speculative evaluation of the next step is voided, and at the end the next
 // step is marked as standing when nothing was accepted.
-__global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep, int spec) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// One replica's step, whole CTA (kAcceptThreads threads); smem_raw: an
+// AcceptSmem.  The body of k_accept and of the persistent step loop.
+__device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned char* smem_raw) {
     AcceptSmem& S = *reinterpret_cast<AcceptSmem*>(smem_raw);
-    const RepDev& R = reps[blockIdx.x];
     const StepDesc D = *R.desc;
     if (D.move == MV_NONE) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x, nwarps = nt >> 5;
@@ -860,6 +865,11 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __re
     }
     PHASE(4);
 #undef PHASE
+}
+
+__global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep, int spec) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    accept_step(reps[blockIdx.x], spec, smem_raw);
 }
 
 }  // namespace gcmc

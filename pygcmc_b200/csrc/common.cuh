@@ -27,7 +27,7 @@ enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_
 // force-bias tilt lambda (Pangali, Rao and Berne): density ~ exp(lambda beta f . d) in the step cube
 constexpr float kFbLambda = 0.5f;
 enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
-enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8, ERR_SITE_TYPE = 16 };
+enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8, ERR_SITE_TYPE = 16, ERR_SYNC = 32 };
 
 // ---------------------------------------------------------------------------
 // exact-rounding float helpers
@@ -335,12 +335,15 @@ struct StepDesc {
     int nvar;      // 1, or 2 for translate/rotate (new, old)
     int nslab;     // work items per pose variant (item z takes window cells z, z + nslab, ...)
     int nw;        // neighbour-row words (0 = no clustering)
-    int items;     // k * nvar * nslab (force-biased steps: k * nslab, the new poses)
+    int items;     // k * nvar * nslab (force-biased and dual steps: k * nslab; tiled: tiles)
     int del_slot;
     int perm_h;
     int fb;        // 1: force-biased translate/rotate (old-pose forces first, then new poses)
     int items_pre; // force-biased steps: k * nslab old-pose items of the first launch; else 0
-    int pad[3];
+    int dual;      // translate / rotate in the pairwise-difference form: items k * nslab, each
+                   // writing the slab's energy change in the new variant's partial and 0 in the old's
+    int margin;    // cells the window reaches beyond R (dual translate steps)
+    int pad;
     U4 perm_key;
 };
 
@@ -424,19 +427,26 @@ struct RepDev {
     float4* fbprop;     // [kMaxPoses * 2] (d or v, invalid flag), (a0, a1, a2, 0) of the old pose
     int* fbcnt;         // [kMaxPoses] old-pose items finished (reset by the last one)
     float* logF;        // [log_cap * log_kmax * 12] F_old, tau_old, F_new, tau_new used
-    // Ewald electrostatics by smooth PME (pme = 1): real-space Coulomb erfc(alpha r)/r,
-    // the reciprocal-space potential phi of the current state on a mesh (FP64),
-    // interpolated at trial sites with order-4 B-splines
     // tiled pose energies (k_energy_tiles): pose blocks of tblk^3 cells, nbk blocks
-    // per axis, windows of tspan cells per axis (min(tblk + 2 range, nc)); per step
-    // the preparation bins the pose entries by block (pbin) and cuts the blocks
-    // into tiles (block, first entry in pbin, entry count, 0)
+    // per axis, windows of tspan cells per axis (min(tblk + 2 range, nc); a translate
+    // step's windows reach dmargin cells further); per step the preparation bins the
+    // pose entries by block (pbin) and cuts the blocks into tiles (block, first entry
+    // in pbin, entry count, entry count of the block's largest tile)
     int tiled;
     int tblk;
     int nbk[3];
     int tspan[3];
     int* pbin;          // [2 * kMaxPoses]
     int4* tiles;        // [2 * kMaxPoses]
+    // translate / rotate energy changes in the pairwise-difference form (dual = 1):
+    // one work item per pose evaluates the old and the new pose together over the
+    // groups within the cutoff of either centre; a translate's new centre lies
+    // within dmargin cells of the old one's, so its windows reach dmargin cells further
+    int dual;
+    int dmargin;
+    // Ewald electrostatics by smooth PME (pme = 1): real-space Coulomb erfc(alpha r)/r,
+    // the reciprocal-space potential phi of the current state on a mesh (FP64),
+    // interpolated at trial sites with order-4 B-splines
     int pme;
     float pme_alpha;
     int pme_n[3];

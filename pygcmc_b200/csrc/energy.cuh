@@ -1,7 +1,9 @@
 // Pose-energy kernel: the batched, cell-listed form of calcEnergy
 // (gcmc/cpp/gcmc_energy.h:142-204).
 //
-// Work item = (pose, variant, z-slab).  One warp per item:
+// Work item = (pose, variant, z-slab), or for a translate / rotate step in the
+// pairwise-difference form (StepDesc.dual) (pose, z-slab) with both poses.
+// One warp per item:
 //   1. builds the pose's sites in shared memory (insertion pose from the RNG,
 //      or the slot's current / moved atoms),
 //   2. walks the cells of its z-slab within R cells of the pose centre, tests
@@ -32,10 +34,21 @@ struct SitePair {
     float2 nx, ny, nz, kq;
 };
 
+// Site s of a translate / rotate pose in the pairwise-difference form: the
+// negated offsets of its old and its new position from the old pose centre
+// (x: old, y: new; the new one in the old centre's periodic frame), and its
+// displacement new - old (from the absolute positions, rounded once) with the
+// Coulomb constant * charge.
+struct DualSite {
+    float2 nx, ny, nz;
+    float4 dk;
+};
+
 struct WarpBuf {
     float4 site[kMaxSites];  // x, y, z relative to the pose centre, Coulomb constant * charge
     int srow[kMaxSites];     // template type * ffY
     SitePair spair[kMaxSites / 2];
+    DualSite dsite[kMaxSites];  // dual items (translate / rotate in the difference form)
     uint2 glist[kGCap];      // included group: (atomStart | image code << 26, atomNum)
     uint32_t alist[kACap];   // atom id  | image code << 26
     float cs_hi[3][4];       // pose centre + image shift (code 0: 0, 1: +L, 2: -L), high part
@@ -113,8 +126,8 @@ __device__ __forceinline__ void flush_atoms_packed(const RepDev& R, const WarpBu
     for (int f = lane; f < na; f += 32) {
         const uint32_t u = B.alist[f];
         const int idx = (int)(u & 0x3FFFFFFu);
-        const float4 a = __ldg(&R.xyzq[idx]);
-        const int ta = __ldg(&R.atype[idx]);
+        const float4 a = R.xyzq[idx];
+        const int ta = R.atype[idx];
         uint32_t c0, c1, c2;
         if (PairImage) {
             const float kx = rintf((a.x - B.cs_hi[0][0]) * R.invL[0]);
@@ -185,8 +198,8 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
     for (int f = lane; f < na; f += 32) {
         const uint32_t u = B.alist[f];
         const int idx = (int)(u & 0x3FFFFFFu);
-        const float4 a = __ldg(&R.xyzq[idx]);
-        const int ta = __ldg(&R.atype[idx]);
+        const float4 a = R.xyzq[idx];
+        const int ta = R.atype[idx];
         uint32_t c0, c1, c2;
         if (PairImage) {  // the atom's image nearest the pose centre
             const float kx = rintf((a.x - B.cs_hi[0][0]) * R.invL[0]);
@@ -242,6 +255,96 @@ __device__ __forceinline__ double flush_atoms(const RepDev& R, const WarpBuf& B,
     return acc;
 }
 
+// One atom's contribution to the energy change E_new - E_old of a translate /
+// rotate pose, sites in the difference form (DualSite), the atom at (ax, ay,
+// az) relative to the old pose centre.  fl bit 0: the atom's group lies within
+// the cutoff of the old centre, bit 1: of the new one.  Both: per site the LJ
+// change lj(new) - lj(old) and the Coulomb change k q_s q_a (1/r_n - 1/r_o),
+// with 1/r_n - 1/r_o = (r_o^2 - r_n^2) / (r_o r_n (r_o + r_n)) and
+// r_o^2 - r_n^2 = (d_o - d_n).(d_o + d_n) = delta.(d_o + d_n): the change comes
+// out to a few ulp of itself instead of as the difference of two terms that
+// are each an order of magnitude larger (under a per-pair minimum image whose
+// old and new shifts differ, 1/r_n - 1/r_o directly).  One side only: +E_new or
+// -E_old terms.  Each pair is the packed (f32x2) form of the single-pose pair
+// energy, x the old pose and y the new one.
+template <bool PairImage>
+__device__ __forceinline__ float dual_atom_e(const RepDev& R, const DualSite* ds, const int* srow, int ns, float ax,
+                                             float ay, float az, float q, int ta, uint32_t fl, const float2* lj) {
+    const float2 mhalf = make_float2(-0.5f, -0.5f), three_half = make_float2(1.5f, 1.5f);
+    const float2 Ax = make_float2(ax, ax), Ay = make_float2(ay, ay), Az = make_float2(az, az);
+    float e = 0.0f;
+#pragma unroll 2
+    for (int s = 0; s < ns; ++s) {
+        const DualSite d = ds[s];
+        float2 dx = __fadd2_rn(Ax, d.nx), dy = __fadd2_rn(Ay, d.ny), dz = __fadd2_rn(Az, d.nz);
+        bool same = true;
+        if (PairImage) {
+            const float kox = rintf(dx.x * R.invL[0]), knx = rintf(dx.y * R.invL[0]);
+            const float koy = rintf(dy.x * R.invL[1]), kny = rintf(dy.y * R.invL[1]);
+            const float koz = rintf(dz.x * R.invL[2]), knz = rintf(dz.y * R.invL[2]);
+            dx = make_float2(fmaf(-kox, R.L[0], dx.x), fmaf(-knx, R.L[0], dx.y));
+            dy = make_float2(fmaf(-koy, R.L[1], dy.x), fmaf(-kny, R.L[1], dy.y));
+            dz = make_float2(fmaf(-koz, R.L[2], dz.x), fmaf(-knz, R.L[2], dz.y));
+            same = kox == knx && koy == kny && koz == knz;
+        }
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        float2 ir = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+        ir = __fmul2_rn(ir, __ffma2_rn(__fmul2_rn(__fmul2_rn(mhalf, r2), ir), ir, three_half));
+        const float2 ir2 = __fmul2_rn(ir, ir);
+        const float2 p = lj[srow[s] + ta];
+        const float2 s2 = __fmul2_rn(make_float2(p.x, p.x), ir2);
+        const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+        const float2 l = __fmul2_rn(make_float2(p.y, p.y), __ffma2_rn(s6, s6, make_float2(-s6.x, -s6.y)));
+        const float kqq = d.dk.w * q;
+        if (fl == 3u) {
+            float dinv;
+            if (same) {
+                const float D = fmaf(d.dk.z, dz.x + dz.y, fmaf(d.dk.y, dy.x + dy.y, d.dk.x * (dx.x + dx.y)));
+                const float2 r = __fmul2_rn(r2, ir);
+                dinv = __fdividef(D * ir.x * ir.y, r.x + r.y);
+            } else {
+                dinv = ir.y - ir.x;
+            }
+            e += fmaf(kqq, dinv, l.y - l.x);
+        } else if (fl == 2u) {
+            e += fmaf(kqq, ir.y, l.y);
+        } else {
+            e -= fmaf(kqq, ir.x, l.x);
+        }
+    }
+    return e;
+}
+
+// The buffered atoms B.alist[0, na) of a dual item: atom id in bits 0-23, the
+// inclusion flags (dual_atom_e) in bits 24-25, the group's image code relative
+// to the old centre in bits 26-31.
+template <bool PairImage>
+__device__ __forceinline__ void flush_dual(const RepDev& R, const WarpBuf& B, int na, int ns, int lane,
+                                           double& acc) {
+    for (int f = lane; f < na; f += 32) {
+        const uint32_t u = B.alist[f];
+        const int idx = (int)(u & 0xFFFFFFu);
+        const float4 a = R.xyzq[idx];
+        const int ta = R.atype[idx];
+        uint32_t c0, c1, c2;
+        if (PairImage) {  // the atom's image nearest the old pose centre
+            const float kx = rintf((a.x - B.cs_hi[0][0]) * R.invL[0]);
+            const float ky = rintf((a.y - B.cs_hi[1][0]) * R.invL[1]);
+            const float kz = rintf((a.z - B.cs_hi[2][0]) * R.invL[2]);
+            c0 = kx > 0.0f ? 1u : (kx < 0.0f ? 2u : 0u);
+            c1 = ky > 0.0f ? 1u : (ky < 0.0f ? 2u : 0u);
+            c2 = kz > 0.0f ? 1u : (kz < 0.0f ? 2u : 0u);
+        } else {
+            const uint32_t code = u >> 26;
+            c0 = code & 3u; c1 = (code >> 2) & 3u; c2 = (code >> 4) & 3u;
+        }
+        const float ax = (a.x - B.cs_hi[0][c0]) - B.cs_lo[0][c0];
+        const float ay = (a.y - B.cs_hi[1][c1]) - B.cs_lo[1][c1];
+        const float az = (a.z - B.cs_hi[2][c2]) - B.cs_lo[2][c2];
+        acc += (double)dual_atom_e<PairImage>(R, B.dsite, B.srow, ns, ax, ay, az, a.w, ta, (u >> 24) & 3u, R.lj);
+    }
+}
+
 // What the cell walk does with each buffer of included atoms: the energy
 // sink sums pair energies; the gradient kernel supplies its own sink.
 struct EnergySink {
@@ -250,6 +353,52 @@ struct EnergySink {
         acc += flush_atoms(R, B, na, ns, lane);
     }
 };
+
+// The sink of a dual item: sums the pairwise energy changes.
+struct DualSink {
+    double acc = 0.0;
+    __device__ __forceinline__ void flush(const RepDev& R, WarpBuf& B, int na, int ns, int lane) {
+        if (R.pair_image) flush_dual<true>(R, B, na, ns, lane, acc);
+        else flush_dual<false>(R, B, na, ns, lane, acc);
+    }
+};
+
+// The new centre of a dual item: its exact coordinates (for the inclusion
+// test) and the same point in the old centre's periodic frame (for the image
+// codes of the groups included for it); the item's window: per axis the first
+// cell (before wrapping) and the cell count, covering R cells around both
+// centres' cells.
+struct DualCentre {
+    float nx, ny, nz;
+    float ux, uy, uz;
+    int w0[3], ws[3];
+};
+
+// Image code of a group centre g relative to a pose centre c (2 bits per
+// axis: 0, 1 = +L, 2 = -L); sets *bad if the image lies more than one box away.
+__device__ __forceinline__ uint32_t image_code(const RepDev& R, float gx, float gy, float gz, float cx, float cy,
+                                               float cz, bool* bad) {
+    const float rx = rintf((gx - cx) * R.invL[0]);
+    const float ry = rintf((gy - cy) * R.invL[1]);
+    const float rz = rintf((gz - cz) * R.invL[2]);
+    *bad = fabsf(rx) > 1.0f || fabsf(ry) > 1.0f || fabsf(rz) > 1.0f;
+    return (rx > 0.0f ? 1u : (rx < 0.0f ? 2u : 0u)) | ((ry > 0.0f ? 1u : (ry < 0.0f ? 2u : 0u)) << 2) |
+           ((rz > 0.0f ? 1u : (rz < 0.0f ? 2u : 0u)) << 4);
+}
+
+// The window of a dual item along axis a: R cells around the cells of both
+// centres (old cell po, new cell pn), the whole axis when that reaches around.
+__device__ __forceinline__ void dual_window(const RepDev& R, int a, int po, int pn, int& w0, int& ws) {
+    const int nc = R.nc[a];
+    int dd = wrapi(pn - po, nc);
+    if (dd > nc / 2) dd -= nc;
+    ws = abs(dd) + 2 * R.range + 1;
+    w0 = po + min(dd, 0) - R.range;
+    if (ws >= nc) {
+        ws = nc;
+        w0 = 0;
+    }
+}
 
 // Expand included groups B.glist[0, ng) into atoms and evaluate them.  Each
 // lane takes one group of a batch of 32, a warp scan of the atom counts gives
@@ -327,28 +476,40 @@ __device__ __forceinline__ void process_groups(const RepDev& R, WarpBuf& B, int 
 __device__ __forceinline__ int wrap_near(int c, int n) {  // c in (-n, 2n)
     return c < 0 ? c + n : (c >= n ? c - n : c);
 }
-template <class Sink>
+//
+// Dual (dc set): a translate / rotate pose with old centre (cx, cy, cz) and new
+// centre dc; the window is dc's (around both centres' cells), every group within
+// the cutoff of either centre is listed with its inclusion flags in bits 24-25
+// of the atom start (dual_atom_e; atom ids stay below 2^24), and a group
+// included for both whose image codes relative to the two centres differ is
+// listed twice, once for each side.
+template <class Sink, bool Dual = false>
 __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                            int self, int c0, int c1, int lane, Sink& sink, int& ngroups,
                                            long long& npair, const int* stop = nullptr, int stop_at = 0,
-                                           int stride = 1) {
+                                           int stride = 1, const DualCentre* dc = nullptr) {
     set_centre(R, B, cx, cy, cz, lane);
     const int pcx = cell_coord(cx, R.start[0], R.invLc[0], R.nc[0]);
     const int pcy = cell_coord(cy, R.start[1], R.invLc[1], R.nc[1]);
     const int pcz = cell_coord(cz, R.start[2], R.invLc[2], R.nc[2]);
-    const int sxy = R.span[0] * R.span[1];
-    const float inv_s0 = 1.0f / (float)R.span[0], inv_sxy = 1.0f / (float)sxy;
+    const int sp0 = Dual ? dc->ws[0] : R.span[0], sp1 = Dual ? dc->ws[1] : R.span[1];
+    const int sp2 = Dual ? dc->ws[2] : R.span[2];
+    const int lo0 = Dual ? dc->w0[0] : pcx - R.range, lo1 = Dual ? dc->w0[1] : pcy - R.range;
+    const int lo2 = Dual ? dc->w0[2] : pcz - R.range;
+    const int sxy = sp0 * sp1;
+    const float inv_s0 = 1.0f / (float)sp0, inv_sxy = 1.0f / (float)sxy;
     const unsigned lt = (1u << lane) - 1u;
     int ng = 0;
+    long long both_atoms = 0;  // dual: atoms listed once for both poses (their pairs count twice)
     for (int base = c0; base < c1; base += 32 * stride) {  // window cells c0, c0 + stride, ... < c1
         const int j = base + lane * stride;
         int cell = 0, cnt = 0;
         if (j < c1) {
             const int jz = (int)(((float)j + 0.5f) * inv_sxy), jxy = j - jz * sxy;
-            const int jy = (int)(((float)jxy + 0.5f) * inv_s0), jx = jxy - jy * R.span[0];
-            const int x = (R.span[0] == R.nc[0]) ? jx : wrap_near(pcx - R.range + jx, R.nc[0]);
-            const int y = (R.span[1] == R.nc[1]) ? jy : wrap_near(pcy - R.range + jy, R.nc[1]);
-            const int z = (R.span[2] == R.nc[2]) ? jz : wrap_near(pcz - R.range + jz, R.nc[2]);
+            const int jy = (int)(((float)jxy + 0.5f) * inv_s0), jx = jxy - jy * sp0;
+            const int x = (sp0 == R.nc[0]) ? jx : wrap_near(lo0 + jx, R.nc[0]);
+            const int y = (sp1 == R.nc[1]) ? jy : wrap_near(lo1 + jy, R.nc[1]);
+            const int z = (sp2 == R.nc[2]) ? jz : wrap_near(lo2 + jz, R.nc[2]);
             cell = (z * R.nc[1] + y) * R.nc[0] + x;
             cnt = R.cell_count[cell];
         }
@@ -369,8 +530,8 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
                 if (__shfl_sync(kFull, v, 0) == stop_at) { c1 = base; ng = -1; break; }
             }
             const int t = t0 + lane;
-            bool inc = false;
-            uint2 packed = make_uint2(0u, 0u);
+            bool inc = false, inc2 = false;
+            uint2 packed = make_uint2(0u, 0u), packed2 = make_uint2(0u, 0u);
             if (t < total) {
                 int lo = 0, hi = 31;  // the last cell whose exclusive prefix is <= t
                 while (lo < hi) {
@@ -378,9 +539,40 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
                     if (B.cexcl[mid] <= t) lo = mid; else hi = mid - 1;
                 }
                 const CellEnt* e = R.cell_ent + B.cbase[lo] + (t - B.cexcl[lo]);
-                const float4 gc = __ldg(&e->c);
-                const int2 sp = __ldg(&e->span);
-                if (__float_as_int(gc.w) != self) {
+                // plain loads (not the read-only path) for the state: a speculative walk reads
+                // records that the accept kernel may be writing meanwhile, and the persistent
+                // step loop reads them after its own accept phase rewrote them
+                const float4 gc = e->c;
+                const int2 sp = e->span;
+                if (Dual) {
+                    if (__float_as_int(gc.w) != self) {
+                        const bool io = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff,
+                                                             R.cut2_lo, R.cut2_hi, R.fast_incl);
+                        const bool in = within_cutoff<false>(dc->nx, dc->ny, dc->nz, gc.x, gc.y, gc.z, R.L, R.invL,
+                                                             R.cutoff, R.cut2_lo, R.cut2_hi, R.fast_incl);
+                        uint32_t co = 0u, cn = 0u;
+                        bool bo = false, bn = false;
+                        if (!R.pair_image) {
+                            if (io) co = image_code(R, gc.x, gc.y, gc.z, cx, cy, cz, &bo);
+                            if (in) cn = image_code(R, gc.x, gc.y, gc.z, dc->ux, dc->uy, dc->uz, &bn);
+                        }
+                        if (bo || bn) {
+                            atomicOr(R.err, ERR_IMAGE);
+                        } else if (io || in) {
+                            // first entry: both sides if their images agree, else the old side
+                            // (or the new one alone); second: the new side of a split group
+                            const bool split = io && in && co != cn;
+                            const uint32_t fl1 = split ? 1u : ((io ? 1u : 0u) | (in ? 2u : 0u));
+                            inc = true;
+                            packed = make_uint2((uint32_t)sp.x | (fl1 << 24) | ((io ? co : cn) << 26), (uint32_t)sp.y);
+                            if (split) {
+                                inc2 = true;
+                                packed2 = make_uint2((uint32_t)sp.x | (2u << 24) | (cn << 26), (uint32_t)sp.y);
+                            }
+                            if (fl1 == 3u) both_atoms += sp.y;
+                        }
+                    }
+                } else if (__float_as_int(gc.w) != self) {
                     inc = within_cutoff<false>(cx, cy, cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
                                                R.cut2_hi, R.fast_incl);
                     if (inc) {
@@ -406,7 +598,12 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
             if (inc) B.glist[ng + __popc(m & lt)] = packed;
             ng += __popc(m);
             ngroups += __popc(m);
-            if (ng > kGCap - 32) {
+            if (Dual) {
+                const unsigned m2 = __ballot_sync(kFull, inc2);
+                if (inc2) B.glist[ng + __popc(m2 & lt)] = packed2;
+                ng += __popc(m2);
+            }
+            if (ng > kGCap - (Dual ? 64 : 32)) {
                 __syncwarp();
                 process_groups(R, B, ng, ns, lane, sink, npair);
                 ng = 0;
@@ -416,6 +613,7 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
     }
     __syncwarp();
     if (ng >= 0) process_groups(R, B, ng, ns, lane, sink, npair);  // ng < 0: stopped
+    if (Dual) npair += (long long)__reduce_add_sync(kFull, (unsigned)both_atoms) * ns;
 }
 
 __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
@@ -631,6 +829,63 @@ __device__ __forceinline__ void keep_sites(const RepDev& R, const StepDesc& D, c
         R.psite[i * kMaxSites + lane] = B.site_abs[lane];
 }
 
+// Translate / rotate pose i of step D in the difference form (one item for
+// both poses): B.dsite, B.srow and the new sites in B.site_abs (for
+// keep_sites); returns the old centre o (the group's centre, the frame of the
+// site offsets), the new one in dc (exact, and unwrapped into o's periodic
+// frame, with the window around both centres' cells) and the residue to skip.
+// The new sites are moved_site's, as in build_pose; offsets and displacements
+// are formed in FP64 from the absolute FP32 positions and rounded once.
+template <class Buf>
+__device__ __forceinline__ void build_pose_dual(const RepDev& R, const StepDesc& D, int i, Buf& B, int lane,
+                                                float& ox, float& oy, float& oz, DualCentre& dc, int& self) {
+    const FragDev& F = R.frag[D.ftype];
+    const int ns = F.nsites;
+    const int res = F.startRes + R.pslot[i];
+    self = res;
+    const int2 sp = R.gspan[res];
+    const float4 gc = R.gcen[res];
+    ox = gc.x; oy = gc.y; oz = gc.z;
+    if (D.move == MV_TRANSLATE) {
+        const float4 c = R.pcen[i];
+        dc.nx = c.x; dc.ny = c.y; dc.nz = c.z;
+    } else {
+        dc.nx = gc.x; dc.ny = gc.y; dc.nz = gc.z;
+    }
+    dc.ux = dc.nx - R.L[0] * rintf((dc.nx - ox) * R.invL[0]);
+    dc.uy = dc.ny - R.L[1] * rintf((dc.ny - oy) * R.invL[1]);
+    dc.uz = dc.nz - R.L[2] * rintf((dc.nz - oz) * R.invL[2]);
+    dual_window(R, 0, cell_coord(ox, R.start[0], R.invLc[0], R.nc[0]),
+                cell_coord(dc.nx, R.start[0], R.invLc[0], R.nc[0]), dc.w0[0], dc.ws[0]);
+    dual_window(R, 1, cell_coord(oy, R.start[1], R.invLc[1], R.nc[1]),
+                cell_coord(dc.ny, R.start[1], R.invLc[1], R.nc[1]), dc.w0[1], dc.ws[1]);
+    dual_window(R, 2, cell_coord(oz, R.start[2], R.invLc[2], R.nc[2]),
+                cell_coord(dc.nz, R.start[2], R.invLc[2], R.nc[2]), dc.w0[2], dc.ws[2]);
+    float px = 0.f, py = 0.f, pz = 0.f;
+    if (lane < ns) {
+        const float4 a = R.xyzq[sp.x + lane];
+        px = a.x; py = a.y; pz = a.z;
+        B.srow[lane] = F.stype[lane] * R.ffY;
+    }
+    const float qx = px, qy = py, qz = pz;
+    moved_site(R, D, i, gc, ns, lane, px, py, pz);
+    if (lane < ns) {
+        const double dox = (double)qx - (double)ox, doy = (double)qy - (double)oy, doz = (double)qz - (double)oz;
+        double dnx = (double)px - (double)ox, dny = (double)py - (double)oy, dnz = (double)pz - (double)oz;
+        dnx -= (double)R.L[0] * rint(dnx / (double)R.L[0]);  // a translate wrapped across the box
+        dny -= (double)R.L[1] * rint(dny / (double)R.L[1]);
+        dnz -= (double)R.L[2] * rint(dnz / (double)R.L[2]);
+        DualSite d;
+        d.nx = make_float2(-(float)dox, -(float)dnx);
+        d.ny = make_float2(-(float)doy, -(float)dny);
+        d.nz = make_float2(-(float)doz, -(float)dnz);
+        d.dk = make_float4((float)(dnx - dox), (float)(dny - doy), (float)(dnz - doz), kCoulomb * F.site[lane].w);
+        B.dsite[lane] = d;
+        B.site_abs[lane] = make_float4(px, py, pz, F.site[lane].w);
+    }
+    __syncwarp();
+}
+
 // The draws of pose i that do not depend on energies, made once per pose by
 // the pose-energy kernels (off the single-CTA accept kernel's critical path):
 // the Gumbel perturbation -ln(-ln u) and ln u of the cluster acceptance draw.
@@ -771,19 +1026,17 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // accept kernel of the step before accepted a move); mode 2 (completion,
 // nrep = 1): nothing if the speculative evaluation of this step stands (the
 // accept kernel books its pair count), else mode 0.
-template <int MinBlocks>
-__global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep,
-                                                                      int mode) {
-    __shared__ WarpBuf bufs[kWarpsE];
-    __shared__ int pre[257];
-    __shared__ int wtot[kWarpsE];
+// The items of one pose-energy launch, whole CTA: warp w of the CTA is warp
+// gw0 + w of the nwarps that share the items; B: this warp's buffer; pre,
+// wtot: 257 and 32 ints of shared memory.  The body of k_energy_t and of the
+// persistent step loop.
+__device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, int nrep, int mode, int gw0,
+                                             int nwarps, WarpBuf& B, int* pre, int* wtot) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (mode == 2 && *reps[0].valid) return;
     items_prefix(nrep, pre, wtot, [&](int r) { return reps[r].desc->items; });
     const int total = pre[nrep];
-    const bool sym = total > (int)(gridDim.x * kWarpsE);  // more items than warps: throughput-bound
-    WarpBuf& B = bufs[warp];
-    for (int it = blockIdx.x * kWarpsE + warp; it < total; it += gridDim.x * kWarpsE) {
+    const bool sym = total > nwarps;  // more items than warps: throughput-bound
+    for (int it = gw0 + warp; it < total; it += nwarps) {
         int lo = 0, hi = nrep;  // find r with pre[r] <= it < pre[r+1]
         while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
         const RepDev& R = reps[lo];
@@ -796,23 +1049,35 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         const int v = q / D.nslab, zi = q - v * D.nslab;
         float cx, cy, cz;
         int self;
-        build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
-        keep_sites(R, D, B, i, v, zi, lane);
         double acc = 0.0;
         int ng = 0;
         long long npair = 0;
-        const int nwin = R.span[0] * R.span[1] * R.span[2];
-        // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
-        // range samples the whole cutoff sphere and the ranges of a pose take equal time)
-        energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
-                     mode == 1 ? R.abort : nullptr, D.step, D.nslab);
-        if (R.pme && zi == 0) {
-            const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
-            acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
+        if (D.dual) {  // translate / rotate: the energy change of both poses in one walk
+            DualCentre dc;
+            build_pose_dual(R, D, i, B, lane, cx, cy, cz, dc, self);
+            keep_sites(R, D, B, i, 0, zi, lane);
+            const int nwin = dc.ws[0] * dc.ws[1] * dc.ws[2];
+            DualSink sink;
+            walk_cells<DualSink, true>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, sink, ng,
+                                       npair, mode == 1 ? R.abort : nullptr, D.step, D.nslab, &dc);
+            acc = sink.acc;
+        } else {
+            build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
+            keep_sites(R, D, B, i, v, zi, lane);
+            const int nwin = R.span[0] * R.span[1] * R.span[2];
+            // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
+            // range samples the whole cutoff sphere and the ranges of a pose take equal time)
+            energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
+                         mode == 1 ? R.abort : nullptr, D.step, D.nslab);
+            if (R.pme && zi == 0) {
+                const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
+                acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
+            }
         }
         acc = warp_sum(acc);
         if (lane == 0) {
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
+            if (D.dual) R.epart[(i * D.nvar + 1) * D.nslab + zi] = 0.0;  // the old variant's share
             atomicAdd(mode == 1 ? R.pairs_pending : &R.counters[2], (unsigned long long)npair);
         }
         if (v == 0 && D.nw > 0) {
@@ -822,6 +1087,16 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         }
         __syncwarp();
     }
+}
+
+template <int MinBlocks>
+__global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep,
+                                                                      int mode) {
+    __shared__ WarpBuf bufs[kWarpsE];
+    __shared__ int pre[257];
+    __shared__ int wtot[32];
+    if (mode == 2 && *reps[0].valid) return;
+    energy_items(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre, wtot);
 }
 
 template __global__ void k_energy_t<3>(const RepDev* __restrict__, int, int);

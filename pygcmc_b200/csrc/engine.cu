@@ -21,6 +21,7 @@
 
 #include "accept.cuh"
 #include "grad.cuh"
+#include "persist.cuh"
 
 using namespace gcmc;
 
@@ -34,6 +35,7 @@ thread_local int g_last_status = GCMC_OK;
 struct RepHost {
     int natoms = 0, ngroups = 0, ncell = 0, cap = 0, ntypes = 0, G = 0, ffX = 0, ffY = 0, mcsteps = 0;
     int nslab = 0, log_cap = 0, log_kmax = 0;
+    int slab_cap = 0;  // per-variant slab partials allocated per pose (>= the largest step split)
     int host_end = 0;
     std::vector<int> startRes, maxNum, moves_host;
     // allocated element count of each device buffer, keyed by the offset of its
@@ -130,6 +132,10 @@ struct gcmc_ctx {
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
     bool tiled = false;  // pose energies by k_energy_tiles (every replica allows it)
     bool pme_any = false; // some replica runs Ewald electrostatics
+    bool persist = false;   // the step loop as one cooperative launch (k_persist) instead of a graph
+    GridSync* d_sync = nullptr;
+    int grid_persist = 0;   // k_persist CTAs (one per SM)
+    long long spin_cap = kPersistSpinCap;
     int gridF = 0;       // k_energy_fb CTAs
     std::vector<int> br_off;  // branch b holds replicas [br_off[b], br_off[b+1])
     // ordering of calls that launch on a caller's stream against the context's
@@ -374,8 +380,23 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
                                         : energy_warps(ctx->device, opt.energy_variant == 1 ? 1 : 0,
                                                        opt.energy_blocks_per_sm, ctx->spec ? 1 : 0);
     h.nslab = std::max(d.span[2], d.max_split);
+    h.slab_cap = std::max(h.nslab, 2 * d.max_split);  // a dual step may split its poses twice as finely
     h.ncell = d.nc[0] * d.nc[1] * d.nc[2];
-    // tiled pose energies: blocks of B^3 cells, windows of B + 2R cells per axis
+    const bool pme_on = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
+    // translate / rotate energy changes in the pairwise-difference form (atom ids
+    // below 2^24 leave bits 24-25 of an atom entry for the inclusion flags); a
+    // translate moves the centre by at most grid_dx (reference proposals) or
+    // trn_step / 2 (symmetric) per axis, i.e. within dmargin cells
+    d.dual = (opt.pair_delta >= 0 && !pme_on && opt.proposal != 2 && I->totalAtomNum < (1 << 24)) ? 1 : 0;
+    {
+        const double shift = opt.proposal == 0 ? (double)I->grid_dx : 0.5 * (double)opt.trn_step;
+        int m = 0;
+        for (int a = 0; a < 3; ++a)
+            m = std::max(m, (int)std::ceil(shift * (1.0 + 1e-6) / ((double)I->cryst[a] / d.nc[a])));
+        d.dmargin = m;
+    }
+    // tiled pose energies: blocks of B^3 cells, windows of B + 2R cells per axis (a
+    // translate step's: B + 2 (R + dmargin))
     {
         const int B = std::max(1, opt.tile_cells > 0 ? opt.tile_cells : Rc);
         d.tblk = B;
@@ -384,13 +405,12 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
             d.nbk[a] = (d.nc[a] + B - 1) / B;
             d.tspan[a] = std::min(B + 2 * Rc, d.nc[a]);
             nblk *= d.nbk[a];
-            nwin *= d.tspan[a];
+            nwin *= std::min(B + 2 * (Rc + (d.dual ? d.dmargin : 0)), d.nc[a]);
         }
         int maxga = 0;
         for (int g = 0; g < in.fragmentInfo[0].startRes; ++g) maxga = std::max(maxga, in.residueInfo[g].atomNum);
         for (int t = 0; t < I->fragTypeNum; ++t) maxga = std::max(maxga, in.fragmentInfo[t].num_atoms);
-        const bool pme_on = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
-        d.tiled = (opt.energy_kernel >= 0 && !pme_on && opt.proposal != 2 && nblk <= kMaxBlocks &&
+        d.tiled = (opt.energy_kernel > 0 && !pme_on && opt.proposal != 2 && nblk <= kMaxBlocks &&
                    nwin <= kTileCells && maxga <= kTileMaxGroupAtoms) ? 1 : 0;
     }
     d.cutoff = I->cutoff;
@@ -505,15 +525,15 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.cell_count, h.ncell); AL(h.cell_ent, (size_t)h.ncell * cap); AL(h.gcell, h.ngroups);
     AL(h.grid, h.G); AL(h.lj, lj.size()); AL(h.moves, h.mcsteps); AL(h.frag, h.ntypes);
     AL(h.totalNum, h.ntypes); AL(h.desc, 1); AL(h.pcen, kMaxPoses); AL(h.pslot, kMaxPoses);
-    AL(h.epart, (size_t)kMaxPoses * 2 * h.nslab); AL(h.nbr, (size_t)kMaxPoses * kMaxWords);
+    AL(h.epart, (size_t)kMaxPoses * 2 * h.slab_cap); AL(h.nbr, (size_t)kMaxPoses * kMaxWords);
     AL(h.counters, 16); AL(h.err, 1);
-    AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.nslab * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
+    AL(h.energy, 1); AL(h.fpart, (size_t)kMaxPoses * 2 * h.slab_cap * 6); AL(h.fbprop, (size_t)kMaxPoses * 2);
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
     AL(h.pbin, 2 * kMaxPoses); AL(h.tiles, 2 * kMaxPoses);
     AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
     if (ctx->spec) {
-        AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.nslab);
+        AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.slab_cap);
         AL(h.nbr2, (size_t)kMaxPoses * kMaxWords); AL(h.pgum2, kMaxPoses); AL(h.plnu2, kMaxPoses);
         AL(h.psite2, (size_t)kMaxPoses * kMaxSites); AL(h.valid2, 2); AL(h.abort2, 2); AL(h.sstep2, 2);
         AL(h.pending2, 2); AL(h.pbin2, 2 * kMaxPoses); AL(h.tiles2, 2 * kMaxPoses);
@@ -604,9 +624,9 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     CK(cudaMemcpyAsync(h.desc, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 16, s));
     CK(cudaMemsetAsync(h.err, 0, sizeof(int), s));
-    CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
+    CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.slab_cap, s));
     CK(cudaMemsetAsync(h.energy, 0, sizeof(double), s));
-    CK(cudaMemsetAsync(h.fpart, 0, sizeof(float) * kMaxPoses * 2 * h.nslab * 6, s));
+    CK(cudaMemsetAsync(h.fpart, 0, sizeof(float) * kMaxPoses * 2 * h.slab_cap * 6, s));
     CK(cudaMemsetAsync(h.fbprop, 0, sizeof(float4) * kMaxPoses * 2, s));
     CK(cudaMemsetAsync(h.fbcnt, 0, sizeof(int) * kMaxPoses, s));
     if (ctx->spec) {
@@ -614,7 +634,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         // every record slot then holds a span of real atoms (or none)
         CK(cudaMemsetAsync(h.cell_ent, 0, sizeof(CellEnt) * (size_t)h.ncell * cap, s));
         CK(cudaMemcpyAsync(h.desc2, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(h.epart2, 0, sizeof(double) * kMaxPoses * 2 * h.nslab, s));
+        CK(cudaMemsetAsync(h.epart2, 0, sizeof(double) * kMaxPoses * 2 * h.slab_cap, s));
         CK(cudaMemsetAsync(h.valid2, 0, sizeof(int) * 2, s));
         CK(cudaMemsetAsync(h.abort2, 0xff, sizeof(int) * 2, s));  // -1: no step voided
         CK(cudaMemsetAsync(h.sstep2, 0, sizeof(int) * 2, s));
@@ -931,10 +951,32 @@ int destroy_impl(gcmc_ctx* ctx) {
     for (auto& h : ctx->reps) free_rep(h);
     if (ctx->d_reps) cudaFree(ctx->d_reps);
     if (ctx->d_reps_b) cudaFree(ctx->d_reps_b);
+    if (ctx->d_sync) cudaFree(ctx->d_sync);
     if (ctx->ev_ctx) cudaEventDestroy(ctx->ev_ctx);
     if (ctx->ev_call) cudaEventDestroy(ctx->ev_call);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+    return GCMC_OK;
+}
+
+// The persistent step loop where it was asked for and the context allows it:
+// no speculation (one-replica contexts speculate instead), no PME (its mesh
+// update runs cuFFT between steps), proposal 0 or 1, the per-pose-warp
+// pose-energy kernel, and one k_persist CTA resident on every SM.
+int setup_persist(gcmc_ctx* ctx, const gcmc_options& opt) {
+    ctx->persist = false;
+    ctx->spin_cap = opt.persist_spin_cap > 0 ? (long long)opt.persist_spin_cap : kPersistSpinCap;
+    if (opt.persistent <= 0 || ctx->spec || ctx->pme_any || ctx->fb || ctx->tiled) return GCMC_OK;
+    int sms = 0, per_sm = 0, coop = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+    if (!coop) return GCMC_OK;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AcceptSmem)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist, kAcceptThreads, sizeof(AcceptSmem)));
+    if (per_sm < 1) return GCMC_OK;
+    if (!ctx->d_sync) CK(cudaMalloc(&ctx->d_sync, sizeof(GridSync)));
+    ctx->grid_persist = sms;
+    ctx->persist = true;
     return GCMC_OK;
 }
 
@@ -994,7 +1036,8 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
         if (cudaGetLastError() != cudaSuccess) st = GCMC_ERR_CUDA;
     }
     if (st == GCMC_OK) st = pme_init_fixed(ctx);
-    if (st == GCMC_OK) st = build_graph(ctx);
+    if (st == GCMC_OK) st = setup_persist(ctx, opt);
+    if (st == GCMC_OK && !ctx->persist) st = build_graph(ctx);
     if (st == GCMC_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) {
         int32_t err = 0;
@@ -1039,15 +1082,23 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const int nb = std::max(1, std::min(opt.branches > 0 ? opt.branches : 1, nrep));
     const int fb = opt.proposal == 2 ? 1 : 0;
     const int evar = opt.energy_variant == 1 ? 1 : 0;
-    if (spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps || fb != ctx->fb ||
-        evar != ctx->evar || ctx->tiled != tiled_before || ctx->pme_any != pme_before) {
-        ctx->fb = fb;
-        ctx->evar = evar;
+    const bool persist_before = ctx->persist;
+    const bool had_graph = ctx->gexec || ctx->gexec_spec[0];
+    const bool shape_changed = spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps ||
+                               fb != ctx->fb || evar != ctx->evar || ctx->tiled != tiled_before ||
+                               ctx->pme_any != pme_before;
+    ctx->fb = fb;
+    ctx->evar = evar;
+    st = setup_persist(ctx, opt);
+    if (st != GCMC_OK) return st;
+    if (shape_changed || ctx->persist != persist_before) {
         st = set_energy_grid(ctx, opt.energy_blocks_per_sm);
         if (st != GCMC_OK) return st;
         split_branches(ctx, nb);
-        st = build_graph(ctx);
-        if (st != GCMC_OK) return st;
+        if (!ctx->persist && (shape_changed || !had_graph)) {
+            st = build_graph(ctx);
+            if (st != GCMC_OK) return st;
+        }
     }
     CK(cudaStreamSynchronize(ctx->stream));
     int32_t err = 0;
@@ -1303,7 +1354,8 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         if (st != GCMC_OK) return st;
         if (trials && n < max_trials)
             trials[n] = gcmc_tune_trial{o.cells_per_cutoff, o.split_items,   o.branches,     o.energy_blocks_per_sm,
-                                        o.energy_variant,   ms,              o.energy_kernel, o.tile_cells};
+                                        o.energy_variant,   ms,              o.energy_kernel, o.tile_cells,
+                                        o.persistent};
         ++n;
         if (ms < best_ms) {
             best_ms = ms;
@@ -1312,15 +1364,22 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         return GCMC_OK;
     };
     int st = GCMC_OK;
-    // coordinate descent: cell grid; the tiled kernel's pose-block edge; the
-    // per-pose-warp kernel (and, if it wins, its work split, register budget and
-    // CTAs per SM); then graph branches
-    for (int R : {1, 2, 3}) {
-        gcmc_options o = cur;
-        o.cells_per_cutoff = R;
-        if (st == GCMC_OK) st = consider(o);
+    // coordinate descent: pose-energy kernel x cell grid; then the tiled kernel's
+    // pose-block edge, or the per-pose-warp kernel's work split, register budget
+    // and CTAs per SM, whichever kernel won; then graph branches; then (several
+    // replicas) the persistent step loop in place of the graph
+    {
+        const gcmc_options base0 = cur;
+        for (int kern : {0, 1})
+            for (int R : {1, 2, 3}) {
+                gcmc_options o = base0;
+                o.energy_kernel = kern;
+                o.cells_per_cutoff = R;
+                o.tile_cells = 0;
+                if (st == GCMC_OK) st = consider(o);
+            }
     }
-    if (cur.energy_kernel >= 0) {
+    if (cur.energy_kernel > 0) {
         const int base_b = cur.tile_cells > 0 ? cur.tile_cells : cur.cells_per_cutoff;
         for (int B : {1, 2, 3}) {
             if (B == base_b) continue;
@@ -1328,11 +1387,7 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
             o.tile_cells = B;
             if (st == GCMC_OK) st = consider(o);
         }
-        gcmc_options o = cur;
-        o.energy_kernel = -1;
-        if (st == GCMC_OK) st = consider(o);
-    }
-    if (cur.energy_kernel < 0) {
+    } else {
         const int base_split = cur.split_items;
         for (int sp : {512, 1024, 2048, 4096, 8192}) {
             if (sp == base_split) continue;
@@ -1358,6 +1413,13 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
         if (nb == base_br || nb > nrep) continue;
         gcmc_options o = cur;
         o.branches = nb;
+        if (st == GCMC_OK) st = consider(o);
+    }
+    // several replicas with the per-pose-warp kernel: the persistent step loop
+    if (nrep > 1 && cur.energy_kernel == 0 && cur.persistent <= 0) {
+        gcmc_options o = cur;
+        o.persistent = 1;
+        o.branches = 1;
         if (st == GCMC_OK) st = consider(o);
     }
     if (ntrials) *ntrials = n;
@@ -1390,6 +1452,17 @@ int gcmc_run(gcmc_ctx* ctx, int32_t nsteps) {
     }
     k_prepare<<<ctx->nrep, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(ctx->d_reps, ctx->nrep);
     CK(cudaGetLastError());
+    if (ctx->persist) {  // the whole step range in one cooperative launch
+        CK(cudaMemsetAsync(ctx->d_sync, 0, sizeof(GridSync), ctx->stream));
+        const RepDev* reps = ctx->d_reps;
+        int nrep = ctx->nrep, nst = need;
+        GridSync* gs = ctx->d_sync;
+        long long cap = ctx->spin_cap;
+        void* args[] = {(void*)&reps, (void*)&nrep, (void*)&nst, (void*)&gs, (void*)&cap};
+        CK(cudaLaunchCooperativeKernel((const void*)k_persist, dim3(ctx->grid_persist), dim3(kAcceptThreads), args,
+                                       sizeof(AcceptSmem), ctx->stream));
+        return GCMC_OK;
+    }
     for (int done = 0; done < need; done += kGraphSteps) CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     return GCMC_OK;
 }

@@ -2,15 +2,18 @@
 // of a step's trial poses, organised around the environment they share.
 //
 // The step's pose entries (pose i, variant v: the new pose, and for a
-// translate / rotate also the old one) are binned by the preparation kernel
-// (bin_entries) into pose blocks of B x B x B cells of the cell grid, and each
-// block into work items ("tiles") of at most kTilePoses entries.  One CTA per
-// tile:
+// translate / rotate also the old one; a translate / rotate step in the
+// pairwise-difference form has one entry per pose for both) are binned by the
+// preparation kernel (bin_entries) into pose blocks of B x B x B cells of the
+// cell grid, and each block into work items ("tiles") of at most kTilePoses
+// entries.  One CTA per tile:
 //   1. builds the tile's poses (one warp each; insertion poses from the RNG,
 //      moved poses from the slot's atoms), keeping new-variant sites for the
 //      accept kernel;
-//   2. stages the block's window -- the cells within R cells of the block,
-//      which hold every group within the cutoff of any pose in it -- into
+//   2. stages the block's window -- the cells within R cells of the block
+//      (R + margin for a translate step, whose new centres lie within margin
+//      cells of the old ones), which hold every group within the cutoff of any
+//      pose in it -- into
 //      shared memory: the window's cell counts, the cells' records (group
 //      centre, id, atom range) and then the groups' atoms (x, y, z, charge,
 //      type), coalesced, once for all the tile's poses (windows larger than the
@@ -20,13 +23,15 @@
 //      fixed split given the pose count), testing every staged centre with the
 //      bit-exact FP32 inclusion distance, compacting the included groups
 //      (ballot) and their atoms, and evaluating atom x site pairs with the
-//      packed FP32 arithmetic of flush_atoms_packed (atoms and the pair table
-//      read from shared memory);
+//      packed FP32 arithmetic of flush_atoms_packed, or of dual_atom_e for a
+//      pose pair in the difference form (atoms and the pair table read from
+//      shared memory);
 //   4. sums each pose's per-warp FP64 partials in warp order into epart (one
 //      entry per pose variant) and, for clustering moves, fills the tile's
 //      poses' rows of the pose-pose bit matrix and the per-pose draws.
-// Energies depend only on the state and the tile's pose count (the staging
-// order is the cells' sorted order), so the speculative and the sequential
+// Energies depend only on the state and the entry count of the pose's block
+// (the staging order is the cells' sorted order, and every tile of a block
+// splits its poses' groups alike), so the speculative and the sequential
 // evaluation of a step are bit-identical.
 #pragma once
 #include "energy.cuh"
@@ -39,7 +44,7 @@ constexpr int kTileAtoms = 5120;  // atoms staged per round
 constexpr int kTileGroups = 1024; // group records staged per round
 constexpr int kTileCells = 1024;  // window cells at most
 constexpr int kTileLJ = 2048;     // pair-table entries kept in shared memory (larger tables: global)
-constexpr int kTileGList = 64;    // per-warp included-group buffer
+constexpr int kTileGList = 128;   // per-warp included-group buffer
 constexpr int kTileAList = 256;   // per-warp included-atom buffer
 constexpr int kTileMaxGroupAtoms = kTileAtoms / 4;  // groups larger than this are not tiled
 constexpr int kMaxBlocks = 4096;  // pose blocks per replica at most
@@ -49,10 +54,13 @@ struct PoseBuf {
     float4 site[kMaxSites];  // x, y, z relative to the pose centre, Coulomb constant * charge
     int srow[kMaxSites];     // template type * ffY
     SitePair spair[kMaxSites / 2];
+    DualSite dsite[kMaxSites];  // dual entries: both poses' sites in the difference form
     float cs_hi[3][4];       // pose centre + image shift, high part and TwoSum error
     float cs_lo[3][4];
     float4 site_abs[kMaxSites];
-    float cx, cy, cz;
+    float cx, cy, cz;        // pose centre (dual: the old one)
+    float nx, ny, nz;        // dual: the new centre, exact
+    float ux, uy, uz;        //   and in the old centre's periodic frame
     int self;
 };
 
@@ -136,8 +144,9 @@ __device__ int bin_entries(const RepDev& R, const StepDesc& D, int* scratch, int
         myb[q] = -1;
         if (e < ne && q * nt < 2 * kMaxPoses) {
             const int i = e / D.nvar, v = e - i * D.nvar;
+            if (D.dual && v == 1) continue;  // dual: one entry per pose (v = 0), binned by its old centre
             float4 c;
-            if (D.move == MV_INSERT || D.move == MV_DELETE || v == 0) c = R.pcen[i];
+            if (D.move == MV_INSERT || D.move == MV_DELETE || (v == 0 && !D.dual)) c = R.pcen[i];
             else c = R.gcen[startRes + R.pslot[i]];  // old pose of a translate / rotate
             myb[q] = pose_block(R, c.x, c.y, c.z);
             myr[q] = atomicAdd(&cnt[myb[q]], 1);
@@ -147,16 +156,22 @@ __device__ int bin_entries(const RepDev& R, const StepDesc& D, int* scratch, int
     for (int b = tid; b < nblk; b += nt) chunks[b] = (cnt[b] + kTilePoses - 1) / kTilePoses;
     __syncthreads();
     // entries by block: cnt becomes each block's first entry
-    block_excl_scan(cnt, nblk, wtot);
+    const int nbinned = block_excl_scan(cnt, nblk, wtot);
     const int ntiles = block_excl_scan(chunks, nblk, wtot);
 #pragma unroll
     for (int q = 0; q < kPer; ++q)
         if (myb[q] >= 0) R.pbin[cnt[myb[q]] + myr[q]] = tid + q * nt;
+    // a block of c entries becomes ceil(c / kTilePoses) tiles of near-equal size, all
+    // evaluated with the warp split of the largest (w = its entry count): a pose's
+    // energy then depends on its block's entry count only, not on which tile the
+    // atomic ranks above put it in
     for (int b = tid; b < nblk; b += nt) {
-        const int first = cnt[b], end = (b + 1 < nblk) ? cnt[b + 1] : ne;
-        int t = chunks[b];
-        for (int f = first; f < end; f += kTilePoses, ++t)
-            R.tiles[t] = make_int4(b, f, min(kTilePoses, end - f), 0);
+        const int first = cnt[b], end = (b + 1 < nblk) ? cnt[b + 1] : nbinned, c = end - first;
+        if (c == 0) continue;
+        const int nt_b = (c + kTilePoses - 1) / kTilePoses, base = c / nt_b, extra = c - base * nt_b;
+        const int pmax = base + (extra > 0 ? 1 : 0);
+        for (int j = 0; j < nt_b; ++j)
+            R.tiles[chunks[b] + j] = make_int4(b, first + j * base + min(j, extra), base + (j < extra ? 1 : 0), pmax);
     }
     __syncthreads();
     return ntiles;
@@ -240,9 +255,47 @@ __device__ __forceinline__ void flush_staged(const RepDev& R, const TileSmem& T,
     }
 }
 
+// Energy changes of the staged atoms in alist[0, na) with the dual pose P
+// (atoms: staged index in bits 0-23, inclusion flags in bits 24-25, image
+// code in bits 26-31).
+template <bool PairImage>
+__device__ __forceinline__ void flush_staged_dual(const RepDev& R, const TileSmem& T, const PoseBuf& P,
+                                                  const uint32_t* alist, int na, int ns, int lane, const float2* lj,
+                                                  double& acc) {
+    for (int f = lane; f < na; f += 32) {
+        const uint32_t u = alist[f];
+        const int idx = (int)(u & 0xFFFFFFu);
+        const float4 a = T.atom[idx];
+        const int ta = T.atype[idx];
+        uint32_t c0, c1, c2;
+        if (PairImage) {
+            const float kx = rintf((a.x - P.cs_hi[0][0]) * R.invL[0]);
+            const float ky = rintf((a.y - P.cs_hi[1][0]) * R.invL[1]);
+            const float kz = rintf((a.z - P.cs_hi[2][0]) * R.invL[2]);
+            c0 = kx > 0.0f ? 1u : (kx < 0.0f ? 2u : 0u);
+            c1 = ky > 0.0f ? 1u : (ky < 0.0f ? 2u : 0u);
+            c2 = kz > 0.0f ? 1u : (kz < 0.0f ? 2u : 0u);
+        } else {
+            const uint32_t code = u >> 26;
+            c0 = code & 3u; c1 = (code >> 2) & 3u; c2 = (code >> 4) & 3u;
+        }
+        const float ax = (a.x - P.cs_hi[0][c0]) - P.cs_lo[0][c0];
+        const float ay = (a.y - P.cs_hi[1][c1]) - P.cs_lo[1][c1];
+        const float az = (a.z - P.cs_hi[2][c2]) - P.cs_lo[2][c2];
+        acc += (double)dual_atom_e<PairImage>(R, P.dsite, P.srow, ns, ax, ay, az, a.w, ta, (u >> 24) & 3u, lj);
+    }
+}
+
 // Expand the included groups glist[0, ng) into staged-atom entries and
 // evaluate them (warp-collective; the staged form of process_groups).
-template <bool PairImage>
+template <bool PairImage, bool Dual>
+__device__ __forceinline__ void flush_any(const RepDev& R, const TileSmem& T, const PoseBuf& P, const uint32_t* alist,
+                                          int na, int ns, int lane, const float2* lj, double& acc) {
+    if (Dual) flush_staged_dual<PairImage>(R, T, P, alist, na, ns, lane, lj, acc);
+    else flush_staged<PairImage>(R, T, P, alist, na, ns, lane, lj, acc);
+}
+
+template <bool PairImage, bool Dual>
 __device__ __forceinline__ void process_staged(const RepDev& R, TileSmem& T, const PoseBuf& P, int warp, int ng,
                                                int ns, int lane, const float2* lj, double& acc, long long& npair) {
     uint32_t* alist = T.alist[warp];
@@ -270,7 +323,7 @@ __device__ __forceinline__ void process_staged(const RepDev& R, TileSmem& T, con
         if (maxcnt <= kTileAList / 2) {
             if (na + total > kTileAList) {
                 __syncwarp();
-                flush_staged<PairImage>(R, T, P, alist, na, ns, lane, lj, acc);
+                flush_any<PairImage, Dual>(R, T, P, alist, na, ns, lane, lj, acc);
                 __syncwarp();
                 na = 0;
             }
@@ -289,7 +342,7 @@ __device__ __forceinline__ void process_staged(const RepDev& R, TileSmem& T, con
                 const int take = min(c0 - done, kTileAList - na);
                 if (take == 0) {
                     __syncwarp();
-                    flush_staged<PairImage>(R, T, P, alist, na, ns, lane, lj, acc);
+                    flush_any<PairImage, Dual>(R, T, P, alist, na, ns, lane, lj, acc);
                     __syncwarp();
                     na = 0;
                     continue;
@@ -301,22 +354,53 @@ __device__ __forceinline__ void process_staged(const RepDev& R, TileSmem& T, con
         }
     }
     __syncwarp();
-    flush_staged<PairImage>(R, T, P, alist, na, ns, lane, lj, acc);
+    flush_any<PairImage, Dual>(R, T, P, alist, na, ns, lane, lj, acc);
     __syncwarp();
 }
 
-// Pose P against the staged groups [g0, g1) (warp-collective).
-template <bool PairImage>
+// Pose P against the staged groups [g0, g1) (warp-collective).  Dual: every
+// group within the cutoff of either centre, with its inclusion flags, listed
+// as in walk_cells.
+template <bool PairImage, bool Dual>
 __device__ __forceinline__ void eval_staged(const RepDev& R, TileSmem& T, const PoseBuf& P, int warp, int g0, int g1,
                                             int ns, int lane, const float2* lj, double& acc, long long& npair) {
     uint2* glist = T.glist[warp];
     const unsigned lt = (1u << lane) - 1u;
     int ng = 0;
+    long long both_atoms = 0;
     for (int base = g0; base < g1; base += 32) {
         const int gi = base + lane;
-        bool inc = false;
-        uint2 packed = make_uint2(0u, 0u);
-        if (gi < g1) {
+        bool inc = false, inc2 = false;
+        uint2 packed = make_uint2(0u, 0u), packed2 = make_uint2(0u, 0u);
+        if (Dual && gi < g1) {
+            const float4 gc = T.gc[gi];
+            if (__float_as_int(gc.w) != P.self) {
+                const bool io = within_cutoff<false>(P.cx, P.cy, P.cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff,
+                                                     R.cut2_lo, R.cut2_hi, R.fast_incl);
+                const bool in = within_cutoff<false>(P.nx, P.ny, P.nz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff,
+                                                     R.cut2_lo, R.cut2_hi, R.fast_incl);
+                uint32_t co = 0u, cn = 0u;
+                bool bo = false, bn = false;
+                if (!PairImage) {
+                    if (io) co = image_code(R, gc.x, gc.y, gc.z, P.cx, P.cy, P.cz, &bo);
+                    if (in) cn = image_code(R, gc.x, gc.y, gc.z, P.ux, P.uy, P.uz, &bn);
+                }
+                if (bo || bn) {
+                    atomicOr(R.err, ERR_IMAGE);
+                } else if (io || in) {
+                    const int2 sg = T.gs[gi];
+                    const bool split = io && in && co != cn;
+                    const uint32_t fl1 = split ? 1u : ((io ? 1u : 0u) | (in ? 2u : 0u));
+                    inc = true;
+                    packed = make_uint2((uint32_t)sg.x | (fl1 << 24) | ((io ? co : cn) << 26), (uint32_t)sg.y);
+                    if (split) {
+                        inc2 = true;
+                        packed2 = make_uint2((uint32_t)sg.x | (2u << 24) | (cn << 26), (uint32_t)sg.y);
+                    }
+                    if (fl1 == 3u) both_atoms += sg.y;
+                }
+            }
+        } else if (gi < g1) {
             const float4 gc = T.gc[gi];
             if (__float_as_int(gc.w) != P.self) {
                 inc = within_cutoff<false>(P.cx, P.cy, P.cz, gc.x, gc.y, gc.z, R.L, R.invL, R.cutoff, R.cut2_lo,
@@ -344,14 +428,20 @@ __device__ __forceinline__ void eval_staged(const RepDev& R, TileSmem& T, const 
         const unsigned m = __ballot_sync(kFull, inc);
         if (inc) glist[ng + __popc(m & lt)] = packed;
         ng += __popc(m);
-        if (ng > kTileGList - 32) {
+        if (Dual) {
+            const unsigned m2 = __ballot_sync(kFull, inc2);
+            if (inc2) glist[ng + __popc(m2 & lt)] = packed2;
+            ng += __popc(m2);
+        }
+        if (ng > kTileGList - (Dual ? 64 : 32)) {
             __syncwarp();
-            process_staged<PairImage>(R, T, P, warp, ng, ns, lane, lj, acc, npair);
+            process_staged<PairImage, Dual>(R, T, P, warp, ng, ns, lane, lj, acc, npair);
             ng = 0;
         }
     }
     __syncwarp();
-    process_staged<PairImage>(R, T, P, warp, ng, ns, lane, lj, acc, npair);
+    process_staged<PairImage, Dual>(R, T, P, warp, ng, ns, lane, lj, acc, npair);
+    if (Dual) npair += (long long)__reduce_add_sync(kFull, (unsigned)both_atoms) * ns;
 }
 
 // A speculative evaluation that has become void (the accept kernel of the step
@@ -372,17 +462,19 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
     const int4 tile = R.tiles[li];
     const int b = tile.x, P = tile.z;
     if (tid < P) T.entry[tid] = R.pbin[tile.y + tid];
-    // window cells: the block's cells and R cells around them
+    // window cells: the block's cells and R (+ margin) cells around them
     const int nb01 = R.nbk[0] * R.nbk[1];
     const int bz = b / nb01, bxy = b - bz * nb01, by = bxy / R.nbk[0], bx = bxy - by * R.nbk[0];
-    const int o[3] = {bx * R.tblk - R.range, by * R.tblk - R.range, bz * R.tblk - R.range};
-    const int W0 = R.tspan[0], W1 = R.tspan[1], W01 = W0 * W1;
-    const int nwin = W01 * R.tspan[2];
+    const int reach = R.range + D.margin;
+    const int o[3] = {bx * R.tblk - reach, by * R.tblk - reach, bz * R.tblk - reach};
+    const int W0 = min(R.tblk + 2 * reach, R.nc[0]), W1 = min(R.tblk + 2 * reach, R.nc[1]);
+    const int W2 = min(R.tblk + 2 * reach, R.nc[2]), W01 = W0 * W1;
+    const int nwin = W01 * W2;
     for (int t = tid; t < nwin; t += nt) {
         const int jz = t / W01, jxy = t - jz * W01, jy = jxy / W0, jx = jxy - jy * W0;
         const int x = (W0 == R.nc[0]) ? jx : wrapi(o[0] + jx, R.nc[0]);
         const int y = (W1 == R.nc[1]) ? jy : wrapi(o[1] + jy, R.nc[1]);
-        const int z = (R.tspan[2] == R.nc[2]) ? jz : wrapi(o[2] + jz, R.nc[2]);
+        const int z = (W2 == R.nc[2]) ? jz : wrapi(o[2] + jz, R.nc[2]);
         const int cell = (z * R.nc[1] + y) * R.nc[0] + x;
         T.cell[t] = cell;
         T.cpre[t] = min(R.cell_count[cell], R.cap);
@@ -400,7 +492,16 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
         PoseBuf& Pb = T.pose[p];
         float cx, cy, cz;
         int self;
-        build_pose(R, D, i, v, Pb, lane, cx, cy, cz, self);
+        if (D.dual) {
+            DualCentre dc;
+            build_pose_dual(R, D, i, Pb, lane, cx, cy, cz, dc, self);
+            if (lane == 0) {
+                Pb.nx = dc.nx; Pb.ny = dc.ny; Pb.nz = dc.nz;
+                Pb.ux = dc.ux; Pb.uy = dc.uy; Pb.uz = dc.uz;
+            }
+        } else {
+            build_pose(R, D, i, v, Pb, lane, cx, cy, cz, self);
+        }
         keep_sites(R, D, Pb, i, v, 0, lane);
         set_centre(R, Pb, cx, cy, cz, lane);
         if (lane == 0) {
@@ -412,8 +513,9 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
     }
     const int nrec = block_excl_scan(T.cpre, nwin, T.wtot);
     if (tid == 0) T.cpre[nwin] = nrec;
-    // warp w evaluates pose w / S over part w % S of each round's groups
-    const int S = max(1, kWarpsT / max(1, P));
+    // warp w evaluates pose w / S over part w % S of each round's groups; S follows the
+    // block's largest tile (tile.w), so every tile of a block splits its poses alike
+    const int S = max(1, kWarpsT / max(1, tile.w));
     const int mp = warp / S, mj = warp - mp * S;
     const bool active = mp < P;
     double acc = 0.0;
@@ -465,8 +567,8 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
         __syncthreads();
         if (active) {
             const int g0 = mj * nfit / S, g1 = (mj + 1) * nfit / S;
-            if (PairImage) eval_staged<true>(R, T, T.pose[mp], warp, g0, g1, ns, lane, lj, acc, npair);
-            else eval_staged<false>(R, T, T.pose[mp], warp, g0, g1, ns, lane, lj, acc, npair);
+            if (D.dual) eval_staged<PairImage, true>(R, T, T.pose[mp], warp, g0, g1, ns, lane, lj, acc, npair);
+            else eval_staged<PairImage, false>(R, T, T.pose[mp], warp, g0, g1, ns, lane, lj, acc, npair);
         }
         r0 += nfit;
         if (tile_voided(R, D, mode, T)) return;
@@ -483,6 +585,7 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
         double e = 0.0;
         for (int j = 0; j < S; ++j) e += T.part[tid][j];
         R.epart[T.entry[tid]] = e;
+        if (D.dual) R.epart[T.entry[tid] + 1] = 0.0;  // the old variant's share of the change
     }
     if (tid == 0) {
         long long np = 0;

@@ -26,7 +26,7 @@ def autotune(systems, options: Options = None, trial_steps: int = 64):
     short runs on temporary contexts (gcmc_autotune).  Returns the options to
     create the :class:`Engine` with and the list of trials
     ``(cells_per_cutoff, split_items, branches, energy_blocks_per_sm, energy_variant, ms_per_step,
-    energy_kernel, tile_cells)``."""
+    energy_kernel, tile_cells, persistent)``."""
     if not isinstance(systems, (list, tuple)):
         systems = [systems]
     base = options if options is not None else default_options()
@@ -37,7 +37,7 @@ def autotune(systems, options: Options = None, trial_steps: int = 64):
     check(lib().gcmc_autotune(len(systems), arr, ctypes.byref(base), int(trial_steps), ctypes.byref(best), trials,
                               32, ctypes.byref(n)), "gcmc_autotune")
     out = [(t.cells_per_cutoff, t.split_items, t.branches, t.energy_blocks_per_sm, t.energy_variant,
-            float(t.ms_per_step), t.energy_kernel, t.tile_cells) for t in trials[: min(n.value, 32)]]
+            float(t.ms_per_step), t.energy_kernel, t.tile_cells, t.persistent) for t in trials[: min(n.value, 32)]]
     return best, out
 
 

@@ -95,28 +95,35 @@ def run_logged(systems, nsteps, **opt):
     return out
 
 
-def test_benchmark_protein_system(oracle_lib):
+# both pose-energy kernels: one warp per pose and cell range (0) and tiled (1)
+KERNELS = pytest.mark.parametrize("kernel", [0, 1], ids=["per_pose", "tiled"])
+
+
+@KERNELS
+def test_benchmark_protein_system(oracle_lib, kernel):
     """The bench's workload exactly: protein_system(seed=1), 6000 fixed atoms, confBias 1000."""
     from pygcmc_b200 import system as S
     n = 256
     s = S.protein_system(seed=1, mcsteps=n)
     assert int(s.meta["n_fixed"]) == 6000 and int(s.fragmentInfo[0]["confBias"]) == 1000
-    (logs, E, final), = run_logged([s], n)
+    (logs, E, final), = run_logged([s], n, energy_kernel=kernel)
     assert set(np.unique(logs["move"])) == {0, 1, 2, 3}
     assert (logs["n_accept"] > 0).any()
-    check_replay(oracle_lib, s, logs, E, final, n, oracle_lib.options(), "protein 6000, confBias 1000")
+    check_replay(oracle_lib, s, logs, E, final, n, oracle_lib.options(), f"protein 6000, confBias 1000, kernel {kernel}")
 
 
-def test_water_box_symmetric_moves(oracle_lib):
+@KERNELS
+def test_water_box_symmetric_moves(oracle_lib, kernel):
     """800 TIP3P waters, 30 A box, muex -5.8 kcal/mol, 55 M, translate in a 1 A cube, rotate <= 15 degrees."""
     from pygcmc_b200 import system as S
     n = 256
     s = S.water_box(n_water=800, box=30.0, seed=1, mcsteps=n)
     rot = float(np.radians(15.0))
-    (logs, E, final), = run_logged([s], n, proposal=1, muex_kcal=1, trn_step=1.0, rot_max=rot)
+    (logs, E, final), = run_logged([s], n, proposal=1, muex_kcal=1, trn_step=1.0, rot_max=rot, energy_kernel=kernel)
     assert set(np.unique(logs["move"])) == {0, 1, 2, 3}
     check_replay(oracle_lib, s, logs, E, final, n,
-                 oracle_lib.options(proposal=1, muex_kcal=1, trn_step=1.0, rot_max=rot), "water 800, 30 A")
+                 oracle_lib.options(proposal=1, muex_kcal=1, trn_step=1.0, rot_max=rot),
+                 f"water 800, 30 A, kernel {kernel}")
 
 
 def test_batched_replica_size_extremes(oracle_lib):

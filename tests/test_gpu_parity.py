@@ -361,16 +361,21 @@ def test_pair_counter_equals_oracle_pairs(oracle_lib, protein_small):
     assert checked >= 1
 
 
-@pytest.mark.parametrize("kernel,tile_cells,cells", [(-1, 0, 2), (0, 1, 2), (0, 3, 2), (0, 0, 1), (0, 0, 3)])
-def test_trajectory_pose_energy_kernels(oracle_lib, protein_small, kernel, tile_cells, cells):
+@pytest.mark.parametrize("kernel,tile_cells,cells,pair_delta", [(0, 0, 2, 0), (1, 1, 2, 0), (1, 3, 2, 0), (1, 0, 1, 0),
+                                                                (1, 0, 3, 0), (0, 0, 2, -1), (1, 0, 2, -1)])
+def test_trajectory_pose_energy_kernels(oracle_lib, protein_small, kernel, tile_cells, cells, pair_delta):
     """Every pose-energy kernel and launch shape replays on the oracle: the
-    per-pose-warp kernel (energy_kernel -1) and the tiled kernel with pose
-    blocks of 1 and 3 cells and cell grids of 1 and 3 cells per cutoff."""
+    per-pose-warp kernel (energy_kernel 0) and the tiled kernel (1) with pose
+    blocks of 1 and 3 cells and cell grids of 1 and 3 cells per cutoff;
+    translate / rotate changes in the pairwise-difference form (pair_delta 0)
+    and as the difference of two evaluations (-1)."""
     check_trajectory(oracle_lib, protein_small, 96, energy_kernel=kernel, tile_cells=tile_cells,
-                     cells_per_cutoff=cells)
+                     cells_per_cutoff=cells, pair_delta=pair_delta)
 
 
-def test_trajectory_water_tiled_pair_image(oracle_lib, water_small):
-    """The small water box takes the per-pair minimum image; the tiled kernel
-    with one-cell pose blocks (more tiles than the default for a small box)."""
-    check_trajectory(oracle_lib, water_small, 96, tile_cells=1)
+@pytest.mark.parametrize("kernel,tile_cells", [(1, 1), (0, 0)])
+def test_trajectory_water_pair_image(oracle_lib, water_small, kernel, tile_cells):
+    """The small water box takes the per-pair minimum image: the tiled kernel
+    with one-cell pose blocks (more tiles than the default for a small box) and
+    the per-pose-warp kernel, translate / rotate changes in the difference form."""
+    check_trajectory(oracle_lib, water_small, 96, energy_kernel=kernel, tile_cells=tile_cells)

@@ -15,10 +15,10 @@ pytestmark = pytest.mark.gpu
 LOG_KMAX = 1024
 
 
-def _run(system, nsteps, speculate, chunks=None):
+def _run(system, nsteps, speculate, chunks=None, kernel=0):
     from pygcmc_b200._native import default_options
     from pygcmc_b200.engine import Engine
-    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, speculate=speculate)
+    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, speculate=speculate, energy_kernel=kernel)
     with Engine(system.copy(), opts) as eng:
         if chunks is None:
             eng.run(nsteps)
@@ -48,12 +48,13 @@ def _same(a, b):
     assert np.array_equal(fin_a.residueInfo["position"], fin_b.residueInfo["position"])
 
 
+@pytest.mark.parametrize("kernel", [0, 1], ids=["per_pose", "tiled"])
 @pytest.mark.parametrize("which", ["protein_small", "water_small"])
-def test_speculation_equals_sequential_order(request, which):
+def test_speculation_equals_sequential_order(request, which, kernel):
     s = request.getfixturevalue(which)
     n = int(s.SimInfo[0]["mcsteps"])
-    on = _run(s, n, 0)
-    off = _run(s, n, -1)
+    on = _run(s, n, 0, kernel=kernel)
+    off = _run(s, n, -1, kernel=kernel)
     _same(on, off)
     kept = int(on[4][6])
     accepted_steps = int((on[0]["n_accept"] > 0).sum())
@@ -62,12 +63,14 @@ def test_speculation_equals_sequential_order(request, which):
     assert int(off[4][6]) == 0
 
 
-def test_speculation_on_the_benchmark_protein():
+@pytest.mark.parametrize("kernel", [0, 1], ids=["per_pose", "tiled"])
+def test_speculation_on_the_benchmark_protein(kernel):
     """6000 atoms, 1000 insertion poses: the one-wave split and the mirrored
-    neighbour blocks of the benchmark workload."""
+    neighbour blocks of the benchmark workload (tiled: blocks holding more
+    poses than one tile, cut into several tiles)."""
     from pygcmc_b200 import system as S
     s = S.protein_system(seed=1, mcsteps=300)
-    _same(_run(s, 300, 0), _run(s, 300, -1))
+    _same(_run(s, 300, 0, kernel=kernel), _run(s, 300, -1, kernel=kernel))
 
 
 def test_speculation_mixed_with_timed_steps(protein_small):
