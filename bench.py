@@ -480,12 +480,15 @@ class RefRunner:
         return float(np.median(t))
 
 
-FB_WORKLOAD = ("force-biased vs plain translate/rotate on the synthetic protein (6000-atom chain, 64 A box, "
-               "8 fragments at their initial counts, confBias 1000, cutoff 12 A), a translate/rotate-only "
-               "schedule (fixed N, equal move probabilities): plain = symmetric moves (translate in a cube of "
-               "half-width 0.5 A, rotate about a uniform axis by <= 10 deg); force-biased = each component of "
-               "the displacement / rotation vector in [-0.5 A, 0.5 A] / [-10 deg, 10 deg] with density "
-               "~exp(beta f d / 2) from the force / torque (Pangali-Rao-Berne), Metropolis-Hastings corrected")
+FB_WORKLOAD = ("force-biased vs plain GCMC on the synthetic protein (6000-atom chain, 64 A box, 8 fragment "
+               "types at bulk counts, confBias 1000, cutoff 12 A): REPLICAS replicas of the system (own RNG "
+               "streams) in one context; plain = symmetric moves (translate in a cube of half-width h, rotate "
+               "about a uniform axis by <= theta); force-biased = each component of the displacement / "
+               "rotation vector in [-h, h] / [-theta, theta] with density ~exp(beta f d / 2) from the force / "
+               "torque (Pangali-Rao-Berne), Metropolis-Hastings corrected; insert / delete identical; both "
+               "scanned over (h, theta) in {(0.5 A, 10 deg), (1 A, 20 deg), (2 A, 40 deg)}; `value` = the "
+               "force-biased run at its best step size")
+FB_SCAN = ((0.5, 10.0), (1.0, 20.0), (2.0, 40.0))
 
 
 def time_engine(eng, stream, flush, chunk, warmup, steps):
@@ -547,84 +550,180 @@ def gradient_throughput(sysm, batches=10, nposes=4096):
             "gradients": "centre of mass (3), quaternion (4), per-type eps and rmin/2 (24 + 24), site charges"}
 
 
-def run_ours_forcebias(args, ws, rank, local):
+def fb_sampling_run(systems, opts, burn, meas, chunk, flush, msd=False):
+    """Burn-in, then `meas` timed steps of every replica (CUDA events on the
+    engine's stream around each chunk, L2 flushed before it): moves/s and, per
+    replica, the integrated autocorrelation times of the total fragment count N
+    and the running energy E over the measured steps (Sokal window), the
+    decorrelated samples meas / max(tau_N, tau_E), translate / rotate acceptance,
+    and with msd=True (fixed-N schedules) the mean square displacement of the
+    fragment centres (unwrapped between chunks) over the measured steps."""
     import torch
     from pygcmc_b200 import analysis as A
-    from pygcmc_b200._native import default_options
     from pygcmc_b200.engine import Engine
+    nrep = len(systems)
+    opts.log_steps = burn + meas
+    opts.log_kmax = 1
+    eng = Engine([x.copy() for x in systems], opts)
+    try:
+        stream = torch.cuda.ExternalStream(eng.stream)
+        eng.run(burn)
+        eng.sync()
+
+        holders = [x.copy() for x in systems] if msd else None
+
+        def centres():
+            out = []
+            for r in range(nrep):
+                st = eng.download(r, into=holders[r])
+                idx = np.concatenate([np.arange(int(f["startRes"]), int(f["startRes"]) + int(f["totalNum"]))
+                                      for f in st.fragmentInfo])
+                out.append(st.residueInfo["position"][idx].astype(np.float64))
+            return out
+
+        box = np.array(systems[0].SimInfo[0]["cryst"], dtype=np.float64)
+        prev = centres() if msd else None
+        disp = [np.zeros_like(c) for c in prev] if msd else None
+        ms = 0.0
+        for c0 in range(0, meas, chunk):
+            n = min(chunk, meas - c0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a.record(stream)
+            eng.run(n)
+            b.record(stream)
+            eng.sync()
+            ms += a.elapsed_time(b)
+            if msd:
+                cur = centres()
+                for r in range(nrep):
+                    d = cur[r] - prev[r]
+                    disp[r] += d - box * np.round(d / box)
+                prev = cur
+        rate = nrep * meas / (ms / 1e3)
+        per_rep = []
+        for r in range(nrep):
+            logs, _ = eng.logs(r)
+            sm = A.sampling_summary(logs[: burn + meas], systems[r].fragmentInfo["totalNum"].astype(np.int64),
+                                    meas / (ms / 1e3), burn=burn)
+            if msd:
+                sm["msd_A2"] = float((disp[r] ** 2).sum(axis=1).mean())
+            per_rep.append(sm)
+        out = {"moves_per_s": round(rate, 1), "ms": round(ms, 2), "replicas": nrep, "burn_steps": burn,
+               "steps": meas,
+               "tau_N_median": float(np.median([x["tau_N"] for x in per_rep])),
+               "tau_E_median": float(np.median([x["tau_E"] for x in per_rep])),
+               "runs_in_tau": float(np.median([meas / x["tau"] for x in per_rep])),
+               "decorrelated_samples_per_s": float(sum(meas / x["tau"] for x in per_rep) / (ms / 1e3)),
+               "trn_rot_accept_per_pose": float(np.mean([x["trn_rot_accept_per_pose"] for x in per_rep])),
+               "mean_N": float(np.mean([x["mean_N"] for x in per_rep]))}
+        if msd:
+            out["msd_A2_per_s"] = float(np.mean([x["msd_A2"] for x in per_rep]) / (ms / 1e3))
+        return out
+    finally:
+        eng.close()
+
+
+def run_ours_forcebias(args, ws, rank, local):
+    """Force-biased against plain GCMC on REPLICAS replicas of the synthetic
+    protein in one context (the batched force-biased line): each method at each
+    step size of FB_SCAN, on the full GCMC schedule (decorrelation of N and E)
+    and on a fixed-N translate/rotate schedule (decorrelation of E and the
+    fragments' mean square displacement per second), after a burn-in; `value`
+    is the force-biased moves/s at the step size with the most decorrelated
+    samples/s on the full schedule."""
+    import torch
+    from pygcmc_b200._native import default_options
     from pygcmc_b200.gpu import runGCMC
     torch.cuda.set_device(local)
-    chunk = args.chunk
+    nrep = args.replicas
     seed = replicas_seed(args.seed, rank)
-    total = (args.warmup + args.steps) * chunk + 256
-    sysm = make_system(seed, total)
-    # translate/rotate-only schedule: fixed N, so the comparison isolates the proposals
+    chunk = 512
+    burn, meas = args.warmup * 1024, args.steps * 1024
+    total = burn + meas + 64
+    base = make_system(seed, total)
+    ntype = len(base.fragmentInfo)
     g = np.random.default_rng(seed + 17)
-    ntype = len(sysm.fragmentInfo)
-    sysm.moveArray = (g.integers(0, ntype, total) * 4 + 2 + g.integers(0, 2, total)).astype(np.int32)
-    init = sysm.fragmentInfo["totalNum"].astype(np.int64).copy()
+    fixed = base.copy()
+    fixed.moveArray = (g.integers(0, ntype, total) * 4 + 2 + g.integers(0, 2, total)).astype(np.int32)
+    systems_full = [base.copy() for _ in range(nrep)]
+    systems_fixed = [fixed.copy() for _ in range(nrep)]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    arms = {"plain": default_options(proposal=1, trn_step=1.0, rot_max=float(np.radians(10.0)), log_steps=total),
-            "force_biased": default_options(proposal=2, fb_trn=0.5, fb_rot=float(np.radians(10.0)),
-                                            log_steps=total)}
-    res, ms_fb, clk = {}, None, None
-    for name, opt in arms.items():
-        eng = Engine(sysm.copy(), opt)
-        stream = torch.cuda.ExternalStream(eng.stream)
-        barrier(ws)
-        clocks = ClockSampler(local) if name == "force_biased" else None
-        ms = max_over_ranks(time_engine(eng, stream, flush, chunk, args.warmup, args.steps), ws)
-        if clocks is not None:
-            clk = clocks.stop()
-        logs, _ = eng.logs()
-        rate = args.steps * chunk / (ms / 1e3)
-        summ = A.sampling_summary(logs[: (args.warmup + args.steps) * chunk], init, rate, burn=args.warmup * chunk)
-        summ["moves_per_s"] = round(rate, 1)
-        if name == "force_biased":
-            ms_fb = ms
-            te, ta, _ = eng.run_profiled(128)
-            summ["avg_energy_launches_us"] = float(te.mean() * 1e3)
-            summ["avg_accept_us"] = float(ta.mean() * 1e3)
-        eng.close()
-        res[name] = summ
-    # end to end: the runGCMC drop-in with force-biased options, host arrays per call
-    e2e_state = sysm.pinned()  # host arrays in page-locked memory
+
+    def opts(method, h, theta):
+        th = float(np.radians(theta))
+        if method == "plain":
+            return default_options(proposal=1, trn_step=2.0 * h, rot_max=th)
+        return default_options(proposal=2, fb_trn=h, fb_rot=th)
+
+    scan = {"plain": [], "force_biased": []}
+    clk = None
+    for method in scan:
+        for h, theta in FB_SCAN:
+            barrier(ws)
+            clocks = ClockSampler(local) if (method == "force_biased" and clk is None) else None
+            full = fb_sampling_run(systems_full, opts(method, h, theta), burn, meas, chunk, flush)
+            if clocks is not None:
+                clk = clocks.stop()
+            fix = fb_sampling_run(systems_fixed, opts(method, h, theta), burn, meas, chunk, flush, msd=True)
+            scan[method].append({"h_A": h, "theta_deg": theta, "full_gcmc": full, "fixed_N": fix})
+    best = {m: max(v, key=lambda e: e["full_gcmc"]["decorrelated_samples_per_s"]) for m, v in scan.items()}
+    best_fix = {m: max(v, key=lambda e: e["fixed_N"]["decorrelated_samples_per_s"]) for m, v in scan.items()}
+    best_msd = {m: max(v, key=lambda e: e["fixed_N"]["msd_A2_per_s"]) for m, v in scan.items()}
+    fbb = best["force_biased"]
+    ms_fb = max_over_ranks(fbb["full_gcmc"]["ms"], ws)
+    value = nrep * meas * ws / (ms_fb / 1e3)
+    # end to end: the runGCMC drop-in with force-biased options (one replica, host arrays per call)
+    e2e_state = base.pinned()
     info = e2e_state.SimInfo
-    info[0]["mcsteps"] = chunk
-    h2d = sum(a.nbytes for a in e2e_state.arrays()[:6]) + 4 * chunk
+    info[0]["mcsteps"] = 8192
+    h2d = sum(x.nbytes for x in e2e_state.arrays()[:6]) + 4 * 8192
     d2h = e2e_state.moved_bytes()
-    fbopt = default_options(proposal=2, fb_trn=0.5, fb_rot=float(np.radians(10.0)))
+    fbopt = opts("force_biased", fbb["h_A"], fbb["theta_deg"])
     times = []
-    for k in range(args.warmup + args.steps):
+    for k in range(4):
         info[0]["seed"] = (seed * 7 + k) & 0xFFFFFFFF
-        mv = np.ascontiguousarray(e2e_state.moveArray[k * chunk:(k + 1) * chunk])  # a page-locked slice
+        mv = np.ascontiguousarray(e2e_state.moveArray[:8192])
         barrier(ws)
         t0 = time.perf_counter()
         runGCMC(info, e2e_state.fragmentInfo, e2e_state.residueInfo, e2e_state.atomInfo, e2e_state.grid,
                 e2e_state.ff, mv, options=fbopt)
-        if k >= args.warmup:
+        if k >= 1:
             times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(times) * 1e3, ws) / 1e3
-    value = args.steps * chunk * ws / (ms_fb / 1e3)
-    fb, pl = res["force_biased"], res["plain"]
+
+    def ratio(d, key, sub):
+        return round(d["force_biased"][sub][key] / max(d["plain"][sub][key], 1e-30), 3)
+
     out = {
-        "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_fb / args.steps, 3), "higher_is_better": True,
+        "metric": METRIC, "value": round(value, 1), "unit": "moves/s", "n_gpus": ws, "steps": meas // chunk,
+        "warmup": burn // chunk, "ms_per_step": round(ms_fb / (meas // chunk), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair terms, fp64 sums/acceptance",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": FB_WORKLOAD, "mc_steps_per_bench_step": chunk, "replicas_per_gpu": 1,
+        "config": {"workload": FB_WORKLOAD.replace("REPLICAS", str(nrep)),
+                   "mc_steps_per_bench_step": chunk * nrep, "replicas_per_gpu": nrep,
                    "parallelism": f"replicas x{ws}", "l2": "flushed (256 MB write) between timed chunks"},
-        "e2e": {"value": round(args.steps * chunk * ws / e2e_s, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC(..., options=proposal 2)"},
-        "forcebias": {"plain": pl, "force_biased": fb,
-                      "decorrelated_samples_per_s_ratio": round(fb["decorrelated_samples_per_s"]
-                                                                / max(pl["decorrelated_samples_per_s"], 1e-30), 3),
-                      "tau": "integrated autocorrelation time (steps) of the total fragment count N and the "
-                             "running energy E, Sokal window c=5, over the timed steps"},
-        "gradient": gradient_throughput(sysm),
-        "gpu_launches": args.steps * (2 + 3 * 32 * ((chunk + 31) // 32)),
+        "e2e": {"value": round(3 * 8192 * ws / e2e_s, 1), "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": 8192,
+                "host_arrays": "page-locked (System.pinned())",
+                "api": "pygcmc_b200.gpu.runGCMC(..., options=proposal 2), one replica per call"},
+        "forcebias": {
+            "scan": scan,
+            "best_full_gcmc": {m: [best[m]["h_A"], best[m]["theta_deg"]] for m in best},
+            "decorrelated_samples_per_s_ratio": ratio(best, "decorrelated_samples_per_s", "full_gcmc"),
+            "fixed_N_decorrelated_samples_per_s_ratio": ratio(best_fix, "decorrelated_samples_per_s", "fixed_N"),
+            "fixed_N_msd_per_s_ratio": ratio(best_msd, "msd_A2_per_s", "fixed_N"),
+            "moves_per_s_ratio": ratio(best, "moves_per_s", "full_gcmc"),
+            "tau": "integrated autocorrelation time (steps) of the total fragment count N and the running "
+                   "energy E per replica, Sokal window c=5, over the measured steps after the burn-in; "
+                   "decorrelated samples/s = sum over replicas of steps / max(tau_N, tau_E) per second",
+        },
+        "gradient": gradient_throughput(base),
         "clocks": clk,
+        # per 512-step chunk: k_set_run_end, k_prepare, then per step two force-bias
+        # pose-energy launches and the accept kernel
+        "gpu_launches": (meas // chunk) * (2 + 3 * chunk),
     }
     return out
 
@@ -826,7 +925,11 @@ def run_probe(args):
         s = S.water_box(seed=args.seed, mcsteps=total)
     else:
         s = make_system(args.seed, total)
-    opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 2)
+    if args.workload == "batched":  # the batch's tuned shape
+        opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 1, split_items=512, energy_variant=1,
+                              pair_delta=args.pair_delta)
+    else:
+        opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 2, pair_delta=args.pair_delta)
     with Engine(s, opt) as eng:
         eng.run(args.probe_warm)
         eng.sync()
@@ -871,6 +974,8 @@ def main():
                          "steps launched kernel by kernel (per-kernel times printed; no bench line)")
     ap.add_argument("--probe-warm", type=int, default=64)
     ap.add_argument("--probe-steps", type=int, default=24)
+    ap.add_argument("--pair-delta", type=int, default=0,
+                    help="probe: translate/rotate changes in the pairwise-difference form (0) or as two evaluations (-1)")
     ap.add_argument("--write-inputs", default="", help=argparse.SUPPRESS)  # reference arm's child process
     ap.add_argument("--mcsteps", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -885,7 +990,7 @@ def main():
         return
     args.warmup = max(args.warmup, 3)
     if args.chunk <= 0:
-        args.chunk = {"batched": 256, "forcebias": 8192, "large": 64}.get(args.workload, 2048)
+        args.chunk = {"batched": 256, "forcebias": 512, "large": 64}.get(args.workload, 2048)
     if args.replicas <= 0:
         args.replicas = 16 if args.workload == "large" else 64
     if args.ref_chunk <= 0:
@@ -913,7 +1018,7 @@ def main():
                 import copy
                 for name, fn, chunk, kw in (("batched", run_ours_batched, 256, {}),
                                             ("water", run_ours, 2048, {"kind": "water"}),
-                                            ("forcebias", run_ours_forcebias, 8192, {})):
+                                            ("forcebias", run_ours_forcebias, 512, {})):
                     sub = copy.copy(args)
                     sub.chunk, sub.no_cpu = chunk, True
                     out[name] = summary(fn(sub, ws, rank, local, **kw))
