@@ -651,6 +651,7 @@ typedef struct {
     const double* sq;
     const int32_t* st;
     int ns;
+    double alpha;  /* > 0: Ewald real-space Coulomb K q q erfc(alpha r) / r */
 } pose64;
 
 /* Visit every included group of a pose (fixed groups, then occupied slots). */
@@ -722,14 +723,21 @@ static void pose_grad64(const pose64* P, const float centre[3], int self, double
                 const double sig = P->ff[2 * tij], eps = P->ff[2 * tij + 1];
                 const double s2 = sig * sig * 100.0 / d2, s6 = s2 * s2 * s2;
                 const double r = sqrt(d2);
-                const double el = OR_COULOMB * P->sq[s] * (double)A->charge / r;
-                const double dd2 = -12.0 * eps * s6 * (2.0 * s6 - 1.0) / d2 - 0.5 * el / d2;
+                double el = OR_COULOMB * P->sq[s] * (double)A->charge / r, gel = el, kr = 1.0 / r;
+                if (P->alpha > 0.0) { /* d/d(d2) of K q q erfc(a r) / r */
+                    const double ec = erfc(P->alpha * r);
+                    el *= ec;
+                    kr *= ec;
+                    gel = el + OR_COULOMB * P->sq[s] * (double)A->charge * 2.0 * P->alpha / sqrt(OR_PI) *
+                                   exp(-P->alpha * P->alpha * d2);
+                }
+                const double dd2 = -12.0 * eps * s6 * (2.0 * s6 - 1.0) / d2 - 0.5 * gel / d2;
                 for (int i = 0; i < 3; ++i) {
                     const double gi = -2.0 * dd2 * d[i];
                     gxyz[3 * s + i] += gi;
                     if (gxyz_l1) gxyz_l1[s] += fabs(gi);
                 }
-                const double gqi = OR_COULOMB * (double)A->charge / r;
+                const double gqi = OR_COULOMB * (double)A->charge * kr;
                 gq[s] += gqi;
                 if (gq_l1) gq_l1[s] += fabs(gqi);
                 if (gff) {
@@ -882,6 +890,19 @@ static double ewald_phi(const ewald_t* E, const double r[3], double* work) {
     return p;
 }
 
+/* grad phi(r): d/dr_d of sum coef (Re S cos th + Im S sin th) = sum coef (Im S cos th - Re S sin th) 2 pi m_d / L_d */
+static void ewald_grad(const ewald_t* E, const double r[3], double* work, double g[3]) {
+    double* wre = work;
+    double* wim = work + E->nk;
+    ewald_term(E, r, wre, wim, work + 2 * E->nk);
+    g[0] = g[1] = g[2] = 0.0;
+    for (int k = 0; k < E->nk; ++k) {
+        const double c = E->coef[k] * (E->sim[k] * wre[k] - E->sre[k] * wim[k]);
+        for (int d = 0; d < 3; ++d) g[d] += c * E->idx[3 * k + d];
+    }
+    for (int d = 0; d < 3; ++d) g[d] *= 2.0 * OR_PI / E->L[d];
+}
+
 void or_ewald_potential(const or_info* info, const or_atomarray* frag, const or_residue* res, const or_atom* atoms,
                         double alpha, const double* pts, int32_t n, double* out, int32_t threads) {
     if (threads <= 0) threads = 1;
@@ -1003,8 +1024,42 @@ static void pose_force64(const sysref* S, const double* ff64, const float (*sx)[
         for (int j = 0; j < 3; ++j) x64[s][j] = sx[s][j];
         q64[s] = sq[s];
     }
-    pose64 P = {S->info, S->frag, S->res, S->atoms, ff64, (const double (*)[3])x64, q64, st, ns};
+    pose64 P = {S->info, S->frag, S->res, S->atoms, ff64, (const double (*)[3])x64, q64, st, ns,
+                S->opt->pme ? (double)S->opt->pme_alpha : 0.0};
     pose_grad64(&P, centre, self, 1.0, g, gq, NULL, gl1, NULL, NULL);
+    if (S->opt->pme) { /* reciprocal-space and molecular terms (ewald_pose_terms) */
+        const double alpha = S->opt->pme_alpha, c = 2.0 * alpha / sqrt(OR_PI);
+        double* work = malloc(sizeof(double) * (2 * S->ew->nk + ewald_tmp_size(S->ew)));
+        for (int s = 0; s < ns; ++s) {
+            double gp[3];
+            ewald_grad(S->ew, x64[s], work, gp);
+            for (int j = 0; j < 3; ++j) {
+                g[3 * s + j] += q64[s] * gp[j];
+                gl1[s] += fabs(q64[s] * gp[j]);
+            }
+            if (self >= 0) {
+                const or_residue* R = &S->res[self];
+                for (int t = 0; t < R->atomNum; ++t) {
+                    const or_atom* A = &S->atoms[R->atomStart + t];
+                    double d[3], d2 = 0.0;
+                    for (int j = 0; j < 3; ++j) {
+                        d[j] = x64[s][j] - (double)A->position[j];
+                        d[j] -= fast_round_d(d[j] / S->info->cryst[j]) * S->info->cryst[j];
+                        d2 += d[j] * d[j];
+                    }
+                    const double r = sqrt(d2);
+                    const double gpr = r < 1e-4 ? -(2.0 / 3.0) * c * alpha * alpha
+                                                : (c * exp(-alpha * alpha * d2) * r - erf(alpha * r)) / (r * d2);
+                    const double w = -OR_COULOMB * q64[s] * (double)A->charge * gpr;
+                    for (int j = 0; j < 3; ++j) {
+                        g[3 * s + j] += w * d[j];
+                        gl1[s] += fabs(w * d[j]);
+                    }
+                }
+            }
+        }
+        free(work);
+    }
     double m[3] = {0.0, 0.0, 0.0};
     for (int s = 0; s < ns; ++s)
         for (int j = 0; j < 3; ++j) m[j] += x64[s][j] / ns;
@@ -1168,7 +1223,6 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
         }
     } else if (S->opt->proposal == 2) {
         /* force-biased translate/rotate with the Metropolis-Hastings correction */
-        if (S->opt->pme) return -4; /* force bias runs without Ewald */
         int n = F->totalNum;
         k = F->confBias < n ? F->confBias : n;
         if (k == 0) goto done;
@@ -1199,8 +1253,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
             for (int s2 = 0; s2 < ns; ++s2)
                 for (int j = 0; j < 3; ++j) old[s2][j] = S->atoms[R->atomStart + s2].position[j];
             double lo = 0.0, ln = 0.0, fo64[6], fn64[6], so[2], sn2[2];
-            double Eo = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])old, sq,
-                                          st, ns, R->position, self, 0, NULL, NULL, &lo);
+            double Eo = step_pose_energy(S, (const float (*)[3])old, sq, st, ns, R->position, self, &lo);
             pose_force64(S, ff64, (const float (*)[3])old, sq, st, ns, R->position, self, fo64, so);
             float fo[6];
             for (int c = 0; c < 6; ++c)
@@ -1245,8 +1298,7 @@ static int32_t do_step(const sysref* S, const int32_t* moves, int step, or_step_
                     }
                 }
             }
-            double En = or_pose_energy_l1(info, S->frag, S->res, S->atoms, S->ff, (const float (*)[3])xyz[i], sq,
-                                          st, ns, cen[i], self, 0, NULL, NULL, &ln);
+            double En = step_pose_energy(S, (const float (*)[3])xyz[i], sq, st, ns, cen[i], self, &ln);
             pose_force64(S, ff64, (const float (*)[3])xyz[i], sq, st, ns, cen[i], self, fn64, sn2);
             for (int c = 0; c < 6; ++c)
                 fnu[i][c] = S->replay_forces ? S->replay_forces[(size_t)i * 12 + 6 + c] : (float)fn64[c];

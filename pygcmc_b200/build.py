@@ -13,7 +13,7 @@ SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "synth.cpp", "as
 HEADERS = [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc"))) if f.endswith(".cuh")] + [
     os.path.join(HERE, "..", "include", "gcmc_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-shared", "-Xcompiler", "-fPIC", "-lcufft"]
+              "-shared", "-Xcompiler", "-fPIC"]
 
 
 def _stale():

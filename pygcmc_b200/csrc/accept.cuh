@@ -575,6 +575,14 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                 if (spec) void_next(R, D.step + 1);
                 const int slot = D.del_slot, last = n - 1;
                 const int gs = F.startRes + slot, gl = F.startRes + last;
+                if (R.pme) {  // the leaving molecule's charges leave the mesh
+                    const int2 sd = R.gspan[gs];
+                    for (int s = 0; s < ns; ++s) {
+                        const float4 a = R.xyzq[sd.x + s];
+                        pme_move_site(R, true, a.x, a.y, a.z, false, 0.f, 0.f, 0.f, a.w);
+                    }
+                    *R.pme_dirty = 1;
+                }
                 cell_remove(R, gs);
                 if (slot != last) {
                     const int2 ss = R.gspan[gs], sl = R.gspan[gl];
@@ -767,8 +775,10 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                 const int2 sp = R.gspan[res];
                 const float4 c = S.c[i];
                 if (lane < ns) {  // the pose's sites as built by the pose-energy kernel
-                    R.xyzq[sp.x + lane] = R.psite[i * kMaxSites + lane];
+                    const float4 p = R.psite[i * kMaxSites + lane];
+                    R.xyzq[sp.x + lane] = p;
                     R.atype[sp.x + lane] = F.stype[lane];
+                    if (R.pme) pme_move_site(R, false, 0.f, 0.f, 0.f, true, p.x, p.y, p.z, p.w);
                 }
                 if (lane == 0) R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
             }
@@ -795,6 +805,10 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                 if (lane < ns) {  // moved sites as built by the pose-energy kernel; the charge stays
                     const float4 p = R.psite[i * kMaxSites + lane];
                     float* dst = reinterpret_cast<float*>(R.xyzq + sp.x + lane);
+                    if (R.pme) {
+                        const float4 o = R.xyzq[sp.x + lane];
+                        pme_move_site(R, true, o.x, o.y, o.z, true, p.x, p.y, p.z, o.w);
+                    }
                     dst[0] = p.x;
                     dst[1] = p.y;
                     dst[2] = p.z;
@@ -830,6 +844,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
     }
     __syncthreads();
     if (tid == 0) {
+        if (R.pme && D.move != MV_DELETE && S.misc[0] > 0) *R.pme_dirty = 1;  // the mesh charges moved
         if (D.move != MV_DELETE) {  // running energy: accepted moves in commit order
             double et = *R.energy;
             const int na = S.misc[0];

@@ -451,6 +451,10 @@ struct RepDev {
     float pme_alpha;
     int pme_n[3];
     const double* pme_phi;  // [n0 * n1 * n2] theta_rec * Q (kJ/mol/e)
+    double* pme_q;          // [n0 * n1 * n2] spread charges of the current state
+    double2* pme_spec;      // [n0 * n1 * (n2 / 2 + 1)] transform workspace
+    const double* pme_g;    // [n0 * n1 * (n2 / 2 + 1)] influence function
+    int* pme_dirty;         // 1: Q changed since phi was computed
     double pme_bgc;         // K pi / (2 V alpha^2): background energy -bgc Q^2
     double pme_qfix;        // total charge of the fixed atoms
 };

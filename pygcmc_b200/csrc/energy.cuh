@@ -35,13 +35,16 @@ struct SitePair {
 };
 
 // Site s of a translate / rotate pose in the pairwise-difference form: the
-// negated offsets of its old and its new position from the old pose centre
-// (x: old, y: new; the new one in the old centre's periodic frame), and its
-// displacement new - old (from the absolute positions, rounded once) with the
-// Coulomb constant * charge.
+// negated offsets so, sn of its old and its new position from the old pose
+// centre (x: old, y: new; the new one in the old centre's periodic frame);
+// twice its displacement delta = sn - so (from the absolute positions, rounded
+// once) with the Coulomb constant * charge; and c = delta.(so + sn) =
+// |sn|^2 - |so|^2 (FP64, rounded once), so that for an atom at offset A
+// r_o^2 - r_n^2 = delta.(d_o + d_n) = 2 delta.A - c.
 struct DualSite {
     float2 nx, ny, nz;
     float4 dk;
+    float c, pad;
 };
 
 struct WarpBuf {
@@ -299,9 +302,13 @@ __device__ __forceinline__ float dual_atom_e(const RepDev& R, const DualSite* ds
         if (fl == 3u) {
             float dinv;
             if (same) {
-                const float D = fmaf(d.dk.z, dz.x + dz.y, fmaf(d.dk.y, dy.x + dy.y, d.dk.x * (dx.x + dx.y)));
-                const float2 r = __fmul2_rn(r2, ir);
-                dinv = __fdividef(D * ir.x * ir.y, r.x + r.y);
+                // r_o^2 - r_n^2: 2 delta.A - c (group image), or delta.(d_o + d_n) under a
+                // per-pair image (the same shift for both, so the pair's own offsets)
+                const float D = PairImage ? 0.5f * fmaf(d.dk.z, dz.x + dz.y, fmaf(d.dk.y, dy.x + dy.y,
+                                                                                d.dk.x * (dx.x + dx.y)))
+                                          : fmaf(d.dk.z, az, fmaf(d.dk.y, ay, fmaf(d.dk.x, ax, -d.c)));
+                // 1/r_n - 1/r_o = D / (r_o r_n (r_o + r_n)) = D (ir_o ir_n)^2 / (ir_o + ir_n)
+                dinv = __fdividef(D * (ir2.x * ir2.y), ir.x + ir.y);
             } else {
                 dinv = ir.y - ir.x;
             }
@@ -879,7 +886,10 @@ __device__ __forceinline__ void build_pose_dual(const RepDev& R, const StepDesc&
         d.nx = make_float2(-(float)dox, -(float)dnx);
         d.ny = make_float2(-(float)doy, -(float)dny);
         d.nz = make_float2(-(float)doz, -(float)dnz);
-        d.dk = make_float4((float)(dnx - dox), (float)(dny - doy), (float)(dnz - doz), kCoulomb * F.site[lane].w);
+        d.dk = make_float4((float)(2.0 * (dnx - dox)), (float)(2.0 * (dny - doy)), (float)(2.0 * (dnz - doz)),
+                           kCoulomb * F.site[lane].w);
+        d.c = (float)((dnx * dnx + dny * dny + dnz * dnz) - (dox * dox + doy * doy + doz * doz));
+        d.pad = 0.0f;
         B.dsite[lane] = d;
         B.site_abs[lane] = make_float4(px, py, pz, F.site[lane].w);
     }
@@ -1029,11 +1039,18 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // The items of one pose-energy launch, whole CTA: warp w of the CTA is warp
 // gw0 + w of the nwarps that share the items; B: this warp's buffer; pre,
 // wtot: 257 and 32 ints of shared memory.  The body of k_energy_t and of the
-// persistent step loop.
+// persistent step loop.  Which: -1 every replica's items; 0 only the items of
+// steps not in the difference form, 1 only those of steps in it (a batch runs
+// the two kinds as separate launches, so that an SM holds one code path's
+// instructions at a time).
+template <int Which>
 __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, int nrep, int mode, int gw0,
                                              int nwarps, WarpBuf& B, int* pre, int* wtot) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    items_prefix(nrep, pre, wtot, [&](int r) { return reps[r].desc->items; });
+    items_prefix(nrep, pre, wtot, [&](int r) {
+        const StepDesc* d = reps[r].desc;
+        return (Which < 0 || (Which == 1) == (d->dual != 0)) ? d->items : 0;
+    });
     const int total = pre[nrep];
     const bool sym = total > nwarps;  // more items than warps: throughput-bound
     for (int it = gw0 + warp; it < total; it += nwarps) {
@@ -1052,7 +1069,7 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
         double acc = 0.0;
         int ng = 0;
         long long npair = 0;
-        if (D.dual) {  // translate / rotate: the energy change of both poses in one walk
+        if (Which != 0 && D.dual) {  // translate / rotate: the energy change of both poses in one walk
             DualCentre dc;
             build_pose_dual(R, D, i, B, lane, cx, cy, cz, dc, self);
             keep_sites(R, D, B, i, 0, zi, lane);
@@ -1061,7 +1078,7 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
             walk_cells<DualSink, true>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, sink, ng,
                                        npair, mode == 1 ? R.abort : nullptr, D.step, D.nslab, &dc);
             acc = sink.acc;
-        } else {
+        } else if (Which != 1) {
             build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
             keep_sites(R, D, B, i, v, zi, lane);
             const int nwin = R.span[0] * R.span[1] * R.span[2];
@@ -1089,18 +1106,23 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
     }
 }
 
-template <int MinBlocks>
+template <int MinBlocks, int Which>
 __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep,
                                                                       int mode) {
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     __shared__ int wtot[32];
     if (mode == 2 && *reps[0].valid) return;
-    energy_items(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre, wtot);
+    energy_items<Which>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre,
+                        wtot);
 }
 
-template __global__ void k_energy_t<3>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<4>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, -1>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, -1>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, 1>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, 1>(const RepDev* __restrict__, int, int);
 
 // Energies of caller-supplied poses (gcmc_energy_poses): item = (pose, slab).
 // The replica descriptor is passed by value so that callers can substitute

@@ -17,7 +17,6 @@
 #include <string>
 #include <vector>
 
-#include <cufft.h>
 
 #include "accept.cuh"
 #include "grad.cuh"
@@ -95,13 +94,11 @@ struct RepHost {
     int pme = 0;
     int pme_n[3] = {0, 0, 0};
     int nfix_atoms = 0;
-    double* pme_qfix = nullptr;   // fixed atoms' spread charges
     double* pme_q = nullptr;      // this step's spread charges
     double* pme_phi = nullptr;    // potential on the mesh
     double2* pme_spec = nullptr;  // half spectrum
     double* pme_g = nullptr;      // influence function on the half spectrum
-    cufftHandle plan_f = 0, plan_b = 0;
-    bool plans = false;
+    int* pme_dirty = nullptr;     // 1: the spread charges changed since phi was computed
     double pme_key[7] = {0, 0, 0, 0, 0, 0, 0};  // mesh, box and alpha the influence function in pme_g is for
     const double* pme_g_for = nullptr;          // the buffer it was written to
 };
@@ -132,6 +129,7 @@ struct gcmc_ctx {
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
     bool tiled = false;  // pose energies by k_energy_tiles (every replica allows it)
     bool pme_any = false; // some replica runs Ewald electrostatics
+    bool dual_any = false; // some replica evaluates translate / rotate changes in the difference form
     bool persist = false;   // the step loop as one cooperative launch (k_persist) instead of a graph
     GridSync* d_sync = nullptr;
     int grid_persist = 0;   // k_persist CTAs (one per SM)
@@ -190,13 +188,8 @@ void free_rep(RepHost& h) {
     dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid);
     dfree(h.desc2); dfree(h.pcen2); dfree(h.pslot2); dfree(h.epart2); dfree(h.nbr2); dfree(h.pgum2); dfree(h.plnu2);
     dfree(h.psite2); dfree(h.valid2); dfree(h.abort2); dfree(h.sstep2); dfree(h.pending2); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
-    dfree(h.pme_qfix); dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g);
+    dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g); dfree(h.pme_dirty);
     dfree(h.pbin); dfree(h.tiles); dfree(h.pbin2); dfree(h.tiles2);
-    if (h.plans) {
-        cufftDestroy(h.plan_f);
-        cufftDestroy(h.plan_b);
-        h.plans = false;
-    }
     h.capn.clear();
 }
 
@@ -265,14 +258,12 @@ int validate(const gcmc_replica_in& in) {
     return GCMC_OK;
 }
 
-// smallest n' >= n whose prime factors are 2, 3, 5, 7 (fast FFT sizes)
+// smallest n' >= n whose prime factors are 2 and 3 (the mesh transforms' line
+// lengths; 0 when that exceeds kFftMax)
 int smooth_size(int n) {
-    for (int m = std::max(n, 1);; ++m) {
-        int x = m;
-        for (int p : {2, 3, 5, 7})
-            while (x % p == 0) x /= p;
-        if (x == 1) return m;
-    }
+    for (int m = std::max(n, 1); m <= kFftMax; ++m)
+        if (fft_size_ok(m)) return m;
+    return 0;
 }
 
 // Smooth-PME influence function on the half spectrum (FP64):
@@ -538,9 +529,8 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         AL(h.psite2, (size_t)kMaxPoses * kMaxSites); AL(h.valid2, 2); AL(h.abort2, 2); AL(h.sstep2, 2);
         AL(h.pending2, 2); AL(h.pbin2, 2 * kMaxPoses); AL(h.tiles2, 2 * kMaxPoses);
     }
-    // smooth PME: mesh, influence function, FFT plans
+    // smooth PME: mesh and influence function
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
-    if (h.pme && opt.proposal == 2) return GCMC_ERR_ARG;  // force bias runs without Ewald
     d.pme = h.pme ? 1 : 0;
     h.nfix_atoms = d.nfixed > 0 ? in.residueInfo[d.nfixed - 1].atomStart + in.residueInfo[d.nfixed - 1].atomNum : 0;
     if (h.pme) {
@@ -549,11 +539,13 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         int n[3];
         for (int a = 0; a < 3; ++a) {
             n[a] = opt.pme_grid[a] > 0 ? opt.pme_grid[a] : smooth_size((int)std::ceil(I->cryst[a] / 1.2));
+            if (n[a] == 0) return GCMC_ERR_LIMIT;      // box edge over 1.2 kFftMax A
             if (n[a] < 8) return GCMC_ERR_ARG;
+            if (!fft_size_ok(n[a])) return GCMC_ERR_LIMIT;  // a mesh size that is not 2^a 3^b <= kFftMax
             d.pme_n[a] = n[a];
         }
         const size_t nr = (size_t)n[0] * n[1] * n[2], nh = (size_t)n[0] * n[1] * (n[2] / 2 + 1);
-        AL(h.pme_qfix, nr); AL(h.pme_q, nr); AL(h.pme_phi, nr); AL(h.pme_spec, nh); AL(h.pme_g, nh);
+        AL(h.pme_q, nr); AL(h.pme_phi, nr); AL(h.pme_spec, nh); AL(h.pme_g, nh); AL(h.pme_dirty, 1);
         // the influence function depends only on the mesh, the box and alpha: kept between refills
         const double key[7] = {(double)n[0], (double)n[1], (double)n[2], (double)I->cryst[0], (double)I->cryst[1],
                                (double)I->cryst[2], alpha};
@@ -565,21 +557,16 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
             h.pme_g_for = h.pme_g;
         }
         CK(cudaMemsetAsync(h.pme_phi, 0, sizeof(double) * nr, ctx->stream));
-        if (!h.plans || n[0] != h.pme_n[0] || n[1] != h.pme_n[1] || n[2] != h.pme_n[2]) {
-            if (h.plans) {
-                cufftDestroy(h.plan_f);
-                cufftDestroy(h.plan_b);
-                h.plans = false;
-            }
-            if (cufftPlan3d(&h.plan_f, n[0], n[1], n[2], CUFFT_D2Z) != CUFFT_SUCCESS) return GCMC_ERR_CUDA;
-            if (cufftPlan3d(&h.plan_b, n[0], n[1], n[2], CUFFT_Z2D) != CUFFT_SUCCESS) {
-                cufftDestroy(h.plan_f);
-                return GCMC_ERR_CUDA;
-            }
-            h.plans = true;
-        }
+        const int fft_smem = 2 * kFftLines * kFftMax * (int)sizeof(double2);
+        CK(cudaFuncSetAttribute(k_pme_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, fft_smem));
+        CK(cudaFuncSetAttribute(k_pme_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, fft_smem));
+        CK(cudaFuncSetAttribute(k_pme_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, fft_smem));
         for (int a = 0; a < 3; ++a) h.pme_n[a] = n[a];
         d.pme_phi = h.pme_phi;
+        d.pme_q = h.pme_q;
+        d.pme_spec = h.pme_spec;
+        d.pme_g = h.pme_g;
+        d.pme_dirty = h.pme_dirty;
         d.pme_bgc = (double)kCoulomb * M_PI / (2.0 * V * alpha * alpha);
         double qf = 0.0;
         for (int a = 0; a < h.nfix_atoms; ++a) qf += (double)in.atomInfo[a].charge;
@@ -676,15 +663,26 @@ int upload_reps(gcmc_ctx* ctx) {
 }
 
 using EnergyKernel = void (*)(const RepDev*, int, int);
-EnergyKernel energy_kernel(int variant) { return variant == 1 ? k_energy_t<4> : k_energy_t<3>; }
+// which: -1 every item; 0 / 1 the items of steps not in / in the difference form
+EnergyKernel energy_kernel(int variant, int which = -1) {
+    if (which == 0) return variant == 1 ? k_energy_t<4, 0> : k_energy_t<3, 0>;
+    if (which == 1) return variant == 1 ? k_energy_t<4, 1> : k_energy_t<3, 1>;
+    return variant == 1 ? k_energy_t<4, -1> : k_energy_t<3, -1>;
+}
 
 // One pose-energy launch over replicas reps[0, n) in `mode` on `grid` CTAs:
 // the tiled kernel when the context is tiled, else the per-pose-warp kernel.
 void launch_energy(const gcmc_ctx* ctx, const RepDev* reps, int n, int mode, int grid, cudaStream_t s) {
-    if (ctx->tiled)
+    if (ctx->tiled) {
         k_energy_tiles<<<grid, kWarpsT * 32, sizeof(TileSmem), s>>>(reps, n, mode);
-    else
+    } else if (n > 1 && ctx->dual_any) {
+        // a batch mixes the two kinds of items: one launch each, so that an SM runs one
+        // code path at a time (both in one launch stalled on instruction fetch)
+        energy_kernel(ctx->evar, 0)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+        energy_kernel(ctx->evar, 1)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+    } else {
         energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+    }
 }
 
 // Dynamic shared memory of the preparation kernels (the pose binning's scratch).
@@ -700,6 +698,9 @@ void finalize_tiling(gcmc_ctx* ctx) {
     bool pme = false;
     for (const auto& h : ctx->reps) pme = pme || h.pme;
     ctx->pme_any = pme;
+    bool dual = false;
+    for (const auto& d : ctx->repdev) dual = dual || d.dual;
+    ctx->dual_any = dual;
 }
 
 // Resident warps of the pose-energy grid for this register variant and CTA cap.
@@ -716,35 +717,42 @@ int energy_warps(int device, int evar, int ebps, int spare_sms) {
 }
 
 
-// Rebuild replica r's PME mesh potential from its current state on stream s:
-// Q = Q_fixed + spread(occupied fragment atoms); phi = IFFT(G * FFT(Q)).
+// Replica r's PME mesh potential from its spread charges on stream s, when
+// they changed since the last update (every pass returns at once otherwise):
+// rows real-to-complex, axis 1, axis 0 with the influence function between
+// its forward and inverse transforms, axis 1 inverse, rows complex-to-real.
 int pme_update(gcmc_ctx* ctx, int r, cudaStream_t s) {
     RepHost& h = ctx->reps[r];
     if (!h.pme) return GCMC_OK;
-    const size_t nr = (size_t)h.pme_n[0] * h.pme_n[1] * h.pme_n[2];
-    const size_t nh = (size_t)h.pme_n[0] * h.pme_n[1] * (h.pme_n[2] / 2 + 1);
-    CK(cudaMemcpyAsync(h.pme_q, h.pme_qfix, sizeof(double) * nr, cudaMemcpyDeviceToDevice, s));
-    k_pme_spread_frag<<<148, 256, 0, s>>>(ctx->d_reps + r, h.pme_q);
-    if (cufftSetStream(h.plan_f, s) != CUFFT_SUCCESS ||
-        cufftExecD2Z(h.plan_f, h.pme_q, reinterpret_cast<cufftDoubleComplex*>(h.pme_spec)) != CUFFT_SUCCESS)
-        return GCMC_ERR_CUDA;
-    k_pme_scale<<<(int)std::min<size_t>((nh + 255) / 256, 4096), 256, 0, s>>>(h.pme_spec, h.pme_g, nh);
-    if (cufftSetStream(h.plan_b, s) != CUFFT_SUCCESS ||
-        cufftExecZ2D(h.plan_b, reinterpret_cast<cufftDoubleComplex*>(h.pme_spec), h.pme_phi) != CUFFT_SUCCESS)
-        return GCMC_ERR_CUDA;
+    const RepDev* rep = ctx->d_reps + r;
+    const int n0 = h.pme_n[0], n1 = h.pme_n[1], n2 = h.pme_n[2], M = n2 / 2 + 1;
+    const int kb = (M + kFftLines - 1) / kFftLines;
+    const int rows = (n0 * n1 + kFftLines - 1) / kFftLines;
+    const size_t sm2 = 2 * kFftLines * (size_t)n2 * sizeof(double2);
+    const size_t sm1 = 2 * kFftLines * (size_t)n1 * sizeof(double2);
+    const size_t sm0 = 2 * kFftLines * (size_t)n0 * sizeof(double2);
+    k_pme_rows_r2c<<<std::min(rows, 4096), kFftThreads, sm2, s>>>(rep);
+    k_pme_axis<<<std::min(n0 * kb, 4096), kFftThreads, sm1, s>>>(rep, 1, -1, 0);
+    k_pme_axis<<<std::min(n1 * kb, 4096), kFftThreads, sm0, s>>>(rep, 0, 0, 1);
+    k_pme_axis<<<std::min(n0 * kb, 4096), kFftThreads, sm1, s>>>(rep, 1, 1, 0);
+    k_pme_rows_c2r<<<std::min(rows, 4096), kFftThreads, sm2, s>>>(rep);
+    k_pme_done<<<1, 32, 0, s>>>(rep);
     CK(cudaGetLastError());
     return GCMC_OK;
 }
 
-// The fixed atoms' spread charges (once per set-up; needs d_reps uploaded).
+// The spread charges of the current state (the fixed atoms and the occupied
+// fragment slots; once per set-up, needs d_reps uploaded), marked dirty.
 int pme_init_fixed(gcmc_ctx* ctx) {
     for (int r = 0; r < ctx->nrep; ++r) {
         RepHost& h = ctx->reps[r];
         if (!h.pme) continue;
         const size_t nr = (size_t)h.pme_n[0] * h.pme_n[1] * h.pme_n[2];
-        CK(cudaMemsetAsync(h.pme_qfix, 0, sizeof(double) * nr, ctx->stream));
+        CK(cudaMemsetAsync(h.pme_q, 0, sizeof(double) * nr, ctx->stream));
         if (h.nfix_atoms > 0)
-            k_pme_spread_range<<<296, 256, 0, ctx->stream>>>(ctx->d_reps + r, h.pme_qfix, 0, h.nfix_atoms);
+            k_pme_spread_range<<<296, 256, 0, ctx->stream>>>(ctx->d_reps + r, h.pme_q, 0, h.nfix_atoms);
+        k_pme_spread_frag<<<148, 256, 0, ctx->stream>>>(ctx->d_reps + r, h.pme_q);
+        CK(cudaMemsetAsync(h.pme_dirty, 1, sizeof(int), ctx->stream));
         CK(cudaGetLastError());
     }
     return GCMC_OK;
@@ -961,7 +969,7 @@ int destroy_impl(gcmc_ctx* ctx) {
 
 // The persistent step loop where it was asked for and the context allows it:
 // no speculation (one-replica contexts speculate instead), no PME (its mesh
-// update runs cuFFT between steps), proposal 0 or 1, the per-pose-warp
+// mesh update runs between steps), proposal 0 or 1, the per-pose-warp
 // pose-energy kernel, and one k_persist CTA resident on every SM.
 int setup_persist(gcmc_ctx* ctx, const gcmc_options& opt) {
     ctx->persist = false;
@@ -1069,7 +1077,7 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const bool spec = spec_eligible(nrep, ins, opt);
     const bool spec_changed = spec != ctx->spec;
     ctx->spec = spec;
-    const bool tiled_before = ctx->tiled, pme_before = ctx->pme_any;
+    const bool tiled_before = ctx->tiled, pme_before = ctx->pme_any, dual_before = ctx->dual_any;
     for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
     if (st != GCMC_OK) return st;
     finalize_tiling(ctx);
@@ -1086,7 +1094,7 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const bool had_graph = ctx->gexec || ctx->gexec_spec[0];
     const bool shape_changed = spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps ||
                                fb != ctx->fb || evar != ctx->evar || ctx->tiled != tiled_before ||
-                               ctx->pme_any != pme_before;
+                               ctx->pme_any != pme_before || ctx->dual_any != dual_before;
     ctx->fb = fb;
     ctx->evar = evar;
     st = setup_persist(ctx, opt);

@@ -90,14 +90,23 @@ struct GradSinkT {
                     const float2 p = __ldg(&R.lj[row + ta]);
                     const float s2 = p.x * ir2;
                     const float s6 = s2 * s2 * s2;
-                    const float uel = sp.w * a.w * ir;
+                    float uel = sp.w * a.w * ir;
+                    float gel = uel;  // -2 r^2 d(U_el)/d(r^2)
+                    float cq = ir;    // d(U_el)/d(K q_s q_a)
+                    if (R.pme) {      // Ewald real space: K q q erfc(alpha r) / r
+                        const float ar = R.pme_alpha * (r2 * ir);
+                        const float ec = erfcf(ar);
+                        uel *= ec;
+                        cq *= ec;
+                        gel = uel + sp.w * a.w * (1.12837917f * R.pme_alpha) * expf(-ar * ar);
+                    }
                     const float t6 = fmaf(2.0f * s6, s6, -s6);
-                    const float G = -fmaf(3.0f * p.y, t6, 0.5f * uel) * ir2;
+                    const float G = -fmaf(3.0f * p.y, t6, 0.5f * gel) * ir2;
                     const float m2 = -2.0f * G;
                     gx = fmaf(m2, dx, gx);  // dU/dx_s = -2 G (atom - site)
                     gy = fmaf(m2, dy, gy);
                     gz = fmaf(m2, dz, gz);
-                    gq = fmaf(kCoulomb * a.w, ir, gq);
+                    gq = fmaf(kCoulomb * a.w, cq, gq);
                     if (WithE) e = fmaf(p.y, fmaf(s6, s6, -s6), e) + uel;
                     if (gtab) {
                         float* g = gtab + ((size_t)s * ffY + ta) * 2;
@@ -238,7 +247,14 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
             sink.w = 1.0f;
             sink.ffY = R.ffY;
             walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair, nullptr, 0, stride);
-            acc = warp_sum((double)sink.e);
+            double epme = 0.0;
+            float pgx = 0.f, pgy = 0.f, pgz = 0.f;
+            if (R.pme && zi == 0) {  // Ewald reciprocal and molecular terms of the pose, once (slab 0)
+                const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
+                epme = pme_pose_lane(R, ns, lane, a.x, a.y, a.z, a.w, self);
+                pme_grad_lane(R, ns, lane, a.x, a.y, a.z, a.w, self, pgx, pgy, pgz);
+            }
+            acc = warp_sum((double)sink.e + epme);
             // per-site gradient (lanes < ns after summing the atom subsets), then
             // force -sum g_s and torque -sum (x_s - m) x g_s about the site centroid
             stages[warp].red[lane] = make_float4(sink.gx, sink.gy, sink.gz, 0.0f);
@@ -251,7 +267,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
                     const float4 t = stages[warp].red[k * ns + lane];
                     gsum.x += t.x; gsum.y += t.y; gsum.z += t.z;
                 }
-                g0 = gsum.x; g1 = gsum.y; g2 = gsum.z;
+                g0 = gsum.x + pgx; g1 = gsum.y + pgy; g2 = gsum.z + pgz;
                 float mx = 0.f, my = 0.f, mz = 0.f;
                 for (int s = 0; s < ns; ++s) { mx += B.site[s].x; my += B.site[s].y; mz += B.site[s].z; }
                 const float inv = 1.0f / (float)ns;

@@ -73,8 +73,12 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_persist(const RepDev* __r
     WarpBuf* bufs = reinterpret_cast<WarpBuf*>(smem_raw);
     int* err = reps[0].err;
     for (int s = 0; s < nsteps; ++s) {
-        energy_items(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
-                     bufs[threadIdx.x >> 5], pre, wtot);
+        // the two kinds of items one after the other (one code path at a time per SM)
+        energy_items<0>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
+                        bufs[threadIdx.x >> 5], pre, wtot);
+        __syncthreads();  // pre / wtot are rewritten by the second prefix
+        energy_items<1>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
+                        bufs[threadIdx.x >> 5], pre, wtot);
         if (!grid_barrier(gs, spin_cap, err, &ok_sh)) return;
         for (int r = blockIdx.x; r < nrep; r += gridDim.x) {
             accept_step(reps[r], 0, smem_raw);

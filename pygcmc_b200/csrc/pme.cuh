@@ -2,12 +2,18 @@
 // Phys. 103 (1995) 8577), FP64 mesh; not in the reference, whose calcEnergy
 // uses a plain cutoff.
 //
-// Per MC step, before the pose energies, each replica's mesh potential is
-// rebuilt: Q = Q_fixed (the fixed atoms' spread charges, made once) + the
-// occupied fragment atoms spread with order-4 cardinal B-splines;
-// phi_mesh = IFFT(G * FFT(Q)) with G(m) = K exp(-pi^2 m^2 / alpha^2) B(m) /
-// (pi V m^2), B the B-spline moduli (cuFFT D2Z / Z2D).  The potential at a
-// point is the same B-spline interpolation of phi_mesh.
+// Each replica keeps its spread charges Q on the mesh: the fixed atoms and the
+// occupied fragment atoms spread with order-4 cardinal B-splines once at
+// set-up; afterwards the accept kernel spreads the change of every accepted
+// move (-q at a molecule's old sites, +q at its new ones) and marks the mesh
+// dirty.  Before a step's pose energies, a dirty mesh's potential is
+// recomputed, phi_mesh = IFFT(G * FFT(Q)) with G(m) = K exp(-pi^2 m^2 /
+// alpha^2) B(m) / (pi V m^2), B the B-spline moduli, by the hand-written FP64
+// transforms of fft.cuh (five passes: rows real-to-complex, axis 1, axis 0
+// with the G product between its forward and inverse transforms, axis 1,
+// rows complex-to-real); after a step that accepted nothing every pass
+// returns at once.  The potential at a point is the same B-spline
+// interpolation of phi_mesh.
 //
 // Energy of a trial pose p (sites r_s, charges q_s) under Ewald:
 //   E(p) = sum_{pairs in the group cutoff} [LJ + K q_s q_a erfc(alpha r) / r]
@@ -22,6 +28,7 @@
 // term of order q^2 / L^3 for these box sizes).
 #pragma once
 #include "common.cuh"
+#include "fft.cuh"
 
 namespace gcmc {
 
@@ -62,6 +69,15 @@ __device__ __forceinline__ void pme_spread_one(const RepDev& R, double* Q, doubl
             for (int c = 0; c < 4; ++c) atomicAdd(row + wrapm((int)fz - c, n2), wab * mz[c]);
         }
     }
+}
+
+// derivatives of bspline4's weights with respect to w
+__device__ __forceinline__ void bspline4_d(double w, double d[4]) {
+    const double c = 1.0 - w;
+    d[0] = 0.5 * w * w;
+    d[1] = 0.5 * (-3.0 * w * w + 2.0 * w + 1.0);
+    d[2] = 0.5 * (3.0 * w * w - 4.0 * w);
+    d[3] = -0.5 * c * c;
 }
 
 // phi at a point by the same interpolation
@@ -110,15 +126,118 @@ __global__ void k_pme_spread_frag(const RepDev* __restrict__ rep, double* Q) {
     }
 }
 
-// spectrum *= G (half spectrum, n0 * n1 * (n2/2 + 1) complex values)
-__global__ void k_pme_scale(double2* __restrict__ spec, const double* __restrict__ G, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double g = G[i];
-        double2 v = spec[i];
-        v.x *= g;
-        v.y *= g;
-        spec[i] = v;
+// ---- the mesh transforms (dynamic shared memory: 2 * kFftLines * n * 16 B,
+// n the pass's line length) ----
+
+__device__ __forceinline__ bool pme_clean(const RepDev& R) {
+    return *reinterpret_cast<const volatile int*>(R.pme_dirty) == 0;
+}
+
+// Rows along axis 2: Q (real, n2 per row) -> spectrum rows (n2 / 2 + 1).
+__global__ void __launch_bounds__(kFftThreads) k_pme_rows_r2c(const RepDev* __restrict__ rep) {
+    const RepDev& R = *rep;
+    if (pme_clean(R)) return;
+    extern __shared__ __align__(16) double2 fbuf[];
+    const int n0 = R.pme_n[0], n1 = R.pme_n[1], n2 = R.pme_n[2], M = n2 / 2 + 1;
+    const int rows = n0 * n1;
+    double2 *b0 = fbuf, *b1 = fbuf + kFftLines * n2;
+    for (int r0 = blockIdx.x * kFftLines; r0 < rows; r0 += gridDim.x * kFftLines) {
+        const int nl = min(kFftLines, rows - r0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nl * n2; e += blockDim.x)
+            b0[e] = make_double2(R.pme_q[(size_t)r0 * n2 + e], 0.0);
+        const double2* out = fft_lines_block(b0, b1, n2, nl, n2, -1);
+        for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
+            const int b = e / M, k = e - b * M;
+            R.pme_spec[(size_t)(r0 + b) * M + k] = out[b * n2 + k];
+        }
     }
+}
+
+// Lines along axis `axis` (0 or 1) of the half spectrum, kFftLines consecutive
+// k2 per CTA: sign -1 forward, +1 inverse; fuse_g: forward, times G, inverse.
+__global__ void __launch_bounds__(kFftThreads) k_pme_axis(const RepDev* __restrict__ rep, int axis, int sign,
+                                                          int fuse_g) {
+    const RepDev& R = *rep;
+    if (pme_clean(R)) return;
+    extern __shared__ __align__(16) double2 fbuf[];
+    const int n0 = R.pme_n[0], n1 = R.pme_n[1], M = R.pme_n[2] / 2 + 1;
+    const int n = axis == 0 ? n0 : n1, other = axis == 0 ? n1 : n0;
+    const size_t stride = axis == 0 ? (size_t)n1 * M : (size_t)M;
+    const int kb = (M + kFftLines - 1) / kFftLines;
+    double2 *b0 = fbuf, *b1 = fbuf + kFftLines * n;
+    for (int w = blockIdx.x; w < other * kb; w += gridDim.x) {
+        const int o = w / kb, k0 = (w - o * kb) * kFftLines;
+        const int nl = min(kFftLines, M - k0);
+        const size_t base = (axis == 0 ? (size_t)o * M : (size_t)o * n1 * M) + k0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < n * kFftLines; e += blockDim.x) {  // consecutive threads: consecutive k2
+            const int i = e / kFftLines, b = e - i * kFftLines;
+            if (b < nl) b0[b * n + i] = R.pme_spec[base + (size_t)i * stride + b];
+        }
+        double2* out = fft_lines_block(b0, b1, n, nl, n, fuse_g ? -1 : sign);
+        if (fuse_g) {
+            for (int e = threadIdx.x; e < n * kFftLines; e += blockDim.x) {
+                const int i = e / kFftLines, b = e - i * kFftLines;
+                if (b < nl) {
+                    const double g = R.pme_g[base + (size_t)i * stride + b];
+                    double2& v = out[b * n + i];
+                    v.x *= g;
+                    v.y *= g;
+                }
+            }
+            double2* other_buf = out == b0 ? b1 : b0;
+            out = fft_lines_block(out, other_buf, n, nl, n, 1);
+        }
+        for (int e = threadIdx.x; e < n * kFftLines; e += blockDim.x) {
+            const int i = e / kFftLines, b = e - i * kFftLines;
+            if (b < nl) R.pme_spec[base + (size_t)i * stride + b] = out[b * n + i];
+        }
+    }
+}
+
+// Rows along axis 2: half spectrum -> phi (real): the row's full Hermitian
+// extension, inverse transform, real part.
+__global__ void __launch_bounds__(kFftThreads) k_pme_rows_c2r(const RepDev* __restrict__ rep) {
+    const RepDev& R = *rep;
+    if (pme_clean(R)) return;
+    extern __shared__ __align__(16) double2 fbuf[];
+    const int n0 = R.pme_n[0], n1 = R.pme_n[1], n2 = R.pme_n[2], M = n2 / 2 + 1;
+    const int rows = n0 * n1;
+    double2 *b0 = fbuf, *b1 = fbuf + kFftLines * n2;
+    double* phi = const_cast<double*>(R.pme_phi);
+    for (int r0 = blockIdx.x * kFftLines; r0 < rows; r0 += gridDim.x * kFftLines) {
+        const int nl = min(kFftLines, rows - r0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nl * n2; e += blockDim.x) {
+            const int b = e / n2, k = e - b * n2;
+            const double2* row = R.pme_spec + (size_t)(r0 + b) * M;
+            double2 v;
+            if (k < M) {
+                v = row[k];
+            } else {
+                v = row[n2 - k];
+                v.y = -v.y;
+            }
+            b0[e] = v;
+        }
+        const double2* out = fft_lines_block(b0, b1, n2, nl, n2, 1);
+        for (int e = threadIdx.x; e < nl * n2; e += blockDim.x) phi[(size_t)r0 * n2 + e] = out[e].x;
+    }
+}
+
+// The mesh potential is current again.
+__global__ void k_pme_done(const RepDev* __restrict__ rep) {
+    if (threadIdx.x == 0) *rep->pme_dirty = 0;
+}
+
+// Spread the change of an accepted move's site: charge q leaves (x0, y0, z0)
+// and arrives at (x1, y1, z1) (either side skipped when its flag is false).
+__device__ __forceinline__ void pme_move_site(const RepDev& R, bool from, float x0, float y0, float z0, bool to,
+                                              float x1, float y1, float z1, float q) {
+    if (q == 0.0f) return;
+    if (from) pme_spread_one(R, R.pme_q, x0, y0, z0, -(double)q);
+    if (to) pme_spread_one(R, R.pme_q, x1, y1, z1, (double)q);
 }
 
 // phi at caller points (diagnostics)
@@ -153,6 +272,68 @@ __device__ __forceinline__ double pme_pose_lane(const RepDev& R, int ns, int lan
         e -= (double)kCoulomb * (double)q * (double)m;
     }
     return e;
+}
+
+// Gradient of pme_pose_lane's terms with respect to lane `lane`'s site
+// position (< ns; zero otherwise): q grad phi(r_s) from the derivative of the
+// B-spline interpolation (d/dx = (n / L) d/du), minus K q sum_t q_t g'(d) d/|d|
+// over the replaced group's atoms (d = r_s - x_t, minimum image).
+__device__ __forceinline__ void pme_grad_lane(const RepDev& R, int ns, int lane, float sx, float sy, float sz,
+                                              float q, int self, float& gx, float& gy, float& gz) {
+    gx = gy = gz = 0.0f;
+    if (lane >= ns || q == 0.0f) return;
+    double mx[4], my[4], mz[4], dx[4], dy[4], dz[4];
+    const double ux = mesh_u(R, sx, 0), uy = mesh_u(R, sy, 1), uz = mesh_u(R, sz, 2);
+    const double fx = floor(ux), fy = floor(uy), fz = floor(uz);
+    bspline4(ux - fx, mx);
+    bspline4(uy - fy, my);
+    bspline4(uz - fz, mz);
+    bspline4_d(ux - fx, dx);
+    bspline4_d(uy - fy, dy);
+    bspline4_d(uz - fz, dz);
+    const int n0 = R.pme_n[0], n1 = R.pme_n[1], n2 = R.pme_n[2];
+    double px = 0.0, py = 0.0, pz = 0.0;
+    for (int a = 0; a < 4; ++a) {
+        const int i0 = wrapm((int)fx - a, n0);
+        for (int b = 0; b < 4; ++b) {
+            const int i1 = wrapm((int)fy - b, n1);
+            const double* row = R.pme_phi + ((size_t)i0 * n1 + i1) * n2;
+            double t = 0.0, tz = 0.0;
+            for (int c = 0; c < 4; ++c) {
+                const double v = row[wrapm((int)fz - c, n2)];
+                t += mz[c] * v;
+                tz += dz[c] * v;
+            }
+            px += dx[a] * my[b] * t;
+            py += mx[a] * dy[b] * t;
+            pz += mx[a] * my[b] * tz;
+        }
+    }
+    double g0 = (double)q * px * n0 / (double)R.L[0];
+    double g1 = (double)q * py * n1 / (double)R.L[1];
+    double g2 = (double)q * pz * n2 / (double)R.L[2];
+    if (self >= 0) {  // d/dr_s of -K q sum_t q_t g(|r_s - x_t|), g(r) = erf(alpha r) / r
+        const int2 sp = R.gspan[self];
+        const double al = (double)R.pme_alpha, c = 1.1283791670955126 * al;  // 2 alpha / sqrt(pi)
+        for (int t = 0; t < sp.y; ++t) {
+            const float4 at = R.xyzq[sp.x + t];
+            double ex = (double)sx - at.x, ey = (double)sy - at.y, ez = (double)sz - at.z;
+            ex -= rint(ex / (double)R.L[0]) * (double)R.L[0];
+            ey -= rint(ey / (double)R.L[1]) * (double)R.L[1];
+            ez -= rint(ez / (double)R.L[2]) * (double)R.L[2];
+            const double r = sqrt(ex * ex + ey * ey + ez * ez);
+            // g'(r) / r (a smooth even function: -(4/3) alpha^3 / sqrt(pi) at r = 0)
+            const double gp = r < 1e-4 ? -(2.0 / 3.0) * c * al * al
+                                       : (c * exp(-al * al * r * r) * r - erf(al * r)) / (r * r * r);
+            const double w = -(double)kCoulomb * q * at.w * gp;
+            g0 += w * ex;
+            g1 += w * ey;
+            g2 += w * ez;
+        }
+    }
+    gx = (float)g0;
+    gy = (float)g1;
+    gz = (float)g2;
 }
 
 }  // namespace gcmc
