@@ -728,11 +728,11 @@ def run_ours_forcebias(args, ws, rank, local):
     return out
 
 
-LARGE_WORKLOAD = ("large periodic slab with Ewald electrostatics: 150 x 150 x 120 A box, 200000 fixed atoms "
-                  "(random-walk chains, 0.09 atoms/A^3, 12 A pore along z), 8 fragment types + TIP3P water "
-                  "(15827 waters, 178915 slots), smooth PME 128 x 128 x 96, order 4, alpha 0.32, FP64 mesh, "
-                  "cutoff 12 A, reference move semantics; REPLICAS replicas of the system (own RNG streams) "
-                  "in one context")
+LARGE_WORKLOAD = ("large periodic slab with Ewald electrostatics and force-biased moves: 150 x 150 x 120 A "
+                  "box, 200000 fixed atoms (random-walk chains, 0.09 atoms/A^3, 12 A pore along z), 8 fragment "
+                  "types + TIP3P water (15827 waters, 178915 slots), smooth PME 128 x 128 x 96, order 4, alpha "
+                  "0.32, FP64 mesh, cutoff 12 A, force-biased translate / rotate (Metropolis-Hastings "
+                  "corrected); REPLICAS replicas of the system (own RNG streams) in one context")
 
 
 def run_ours_large(args, ws, rank, local):
@@ -748,7 +748,8 @@ def run_ours_large(args, ws, rank, local):
     t0 = time.perf_counter()
     base = S.slab_system(seed=args.seed + rank, mcsteps=total)
     t_gen = time.perf_counter() - t0
-    opt = default_options(pme=1, pme_alpha=0.32, branches=min(4, nrep))
+    # force-biased translate / rotate under Ewald, as the large configuration asks
+    opt = default_options(pme=1, pme_alpha=0.32, branches=min(4, nrep), proposal=2)
     for a, n in enumerate((128, 128, 96)):
         opt.pme_grid[a] = n
     eng = Engine([base.copy() for _ in range(nrep)], opt)
@@ -794,7 +795,7 @@ def run_ours_large(args, ws, rank, local):
         "config": {"workload": LARGE_WORKLOAD.replace("REPLICAS", str(nrep)), "replicas_per_gpu": nrep,
                    "mc_steps_per_bench_step": chunk, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (state + meshes of all replicas)", "generate_s": round(t_gen, 2),
-                   "proposals": "reference (force-biased moves run without Ewald)"},
+                   "proposals": "force-biased translate / rotate (h 0.5 A, 10 deg), uniform SO(3) insertion"},
         "e2e": {"value": round(min(args.steps, 3) * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
                 "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
@@ -804,7 +805,10 @@ def run_ours_large(args, ws, rank, local):
                      "peak_source": f"nominal FP32: {sms} SMs x 128 lanes x 2 x {sm_max:.0f} MHz",
                      "avg_step_us_pme_and_energy": e_ms / 16 * 1e3, "avg_accept_us": a_ms / 16 * 1e3,
                      "traffic": None},
-        "gpu_launches": args.steps * (2 + 32 * ((chunk + 31) // 32) * (2 * nrep + 2 * opt.branches)),
+        # per chunk: k_set_run_end, k_prepare; per graph step: each replica's six mesh-update
+        # launches (which return at once when no charge moved), then per branch two force-bias
+        # pose-energy launches and the accept kernel
+        "gpu_launches": args.steps * (2 + 32 * ((chunk + 31) // 32) * (6 * nrep + 3 * opt.branches)),
         "clocks": clk,
     }
 
@@ -930,6 +934,10 @@ def run_probe(args):
                               pair_delta=args.pair_delta)
     else:
         opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 2, pair_delta=args.pair_delta)
+    if args.probe_pme > 0:  # Ewald electrostatics on a probe_pme^3 mesh
+        opt.pme = 1
+        for a in range(3):
+            opt.pme_grid[a] = args.probe_pme
     with Engine(s, opt) as eng:
         eng.run(args.probe_warm)
         eng.sync()
@@ -974,6 +982,7 @@ def main():
                          "steps launched kernel by kernel (per-kernel times printed; no bench line)")
     ap.add_argument("--probe-warm", type=int, default=64)
     ap.add_argument("--probe-steps", type=int, default=24)
+    ap.add_argument("--probe-pme", type=int, default=0, help="probe: Ewald electrostatics on an N^3 mesh")
     ap.add_argument("--pair-delta", type=int, default=0,
                     help="probe: translate/rotate changes in the pairwise-difference form (0) or as two evaluations (-1)")
     ap.add_argument("--write-inputs", default="", help=argparse.SUPPRESS)  # reference arm's child process

@@ -343,7 +343,9 @@ struct StepDesc {
     int dual;      // translate / rotate in the pairwise-difference form: items k * nslab, each
                    // writing the slab's energy change in the new variant's partial and 0 in the old's
     int margin;    // cells the window reaches beyond R (dual translate steps)
-    int pad;
+    int queue[2];  // pose-energy work counters of a launch whose first replica this is: [0] plain or
+                   // all items, [1] difference-form items; each launch's last CTA resets its counter
+    int done[2];   //   and this count of finished CTAs to 0
     U4 perm_key;
 };
 

@@ -1043,9 +1043,12 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // steps not in the difference form, 1 only those of steps in it (a batch runs
 // the two kinds as separate launches, so that an SM holds one code path's
 // instructions at a time).
+// queue (optional): a counter, zero before the launch, from which warps take
+// their next item (the items' results do not depend on which warp takes them);
+// without it warp g takes items g, g + nwarps, ...
 template <int Which>
 __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, int nrep, int mode, int gw0,
-                                             int nwarps, WarpBuf& B, int* pre, int* wtot) {
+                                             int nwarps, WarpBuf& B, int* pre, int* wtot, int* queue = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     items_prefix(nrep, pre, wtot, [&](int r) {
         const StepDesc* d = reps[r].desc;
@@ -1053,7 +1056,13 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
     });
     const int total = pre[nrep];
     const bool sym = total > nwarps;  // more items than warps: throughput-bound
-    for (int it = gw0 + warp; it < total; it += nwarps) {
+    auto next_item = [&](int prev) {
+        if (!queue) return prev < 0 ? gw0 + warp : prev + nwarps;
+        int v = 0;
+        if (lane == 0) v = atomicAdd(queue, 1);
+        return __shfl_sync(kFull, v, 0);
+    };
+    for (int it = next_item(-1); it < total; it = next_item(it)) {
         int lo = 0, hi = nrep;  // find r with pre[r] <= it < pre[r+1]
         while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
         const RepDev& R = reps[lo];
@@ -1113,8 +1122,25 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     __shared__ int pre[257];
     __shared__ int wtot[32];
     if (mode == 2 && *reps[0].valid) return;
+    // several replicas (throughput-bound launches): warps take items from a counter, which
+    // balances uneven items; one replica (latency-bound, about one item per warp): a fixed
+    // stride, which saves the counter's round trip per item
+    StepDesc* d0 = reps[0].desc;
+    const int q = Which == 1 ? 1 : 0;
     energy_items<Which>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre,
-                        wtot);
+                        wtot, nrep > 1 ? &d0->queue[q] : nullptr);
+    if (nrep == 1) return;
+    // the last CTA to finish resets the counter for the next launch (every warp has taken
+    // its last item once its CTA arrives here)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&d0->done[q], 1) == (int)gridDim.x - 1) {
+            d0->queue[q] = 0;
+            d0->done[q] = 0;
+            __threadfence();
+        }
+    }
 }
 
 template __global__ void k_energy_t<3, -1>(const RepDev* __restrict__, int, int);
