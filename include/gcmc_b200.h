@@ -145,6 +145,11 @@ typedef struct {
     int32_t persist_spin_cap; /* polls a CTA waits at the persistent loop's grid
                             barrier before it gives up, raises device error bit 5
                             and ends the launch (0 = 2^24, over a second)        */
+    int32_t pose_split;  /* per-pose-warp kernel: 0 = every pose's cell window split into
+                            the same number of ranges; 1 = each pose's window split in
+                            proportion to its estimated work (the fixed atoms in the
+                            windows of its centre's cell), the same total (an
+                            autotuner candidate; slower than 0 on one replica)      */
 } gcmc_options;
 
 /* One autotuner trial (gcmc_autotune). */

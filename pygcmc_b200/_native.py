@@ -23,7 +23,7 @@ class Options(ctypes.Structure):
                 ("step_offset", ctypes.c_uint32), ("pme", c_int), ("pme_alpha", ctypes.c_float),
                 ("pme_grid", c_int * 3), ("energy_variant", c_int), ("speculate", c_int),
                 ("energy_kernel", c_int), ("tile_cells", c_int), ("pair_delta", c_int),
-                ("persistent", c_int), ("persist_spin_cap", c_int)]
+                ("persistent", c_int), ("persist_spin_cap", c_int), ("pose_split", c_int)]
 
 
 class TuneTrial(ctypes.Structure):

@@ -177,6 +177,56 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return v;
 }
 
+// Per-pose ranges of the per-pose-warp kernel in proportion to each pose
+// variant's work, estimated as the fixed atoms in the windows of its centre's
+// cell (wcost) plus kCellWork atoms' worth per window cell: the poses inside a
+// dense protein get more, and shorter, ranges than those in the open box, so
+// that the items of one launch take similar times.  Whole CTA; scratch: 2 *
+// kMaxPoses ints.  Slots s = v k + i (the new variants first, so that the
+// new-variant items are the list's first ones; a step in the difference form has
+// v = 0 only); entry e = i nvar + v.  The total stays the uniform split's
+// `budget` items (up to rounding).  Writes pnslab and pitem; returns the item
+// count and the largest split in *nmax.
+constexpr int kCellWork = 4;
+__device__ int split_entries(const RepDev& R, const StepDesc& D, int budget, int* scratch, int* wtot, int* nmax_sh) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int nv = D.dual ? 1 : D.nvar;
+    const int nslots = D.k * nv;
+    const int startRes = D.move == MV_INSERT ? 0 : R.frag[D.ftype].startRes;
+    const int nwin = R.span[0] * R.span[1] * R.span[2];
+    const int cap = min(255, R.max_split * (D.dual ? 2 : 1));
+    auto cost = [&](int s) {
+        const int v = s / D.k, i = s - v * D.k;
+        float4 c;
+        if (D.move == MV_INSERT || D.move == MV_DELETE || (v == 0 && !D.dual)) c = R.pcen[i];
+        else c = R.gcen[startRes + R.pslot[i]];
+        return R.wcost[cell_of(R, c.x, c.y, c.z)] + kCellWork * nwin;
+    };
+    for (int s = tid; s < nslots; s += nt) scratch[s] = cost(s);
+    if (tid == 0) *nmax_sh = 1;
+    __syncthreads();
+    const double total = (double)block_excl_scan(scratch, nslots, wtot);
+    for (int s = tid; s < nslots; s += nt) {
+        const int n = max(1, min(cap, (int)((double)budget * (double)cost(s) / total + 0.5)));
+        scratch[s] = n;
+        const int v = s / D.k, i = s - v * D.k;
+        const int e = i * D.nvar + v;
+        R.pnslab[e] = n;
+        if (D.dual) R.pnslab[e + 1] = n;  // the old variant's zero partials
+        atomicMax(nmax_sh, n);
+    }
+    __syncthreads();
+    const int items = block_excl_scan(scratch, nslots, wtot);
+    for (int s = tid; s < nslots; s += nt) {
+        const int v = s / D.k, i = s - v * D.k;
+        const int e = i * D.nvar + v;
+        const int off = scratch[s], n = (s + 1 < nslots ? scratch[s + 1] : items) - off;
+        for (int z = 0; z < n; ++z) R.pitem[off + z] = (e << 8) | z;
+    }
+    __syncthreads();
+    return items;
+}
+
 // ---- next-step preparation (whole CTA) ----
 // scratch: kBinScratchBytes of shared memory for the tiled contexts' pose binning.
 __device__ void prepare_step(const RepDev& R, int step, int* scratch) {
@@ -259,14 +309,25 @@ __device__ void prepare_step(const RepDev& R, int step, int* scratch) {
             R.pcen[i] = c;
         }
     }
+    __shared__ int nmax_sh;
     if (R.tiled && D.move != MV_NONE && D.k > 0) {
         __syncthreads();  // centres and slots written above
         const int ntiles = bin_entries(R, D, scratch, wtot_sh);
         if (tid == 0) Dsh.items = ntiles;
+    } else if (R.wcost && D.move != MV_NONE && D.k > 0 && !R.fb) {  // (the force-bias kernel splits alike)
+        __syncthreads();  // centres and slots written above
+        const int items = split_entries(R, D, D.items, scratch, wtot_sh, &nmax_sh);
+        if (tid == 0) {
+            Dsh.items = items;
+            Dsh.nslab = nmax_sh;
+            Dsh.varslab = 1;
+        }
     }
     if (tid == 0) {
         StepDesc Dw = D;
         Dw.items = Dsh.items;
+        Dw.nslab = Dsh.nslab;
+        Dw.varslab = Dsh.varslab;
         *R.desc = Dw;
     }
     __syncthreads();
@@ -527,10 +588,12 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
     const double* ep = stage_e ? Ep : R.epart;
     for (int i = tid; i < k; i += nt) {
         double e = 0.0;
-        for (int z = 0; z < D.nslab; ++z) e += ep[(i * D.nvar) * D.nslab + z];
+        const int n0 = D.varslab ? R.pnslab[i * D.nvar] : D.nslab;
+        for (int z = 0; z < n0; ++z) e += ep[(i * D.nvar) * D.nslab + z];
         if (D.nvar == 2) {
+            const int n1 = D.varslab ? R.pnslab[i * 2 + 1] : D.nslab;
             double eo = 0.0;
-            for (int z = 0; z < D.nslab; ++z) eo += ep[(i * 2 + 1) * D.nslab + z];
+            for (int z = 0; z < n1; ++z) eo += ep[(i * 2 + 1) * D.nslab + z];
             e = e - eo;
         }
         e += bg;

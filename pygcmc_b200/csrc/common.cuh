@@ -343,6 +343,9 @@ struct StepDesc {
     int dual;      // translate / rotate in the pairwise-difference form: items k * nslab, each
                    // writing the slab's energy change in the new variant's partial and 0 in the old's
     int margin;    // cells the window reaches beyond R (dual translate steps)
+    int varslab;   // 1: the per-pose-warp kernel's items come from pitem, each pose variant split
+                   // into pnslab ranges in proportion to its window's work (nslab: their maximum)
+    int pad2[3];
     int queue[2];  // pose-energy work counters of a launch whose first replica this is: [0] plain or
                    // all items, [1] difference-form items; each launch's last CTA resets its counter
     int done[2];   //   and this count of finished CTAs to 0
@@ -440,6 +443,12 @@ struct RepDev {
     int tspan[3];
     int* pbin;          // [2 * kMaxPoses]
     int4* tiles;        // [2 * kMaxPoses]
+    // per-pose splits of the per-pose-warp kernel: each cell's window work (atoms of the fixed
+    // groups in the cells within R of it), and per step the ranges of each pose variant
+    // (entry e = i * nvar + v) and the item list (e << 8 | range)
+    const int* wcost;   // [ncell]
+    int* pnslab;        // [2 * kMaxPoses]
+    int* pitem;         // [2 * kMaxPoses * slab cap]
     // translate / rotate energy changes in the pairwise-difference form (dual = 1):
     // one work item per pose evaluates the old and the new pose together over the
     // groups within the cutoff of either centre; a translate's new centre lies

@@ -910,8 +910,8 @@ __device__ __forceinline__ void pose_draws(const RepDev& R, const StepDesc& D, i
 // "within cutoff" bit matrix (host distance form, bit-exact).  The row of pose
 // 32 w also makes the energy-independent draws of the 32 poses of word w, one
 // per lane.
-__device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int i, int zi, int lane) {
-    const int w0 = zi * D.nw / D.nslab, w1 = (zi + 1) * D.nw / D.nslab;
+__device__ __forceinline__ void nbr_rows(const RepDev& R, const StepDesc& D, int i, int zi, int nsl, int lane) {
+    const int w0 = zi * D.nw / nsl, w1 = (zi + 1) * D.nw / nsl;
     const float4 ci = R.pcen[i];
     for (int w = w0; w < w1; ++w) {
         const int j = 32 * w + lane;
@@ -984,12 +984,14 @@ __device__ __forceinline__ void nbr_block(const RepDev& R, const StepDesc& D, in
 // nw (nw + 1) / 2 items compute a block each (half the distance tests);
 // otherwise every item computes its slab's share of pose i's row, which keeps
 // each item's latency short.  Both give the same matrix.
-__device__ __forceinline__ void nbr_share(const RepDev& R, const StepDesc& D, int i, int zi, int lane, bool sym) {
+// (i, zi): the item's pose and range of nsl; task: its index among the step's
+// new-variant items (at least k of them, more than the nw (nw + 1) / 2 blocks).
+__device__ __forceinline__ void nbr_share(const RepDev& R, const StepDesc& D, int i, int zi, int nsl, int task,
+                                          int lane, bool sym) {
     if (sym) {
-        const int p = i * D.nslab + zi;
-        if (p < D.nw * (D.nw + 1) / 2) nbr_block(R, D, p, lane);
+        if (task < D.nw * (D.nw + 1) / 2) nbr_block(R, D, task, lane);
     } else {
-        nbr_rows(R, D, i, zi, lane);
+        nbr_rows(R, D, i, zi, nsl, lane);
     }
 }
 
@@ -1068,11 +1070,23 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
         const RepDev& R = reps[lo];
         const StepDesc D = *R.desc;
         const int local = it - pre[lo];
-        // pose fastest: the ranges of one pose go to different CTAs (and SMs), so the
-        // items of a heavy pose do not share one SM's issue slots
-        const int q = local / max(1, D.k);
-        const int i = local - q * D.k;
-        const int v = q / D.nslab, zi = q - v * D.nslab;
+        int i, v, zi, nsl;
+        if (D.varslab) {  // the preparation's list: pose variant e's range zi of pnslab[e]
+            const int pk = R.pitem[local];
+            const int e = pk >> 8;
+            zi = pk & 255;
+            i = e / D.nvar;
+            v = e - i * D.nvar;
+            nsl = R.pnslab[e];
+        } else {
+            // pose fastest: the ranges of one pose go to different CTAs (and SMs), so the
+            // items of a heavy pose do not share one SM's issue slots
+            const int q = local / max(1, D.k);
+            i = local - q * D.k;
+            v = q / D.nslab;
+            zi = q - v * D.nslab;
+            nsl = D.nslab;
+        }
         float cx, cy, cz;
         int self;
         double acc = 0.0;
@@ -1085,7 +1099,7 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
             const int nwin = dc.ws[0] * dc.ws[1] * dc.ws[2];
             DualSink sink;
             walk_cells<DualSink, true>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, sink, ng,
-                                       npair, mode == 1 ? R.abort : nullptr, D.step, D.nslab, &dc);
+                                       npair, mode == 1 ? R.abort : nullptr, D.step, nsl, &dc);
             acc = sink.acc;
         } else if (Which != 1) {
             build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
@@ -1094,7 +1108,7 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
             // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
             // range samples the whole cutoff sphere and the ranges of a pose take equal time)
             energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
-                         mode == 1 ? R.abort : nullptr, D.step, D.nslab);
+                         mode == 1 ? R.abort : nullptr, D.step, nsl);
             if (R.pme && zi == 0) {
                 const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
                 acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
@@ -1109,7 +1123,8 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
         if (v == 0 && D.nw > 0) {
             int stop = 0;
             if (mode == 1 && lane == 0) stop = *reinterpret_cast<const volatile int*>(R.abort) == D.step;
-            if (!__shfl_sync(kFull, stop, 0)) nbr_share(R, D, i, zi, lane, sym);
+            if (!__shfl_sync(kFull, stop, 0))
+                nbr_share(R, D, i, zi, nsl, D.varslab ? local : i * D.nslab + zi, lane, sym);
         }
         __syncwarp();
     }

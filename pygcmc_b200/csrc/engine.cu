@@ -86,6 +86,11 @@ struct RepHost {
     int4* tiles = nullptr;     //   and its tiles
     int* pbin2 = nullptr;      //   (the speculating copy's)
     int4* tiles2 = nullptr;
+    int* wcost = nullptr;      // per-pose-warp kernel: each cell's window work (fixed atoms)
+    int* pnslab = nullptr;     //   the step's ranges per pose variant
+    int* pitem = nullptr;      //   and its item list
+    int* pnslab2 = nullptr;    //   (the speculating copy's)
+    int* pitem2 = nullptr;
     float* fpart = nullptr;
     float4* fbprop = nullptr;
     int* fbcnt = nullptr;
@@ -190,6 +195,7 @@ void free_rep(RepHost& h) {
     dfree(h.psite2); dfree(h.valid2); dfree(h.abort2); dfree(h.sstep2); dfree(h.pending2); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g); dfree(h.pme_dirty);
     dfree(h.pbin); dfree(h.tiles); dfree(h.pbin2); dfree(h.tiles2);
+    dfree(h.wcost); dfree(h.pnslab); dfree(h.pitem); dfree(h.pnslab2); dfree(h.pitem2);
     h.capn.clear();
 }
 
@@ -522,12 +528,52 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.fbcnt, kMaxPoses); AL(h.pgum, kMaxPoses); AL(h.plnu, kMaxPoses);
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
     AL(h.pbin, 2 * kMaxPoses); AL(h.tiles, 2 * kMaxPoses);
+    AL(h.wcost, h.ncell); AL(h.pnslab, 2 * kMaxPoses); AL(h.pitem, (size_t)2 * kMaxPoses * h.slab_cap);
     AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
     if (ctx->spec) {
         AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.slab_cap);
         AL(h.nbr2, (size_t)kMaxPoses * kMaxWords); AL(h.pgum2, kMaxPoses); AL(h.plnu2, kMaxPoses);
         AL(h.psite2, (size_t)kMaxPoses * kMaxSites); AL(h.valid2, 2); AL(h.abort2, 2); AL(h.sstep2, 2);
         AL(h.pending2, 2); AL(h.pbin2, 2 * kMaxPoses); AL(h.tiles2, 2 * kMaxPoses);
+        AL(h.pnslab2, 2 * kMaxPoses); AL(h.pitem2, (size_t)2 * kMaxPoses * h.slab_cap);
+    }
+    // each cell's window work: the fixed atoms in the cells within R of it (box sums along
+    // each axis, periodic; the whole axis where the window spans it)
+    if (opt.pose_split > 0) {
+        const int n0 = d.nc[0], n1 = d.nc[1], n2 = d.nc[2];
+        std::vector<int> cnt((size_t)h.ncell, 0), tmp((size_t)h.ncell, 0);
+        for (int g = 0; g < d.nfixed; ++g) {
+            int c[3];
+            for (int a = 0; a < 3; ++a) {
+                const double u = ((double)in.residueInfo[g].position[a] - (double)d.start[a]) * (double)d.invLc[a];
+                int x = (int)std::floor(u);
+                x %= d.nc[a];
+                c[a] = x < 0 ? x + d.nc[a] : x;
+            }
+            cnt[((size_t)c[2] * n1 + c[1]) * n0 + c[0]] += in.residueInfo[g].atomNum;
+        }
+        auto box = [&](std::vector<int>& src, std::vector<int>& dst, int a) {
+            const int n = d.nc[a], R = d.range;
+            const bool whole = d.span[a] == n;
+            for (int z = 0; z < n2; ++z)
+                for (int y = 0; y < n1; ++y)
+                    for (int x = 0; x < n0; ++x) {
+                        int co[3] = {x, y, z};
+                        long long sum = 0;
+                        const int lo = whole ? 0 : co[a] - R, hi = whole ? n - 1 : co[a] + R;
+                        for (int t = lo; t <= hi; ++t) {
+                            int q[3] = {x, y, z};
+                            q[a] = ((t % n) + n) % n;
+                            sum += src[((size_t)q[2] * n1 + q[1]) * n0 + q[0]];
+                        }
+                        dst[((size_t)z * n1 + y) * n0 + x] = (int)std::min<long long>(sum, 1ll << 30);
+                    }
+        };
+        box(cnt, tmp, 0);
+        box(tmp, cnt, 1);
+        box(cnt, tmp, 2);
+        CK(cudaMemcpyAsync(h.wcost, tmp.data(), sizeof(int) * h.ncell, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));  // tmp is a host temporary
     }
     // smooth PME: mesh and influence function
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
@@ -637,11 +683,14 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.energy = h.energy; d.pgum = h.pgum; d.psite = h.psite; d.plnu = h.plnu; d.fpart = h.fpart; d.fbprop = h.fbprop; d.fbcnt = h.fbcnt;
     d.logF = (h.log_cap > 0 && d.fb) ? h.logF : nullptr;
     d.pbin = h.pbin; d.tiles = h.tiles;
+    d.wcost = opt.pose_split > 0 ? h.wcost : nullptr;
+    d.pnslab = h.pnslab; d.pitem = h.pitem;
     if (ctx->spec) {
         RepDev& b = ctx->repdev_b;
         b = d;
         b.desc = h.desc2; b.pcen = h.pcen2; b.pslot = h.pslot2; b.epart = h.epart2; b.nbr = h.nbr2;
         b.pgum = h.pgum2; b.plnu = h.plnu2; b.psite = h.psite2; b.pbin = h.pbin2; b.tiles = h.tiles2;
+        b.pnslab = h.pnslab2; b.pitem = h.pitem2;
         d.valid = h.valid2; d.pairs_pending = h.pending2; d.abort = h.abort2; d.spec_step = h.sstep2;
         b.valid = h.valid2 + 1; b.pairs_pending = h.pending2 + 1; b.abort = h.abort2 + 1; b.spec_step = h.sstep2 + 1;
     }
@@ -685,8 +734,9 @@ void launch_energy(const gcmc_ctx* ctx, const RepDev* reps, int n, int mode, int
     }
 }
 
-// Dynamic shared memory of the preparation kernels (the pose binning's scratch).
-size_t prep_smem(const gcmc_ctx* ctx) { return ctx->tiled ? (size_t)kBinScratchBytes : 0; }
+// Dynamic shared memory of the preparation kernels (the pose binning's or the
+// per-pose split's scratch).
+size_t prep_smem(const gcmc_ctx*) { return (size_t)kBinScratchBytes; }
 
 // The context is tiled when every replica allows it; otherwise no replica is.
 void finalize_tiling(gcmc_ctx* ctx) {
@@ -1413,6 +1463,11 @@ int gcmc_autotune(int32_t nrep, const gcmc_replica_in* reps, const gcmc_options*
             if (e == base_e) continue;
             gcmc_options o = cur;
             o.energy_blocks_per_sm = e;
+            if (st == GCMC_OK) st = consider(o);
+        }
+        {
+            gcmc_options o = cur;
+            o.pose_split = cur.pose_split > 0 ? 0 : 1;
             if (st == GCMC_OK) st = consider(o);
         }
     }

@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
                 R.pcen[i] = fb_propose(R, D, i, fo, gc, R.fbprop + 2 * i);
             }
         } else if (v == 0 && D.nw > 0) {  // this item's share of the neighbour bit matrix
-            nbr_share(R, D, i, zi, lane, sym);
+            nbr_share(R, D, i, zi, D.nslab, i * D.nslab + zi, lane, sym);
         }
         __syncwarp();
     }

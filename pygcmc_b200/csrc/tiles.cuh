@@ -601,7 +601,7 @@ __device__ void tile_item(const RepDev& R, const StepDesc& D, int li, TileSmem& 
             for (int p = warp; p < P; p += kWarpsT) {
                 const int e = T.entry[p];
                 const int i = e / D.nvar, v = e - i * D.nvar;
-                if (v == 0) nbr_rows(R, D, i, 0, lane);
+                if (v == 0) nbr_rows(R, D, i, 0, 1, lane);
             }
         }
     }

@@ -379,3 +379,10 @@ def test_trajectory_water_pair_image(oracle_lib, water_small, kernel, tile_cells
     with one-cell pose blocks (more tiles than the default for a small box) and
     the per-pose-warp kernel, translate / rotate changes in the difference form."""
     check_trajectory(oracle_lib, water_small, 96, energy_kernel=kernel, tile_cells=tile_cells)
+
+
+@pytest.mark.parametrize("which,proposal", [("protein_small", 0), ("water_small", 1)])
+def test_trajectory_proportional_pose_split(request, oracle_lib, which, proposal):
+    """The per-pose ranges in proportion to each pose's estimated window work
+    (pose_split 1): the trajectory replays on the oracle as with uniform ranges."""
+    check_trajectory(oracle_lib, request.getfixturevalue(which), 96, proposal=proposal, pose_split=1)

@@ -15,10 +15,10 @@ pytestmark = pytest.mark.gpu
 LOG_KMAX = 1024
 
 
-def _run(system, nsteps, speculate, chunks=None, kernel=0):
+def _run(system, nsteps, speculate, chunks=None, kernel=0, **kw):
     from pygcmc_b200._native import default_options
     from pygcmc_b200.engine import Engine
-    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, speculate=speculate, energy_kernel=kernel)
+    opts = default_options(log_steps=nsteps, log_kmax=LOG_KMAX, speculate=speculate, energy_kernel=kernel, **kw)
     with Engine(system.copy(), opts) as eng:
         if chunks is None:
             eng.run(nsteps)
@@ -105,3 +105,10 @@ def test_dropin_refills_switching_speculation(protein_small, water_small):
         a = _occupied_atoms(s)
         assert np.array_equal(s.atomInfo["position"][a], fin.atomInfo["position"][a])
     assert lib().gcmc_release_cache() == 0
+
+
+def test_speculation_with_proportional_pose_split(protein_small):
+    """Per-pose ranges in proportion to the estimated window work (pose_split 1):
+    the speculative and the sequential orders stay bit-identical."""
+    n = int(protein_small.SimInfo[0]["mcsteps"])
+    _same(_run(protein_small, n, 0, pose_split=1), _run(protein_small, n, -1, pose_split=1))
