@@ -525,6 +525,10 @@ __device__ __forceinline__ void void_next(const RepDev& R, int step) {
 // step is marked as standing when nothing was accepted.
 // One replica's step, whole CTA (kAcceptThreads threads); smem_raw: an
 // AcceptSmem.  The body of k_accept and of the persistent step loop.
+// Pme: the replica may run Ewald electrostatics (the background term and the
+// mesh charge updates are compiled in only then; they add registers to every
+// phase of the kernel).
+template <bool Pme>
 __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned char* smem_raw) {
     AcceptSmem& S = *reinterpret_cast<AcceptSmem*>(smem_raw);
     const StepDesc D = *R.desc;
@@ -574,7 +578,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
     // ---- phase 0: pose energies (sum of slab partials; dE for translate/rotate)
     const bool logging = R.log != nullptr && D.step < R.log_cap;
     double bg = 0.0;  // Ewald: change of the neutralising-background energy -bgc Q^2
-    if (R.pme && (D.move == MV_INSERT || D.move == MV_DELETE)) {
+    if (Pme && R.pme && (D.move == MV_INSERT || D.move == MV_DELETE)) {
         double Q = R.pme_qfix;
         for (int t = 0; t < R.ntypes; ++t) Q += (double)R.totalNum[t] * R.frag[t].qnet;
         const double dq = D.move == MV_INSERT ? F.qnet : -F.qnet;
@@ -638,7 +642,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                 if (spec) void_next(R, D.step + 1);
                 const int slot = D.del_slot, last = n - 1;
                 const int gs = F.startRes + slot, gl = F.startRes + last;
-                if (R.pme) {  // the leaving molecule's charges leave the mesh
+                if (Pme && R.pme) {  // the leaving molecule's charges leave the mesh
                     const int2 sd = R.gspan[gs];
                     for (int s = 0; s < ns; ++s) {
                         const float4 a = R.xyzq[sd.x + s];
@@ -841,7 +845,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                     const float4 p = R.psite[i * kMaxSites + lane];
                     R.xyzq[sp.x + lane] = p;
                     R.atype[sp.x + lane] = F.stype[lane];
-                    if (R.pme) pme_move_site(R, false, 0.f, 0.f, 0.f, true, p.x, p.y, p.z, p.w);
+                    if (Pme && R.pme) pme_move_site(R, false, 0.f, 0.f, 0.f, true, p.x, p.y, p.z, p.w);
                 }
                 if (lane == 0) R.gcen[res] = make_float4(c.x, c.y, c.z, 0.0f);
             }
@@ -868,7 +872,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
                 if (lane < ns) {  // moved sites as built by the pose-energy kernel; the charge stays
                     const float4 p = R.psite[i * kMaxSites + lane];
                     float* dst = reinterpret_cast<float*>(R.xyzq + sp.x + lane);
-                    if (R.pme) {
+                    if (Pme && R.pme) {
                         const float4 o = R.xyzq[sp.x + lane];
                         pme_move_site(R, true, o.x, o.y, o.z, true, p.x, p.y, p.z, o.w);
                     }
@@ -907,7 +911,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
     }
     __syncthreads();
     if (tid == 0) {
-        if (R.pme && D.move != MV_DELETE && S.misc[0] > 0) *R.pme_dirty = 1;  // the mesh charges moved
+        if (Pme && R.pme && D.move != MV_DELETE && S.misc[0] > 0) *R.pme_dirty = 1;  // the mesh charges moved
         if (D.move != MV_DELETE) {  // running energy: accepted moves in commit order
             double et = *R.energy;
             const int na = S.misc[0];
@@ -945,9 +949,12 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
 #undef PHASE
 }
 
+template <bool Pme>
 __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep, int spec) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    accept_step(reps[blockIdx.x], spec, smem_raw);
+    accept_step<Pme>(reps[blockIdx.x], spec, smem_raw);
 }
+template __global__ void k_accept<false>(const RepDev* __restrict__, int, int);
+template __global__ void k_accept<true>(const RepDev* __restrict__, int, int);
 
 }  // namespace gcmc

@@ -246,9 +246,12 @@ __device__ __forceinline__ void flush_atoms_t(const RepDev& R, const WarpBuf& B,
 // This lane's FP64 sum of the pair energies of the buffered atoms.  (Inlined:
 // an out-of-line copy shared by the call sites measured slower, as the call
 // makes the kernels spill around it.)
+// Ew = 0: the replica never runs Ewald electrostatics (the Ewald loops are not
+// compiled in: they add registers to the kernel around them).
+template <int Ew = 1>
 __device__ __forceinline__ double flush_atoms(const RepDev& R, const WarpBuf& B, int na, int ns, int lane) {
     double acc = 0.0;
-    if (R.pme) {
+    if (Ew && R.pme) {
         if (R.pair_image) flush_atoms_t<true, true>(R, B, na, ns, lane, acc);
         else flush_atoms_t<false, true>(R, B, na, ns, lane, acc);
     } else {
@@ -354,10 +357,11 @@ __device__ __forceinline__ void flush_dual(const RepDev& R, const WarpBuf& B, in
 
 // What the cell walk does with each buffer of included atoms: the energy
 // sink sums pair energies; the gradient kernel supplies its own sink.
+template <int Ew = 1>
 struct EnergySink {
     double acc = 0.0;
     __device__ __forceinline__ void flush(const RepDev& R, WarpBuf& B, int na, int ns, int lane) {
-        acc += flush_atoms(R, B, na, ns, lane);
+        acc += flush_atoms<Ew>(R, B, na, ns, lane);
     }
 };
 
@@ -623,11 +627,12 @@ __device__ __forceinline__ void walk_cells(const RepDev& R, WarpBuf& B, int ns, 
     if (Dual) npair += (long long)__reduce_add_sync(kFull, (unsigned)both_atoms) * ns;
 }
 
+template <int Ew = 1>
 __device__ __forceinline__ void energy_cells(const RepDev& R, WarpBuf& B, int ns, float cx, float cy, float cz,
                                              int self, int c0, int c1, int lane, double& acc, int& ngroups,
                                              long long& npair, const int* stop = nullptr, int stop_at = 0,
                                              int stride = 1) {
-    EnergySink sink;
+    EnergySink<Ew> sink;
     sink.acc = acc;
     walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ngroups, npair, stop, stop_at, stride);
     acc = sink.acc;
@@ -1048,7 +1053,7 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // queue (optional): a counter, zero before the launch, from which warps take
 // their next item (the items' results do not depend on which warp takes them);
 // without it warp g takes items g, g + nwarps, ...
-template <int Which>
+template <int Which, int Ew = 1>
 __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, int nrep, int mode, int gw0,
                                              int nwarps, WarpBuf& B, int* pre, int* wtot, int* queue = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1107,9 +1112,9 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
             const int nwin = R.span[0] * R.span[1] * R.span[2];
             // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
             // range samples the whole cutoff sphere and the ranges of a pose take equal time)
-            energy_cells(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
-                         mode == 1 ? R.abort : nullptr, D.step, nsl);
-            if (R.pme && zi == 0) {
+            energy_cells<Ew>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
+                             mode == 1 ? R.abort : nullptr, D.step, nsl);
+            if (Ew && R.pme && zi == 0) {
                 const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
                 acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
             }
@@ -1130,7 +1135,7 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
     }
 }
 
-template <int MinBlocks, int Which>
+template <int MinBlocks, int Which, int Ew>
 __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepDev* __restrict__ reps, int nrep,
                                                                       int mode) {
     __shared__ WarpBuf bufs[kWarpsE];
@@ -1142,8 +1147,8 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     // stride, which saves the counter's round trip per item
     StepDesc* d0 = reps[0].desc;
     const int q = Which == 1 ? 1 : 0;
-    energy_items<Which>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre,
-                        wtot, nrep > 1 ? &d0->queue[q] : nullptr);
+    energy_items<Which, Ew>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5],
+                            pre, wtot, nrep > 1 ? &d0->queue[q] : nullptr);
     if (nrep == 1) return;
     // the last CTA to finish resets the counter for the next launch (every warp has taken
     // its last item once its CTA arrives here)
@@ -1158,12 +1163,14 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     }
 }
 
-template __global__ void k_energy_t<3, -1>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<4, -1>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<3, 0>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<4, 0>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<3, 1>(const RepDev* __restrict__, int, int);
-template __global__ void k_energy_t<4, 1>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, -1, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, -1, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, 0, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, 0, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, 1, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<4, 1, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, -1, 1>(const RepDev* __restrict__, int, int);  // Ewald contexts
+template __global__ void k_energy_t<4, -1, 1>(const RepDev* __restrict__, int, int);
 
 // Energies of caller-supplied poses (gcmc_energy_poses): item = (pose, slab).
 // The replica descriptor is passed by value so that callers can substitute

@@ -712,11 +712,13 @@ int upload_reps(gcmc_ctx* ctx) {
 }
 
 using EnergyKernel = void (*)(const RepDev*, int, int);
-// which: -1 every item; 0 / 1 the items of steps not in / in the difference form
-EnergyKernel energy_kernel(int variant, int which = -1) {
-    if (which == 0) return variant == 1 ? k_energy_t<4, 0> : k_energy_t<3, 0>;
-    if (which == 1) return variant == 1 ? k_energy_t<4, 1> : k_energy_t<3, 1>;
-    return variant == 1 ? k_energy_t<4, -1> : k_energy_t<3, -1>;
+// which: -1 every item; 0 / 1 the items of steps not in / in the difference form;
+// ew: the Ewald code paths compiled in (contexts with a replica under Ewald)
+EnergyKernel energy_kernel(int variant, int which = -1, bool ew = false) {
+    if (ew) return variant == 1 ? k_energy_t<4, -1, 1> : k_energy_t<3, -1, 1>;
+    if (which == 0) return variant == 1 ? k_energy_t<4, 0, 0> : k_energy_t<3, 0, 0>;
+    if (which == 1) return variant == 1 ? k_energy_t<4, 1, 0> : k_energy_t<3, 1, 0>;
+    return variant == 1 ? k_energy_t<4, -1, 0> : k_energy_t<3, -1, 0>;
 }
 
 // One pose-energy launch over replicas reps[0, n) in `mode` on `grid` CTAs:
@@ -724,15 +726,20 @@ EnergyKernel energy_kernel(int variant, int which = -1) {
 void launch_energy(const gcmc_ctx* ctx, const RepDev* reps, int n, int mode, int grid, cudaStream_t s) {
     if (ctx->tiled) {
         k_energy_tiles<<<grid, kWarpsT * 32, sizeof(TileSmem), s>>>(reps, n, mode);
-    } else if (n > 1 && ctx->dual_any) {
+    } else if (n > 1 && ctx->dual_any && !ctx->pme_any) {
         // a batch mixes the two kinds of items: one launch each, so that an SM runs one
         // code path at a time (both in one launch stalled on instruction fetch)
         energy_kernel(ctx->evar, 0)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
         energy_kernel(ctx->evar, 1)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
     } else {
-        energy_kernel(ctx->evar)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+        energy_kernel(ctx->evar, -1, ctx->pme_any)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
     }
 }
+
+// The accept kernel of the context: with the Ewald code paths when a replica
+// runs Ewald electrostatics.
+using AcceptKernel = void (*)(const RepDev*, int, int);
+AcceptKernel accept_kernel(const gcmc_ctx* ctx) { return ctx->pme_any ? k_accept<true> : k_accept<false>; }
 
 // Dynamic shared memory of the preparation kernels (the pose binning's or the
 // per-pose split's scratch).
@@ -899,7 +906,7 @@ int build_spec_graph(gcmc_ctx* ctx, int parity) {
             k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(cur, 1);
             launch_energy(ctx, cur, 1, 2, ctx->gridE, ctx->stream);
             if (e == cudaSuccess) e = cudaEventRecord(evF[i], ctx->stream);
-            k_accept<<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);
+            k_accept<false><<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);  // (speculating: no Ewald)
             if (e == cudaSuccess) e = cudaEventRecord(evA[i], ctx->stream);
             if (i > 0 && e == cudaSuccess) e = cudaStreamWaitEvent(sp, evA[i - 1], 0);
             k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), sp>>>(nxt, 0);
@@ -975,7 +982,7 @@ int build_graph(gcmc_ctx* ctx) {
                 } else {
                     launch_energy(ctx, ctx->d_reps + r0, cnt, 0, grid, side[b]);
                 }
-                k_accept<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt, 0);
+                accept_kernel(ctx)<<<cnt, kAcceptThreads, sizeof(AcceptSmem), side[b]>>>(ctx->d_reps + r0, cnt, 0);
             }
             if (e == cudaSuccess) e = cudaGetLastError();
         }
@@ -1081,7 +1088,9 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     if (st == GCMC_OK && cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) st = upload_reps(ctx);
     if (st == GCMC_OK) {
-        if (cudaFuncSetAttribute(k_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_accept<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(AcceptSmem)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_accept<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(AcceptSmem)) != cudaSuccess)
             st = GCMC_ERR_CUDA;
     }
@@ -1562,7 +1571,7 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
             launch_energy(ctx, ctx->d_reps, ctx->nrep, 0, ctx->gridE, ctx->stream);
         }
         CK(cudaEventRecord(ev[3 * i + 1], ctx->stream));
-        k_accept<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);
+        accept_kernel(ctx)<<<ctx->nrep, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(ctx->d_reps, ctx->nrep, 0);
         CK(cudaEventRecord(ev[3 * i + 2], ctx->stream));
     }
     CK(cudaGetLastError());

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
         long long npair = 0;
         double acc = 0.0;
         if (!fbitem) {
-            EnergySink sink;
+            EnergySink<> sink;
             walk_cells(R, B, ns, cx, cy, cz, self, c0, c1, lane, sink, ng, npair, nullptr, 0, stride);
             acc = warp_sum(sink.acc);
         } else {

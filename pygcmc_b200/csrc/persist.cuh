@@ -74,14 +74,14 @@ __global__ void __launch_bounds__(kAcceptThreads, 1) k_persist(const RepDev* __r
     int* err = reps[0].err;
     for (int s = 0; s < nsteps; ++s) {
         // the two kinds of items one after the other (one code path at a time per SM)
-        energy_items<0>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
+        energy_items<0, 0>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
                         bufs[threadIdx.x >> 5], pre, wtot);
         __syncthreads();  // pre / wtot are rewritten by the second prefix
-        energy_items<1>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
+        energy_items<1, 0>(reps, nrep, 0, blockIdx.x * kPersistWarps, gridDim.x * kPersistWarps,
                         bufs[threadIdx.x >> 5], pre, wtot);
         if (!grid_barrier(gs, spin_cap, err, &ok_sh)) return;
         for (int r = blockIdx.x; r < nrep; r += gridDim.x) {
-            accept_step(reps[r], 0, smem_raw);
+            accept_step<false>(reps[r], 0, smem_raw);  // (no Ewald in the persistent loop)
             __syncthreads();
         }
         if (!grid_barrier(gs, spin_cap, err, &ok_sh)) return;
