@@ -319,7 +319,7 @@ def run_ours_batched(args, ws, rank, local):
     accept launch per MC step, replayed from a CUDA graph); the launch shape
     comes from the autotuner, run before the timed region."""
     import torch
-    from pygcmc_b200._native import default_options
+    from pygcmc_b200._native import Options, default_options
     from pygcmc_b200.engine import Engine, autotune
     from pygcmc_b200.gpu import runGCMC_batch
     torch.cuda.set_device(local)
@@ -362,7 +362,10 @@ def run_ours_batched(args, ws, rank, local):
     eng.close()
     # end to end: the batched drop-in with host arrays (upload, run, download per call)
     state = [x.pinned() for x in systems]  # host arrays in page-locked memory
-    h2d = sum(sum(a.nbytes for a in s.arrays()[:6]) + 4 * chunk for s in state)
+    # the cavity grids travel as voxel bit sets (Options.grid_bits; the same points)
+    e2e_opt = Options.from_buffer_copy(best)
+    e2e_opt.grid_bits = 1
+    h2d = sum(sum(a.nbytes for a in s.arrays_for(e2e_opt)[:6]) + 4 * chunk for s in state)
     d2h = sum(s.moved_bytes() for s in state)
     full_moves = [s.moveArray for s in state]  # page-locked; each call takes a slice of it
     e2e_times = []
@@ -373,7 +376,7 @@ def run_ours_batched(args, ws, rank, local):
             s.moveArray = np.ascontiguousarray(full_moves[r][k * chunk:(k + 1) * chunk])
         barrier(ws)
         t0 = time.perf_counter()
-        runGCMC_batch(state, best)
+        runGCMC_batch(state, e2e_opt)
         if k >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(e2e_times) * 1e3, ws) / 1e3
@@ -403,7 +406,8 @@ def run_ours_batched(args, ws, rank, local):
         "generate_s": round(t_gen, 2),
         "e2e": {"value": round(args.steps * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)",
+                "cavity_grid": "voxel bit sets (Options.grid_bits = 1)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies, all replicas)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 5),
@@ -738,7 +742,7 @@ LARGE_WORKLOAD = ("large periodic slab with Ewald electrostatics and force-biase
 def run_ours_large(args, ws, rank, local):
     import torch
     from pygcmc_b200 import system as S
-    from pygcmc_b200._native import default_options
+    from pygcmc_b200._native import Options, default_options
     from pygcmc_b200.engine import Engine
     from pygcmc_b200.gpu import runGCMC_batch
     torch.cuda.set_device(local)
@@ -765,10 +769,12 @@ def run_ours_large(args, ws, rank, local):
     eng.close()
     # end to end: the batched drop-in with host arrays (all replicas per call)
     state = [base.pinned() for _ in range(nrep)]  # host arrays in page-locked memory
+    e2e_opt = Options.from_buffer_copy(opt)
+    e2e_opt.grid_bits = 1  # the cavity grids travel as voxel bit sets (the same points)
     full_moves = [st.moveArray for st in state]
     for r, st in enumerate(state):
         st.SimInfo[0]["mcsteps"] = chunk
-    h2d = sum(sum(a.nbytes for a in s_.arrays()[:6]) + 4 * chunk for s_ in state)
+    h2d = sum(sum(a.nbytes for a in s_.arrays_for(e2e_opt)[:6]) + 4 * chunk for s_ in state)
     d2h = sum(s_.moved_bytes() for s_ in state)
     times = []
     for k in range(args.warmup + min(args.steps, 3)):
@@ -777,7 +783,7 @@ def run_ours_large(args, ws, rank, local):
             st.moveArray = np.ascontiguousarray(full_moves[r][k * chunk:(k + 1) * chunk])
         barrier(ws)
         t0 = time.perf_counter()
-        runGCMC_batch(state, opt)
+        runGCMC_batch(state, e2e_opt)
         if k >= args.warmup:
             times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(times) * 1e3, ws) / 1e3
@@ -798,7 +804,8 @@ def run_ours_large(args, ws, rank, local):
                    "proposals": "force-biased translate / rotate (h 0.5 A, 10 deg), uniform SO(3) insertion"},
         "e2e": {"value": round(min(args.steps, 3) * chunk * nrep * ws / e2e_s, 1), "unit": "moves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "mc_steps_per_call": chunk,
-                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)"},
+                "host_arrays": "page-locked (System.pinned())", "api": "pygcmc_b200.gpu.runGCMC_batch (all replicas per call)",
+                "cavity_grid": "voxel bit sets (Options.grid_bits = 1)"},
         "roofline": {"bound": "fp32", "kernel": "k_energy (pose energies incl. erfc and PME interpolation)",
                      "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 5), "flops_per_pair": FLOPS_PER_PAIR,

@@ -150,7 +150,28 @@ typedef struct {
                             proportion to its estimated work (the fixed atoms in the
                             windows of its centre's cell), the same total (an
                             autotuner candidate; slower than 0 on one replica)      */
+    int32_t grid_bits;   /* 0 = the `grid` argument of the run entry points is the
+                            reference's float list of insertion base points (x, y, z
+                            per point); 1 = it is a gcmc_grid_bits record: the same
+                            points as a voxel bit set, 1 bit per voxel instead of
+                            12 bytes per point, expanded on the device (no
+                            counterpart in the reference)                         */
 } gcmc_options;
+
+/* Cavity grid as a voxel bit set (gcmc_options.grid_bits = 1): this header,
+ * followed directly by ceil(n[0] n[1] n[2] / 32) uint32 words; bit (v % 32) of
+ * word v / 32 marks voxel v = (x n[1] + y) n[2] + z.  Insertion base point k is
+ * the k-th marked voxel in increasing v, at ((float)(x dx + start[0]), ...),
+ * each coordinate an FP64 product and sum rounded once to float -- the points
+ * and the order gcmc_cavity_grid writes, so both forms give the same chains.
+ * InfoStruct.totalGridNum must equal the number of marked voxels (else device
+ * error bit 6 and GCMC_ERR_ARG); bits past the last voxel are ignored. */
+typedef struct {
+    double start[3];     /* lower corner of voxel (0, 0, 0)                         */
+    double dx;           /* voxel edge                                              */
+    int32_t n[3];        /* voxels per axis                                         */
+    int32_t pad;
+} gcmc_grid_bits;        /* 48 B */
 
 /* One autotuner trial (gcmc_autotune). */
 typedef struct {
@@ -262,7 +283,9 @@ int gcmc_phase_cycles(gcmc_ctx* ctx, int32_t rep, int64_t* out8);
  * outside the pair table -- gcmc_energy_poses_noalloc, whose device inputs the
  * host does not read; such a pose's energy is NaN; bit 5 the persistent step
  * loop's grid barrier waited longer than gcmc_options.persist_spin_cap, in
- * replica 0's word). */
+ * replica 0's word; bit 6 a gcmc_grid_bits record whose marked voxels do not
+ * number InfoStruct.totalGridNum -- the run entry points report it as
+ * GCMC_ERR_ARG). */
 int gcmc_device_error(gcmc_ctx* ctx, int32_t* err);
 /* The cudaStream_t the context launches on. */
 void* gcmc_stream(gcmc_ctx* ctx);
@@ -370,6 +393,11 @@ int gcmc_synth_chain_slab(int n, float lo0, float hi0, float lo1, float hi1, flo
  * where the reference exits (dataset.py:95-97). */
 int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
                      double* start, float* pts, int64_t cap, int64_t* npts, double* factor);
+/* The same grid as a gcmc_grid_bits record (no counterpart in the reference):
+ * *hdr and words[cap_words] (words == NULL: header and counts only); *nwords =
+ * ceil(voxels / 32), *npts = marked voxels.  Errors as gcmc_cavity_grid. */
+int gcmc_cavity_bits(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                     gcmc_grid_bits* hdr, uint32_t* words, int64_t cap_words, int64_t* nwords, int64_t* npts);
 /* set_fixCut (gcmc/python/dataset.py:175-188): group id per atom (a new group
  * starts more than fix_cutoff from the current group's first atom); returns the
  * number of groups. */

@@ -23,7 +23,8 @@ class Options(ctypes.Structure):
                 ("step_offset", ctypes.c_uint32), ("pme", c_int), ("pme_alpha", ctypes.c_float),
                 ("pme_grid", c_int * 3), ("energy_variant", c_int), ("speculate", c_int),
                 ("energy_kernel", c_int), ("tile_cells", c_int), ("pair_delta", c_int),
-                ("persistent", c_int), ("persist_spin_cap", c_int), ("pose_split", c_int)]
+                ("persistent", c_int), ("persist_spin_cap", c_int), ("pose_split", c_int),
+                ("grid_bits", c_int)]
 
 
 class TuneTrial(ctypes.Structure):
@@ -72,6 +73,8 @@ def lib():
                                                      ctypes.c_int64, c_void, ctypes.c_int64]),
         "gcmc_cavity_grid": (c_int, [c_int, c_void, c_void, ctypes.c_double, c_int, c_void, c_void, ctypes.c_int64,
                                      P(ctypes.c_int64), P(ctypes.c_double)]),
+        "gcmc_cavity_bits": (c_int, [c_int, c_void, c_void, ctypes.c_double, c_int, c_void, c_void, ctypes.c_int64,
+                                     P(ctypes.c_int64), P(ctypes.c_int64)]),
         "gcmc_fix_groups": (ctypes.c_int32, [c_int, c_void, ctypes.c_double, c_void]),
         "gcmc_group_centres": (c_int, [c_int, c_void, c_void, c_void, c_void]),
         "gcmc_fill_layout": (c_int, [c_int, c_void, c_void, c_void, c_void, c_int, c_void, c_void, c_void, c_void,
@@ -138,7 +141,7 @@ def default_options(**kw):
 
 
 EXPORTS = ["runGCMC_cuda", "gcmc_run_gcmc", "gcmc_run_batch", "gcmc_energy_grad", "gcmc_get_forces", "gcmc_pme_potential",
-           "gcmc_cavity_grid", "gcmc_fix_groups", "gcmc_group_centres", "gcmc_fill_layout", "gcmc_pdb_fragment_lines",
+           "gcmc_cavity_grid", "gcmc_cavity_bits", "gcmc_fix_groups", "gcmc_group_centres", "gcmc_fill_layout", "gcmc_pdb_fragment_lines",
            "gcmc_energy_total", "gcmc_autotune", "gcmc_release_cache", "gcmc_last_status", "gcmc_status_string", "gcmc_default_options",
            "gcmc_create", "gcmc_run", "gcmc_run_profiled", "gcmc_sync", "gcmc_download", "gcmc_get_logs", "gcmc_counters",
            "gcmc_device_error", "gcmc_phase_cycles", "gcmc_stream", "gcmc_destroy", "gcmc_energy_poses",

@@ -11,6 +11,7 @@
 // by truncation and Python's non-negative modulo.  Differences are deliberate
 // and few: empty voxels come out in lexicographic (x, y, z) order instead of
 // Python set order, and unused slots are zero-filled.
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -38,13 +39,17 @@ inline void centre_of(const double* xyz, int64_t start, int32_t count, float out
     for (int c = 0; c < 3; ++c) out[c] = (float)((double)acc[c] / n);
 }
 
-}  // namespace
+// The voxel lattice of get_grid and which voxels hold an atom (occ empty
+// without cavity bias: every voxel of a 1 A grid is a base point).
+struct CavityVoxels {
+    double start[3], dx, factor;
+    int64_t nv[3], nempty;
+    std::vector<uint8_t> occ;
+};
 
-extern "C" {
-
-int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
-                     double* start, float* pts, int64_t cap, int64_t* npts, double* factor) {
-    if (n < 1 || !xyz || !cryst || !start || !npts || !factor) return GCMC_ERR_ARG;
+int cavity_voxels(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                  CavityVoxels* cv) {
+    if (n < 1 || !xyz || !cryst) return GCMC_ERR_ARG;
     double lo[3], hi[3];
     for (int c = 0; c < 3; ++c) lo[c] = hi[c] = xyz[c];
     for (int32_t a = 1; a < n; ++a)
@@ -52,41 +57,84 @@ int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double g
             lo[c] = std::fmin(lo[c], xyz[3 * a + c]);
             hi[c] = std::fmax(hi[c], xyz[3 * a + c]);
         }
-    double end[3];
-    int64_t nv[3];
-    const double dx = cavity_bias ? grid_dx : 1.0;
+    cv->dx = cavity_bias ? grid_dx : 1.0;
     for (int c = 0; c < 3; ++c) {
         const double centre = (lo[c] + hi[c]) / 2.0;
-        start[c] = centre - cryst[c] / 2.0;
-        end[c] = centre + cryst[c] / 2.0;
-        nv[c] = (int64_t)((end[c] - start[c]) / dx);
-        if (nv[c] < 1) return GCMC_ERR_ARG;
+        cv->start[c] = centre - cryst[c] / 2.0;
+        const double end = centre + cryst[c] / 2.0;
+        cv->nv[c] = (int64_t)((end - cv->start[c]) / cv->dx);
+        if (cv->nv[c] < 1) return GCMC_ERR_ARG;
     }
-    const int64_t total = nv[0] * nv[1] * nv[2];
-    std::vector<uint8_t> occ(cavity_bias ? (size_t)total : 0, 0);
-    if (cavity_bias)
+    const int64_t total = cv->nv[0] * cv->nv[1] * cv->nv[2];
+    cv->occ.clear();
+    int64_t nocc = 0;
+    if (cavity_bias) {
+        cv->occ.assign((size_t)total, 0);
         for (int32_t a = 0; a < n; ++a) {
             int64_t v[3];
-            for (int c = 0; c < 3; ++c) v[c] = pymod((int64_t)std::trunc((xyz[3 * a + c] - start[c]) / dx), nv[c]);
-            occ[(size_t)((v[0] * nv[1] + v[1]) * nv[2] + v[2])] = 1;
+            for (int c = 0; c < 3; ++c)
+                v[c] = pymod((int64_t)std::trunc((xyz[3 * a + c] - cv->start[c]) / cv->dx), cv->nv[c]);
+            uint8_t& o = cv->occ[(size_t)((v[0] * cv->nv[1] + v[1]) * cv->nv[2] + v[2])];
+            nocc += !o;
+            o = 1;
         }
-    int64_t ne = 0;
-    for (int64_t i = 0; i < total; ++i) ne += cavity_bias ? !occ[(size_t)i] : 1;
-    *npts = ne;
-    *factor = cavity_bias ? (double)ne / (double)total : 1.0;
-    if (cavity_bias && *factor < 0.05) return GCMC_ERR_ARG;  // the reference exits here (dataset.py:95-97)
+    }
+    cv->nempty = total - nocc;
+    cv->factor = cavity_bias ? (double)cv->nempty / (double)total : 1.0;
+    return GCMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcmc_cavity_grid(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                     double* start, float* pts, int64_t cap, int64_t* npts, double* factor) {
+    if (!start || !npts || !factor) return GCMC_ERR_ARG;
+    CavityVoxels cv;
+    const int st = cavity_voxels(n, xyz, cryst, grid_dx, cavity_bias, &cv);
+    if (st != GCMC_OK) return st;
+    for (int c = 0; c < 3; ++c) start[c] = cv.start[c];
+    *npts = cv.nempty;
+    *factor = cv.factor;
+    if (cavity_bias && cv.factor < 0.05) return GCMC_ERR_ARG;  // the reference exits here (dataset.py:95-97)
     if (!pts) return GCMC_OK;
-    if (cap < ne) return GCMC_ERR_LIMIT;
+    if (cap < cv.nempty) return GCMC_ERR_LIMIT;
     int64_t k = 0;
-    for (int64_t x = 0; x < nv[0]; ++x)
-        for (int64_t y = 0; y < nv[1]; ++y)
-            for (int64_t z = 0; z < nv[2]; ++z) {
-                if (cavity_bias && occ[(size_t)((x * nv[1] + y) * nv[2] + z)]) continue;
-                pts[3 * k] = (float)((double)x * dx + start[0]);
-                pts[3 * k + 1] = (float)((double)y * dx + start[1]);
-                pts[3 * k + 2] = (float)((double)z * dx + start[2]);
+    for (int64_t x = 0; x < cv.nv[0]; ++x)
+        for (int64_t y = 0; y < cv.nv[1]; ++y)
+            for (int64_t z = 0; z < cv.nv[2]; ++z) {
+                if (!cv.occ.empty() && cv.occ[(size_t)((x * cv.nv[1] + y) * cv.nv[2] + z)]) continue;
+                pts[3 * k] = (float)((double)x * cv.dx + cv.start[0]);
+                pts[3 * k + 1] = (float)((double)y * cv.dx + cv.start[1]);
+                pts[3 * k + 2] = (float)((double)z * cv.dx + cv.start[2]);
                 ++k;
             }
+    return GCMC_OK;
+}
+
+int gcmc_cavity_bits(int32_t n, const double* xyz, const double* cryst, double grid_dx, int32_t cavity_bias,
+                     gcmc_grid_bits* hdr, uint32_t* words, int64_t cap_words, int64_t* nwords, int64_t* npts) {
+    if (!hdr || !nwords || !npts) return GCMC_ERR_ARG;
+    CavityVoxels cv;
+    const int st = cavity_voxels(n, xyz, cryst, grid_dx, cavity_bias, &cv);
+    if (st != GCMC_OK) return st;
+    for (int c = 0; c < 3; ++c) {
+        if (cv.nv[c] > INT32_MAX) return GCMC_ERR_LIMIT;
+        hdr->start[c] = cv.start[c];
+        hdr->n[c] = (int32_t)cv.nv[c];
+    }
+    hdr->dx = cv.dx;
+    hdr->pad = 0;
+    const int64_t total = cv.nv[0] * cv.nv[1] * cv.nv[2];
+    *nwords = (total + 31) / 32;
+    *npts = cv.nempty;
+    if (cavity_bias && cv.factor < 0.05) return GCMC_ERR_ARG;
+    if (!words) return GCMC_OK;
+    if (cap_words < *nwords) return GCMC_ERR_LIMIT;
+    std::memset(words, 0, sizeof(uint32_t) * (size_t)*nwords);
+    for (int64_t v = 0; v < total; ++v)
+        if (cv.occ.empty() || !cv.occ[(size_t)v]) words[v >> 5] |= 1u << (v & 31);
     return GCMC_OK;
 }
 

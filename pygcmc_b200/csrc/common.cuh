@@ -27,7 +27,10 @@ enum : uint32_t { RP_INSERT = 1, RP_DELETE = 2, RP_MOVE = 3, RP_CLUSTER = 4, RP_
 // force-bias tilt lambda (Pangali, Rao and Berne): density ~ exp(lambda beta f . d) in the step cube
 constexpr float kFbLambda = 0.5f;
 enum : int { MV_NONE = -1, MV_INSERT = 0, MV_DELETE = 1, MV_TRANSLATE = 2, MV_ROTATE = 3 };
-enum : int { ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8, ERR_SITE_TYPE = 16, ERR_SYNC = 32 };
+enum : int {
+    ERR_CELL_OVERFLOW = 1, ERR_IMAGE = 2, ERR_SLOT = 4, ERR_POSES = 8, ERR_SITE_TYPE = 16, ERR_SYNC = 32,
+    ERR_GRID_BITS = 64
+};
 
 // ---------------------------------------------------------------------------
 // exact-rounding float helpers

@@ -9,12 +9,16 @@
 // (build_spec_graph): the next step is prepared and its pose energies
 // evaluated beside the accept kernel, and kept when the step accepts nothing.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 
@@ -31,11 +35,61 @@ static_assert(kGraphSteps % 2 == 0, "a speculating graph ends on its start parit
 constexpr int kMaxRep = 256;
 thread_local int g_last_status = GCMC_OK;
 
+// GCMC_B200_TRACE=1 (read once): every drop-in call (gcmc_run_gcmc,
+// runGCMC_cuda, gcmc_run_batch) prints its phases' host wall times to stderr.
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("GCMC_B200_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+// phase stamps of the current call (refill: validated, host set-up done, set-up enqueued)
+thread_local double g_trace[4];
+// host set-up split, host time summed over the call's replicas (and threads):
+// layout and cell sizing, allocations, per-cell work table and PME host set-up,
+// uploads enqueued
+std::atomic<long long> g_setup_ns[4];
+
+// fn(r) for r in [0, n) on up to 16 host threads (inline for one replica or
+// one hardware thread); a worker first selects `device` (>= 0) for its CUDA
+// calls.  Returns the first failing replica's status.
+template <class F>
+int for_each_rep(int n, int device, F fn) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::min(n, std::min(hw, 16));
+    std::vector<int> st(n, GCMC_OK);
+    if (nt <= 1) {
+        for (int r = 0; r < n; ++r)
+            if ((st[r] = fn(r)) != GCMC_OK) return st[r];
+        return GCMC_OK;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(nt);
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            if (device >= 0 && cudaSetDevice(device) != cudaSuccess) {
+                cudaGetLastError();
+                for (int r = t; r < n; r += nt) st[r] = GCMC_ERR_CUDA;
+                return;
+            }
+            for (int r = t; r < n; r += nt) st[r] = fn(r);
+        });
+    for (auto& th : pool) th.join();
+    for (int r = 0; r < n; ++r)
+        if (st[r] != GCMC_OK) return st[r];
+    return GCMC_OK;
+}
+
 struct RepHost {
     int natoms = 0, ngroups = 0, ncell = 0, cap = 0, ntypes = 0, G = 0, ffX = 0, ffY = 0, mcsteps = 0;
     int nslab = 0, log_cap = 0, log_kmax = 0;
     int slab_cap = 0;  // per-variant slab partials allocated per pose (>= the largest step split)
     int host_end = 0;
+    int2 frag_atoms = make_int2(0, 0);  // atom range of the fragment slots (the caller's layout)
     std::vector<int> startRes, maxNum, moves_host;
     // allocated element count of each device buffer, keyed by the offset of its
     // pointer member (grown on demand, reused on refill)
@@ -50,6 +104,8 @@ struct RepHost {
     Atom* raw_atoms = nullptr;      // the caller's arrays as uploaded, unpacked on the device
     residue* raw_groups = nullptr;
     float* raw_grid = nullptr;
+    uint32_t* raw_bits = nullptr;   // gcmc_grid_bits words as uploaded
+    int* bits_blk = nullptr;        // per-block marked-voxel counts, then offsets (+ total)
     int* gcell = nullptr;
     float4* grid = nullptr;
     float2* lj = nullptr;
@@ -190,7 +246,7 @@ void free_rep(RepHost& h) {
     dfree(h.desc); dfree(h.pcen); dfree(h.pslot); dfree(h.epart); dfree(h.nbr); dfree(h.log);
     dfree(h.logE); dfree(h.counters); dfree(h.err);
     dfree(h.energy); dfree(h.pgum); dfree(h.psite);
-    dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid);
+    dfree(h.raw_atoms); dfree(h.raw_groups); dfree(h.raw_grid); dfree(h.raw_bits); dfree(h.bits_blk);
     dfree(h.desc2); dfree(h.pcen2); dfree(h.pslot2); dfree(h.epart2); dfree(h.nbr2); dfree(h.pgum2); dfree(h.plnu2);
     dfree(h.psite2); dfree(h.valid2); dfree(h.abort2); dfree(h.sstep2); dfree(h.pending2); dfree(h.plnu); dfree(h.fpart); dfree(h.fbprop); dfree(h.fbcnt); dfree(h.logF);
     dfree(h.pme_q); dfree(h.pme_phi); dfree(h.pme_spec); dfree(h.pme_g); dfree(h.pme_dirty);
@@ -209,7 +265,8 @@ int host_cell(float x, float start, float invLc, int nc) {
     return c < 0 ? c + nc : c;
 }
 
-int validate(const gcmc_replica_in& in) {
+// frag_atoms (optional): the atom range [x, y) the fragment slots cover (empty: x >= y)
+int validate(const gcmc_replica_in& in, int2* frag_atoms = nullptr) {
     const InfoStruct* I = in.info;
     if (!I || !in.fragmentInfo || !in.residueInfo || !in.atomInfo || !in.ff) return GCMC_ERR_ARG;
     if (I->fragTypeNum < 1 || I->totalResNum < 0 || I->totalAtomNum < 0 || I->mcsteps < 0) return GCMC_ERR_ARG;
@@ -224,6 +281,7 @@ int validate(const gcmc_replica_in& in) {
     int prev_end = F[0].startRes;
     if (prev_end < 0) return GCMC_ERR_ARG;
     bool any_insert = false;
+    int alo = I->totalAtomNum, ahi = 0;
     for (int t = 0; t < I->fragTypeNum; ++t) {
         const AtomArray& f = F[t];
         if (f.num_atoms < 1 || f.num_atoms > kMaxSites) return GCMC_ERR_LIMIT;
@@ -238,6 +296,8 @@ int validate(const gcmc_replica_in& in) {
             const residue& r = R[f.startRes + j];
             if (r.atomNum != f.num_atoms || r.atomStart < 0 || r.atomStart + r.atomNum > I->totalAtomNum)
                 return GCMC_ERR_ARG;
+            alo = std::min(alo, r.atomStart);
+            ahi = std::max(ahi, r.atomStart + r.atomNum);
         }
         for (int j = 0; j < f.totalNum; ++j) {
             const residue& r = R[f.startRes + j];
@@ -261,6 +321,7 @@ int validate(const gcmc_replica_in& in) {
         if ((mv & 3) == 0) any_insert = true;
     }
     if (any_insert && (I->totalGridNum < 1 || !in.grid)) return GCMC_ERR_ARG;
+    if (frag_atoms) *frag_atoms = make_int2(alo, ahi);
     return GCMC_OK;
 }
 
@@ -330,6 +391,104 @@ __global__ void k_unpack_grid(const float* __restrict__ in, float4* __restrict__
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         grid[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
 }
+
+// Cavity grid from a gcmc_grid_bits record: base point k = the k-th marked
+// voxel.  Three launches, one word per thread: marked voxels per block of
+// kBitsThreads words (k_bits_count), an exclusive scan of the block counts with
+// the total checked against the expected point count (k_bits_scan), and the
+// points of each word at its offset (k_bits_expand).
+constexpr int kBitsThreads = 256;
+constexpr long long kIntMax = 0x7fffffffll;
+
+// the marked bits of word w (bits past the last voxel cleared)
+__device__ __forceinline__ uint32_t bits_word(const uint32_t* words, long long w, long long nvox) {
+    uint32_t b = words[w];
+    const long long rest = nvox - w * 32;
+    if (rest < 32) b &= (1u << rest) - 1u;
+    return b;
+}
+
+// Exclusive prefix of v over the block (kBitsThreads threads); *total = the sum.
+__device__ __forceinline__ int bits_block_scan(int v, int* total) {
+    __shared__ int warp_sum[kBitsThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    int before = 0, all = 0;
+    for (int w = 0; w < kBitsThreads / 32; ++w) {
+        if (w < wid) before += warp_sum[w];
+        all += warp_sum[w];
+    }
+    __syncthreads();
+    *total = all;
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kBitsThreads) k_bits_count(const uint32_t* __restrict__ words, long long nwords,
+                                                              long long nvox, int* __restrict__ blk) {
+    const long long w = (long long)blockIdx.x * kBitsThreads + threadIdx.x;
+    const int c = w < nwords ? __popc(bits_word(words, w, nvox)) : 0;
+    int total = 0;
+    bits_block_scan(c, &total);
+    if (threadIdx.x == 0) blk[blockIdx.x] = total;
+}
+
+// One CTA: blk[0, nblk) -> exclusive offsets; blk[nblk] = total; error bit when total != expect.
+__global__ void __launch_bounds__(kBitsThreads) k_bits_scan(int* __restrict__ blk, int nblk, int expect,
+                                                             int* __restrict__ err) {
+    long long carry = 0;
+    for (int b0 = 0; b0 < nblk; b0 += kBitsThreads) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < nblk ? blk[b] : 0;
+        int total = 0;
+        const int ex = bits_block_scan(v, &total);
+        if (b < nblk) blk[b] = (int)(carry + ex < kIntMax ? carry + ex : kIntMax);
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        blk[nblk] = (int)(carry < kIntMax ? carry : kIntMax);
+        if (carry != expect) atomicOr(err, ERR_GRID_BITS);
+    }
+}
+
+__global__ void __launch_bounds__(kBitsThreads) k_bits_expand(const uint32_t* __restrict__ words, long long nwords,
+                                                               long long nvox, const int* __restrict__ blk, int n1,
+                                                               int n2, double s0, double s1, double s2, double dx,
+                                                               float4* __restrict__ grid, int npts) {
+    const long long w = (long long)blockIdx.x * kBitsThreads + threadIdx.x;
+    uint32_t b = w < nwords ? bits_word(words, w, nvox) : 0u;
+    int total = 0;
+    long long k = (long long)blk[blockIdx.x] + bits_block_scan(__popc(b), &total);
+    if (!b) return;
+    // voxel of the word's first bit, then walk z (and carry into y, x) bit by bit
+    const long long plane = (long long)n1 * n2, v0 = w * 32;
+    long long x = v0 / plane;
+    const long long r0 = v0 - x * plane;
+    int y = (int)(r0 / n2), z = (int)(r0 - (long long)y * n2);
+    int at = 0;
+    while (b) {
+        const int bit = __ffs(b) - 1;
+        b &= b - 1u;
+        for (; at < bit; ++at)
+            if (++z == n2) {
+                z = 0;
+                if (++y == n1) {
+                    y = 0;
+                    ++x;
+                }
+            }
+        if (k < npts)
+            grid[k] = make_float4(__double2float_rn(__dadd_rn(__dmul_rn((double)x, dx), s0)),
+                                  __double2float_rn(__dadd_rn(__dmul_rn((double)y, dx), s1)),
+                                  __double2float_rn(__dadd_rn(__dmul_rn((double)z, dx), s2)), 0.0f);
+        ++k;
+    }
+}
 int unpack_blocks(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
 
 int energy_warps(int device, int evar, int ebps, int spare_sms);
@@ -341,6 +500,14 @@ bool spec_eligible(int nrep, const gcmc_replica_in* ins, const gcmc_options& opt
 }
 
 int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_options& opt) {
+    const bool trace = trace_on();
+    double tp = trace ? now_ms() : 0.0;
+    auto stamp = [&](int k) {
+        if (!trace) return;
+        const double t = now_ms();
+        g_setup_ns[k] += (long long)((t - tp) * 1e6);
+        tp = t;
+    };
     const InfoStruct* I = in.info;
     RepHost& h = ctx->reps[r];
     RepDev& d = ctx->repdev[r];
@@ -512,6 +679,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         h.maxNum.push_back(f.maxNum);
     }
 
+    stamp(0);
     int st;
 #define AL(ptr, n)                                                                          \
     do {                                                                                    \
@@ -529,7 +697,27 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     AL(h.psite, (size_t)kMaxPoses * kMaxSites);
     AL(h.pbin, 2 * kMaxPoses); AL(h.tiles, 2 * kMaxPoses);
     AL(h.wcost, h.ncell); AL(h.pnslab, 2 * kMaxPoses); AL(h.pitem, (size_t)2 * kMaxPoses * h.slab_cap);
-    AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups); AL(h.raw_grid, (size_t)3 * h.G);
+    AL(h.raw_atoms, h.natoms); AL(h.raw_groups, h.ngroups);
+    // the cavity grid as the caller holds it: the reference's float list, or a voxel bit set
+    gcmc_grid_bits gb{};
+    long long nvox = 0, nwords = 0;
+    int nblk = 0;
+    if (opt.grid_bits && h.G > 0) {
+        std::memcpy(&gb, in.grid, sizeof(gb));
+        if (!(gb.dx > 0.0) || !std::isfinite(gb.dx)) return GCMC_ERR_ARG;
+        nvox = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (gb.n[a] < 1 || !std::isfinite(gb.start[a])) return GCMC_ERR_ARG;
+            nvox *= gb.n[a];
+            if (nvox > (1ll << 36)) return GCMC_ERR_LIMIT;
+        }
+        if (h.G > nvox) return GCMC_ERR_ARG;
+        nwords = (nvox + 31) / 32;
+        nblk = (int)((nwords + kBitsThreads - 1) / kBitsThreads);
+        AL(h.raw_bits, (size_t)nwords); AL(h.bits_blk, (size_t)nblk + 1); AL(h.raw_grid, 1);
+    } else {
+        AL(h.raw_grid, (size_t)3 * h.G);
+    }
     if (ctx->spec) {
         AL(h.desc2, 1); AL(h.pcen2, kMaxPoses); AL(h.pslot2, kMaxPoses); AL(h.epart2, (size_t)kMaxPoses * 2 * h.slab_cap);
         AL(h.nbr2, (size_t)kMaxPoses * kMaxWords); AL(h.pgum2, kMaxPoses); AL(h.plnu2, kMaxPoses);
@@ -537,6 +725,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         AL(h.pending2, 2); AL(h.pbin2, 2 * kMaxPoses); AL(h.tiles2, 2 * kMaxPoses);
         AL(h.pnslab2, 2 * kMaxPoses); AL(h.pitem2, (size_t)2 * kMaxPoses * h.slab_cap);
     }
+    stamp(1);
     // each cell's window work: the fixed atoms in the cells within R of it (box sums along
     // each axis, periodic; the whole axis where the window spans it)
     if (opt.pose_split > 0) {
@@ -572,8 +761,8 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         box(cnt, tmp, 0);
         box(tmp, cnt, 1);
         box(cnt, tmp, 2);
+        // (a copy from pageable memory is staged before the call returns: tmp may go)
         CK(cudaMemcpyAsync(h.wcost, tmp.data(), sizeof(int) * h.ncell, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));  // tmp is a host temporary
     }
     // smooth PME: mesh and influence function
     h.pme = opt.pme > 0 || (opt.pme == 0 && I->PME != 0);
@@ -626,6 +815,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         if (d.fb) AL(h.logF, (size_t)h.log_cap * h.log_kmax * 12);
     }
 #undef AL
+    stamp(2);
     cudaStream_t s = ctx->stream;
     if (h.natoms > 0) {
         CK(cudaMemcpyAsync(h.raw_atoms, in.atomInfo, sizeof(Atom) * h.natoms, cudaMemcpyHostToDevice, s));
@@ -637,10 +827,10 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     }
     CK(cudaMemsetAsync(h.cell_count, 0, sizeof(int) * h.ncell, s));
     CK(cudaMemsetAsync(h.gcell, 0xff, sizeof(int) * std::max(1, h.ngroups), s));
-    if (h.G > 0) {
+    if (h.G > 0 && !opt.grid_bits) {
         CK(cudaMemcpyAsync(h.raw_grid, in.grid, sizeof(float) * 3 * (size_t)h.G, cudaMemcpyHostToDevice, s));
         k_unpack_grid<<<unpack_blocks(h.G), 256, 0, s>>>(h.raw_grid, h.grid, h.G);
-    } else {
+    } else if (h.G == 0) {
         CK(cudaMemsetAsync(h.grid, 0, sizeof(float4), s));
     }
     CK(cudaGetLastError());
@@ -657,6 +847,19 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     CK(cudaMemcpyAsync(h.desc, &d0, sizeof(StepDesc), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(h.counters, 0, sizeof(unsigned long long) * 16, s));
     CK(cudaMemsetAsync(h.err, 0, sizeof(int), s));
+    if (h.log_cap > 0) {  // entries past a step's pose count read as zeros
+        CK(cudaMemsetAsync(h.logE, 0, sizeof(double) * (size_t)h.log_cap * h.log_kmax, s));
+        if (d.fb) CK(cudaMemsetAsync(h.logF, 0, sizeof(float) * (size_t)h.log_cap * h.log_kmax * 12, s));
+    }
+    if (nblk > 0) {  // after the error word is cleared: the scan reports a count mismatch there
+        CK(cudaMemcpyAsync(h.raw_bits, reinterpret_cast<const char*>(in.grid) + sizeof(gcmc_grid_bits),
+                           sizeof(uint32_t) * (size_t)nwords, cudaMemcpyHostToDevice, s));
+        k_bits_count<<<nblk, kBitsThreads, 0, s>>>(h.raw_bits, nwords, nvox, h.bits_blk);
+        k_bits_scan<<<1, kBitsThreads, 0, s>>>(h.bits_blk, nblk, h.G, h.err);
+        k_bits_expand<<<nblk, kBitsThreads, 0, s>>>(h.raw_bits, nwords, nvox, h.bits_blk, gb.n[1], gb.n[2],
+                                                    gb.start[0], gb.start[1], gb.start[2], gb.dx, h.grid, h.G);
+        CK(cudaGetLastError());
+    }
     CK(cudaMemsetAsync(h.epart, 0, sizeof(double) * kMaxPoses * 2 * h.slab_cap, s));
     CK(cudaMemsetAsync(h.energy, 0, sizeof(double), s));
     CK(cudaMemsetAsync(h.fpart, 0, sizeof(float) * kMaxPoses * 2 * h.slab_cap * 6, s));
@@ -674,6 +877,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
         CK(cudaMemsetAsync(h.pending2, 0, sizeof(unsigned long long) * 2, s));
     }
 
+    stamp(3);
     d.xyzq = h.xyzq; d.atype = h.atype; d.gcen = h.gcen; d.gspan = h.gspan;
     d.cell_count = h.cell_count; d.cell_ent = h.cell_ent; d.gcell = h.gcell;
     d.grid = h.grid; d.lj = h.lj; d.moves = h.moves; d.frag = h.frag; d.totalNum = h.totalNum;
@@ -1052,8 +1256,9 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     gcmc_options opt;
     if (optp) opt = *optp; else gcmc_default_options(&opt);
     if (opt.proposal < 0 || opt.proposal > 2) return GCMC_ERR_ARG;
-    for (int r = 0; r < nrep; ++r) {
-        int st = validate(ins[r]);
+    std::vector<int2> frag_atoms(nrep);
+    {
+        const int st = for_each_rep(nrep, -1, [&](int r) { return validate(ins[r], &frag_atoms[r]); });
         if (st != GCMC_OK) return st;
     }
     int ndev = 0;
@@ -1082,8 +1287,9 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     }
     ctx->reps.resize(nrep);
     ctx->repdev.resize(nrep);
+    for (int r = 0; r < nrep; ++r) ctx->reps[r].frag_atoms = frag_atoms[r];
     ctx->spec = spec_eligible(nrep, ins, opt);
-    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
+    if (st == GCMC_OK) st = for_each_rep(nrep, ctx->device, [&](int r) { return setup_rep(ctx, r, ins[r], opt); });
     if (st == GCMC_OK) finalize_tiling(ctx);
     if (st == GCMC_OK && cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) st = upload_reps(ctx);
@@ -1109,7 +1315,7 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     if (st == GCMC_OK) {
         int32_t err = 0;
         gcmc_device_error(ctx, &err);
-        if (err) st = GCMC_ERR_DEVICE;
+        if (err) st = (err & ERR_GRID_BITS) ? GCMC_ERR_ARG : GCMC_ERR_DEVICE;
     }
     if (st != GCMC_OK) {
         cudaGetLastError();
@@ -1130,15 +1336,19 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     if (optp) opt = *optp; else gcmc_default_options(&opt);
     if (opt.proposal < 0 || opt.proposal > 2) return GCMC_ERR_ARG;
     int st = GCMC_OK;
-    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = validate(ins[r]);
+    std::vector<int2> frag_atoms(nrep);
+    st = for_each_rep(nrep, -1, [&](int r) { return validate(ins[r], &frag_atoms[r]); });
     if (st != GCMC_OK) return st;
     CK(cudaStreamSynchronize(ctx->stream));
+    for (int r = 0; r < nrep; ++r) ctx->reps[r].frag_atoms = frag_atoms[r];
+    if (trace_on()) g_trace[0] = now_ms();
     const bool spec = spec_eligible(nrep, ins, opt);
     const bool spec_changed = spec != ctx->spec;
     ctx->spec = spec;
     const bool tiled_before = ctx->tiled, pme_before = ctx->pme_any, dual_before = ctx->dual_any;
-    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = setup_rep(ctx, r, ins[r], opt);
+    st = for_each_rep(nrep, ctx->device, [&](int r) { return setup_rep(ctx, r, ins[r], opt); });
     if (st != GCMC_OK) return st;
+    if (trace_on()) g_trace[1] = now_ms();
     finalize_tiling(ctx);
     st = upload_reps(ctx);
     if (st != GCMC_OK) return st;
@@ -1167,10 +1377,11 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
             if (st != GCMC_OK) return st;
         }
     }
+    if (trace_on()) g_trace[2] = now_ms();
     CK(cudaStreamSynchronize(ctx->stream));
     int32_t err = 0;
     gcmc_device_error(ctx, &err);
-    return err ? GCMC_ERR_DEVICE : GCMC_OK;
+    return err ? ((err & ERR_GRID_BITS) ? GCMC_ERR_ARG : GCMC_ERR_DEVICE) : GCMC_OK;
 }
 
 // The contexts kept by gcmc_run_gcmc / runGCMC_cuda (one replica) and by
@@ -1182,40 +1393,61 @@ gcmc_ctx* g_batch = nullptr;
 // What a run can change in the caller's arrays, written back in place: the
 // fragment types' counts, the fragment residues' centres and the atoms of the
 // fragment slots (fixed groups and atoms never move, so their entries already
-// hold the device's values).
-int download_moved(gcmc_ctx* ctx, int r, const gcmc_replica_in& in) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    RepHost& h = ctx->reps[r];
-    AtomArray* frag = const_cast<AtomArray*>(in.fragmentInfo);
-    residue* res = const_cast<residue*>(in.residueInfo);
-    Atom* atoms = const_cast<Atom*>(in.atomInfo);
-    std::vector<int> tot(h.ntypes);
-    CK(cudaMemcpy(tot.data(), h.totalNum, sizeof(int) * h.ntypes, cudaMemcpyDeviceToHost));
-    for (int t = 0; t < h.ntypes; ++t) frag[t].totalNum = tot[t];
-    const int g0 = frag[0].startRes, g1 = h.ngroups;
-    if (g1 <= g0) return GCMC_OK;
-    std::vector<float4> gcen(g1 - g0);
-    CK(cudaMemcpy(gcen.data(), h.gcen + g0, sizeof(float4) * (g1 - g0), cudaMemcpyDeviceToHost));
-    int lo = h.natoms, hi = 0;
-    for (int g = g0; g < g1; ++g) {
-        res[g].position[0] = gcen[g - g0].x;
-        res[g].position[1] = gcen[g - g0].y;
-        res[g].position[2] = gcen[g - g0].z;
-        lo = std::min(lo, res[g].atomStart);
-        hi = std::max(hi, res[g].atomStart + res[g].atomNum);
+// hold the device's values).  k_pack_moved writes the current state in the
+// caller's layout into the upload buffers (which hold the caller's arrays as
+// uploaded, so the fields a run never changes keep the caller's values), and
+// one copy per range lands it in place.
+__global__ void k_pack_moved(const float4* __restrict__ gcen, residue* __restrict__ groups, int g0, int g1,
+                             const float4* __restrict__ xyzq, const int* __restrict__ atype, Atom* __restrict__ atoms,
+                             int a0, int a1) {
+    const int ng = g1 - g0, na = a1 - a0, n = ng > na ? ng : na;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i < ng) {
+            const float4 c = gcen[g0 + i];
+            residue& R = groups[g0 + i];
+            R.position[0] = c.x;
+            R.position[1] = c.y;
+            R.position[2] = c.z;
+        }
+        if (i < na) {
+            const float4 p = xyzq[a0 + i];
+            Atom& A = atoms[a0 + i];
+            A.position[0] = p.x;
+            A.position[1] = p.y;
+            A.position[2] = p.z;
+            A.charge = p.w;
+            A.type = atype[a0 + i];
+        }
     }
-    if (hi <= lo) return GCMC_OK;
-    std::vector<float4> xyzq(hi - lo);
-    std::vector<int> atype(hi - lo);
-    CK(cudaMemcpy(xyzq.data(), h.xyzq + lo, sizeof(float4) * (hi - lo), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(atype.data(), h.atype + lo, sizeof(int) * (hi - lo), cudaMemcpyDeviceToHost));
-    for (int a = lo; a < hi; ++a) {
-        const float4 p = xyzq[a - lo];
-        atoms[a].position[0] = p.x;
-        atoms[a].position[1] = p.y;
-        atoms[a].position[2] = p.z;
-        atoms[a].charge = p.w;
-        atoms[a].type = atype[a - lo];
+}
+
+// Every replica's changes into the caller's arrays (one stream sync).
+int download_moved(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins) {
+    cudaStream_t s = ctx->stream;
+    std::vector<std::vector<int>> tot(nrep);
+    for (int r = 0; r < nrep; ++r) {
+        RepHost& h = ctx->reps[r];
+        const gcmc_replica_in& in = ins[r];
+        tot[r].resize(h.ntypes);
+        CK(cudaMemcpyAsync(tot[r].data(), h.totalNum, sizeof(int) * h.ntypes, cudaMemcpyDeviceToHost, s));
+        const int g0 = in.fragmentInfo[0].startRes, g1 = h.ngroups;
+        const int a0 = h.frag_atoms.x, a1 = h.frag_atoms.y;
+        if (g1 <= g0 && a1 <= a0) continue;
+        const int n = std::max(g1 - g0, a1 - a0);
+        k_pack_moved<<<unpack_blocks(n), 256, 0, s>>>(h.gcen, h.raw_groups, g0, g1, h.xyzq, h.atype, h.raw_atoms,
+                                                      a0, a1);
+        CK(cudaGetLastError());
+        if (g1 > g0)
+            CK(cudaMemcpyAsync(const_cast<residue*>(in.residueInfo) + g0, h.raw_groups + g0,
+                               sizeof(residue) * (g1 - g0), cudaMemcpyDeviceToHost, s));
+        if (a1 > a0)
+            CK(cudaMemcpyAsync(const_cast<Atom*>(in.atomInfo) + a0, h.raw_atoms + a0, sizeof(Atom) * (a1 - a0),
+                               cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    for (int r = 0; r < nrep; ++r) {
+        AtomArray* frag = const_cast<AtomArray*>(ins[r].fragmentInfo);
+        for (int t = 0; t < ctx->reps[r].ntypes; ++t) frag[t].totalNum = tot[r][t];
     }
     return GCMC_OK;
 }
@@ -1229,7 +1461,15 @@ int cached_run(gcmc_ctx** slot, int nrep, const gcmc_replica_in* ins, const gcmc
         return GCMC_ERR_NODEVICE;
     }
     int st = GCMC_OK;
+    const bool trace = trace_on();
+    const double t0 = trace ? now_ms() : 0.0;
+    bool refilled = false;
+    if (trace) {
+        g_trace[0] = g_trace[1] = g_trace[2] = t0;
+        for (auto& x : g_setup_ns) x = 0;
+    }
     if (*slot && (*slot)->device == dev && (*slot)->nrep == nrep) {
+        refilled = true;
         st = refill_impl(*slot, nrep, ins, opt);
         if (st != GCMC_OK) {  // drop the cached context and start afresh
             destroy_impl(*slot);
@@ -1247,11 +1487,29 @@ int cached_run(gcmc_ctx** slot, int nrep, const gcmc_replica_in* ins, const gcmc
             return st;
         }
     }
+    const double t1 = trace ? now_ms() : 0.0;
     int most = 0;
     for (int r = 0; r < nrep; ++r) most = std::max(most, (int)ins[r].info->mcsteps);
     st = gcmc_run(*slot, most);
     if (st == GCMC_OK) st = gcmc_sync(*slot);
-    for (int r = 0; r < nrep && st == GCMC_OK; ++r) st = download_moved(*slot, r, ins[r]);
+    const double t2 = trace ? now_ms() : 0.0;
+    if (st == GCMC_OK) st = download_moved(*slot, nrep, ins);
+    if (trace) {
+        const double t3 = now_ms();
+        if (refilled)
+            std::fprintf(stderr,
+                         "gcmc_b200 trace: %d replicas, %d steps: validate %.3f ms, host set-up %.3f ms "
+                         "(host time over threads: layout %.3f, allocations %.3f, tables %.3f, uploads %.3f), "
+                         "enqueue %.3f ms, device set-up %.3f ms, run %.3f ms, download %.3f ms\n",
+                         nrep, most, g_trace[0] - t0, g_trace[1] - g_trace[0], g_setup_ns[0] * 1e-6,
+                         g_setup_ns[1] * 1e-6, g_setup_ns[2] * 1e-6, g_setup_ns[3] * 1e-6, g_trace[2] - g_trace[1],
+                         t1 - g_trace[2], t2 - t1, t3 - t2);
+        else
+            std::fprintf(stderr,
+                         "gcmc_b200 trace: %d replicas, %d steps: new context %.3f ms, run %.3f ms, "
+                         "download %.3f ms\n",
+                         nrep, most, t1 - t0, t2 - t1, t3 - t2);
+    }
     if (st != GCMC_OK) {
         destroy_impl(*slot);
         *slot = nullptr;

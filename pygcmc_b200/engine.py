@@ -13,10 +13,10 @@ from . import values as V
 from ._native import Options, ReplicaIn, TuneTrial, check, default_options, lib, ptr
 
 
-def _replica_array(systems):
+def _replica_array(systems, options=None):
     arr = (ReplicaIn * len(systems))()
     for i, s in enumerate(systems):
-        arr[i] = ReplicaIn(*[ptr(x) for x in s.arrays()])
+        arr[i] = ReplicaIn(*[ptr(x) for x in s.arrays_for(options)])
     return arr
 
 
@@ -30,7 +30,7 @@ def autotune(systems, options: Options = None, trial_steps: int = 64):
     if not isinstance(systems, (list, tuple)):
         systems = [systems]
     base = options if options is not None else default_options()
-    arr = _replica_array(systems)
+    arr = _replica_array(systems, base)
     best = Options()
     trials = (TuneTrial * 32)()
     n = ctypes.c_int32(0)
@@ -50,7 +50,7 @@ class Engine:
             systems = [systems]
         self.systems = list(systems)
         self.options = options if options is not None else default_options()
-        arr = _replica_array(self.systems)
+        arr = _replica_array(self.systems, self.options)
         self._in = arr
         h = ctypes.c_void_p()
         check(lib().gcmc_create(len(self.systems), arr, ctypes.byref(self.options),

@@ -17,12 +17,27 @@ from ._native import GcmcError, check, default_options, lib, ptr
 __all__ = ["runGCMC", "GcmcError", "validate_arrays"]
 
 
-def validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray):
-    """Dtype, contiguity and size checks against the sizes recorded in SimInfo."""
+GRID_BITS_HEADER = 48  # sizeof(gcmc_grid_bits)
+
+
+def grid_bits_size(rec) -> int:
+    """Bytes a gcmc_grid_bits record needs: the header plus ceil(voxels / 32) words."""
+    if rec.size < GRID_BITS_HEADER:
+        raise ValueError(f"grid holds {rec.size} bytes, a gcmc_grid_bits header needs {GRID_BITS_HEADER}")
+    n = np.frombuffer(rec[32:44].tobytes(), dtype=np.int32)
+    if (n < 1).any():
+        raise ValueError("gcmc_grid_bits: voxel counts must be >= 1")
+    return GRID_BITS_HEADER + 4 * ((int(n[0]) * int(n[1]) * int(n[2]) + 31) // 32)
+
+
+def validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, grid_bits=False):
+    """Dtype, contiguity and size checks against the sizes recorded in SimInfo
+    (``grid_bits``: ``grid`` is a uint8 gcmc_grid_bits record instead of the
+    float list)."""
     spec = [("SimInfo", SimInfo, V.Info_dtype), ("fragmentInfo", fragmentInfo, V.AtomArray_dtype),
             ("residueInfo", residueInfo, V.Residue_dtype), ("atomInfo", atomInfo, V.Atom_dtype),
-            ("grid", grid, np.dtype(np.float32)), ("ff", ff, np.dtype(np.float32)),
-            ("moveArray", moveArray, np.dtype(np.int32))]
+            ("grid", grid, np.dtype(np.uint8) if grid_bits else np.dtype(np.float32)),
+            ("ff", ff, np.dtype(np.float32)), ("moveArray", moveArray, np.dtype(np.int32))]
     for name, a, dt in spec:
         if not isinstance(a, np.ndarray):
             raise TypeError(f"{name} must be a numpy array")
@@ -34,7 +49,7 @@ def validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, move
     need = [("fragmentInfo", fragmentInfo, int(info["fragTypeNum"])),
             ("residueInfo", residueInfo, int(info["totalResNum"])),
             ("atomInfo", atomInfo, int(info["totalAtomNum"])),
-            ("grid", grid, 3 * int(info["totalGridNum"])),
+            ("grid", grid, grid_bits_size(grid) if grid_bits else 3 * int(info["totalGridNum"])),
             ("ff", ff, 2 * int(info["ffXNum"]) * int(info["ffYNum"])),
             ("moveArray", moveArray, int(info["mcsteps"]))]
     for name, a, n in need:
@@ -82,13 +97,16 @@ def runGCMC(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, o
 
     ``options`` (optional, not part of the reference signature) is a
     :class:`pygcmc_b200._native.Options`; the default is the reference's
-    semantics (``proposal=0``, ``muex_kcal=0``).
+    semantics (``proposal=0``, ``muex_kcal=0``).  With ``options.grid_bits``
+    set, ``grid`` is a gcmc_grid_bits record
+    (:func:`pygcmc_b200.system.cavity_bits`) instead of the float list.
     """
-    validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
-    show = int(SimInfo[0]["showInfo"]) > 0
+    opt = options if options is not None else default_options()
+    bits = bool(opt.grid_bits)
+    validate_arrays(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray, grid_bits=bits)
+    show = int(SimInfo[0]["showInfo"]) > 0 and not bits
     if show:
         print_all_info(SimInfo, fragmentInfo, residueInfo, atomInfo, grid, ff, moveArray)
-    opt = options if options is not None else default_options()
     st = lib().gcmc_run_gcmc(ptr(SimInfo), ptr(fragmentInfo), ptr(residueInfo), ptr(atomInfo), ptr(grid),
                              ptr(ff), ptr(moveArray), __import__("ctypes").byref(opt))
     check(st, "runGCMC")
@@ -103,15 +121,19 @@ def runGCMC_batch(replicas, options=None):
     runGCMC arrays -- runs its ``mcsteps`` steps in one device context (one
     pose-energy launch and one accept launch per MC step for all of them; a
     single replica speculates instead, see ``Options.speculate``), and
-    each replica's fragmentInfo/residueInfo/atomInfo are updated in place."""
+    each replica's fragmentInfo/residueInfo/atomInfo are updated in place.
+    With ``options.grid_bits`` set, each System's ``grid_bits`` record (or a
+    tuple's fifth array, a gcmc_grid_bits record) goes in place of the float
+    grid."""
     import ctypes
     from ._native import ReplicaIn
-    arrays = [r.arrays() if hasattr(r, "arrays") else tuple(r) for r in replicas]
+    opt = options if options is not None else default_options()
+    bits = bool(opt.grid_bits)
+    arrays = [r.arrays_for(opt) if hasattr(r, "arrays_for") else tuple(r) for r in replicas]
     for a in arrays:
-        validate_arrays(*a)
+        validate_arrays(*a, grid_bits=bits)
     arr = (ReplicaIn * len(arrays))()
     for i, a in enumerate(arrays):
         arr[i] = ReplicaIn(*[ptr(x) for x in a])
-    opt = options if options is not None else default_options()
     check(lib().gcmc_run_batch(len(arrays), arr, ctypes.byref(opt)), "runGCMC_batch")
     return None

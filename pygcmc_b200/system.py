@@ -45,13 +45,27 @@ class System:
     ff: np.ndarray
     moveArray: np.ndarray
     meta: dict = dataclasses.field(default_factory=dict)
+    # the cavity grid as a gcmc_grid_bits record (uint8: 48-byte header + voxel words), or None
+    grid_bits: Optional[np.ndarray] = None
 
     def arrays(self):
         return (self.SimInfo, self.fragmentInfo, self.residueInfo, self.atomInfo, self.grid, self.ff,
                 self.moveArray)
 
+    def arrays_for(self, options=None):
+        """The seven arrays a run entry point takes under ``options``: with
+        ``options.grid_bits`` set, the ``grid`` slot carries the voxel bit set
+        (:attr:`grid_bits`) instead of the float list."""
+        a = self.arrays()
+        if options is not None and getattr(options, "grid_bits", 0):
+            if self.grid_bits is None:
+                raise ValueError("options.grid_bits is set but this System carries no grid_bits record")
+            a = a[:4] + (self.grid_bits,) + a[5:]
+        return a
+
     def copy(self) -> "System":
-        return System(*(a.copy() for a in self.arrays()), meta=dict(self.meta))
+        return System(*(a.copy() for a in self.arrays()), meta=dict(self.meta),
+                      grid_bits=None if self.grid_bits is None else self.grid_bits.copy())
 
     def pinned(self) -> "System":
         """A copy whose arrays live in page-locked host memory (needs torch with
@@ -59,13 +73,14 @@ class System:
         directly instead of through the driver's staging buffers."""
         import torch
         keep, arrs = [], []
-        for a in self.arrays():
+        extra = () if self.grid_bits is None else (self.grid_bits,)
+        for a in self.arrays() + extra:
             buf = torch.empty(max(1, a.nbytes), dtype=torch.uint8, pin_memory=True)
             v = buf.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
             v[...] = a
             keep.append(buf)
             arrs.append(v)
-        out = System(*arrs, meta=dict(self.meta))
+        out = System(*arrs[:7], meta=dict(self.meta), grid_bits=arrs[7] if extra else None)
         out._page_locked = keep  # the buffers the arrays view
         return out
 
@@ -118,6 +133,33 @@ def cavity_grid(xyz: np.ndarray, cryst: Sequence[float], grid_dx: float = 1.0, c
                              ptr(pts), n.value, ctypes.byref(n), ctypes.byref(factor)), "gcmc_cavity_grid")
     dx = float(grid_dx) if cavity_bias else 1.0
     return [float(v) for v in start], pts, factor.value, dx
+
+
+GRID_BITS_HEADER = 48  # sizeof(gcmc_grid_bits)
+
+
+def cavity_bits(xyz: np.ndarray, cryst: Sequence[float], grid_dx: float = 1.0, cavity_bias: bool = True):
+    """The grid of :func:`cavity_grid` as a ``gcmc_grid_bits`` record
+    (``gcmc_cavity_bits``): a uint8 array holding the 48-byte header (voxel
+    (0, 0, 0) corner, edge, voxels per axis) and one bit per voxel, set for the
+    insertion base points.  Runs with ``Options.grid_bits = 1`` take it in
+    place of the float list: the same points in the same order, 1 bit per voxel
+    instead of 12 bytes per point on the way to the device."""
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    cr = np.ascontiguousarray([float(c) for c in cryst], dtype=np.float64)
+    nw, npts = ctypes.c_int64(0), ctypes.c_int64(0)
+    hdr = np.zeros(GRID_BITS_HEADER, np.uint8)
+    L = lib()
+    st = L.gcmc_cavity_bits(len(xyz), ptr(xyz), ptr(cr), float(grid_dx), int(bool(cavity_bias)), ptr(hdr), None, 0,
+                            ctypes.byref(nw), ctypes.byref(npts))
+    if st == 2 and cavity_bias:
+        raise ValueError("cavity_bias_factor is too small (< 0.05); decrease the grid spacing")
+    check(st, "gcmc_cavity_bits")
+    out = np.zeros(GRID_BITS_HEADER + 4 * nw.value, np.uint8)
+    words = out[GRID_BITS_HEADER:].view(np.uint32)
+    check(L.gcmc_cavity_bits(len(xyz), ptr(xyz), ptr(cr), float(grid_dx), int(bool(cavity_bias)), ptr(out),
+                             ptr(words), nw.value, ctypes.byref(nw), ctypes.byref(npts)), "gcmc_cavity_bits")
+    return out
 
 
 def move_array(nsteps: int, names: Sequence[str], mctime: Sequence[float],
@@ -392,11 +434,13 @@ def water_box(n_water: int = 800, box: float = 30.0, seed: int = 1, mcsteps: int
     if moves is None:
         moves = move_array_np(mcsteps, ["SOL"], [1.0], seed=seed)
     tpl_c = {"xyz": tpl, "q": np.array([-0.834, 0.417, 0.417]), "type": np.array([0, 1, 1])}
-    return assemble(names=["SOL"], templates=[tpl_c], initial=[waters], fixed_xyz=np.zeros((0, 3)),
-                    fixed_q=np.zeros(0), fixed_type=np.zeros(0, int), fixed_group=np.zeros(0, int),
-                    muex=[muex], conc=[conc], conf_bias=[conf_bias], mctime=[1.0], cryst=L, cutoff=cutoff,
-                    grid_dx=dx, start=start, grid=grid, cavity_factor=cav, ff=ff, n_frag_types_ff=len(t1),
-                    n_types_ff=len(t2), moves=moves, seed=seed)
+    s = assemble(names=["SOL"], templates=[tpl_c], initial=[waters], fixed_xyz=np.zeros((0, 3)),
+                 fixed_q=np.zeros(0), fixed_type=np.zeros(0, int), fixed_group=np.zeros(0, int),
+                 muex=[muex], conc=[conc], conf_bias=[conf_bias], mctime=[1.0], cryst=L, cutoff=cutoff,
+                 grid_dx=dx, start=start, grid=grid, cavity_factor=cav, ff=ff, n_frag_types_ff=len(t1),
+                 n_types_ff=len(t2), moves=moves, seed=seed)
+    s.grid_bits = cavity_bits(xyz_all, L, grid_dx)
+    return s
 
 
 def protein_system(seed: int = 1, n_atoms: int = 6000, box: float = 64.0, radius: float = 24.0,
@@ -476,6 +520,7 @@ def protein_system(seed: int = 1, n_atoms: int = 6000, box: float = 64.0, radius
                  conf_bias=[conf_bias] * n_frag, mctime=[1.0] * n_frag, cryst=L, cutoff=cutoff, grid_dx=dx,
                  start=start, grid=grid, cavity_factor=cav, ff=ff, n_frag_types_ff=len(t1), n_types_ff=len(t2),
                  moves=moves, seed=seed)
+    s.grid_bits = cavity_bits(all_xyz, L, grid_dx)
     s.meta.update({"chain_breaks": int(nbreak.value), "n_fixed": n_atoms, "box": box,
                    # per-type CHARMM parameters in the ff column order (t2); rows are t2[:ffX]
                    "lj_types": {"names": list(t2), "eps_kcal": np.array([eps[tnames.index(n)] for n in t2]),
@@ -581,6 +626,7 @@ def slab_system(seed: int = 1, n_atoms: int = 200_000, box=(150.0, 150.0, 120.0)
                  fixed_group=groups, muex=muex, conc=concs, conf_bias=[conf_bias] * nt, mctime=[1.0] * nt, cryst=L,
                  cutoff=cutoff, grid_dx=dx, start=start, grid=grid, cavity_factor=cav, ff=ff,
                  n_frag_types_ff=len(t1), n_types_ff=len(t2), moves=moves, seed=seed)
+    s.grid_bits = cavity_bits(existing.astype(np.float64), L, grid_dx)
     s.meta.update({"chain_breaks": int(nbreak.value), "n_fixed": n_atoms, "box": tuple(L), "slab_thickness": thick,
                    "lj_types": {"names": list(t2),
                                 "eps_kcal": np.array([(eps[tnames.index(n)] if n in tnames else

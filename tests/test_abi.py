@@ -30,7 +30,8 @@ def test_c_struct_sizes(tmp_path):
     src.write_text('#include "gcmc_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
                    'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(Atom), sizeof(AtomArray),'
                    ' sizeof(InfoStruct), sizeof(residue), sizeof(gcmc_options), sizeof(gcmc_step_log),'
-                   ' offsetof(AtomArray, atoms));return 0;}\n')
+                   ' offsetof(AtomArray, atoms));printf("%zu %zu\\n", sizeof(gcmc_grid_bits),'
+                   ' offsetof(gcmc_grid_bits, n));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
     out = [int(x) for x in subprocess.check_output([str(exe)]).split()]
@@ -40,6 +41,8 @@ def test_c_struct_sizes(tmp_path):
     assert out[4] == ctypes.sizeof(Options)
     assert out[5] == StepLog_dtype.itemsize
     assert out[6] == AtomArray_dtype.fields["atoms"][1]
+    from pygcmc_b200.gpu import GRID_BITS_HEADER
+    assert out[7:9] == [GRID_BITS_HEADER, 32]
 
 
 def test_library_exports_every_declared_symbol(native_lib):

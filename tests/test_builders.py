@@ -30,6 +30,48 @@ def test_cavity_grid_matches_reference(gold):
     assert mine == ref and len(grid) == len(gold["ref_grid"])
 
 
+def expand_bits(rec):
+    """CPU expansion of a gcmc_grid_bits record: the marked voxels in increasing
+    voxel index, each corner an FP64 product and sum rounded once to float."""
+    start = np.frombuffer(rec[0:24].tobytes(), np.float64)
+    dx = float(np.frombuffer(rec[24:32].tobytes(), np.float64)[0])
+    n = np.frombuffer(rec[32:44].tobytes(), np.int32).astype(np.int64)
+    words = np.frombuffer(rec[48:].tobytes(), np.uint32)
+    bits = np.unpackbits(words.view(np.uint8), bitorder="little")[: n.prod()]
+    v = np.flatnonzero(bits).astype(np.int64)
+    x, r = np.divmod(v, n[1] * n[2])
+    y, z = np.divmod(r, n[2])
+    return np.stack([x * dx + start[0], y * dx + start[1], z * dx + start[2]], axis=1).astype(np.float32)
+
+
+@pytest.mark.parametrize("bias,dx", [(True, 1.0), (True, 0.7), (False, 1.0)])
+def test_cavity_bits_expand_to_the_float_grid(gold, bias, dx):
+    from pygcmc_b200.system import cavity_bits, cavity_grid
+    start, grid, cav, gdx = cavity_grid(all_atoms(gold), gold["cryst"], dx, cavity_bias=bias)
+    rec = cavity_bits(all_atoms(gold), gold["cryst"], dx, cavity_bias=bias)
+    assert rec.dtype == np.uint8
+    np.testing.assert_array_equal(np.frombuffer(rec[0:24].tobytes(), np.float64), start)
+    assert float(np.frombuffer(rec[24:32].tobytes(), np.float64)[0]) == gdx
+    pts = expand_bits(rec)
+    np.testing.assert_array_equal(pts.view(np.uint32), grid.reshape(-1, 3).view(np.uint32))
+
+
+def test_cavity_bits_of_the_reference_grid(gold):
+    from pygcmc_b200.system import cavity_bits
+    pts = expand_bits(cavity_bits(all_atoms(gold), gold["cryst"], 1.0))
+    assert {tuple(p) for p in pts.tolist()} == {tuple(p) for p in gold["ref_grid"].reshape(-1, 3).tolist()}
+    assert len(pts) * 3 == len(gold["ref_grid"])
+
+
+def test_builders_attach_the_bit_set(protein_small, water_small):
+    for s in (protein_small, water_small):
+        pts = expand_bits(s.grid_bits)
+        assert len(pts) == int(s.SimInfo[0]["totalGridNum"])
+        np.testing.assert_array_equal(pts.reshape(-1).view(np.uint32), s.grid.view(np.uint32))
+        c = s.copy()
+        assert c.grid_bits is not s.grid_bits and np.array_equal(c.grid_bits, s.grid_bits)
+
+
 def test_move_schedule_matches_reference(gold):
     from pygcmc_b200.system import move_array
     mv = move_array(500, ["WAT3", "LIN4"], [1.0, 2.0], rng=random.Random(1234))
