@@ -1032,6 +1032,77 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
     __syncthreads();
 }
 
+// One item of a pose-energy launch (whole warp): item `it` of the replicas'
+// items numbered by the prefix pre (pre[r] = items of the replicas before r).
+// sym: more items than warps (throughput-bound; see nbr_share).  Which: the
+// kinds of items this code path handles (-1 both, 0 / 1 the steps not in / in
+// the difference form).
+template <int Which, int Ew>
+__device__ __forceinline__ void energy_item(const RepDev* __restrict__ reps, int nrep, int mode, WarpBuf& B,
+                                            const int* pre, int it, int lane, bool sym) {
+    int lo = 0, hi = nrep;  // find r with pre[r] <= it < pre[r+1]
+    while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
+    const RepDev& R = reps[lo];
+    const StepDesc D = *R.desc;
+    const int local = it - pre[lo];
+    int i, v, zi, nsl;
+    if (D.varslab) {  // the preparation's list: pose variant e's range zi of pnslab[e]
+        const int pk = R.pitem[local];
+        const int e = pk >> 8;
+        zi = pk & 255;
+        i = e / D.nvar;
+        v = e - i * D.nvar;
+        nsl = R.pnslab[e];
+    } else {
+        // pose fastest: the ranges of one pose go to different CTAs (and SMs), so the
+        // items of a heavy pose do not share one SM's issue slots
+        const int q = local / max(1, D.k);
+        i = local - q * D.k;
+        v = q / D.nslab;
+        zi = q - v * D.nslab;
+        nsl = D.nslab;
+    }
+    float cx, cy, cz;
+    int self;
+    double acc = 0.0;
+    int ng = 0;
+    long long npair = 0;
+    if (Which != 0 && D.dual) {  // translate / rotate: the energy change of both poses in one walk
+        DualCentre dc;
+        build_pose_dual(R, D, i, B, lane, cx, cy, cz, dc, self);
+        keep_sites(R, D, B, i, 0, zi, lane);
+        const int nwin = dc.ws[0] * dc.ws[1] * dc.ws[2];
+        DualSink sink;
+        walk_cells<DualSink, true>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, sink, ng,
+                                   npair, mode == 1 ? R.abort : nullptr, D.step, nsl, &dc);
+        acc = sink.acc;
+    } else if (Which != 1) {
+        build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
+        keep_sites(R, D, B, i, v, zi, lane);
+        const int nwin = R.span[0] * R.span[1] * R.span[2];
+        // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
+        // range samples the whole cutoff sphere and the ranges of a pose take equal time)
+        energy_cells<Ew>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
+                         mode == 1 ? R.abort : nullptr, D.step, nsl);
+        if (Ew && R.pme && zi == 0) {
+            const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
+            acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
+        }
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) {
+        R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
+        if (D.dual) R.epart[(i * D.nvar + 1) * D.nslab + zi] = 0.0;  // the old variant's share
+        atomicAdd(mode == 1 ? R.pairs_pending : &R.counters[2], (unsigned long long)npair);
+    }
+    if (v == 0 && D.nw > 0) {
+        int stop = 0;
+        if (mode == 1 && lane == 0) stop = *reinterpret_cast<const volatile int*>(R.abort) == D.step;
+        if (!__shfl_sync(kFull, stop, 0))
+            nbr_share(R, D, i, zi, nsl, D.varslab ? local : i * D.nslab + zi, lane, sym);
+    }
+}
+
 // One launch per MC step: every replica's (pose, variant, slab) items.
 // Two register budgets of the same kernel, picked per context (gcmc_options.
 // energy_variant, autotuned): MinBlocks = 3 CTAs per SM (up to 85 registers,
@@ -1047,9 +1118,10 @@ __device__ __forceinline__ void items_prefix(int nrep, int* pre, int* wtot, Item
 // gw0 + w of the nwarps that share the items; B: this warp's buffer; pre,
 // wtot: 257 and 32 ints of shared memory.  The body of k_energy_t and of the
 // persistent step loop.  Which: -1 every replica's items; 0 only the items of
-// steps not in the difference form, 1 only those of steps in it (a batch runs
-// the two kinds as separate launches, so that an SM holds one code path's
-// instructions at a time).
+// steps not in the difference form, 1 only those of steps in it (the
+// persistent step loop runs the two kinds one after the other, so that an SM
+// holds one code path's instructions at a time; a batched launch runs both
+// kinds SM-affine, energy_items_affine).
 // queue (optional): a counter, zero before the launch, from which warps take
 // their next item (the items' results do not depend on which warp takes them);
 // without it warp g takes items g, g + nwarps, ...
@@ -1070,68 +1142,47 @@ __device__ __forceinline__ void energy_items(const RepDev* __restrict__ reps, in
         return __shfl_sync(kFull, v, 0);
     };
     for (int it = next_item(-1); it < total; it = next_item(it)) {
-        int lo = 0, hi = nrep;  // find r with pre[r] <= it < pre[r+1]
-        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
-        const RepDev& R = reps[lo];
-        const StepDesc D = *R.desc;
-        const int local = it - pre[lo];
-        int i, v, zi, nsl;
-        if (D.varslab) {  // the preparation's list: pose variant e's range zi of pnslab[e]
-            const int pk = R.pitem[local];
-            const int e = pk >> 8;
-            zi = pk & 255;
-            i = e / D.nvar;
-            v = e - i * D.nvar;
-            nsl = R.pnslab[e];
-        } else {
-            // pose fastest: the ranges of one pose go to different CTAs (and SMs), so the
-            // items of a heavy pose do not share one SM's issue slots
-            const int q = local / max(1, D.k);
-            i = local - q * D.k;
-            v = q / D.nslab;
-            zi = q - v * D.nslab;
-            nsl = D.nslab;
-        }
-        float cx, cy, cz;
-        int self;
-        double acc = 0.0;
-        int ng = 0;
-        long long npair = 0;
-        if (Which != 0 && D.dual) {  // translate / rotate: the energy change of both poses in one walk
-            DualCentre dc;
-            build_pose_dual(R, D, i, B, lane, cx, cy, cz, dc, self);
-            keep_sites(R, D, B, i, 0, zi, lane);
-            const int nwin = dc.ws[0] * dc.ws[1] * dc.ws[2];
-            DualSink sink;
-            walk_cells<DualSink, true>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, sink, ng,
-                                       npair, mode == 1 ? R.abort : nullptr, D.step, nsl, &dc);
-            acc = sink.acc;
-        } else if (Which != 1) {
-            build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
-            keep_sites(R, D, B, i, v, zi, lane);
-            const int nwin = R.span[0] * R.span[1] * R.span[2];
-            // range zi of the pose's window: cells zi, zi + nslab, ... (interleaved, so that every
-            // range samples the whole cutoff sphere and the ranges of a pose take equal time)
-            energy_cells<Ew>(R, B, R.frag[D.ftype].nsites, cx, cy, cz, self, zi, nwin, lane, acc, ng, npair,
-                             mode == 1 ? R.abort : nullptr, D.step, nsl);
-            if (Ew && R.pme && zi == 0) {
-                const float4 a = B.site_abs[lane < kMaxSites ? lane : 0];
-                acc += pme_pose_lane(R, R.frag[D.ftype].nsites, lane, a.x, a.y, a.z, a.w, self);
-            }
-        }
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
-            if (D.dual) R.epart[(i * D.nvar + 1) * D.nslab + zi] = 0.0;  // the old variant's share
-            atomicAdd(mode == 1 ? R.pairs_pending : &R.counters[2], (unsigned long long)npair);
-        }
-        if (v == 0 && D.nw > 0) {
-            int stop = 0;
-            if (mode == 1 && lane == 0) stop = *reinterpret_cast<const volatile int*>(R.abort) == D.step;
-            if (!__shfl_sync(kFull, stop, 0))
-                nbr_share(R, D, i, zi, nsl, D.varslab ? local : i * D.nslab + zi, lane, sym);
-        }
+        energy_item<Which, Ew>(reps, nrep, mode, B, pre, it, lane, sym);
         __syncwarp();
+    }
+}
+
+// Both kinds of items in one launch (a batch whose replicas' steps lie in and
+// out of the difference form): the warps of an SM take the kind its SM index
+// selects, the SMs split between the kinds in proportion to their item counts,
+// so that an SM fetches one code path's instructions; a warp whose kind has run
+// out then takes the other kind's remaining items.  Items come from the
+// counters queue[0] (steps not in the difference form) and queue[1] (steps in
+// it), zero before the launch; pre0 / pre1: 257 ints of shared memory each.
+template <int Ew>
+__device__ __forceinline__ void energy_items_affine(const RepDev* __restrict__ reps, int nrep, int mode, int nwarps,
+                                                    WarpBuf& B, int* pre0, int* pre1, int* wtot, int* queue) {
+    const int lane = threadIdx.x & 31;
+    items_prefix(nrep, pre0, wtot, [&](int r) {
+        const StepDesc* d = reps[r].desc;
+        return d->dual ? 0 : d->items;
+    });
+    items_prefix(nrep, pre1, wtot, [&](int r) {
+        const StepDesc* d = reps[r].desc;
+        return d->dual ? d->items : 0;
+    });
+    const int t0 = pre0[nrep], t1 = pre1[nrep];
+    const bool sym = t0 + t1 > nwarps;
+    unsigned smid, nsm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+    int kind = ((long long)smid * (t0 + t1) < (long long)t0 * nsm) ? 0 : 1;
+    for (int pass = 0; pass < 2; ++pass, kind ^= 1) {
+        const int total = kind ? t1 : t0;
+        for (;;) {
+            int v = 0;
+            if (lane == 0) v = atomicAdd(&queue[kind], 1);
+            const int it = __shfl_sync(kFull, v, 0);
+            if (it >= total) break;
+            if (kind == 0) energy_item<0, Ew>(reps, nrep, mode, B, pre0, it, lane, sym);
+            else energy_item<1, Ew>(reps, nrep, mode, B, pre1, it, lane, sym);
+            __syncwarp();
+        }
     }
 }
 
@@ -1147,8 +1198,14 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     // stride, which saves the counter's round trip per item
     StepDesc* d0 = reps[0].desc;
     const int q = Which == 1 ? 1 : 0;
-    energy_items<Which, Ew>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5],
-                            pre, wtot, nrep > 1 ? &d0->queue[q] : nullptr);
+    if (Which == 2) {  // both kinds, SM-affine (batches only)
+        __shared__ int pre1[257];
+        energy_items_affine<Ew>(reps, nrep, mode, gridDim.x * kWarpsE, bufs[threadIdx.x >> 5], pre, pre1, wtot,
+                                d0->queue);
+    } else {
+        energy_items<Which, Ew>(reps, nrep, mode, blockIdx.x * kWarpsE, gridDim.x * kWarpsE,
+                                bufs[threadIdx.x >> 5], pre, wtot, nrep > 1 ? &d0->queue[q] : nullptr);
+    }
     if (nrep == 1) return;
     // the last CTA to finish resets the counter for the next launch (every warp has taken
     // its last item once its CTA arrives here)
@@ -1157,6 +1214,7 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
         __threadfence();
         if (atomicAdd(&d0->done[q], 1) == (int)gridDim.x - 1) {
             d0->queue[q] = 0;
+            if (Which == 2) d0->queue[1] = 0;
             d0->done[q] = 0;
             __threadfence();
         }
@@ -1169,6 +1227,8 @@ template __global__ void k_energy_t<3, 0, 0>(const RepDev* __restrict__, int, in
 template __global__ void k_energy_t<4, 0, 0>(const RepDev* __restrict__, int, int);
 template __global__ void k_energy_t<3, 1, 0>(const RepDev* __restrict__, int, int);
 template __global__ void k_energy_t<4, 1, 0>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_t<3, 2, 0>(const RepDev* __restrict__, int, int);  // both kinds, SM-affine
+template __global__ void k_energy_t<4, 2, 0>(const RepDev* __restrict__, int, int);
 template __global__ void k_energy_t<3, -1, 1>(const RepDev* __restrict__, int, int);  // Ewald contexts
 template __global__ void k_energy_t<4, -1, 1>(const RepDev* __restrict__, int, int);
 

@@ -922,6 +922,7 @@ EnergyKernel energy_kernel(int variant, int which = -1, bool ew = false) {
     if (ew) return variant == 1 ? k_energy_t<4, -1, 1> : k_energy_t<3, -1, 1>;
     if (which == 0) return variant == 1 ? k_energy_t<4, 0, 0> : k_energy_t<3, 0, 0>;
     if (which == 1) return variant == 1 ? k_energy_t<4, 1, 0> : k_energy_t<3, 1, 0>;
+    if (which == 2) return variant == 1 ? k_energy_t<4, 2, 0> : k_energy_t<3, 2, 0>;
     return variant == 1 ? k_energy_t<4, -1, 0> : k_energy_t<3, -1, 0>;
 }
 
@@ -931,10 +932,9 @@ void launch_energy(const gcmc_ctx* ctx, const RepDev* reps, int n, int mode, int
     if (ctx->tiled) {
         k_energy_tiles<<<grid, kWarpsT * 32, sizeof(TileSmem), s>>>(reps, n, mode);
     } else if (n > 1 && ctx->dual_any && !ctx->pme_any) {
-        // a batch mixes the two kinds of items: one launch each, so that an SM runs one
-        // code path at a time (both in one launch stalled on instruction fetch)
-        energy_kernel(ctx->evar, 0)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
-        energy_kernel(ctx->evar, 1)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
+        // a batch mixes the two kinds of items: one launch whose SMs each take one kind
+        // (an SM that ran both code paths at once stalled on instruction fetch)
+        energy_kernel(ctx->evar, 2)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
     } else {
         energy_kernel(ctx->evar, -1, ctx->pme_any)<<<grid, kWarpsE * 32, 0, s>>>(reps, n, mode);
     }
