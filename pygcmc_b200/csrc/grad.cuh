@@ -191,13 +191,17 @@ __global__ void __launch_bounds__(kWarpsG * 32)
 // ---------------------------------------------------------------------------
 // Pose energies with forces for force-biased translate/rotate steps.
 //
-// phase 1: items (pose i, slab) of the OLD poses: energy partial (variant 1)
-//          and force/torque partials; the last item of a pose to finish (a
-//          per-pose counter after a fence) sums them in slab order and draws
-//          the pose's proposal (new centre, d, z).
-// phase 2: the step's ordinary items, except that a force-biased step's items
-//          are (pose i, slab) of the NEW poses (variant 0) with forces.
-// Non-force-biased steps have no phase-1 items and run the energy path.
+// phase 1: items (pose i, slab) of the OLD poses of force-biased steps:
+//          energy partial (variant 1) and force/torque partials; the last item
+//          of a pose to finish (a per-pose counter after a fence) sums them in
+//          slab order and draws the pose's proposal (new centre, d, z).  The
+//          ordinary items of the other steps (insert / delete), which depend on
+//          no proposal, run here too.
+// phase 2: items (pose i, slab) of the NEW poses (variant 0) of force-biased
+//          steps, with forces.
+// Several replicas: warps take items from a counter per phase (the step
+// descriptor of the first replica; the launch's last CTA resets it), which
+// balances uneven items; one replica: a fixed stride.
 // ---------------------------------------------------------------------------
 // (Five CTAs per SM: at most 102 registers a thread, the budget that keeps
 // 20 warps per SM resident.)
@@ -209,18 +213,27 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     items_prefix(nrep, pre, wtot, [&](int r) {
         const StepDesc* d = reps[r].desc;
-        return phase == 1 ? d->items_pre : d->items;
+        return phase == 1 ? (d->fb ? d->items_pre : d->items) : (d->fb ? d->items : 0);
     });
     const int total = pre[nrep];
-    const bool sym = total > (int)(gridDim.x * kWarpsG);
+    const int nwarps = (int)(gridDim.x * kWarpsG);
+    const bool sym = total > nwarps;
     WarpBuf& B = bufs[warp];
-    for (int it = blockIdx.x * kWarpsG + warp; it < total; it += gridDim.x * kWarpsG) {
+    StepDesc* d0 = reps[0].desc;
+    const int qi = phase == 1 ? 0 : 1;
+    auto next_item = [&](int prev) {
+        if (nrep == 1) return prev < 0 ? (int)blockIdx.x * kWarpsG + warp : prev + nwarps;
+        int v = 0;
+        if (lane == 0) v = atomicAdd(&d0->queue[qi], 1);
+        return __shfl_sync(kFull, v, 0);
+    };
+    for (int it = next_item(-1); it < total; it = next_item(it)) {
         int lo = 0, hi = nrep;
         while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
         const RepDev& R = reps[lo];
         const StepDesc D = *R.desc;
         const int local = it - pre[lo];
-        const bool fbitem = phase == 1 || D.fb;
+        const bool fbitem = D.fb != 0;
         const int q = local / max(1, D.k);  // pose fastest, as in k_energy_t
         const int i = local - q * D.k;
         const int v = fbitem ? (phase == 1 ? 1 : 0) : q / D.nslab;
@@ -228,7 +241,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
         float cx, cy, cz;
         int self;
         build_pose(R, D, i, v, B, lane, cx, cy, cz, self);
-        if (phase != 1) keep_sites(R, D, B, i, v, zi, lane);
+        if (!(phase == 1 && fbitem)) keep_sites(R, D, B, i, v, zi, lane);
         const int ns = R.frag[D.ftype].nsites;
         const int nwin = R.span[0] * R.span[1] * R.span[2];
         const int c0 = zi, c1 = nwin;  // interleaved range: cells zi, zi + nslab, ...
@@ -288,7 +301,7 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
             R.epart[(i * D.nvar + v) * D.nslab + zi] = acc;
             atomicAdd(&R.counters[2], (unsigned long long)npair);
         }
-        if (phase == 1) {  // the last item of pose i draws its proposal
+        if (phase == 1 && fbitem) {  // the last item of pose i draws its proposal
             int last = 0;
             if (lane == 0) {
                 __threadfence();
@@ -308,6 +321,17 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
             nbr_share(R, D, i, zi, D.nslab, i * D.nslab + zi, lane, sym);
         }
         __syncwarp();
+    }
+    if (nrep == 1) return;
+    // the last CTA to finish resets the counter for the next launch
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&d0->done[qi], 1) == (int)gridDim.x - 1) {
+            d0->queue[qi] = 0;
+            d0->done[qi] = 0;
+            __threadfence();
+        }
     }
 }
 
