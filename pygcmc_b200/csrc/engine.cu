@@ -1167,16 +1167,16 @@ int build_graph(gcmc_ctx* ctx) {
         st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) {
         side[0] = ctx->stream;
-        double tot = 0.0;
-        for (int r = 0; r < ctx->nrep; ++r) tot += (double)ctx->reps[r].natoms + 1.0;
         cudaError_t e = cudaEventRecord(ev[0], ctx->stream);
         for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(side[b], ev[0], 0);
         for (int b = 0; b < nb && e == cudaSuccess; ++b) {
             const int r0 = ctx->br_off[b], cnt = ctx->br_off[b + 1] - r0;
-            double part = 0.0;
-            for (int r = r0; r < r0 + cnt; ++r) part += (double)ctx->reps[r].natoms + 1.0;
-            const int grid = nb == 1 ? ctx->gridE : std::max(1, (int)std::ceil(ctx->gridE * part / tot));
-            const int gridf = nb == 1 ? ctx->gridF : std::max(1, (int)std::ceil(ctx->gridF * part / tot));
+            // every branch's pose-energy launch on the whole grid: its warps take items from
+            // the branch's own counter, so a branch whose neighbour sits in its accept kernel
+            // (one CTA per replica) spreads over the SMs left free (a grid in proportion to
+            // the branch's atoms left them idle: 358 against 306 us per 64-replica step)
+            const int grid = ctx->gridE;
+            const int gridf = ctx->gridF;
             for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) {
                 for (int r = r0; r < r0 + cnt; ++r)
                     if (pme_update(ctx, r, side[b]) != GCMC_OK) e = cudaErrorUnknown;
