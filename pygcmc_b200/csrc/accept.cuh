@@ -371,6 +371,7 @@ __global__ void k_set_run_end(RepDev* reps, int nrep, int nsteps) {
 // copy's step again from the current state unless its speculation stands.
 __global__ void __launch_bounds__(kAcceptThreads) k_prep_spec(const RepDev* __restrict__ reps, int mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();  // the completion pose-energy launch may start (it waits for this grid's results)
     int* scratch = reinterpret_cast<int*>(smem_raw);
     const RepDev& R = reps[0];
     if (mode == 0) {
@@ -952,6 +953,7 @@ __device__ __forceinline__ void accept_step(const RepDev& R, int spec, unsigned 
 template <bool Pme>
 __global__ void __launch_bounds__(kAcceptThreads, 1) k_accept(const RepDev* __restrict__ reps, int nrep, int spec) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_wait();  // a speculating graph launches this kernel as a dependent of the pose energies
     accept_step<Pme>(reps[blockIdx.x], spec, smem_raw);
 }
 template __global__ void k_accept<false>(const RepDev* __restrict__, int, int);

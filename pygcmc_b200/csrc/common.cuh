@@ -98,6 +98,15 @@ __device__ __forceinline__ bool within_cutoff(float ax, float ay, float az, floa
     return (Host ? dist_host(ax, ay, az, bx, by, bz, L) : dist_group(ax, ay, az, bx, by, bz, L)) <= cutoff;
 }
 
+// Programmatic dependent launch (PTX griddepcontrol): a kernel launched as a
+// programmatic dependent of the kernel before it in its stream may start while
+// that kernel runs; pdl_wait blocks until the prerequisite grid has completed
+// and its memory operations are visible (it returns at once when the kernel
+// was launched normally), and pdl_trigger lets this grid's dependents be
+// scheduled once every CTA of it has triggered or exited.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter (step, index,
 // purpose<<16 | draw, 0), key (seed, replica).

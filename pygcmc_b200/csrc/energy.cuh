@@ -1192,7 +1192,13 @@ __global__ void __launch_bounds__(kWarpsE * 32, MinBlocks) k_energy_t(const RepD
     __shared__ WarpBuf bufs[kWarpsE];
     __shared__ int pre[257];
     __shared__ int wtot[32];
+    // the completion launch of a speculating graph is a programmatic dependent of the step's
+    // re-preparation: a standing step (valid, set by the accept kernel of the step before,
+    // which completed before the re-preparation began) returns at once; otherwise wait for
+    // the re-preparation's results.  Then the accept kernel may be scheduled.
     if (mode == 2 && *reps[0].valid) return;
+    pdl_wait();
+    pdl_trigger();
     // several replicas (throughput-bound launches): warps take items from a counter, which
     // balances uneven items; one replica (latency-bound, about one item per warp): a fixed
     // stride, which saves the counter's round trip per item

@@ -1083,7 +1083,29 @@ void split_branches(gcmc_ctx* ctx, int nb) {
 // once P and F_e are done, on the SMs that A leaves free, stopping early when
 // A accepts a move.  F_p of step j + 1 waits for A and S.  One graph per
 // parity of the run's first step (kGraphSteps is even).
-int build_spec_graph(gcmc_ctx* ctx, int parity) {
+// Launch of `kernel` on s as a programmatic dependent of the kernel before it in
+// s: it may be scheduled once every CTA of that kernel has triggered (pdl_trigger)
+// and waits in pdl_wait for that kernel's results, so its launch latency overlaps
+// the kernel before it.
+template <class... Args, class... Act>
+cudaError_t launch_dependent(void (*kernel)(Args...), int grid, int block, size_t smem, cudaStream_t s,
+                             Act... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// pdl: the step's completion pose-energy launch and accept kernel as programmatic
+// dependents of the kernels before them (F_p -> F_e -> accept).
+int build_spec_graph(gcmc_ctx* ctx, int parity, bool pdl) {
     cudaStream_t sp = nullptr, ss = nullptr;
     cudaEvent_t ev[4 * kGraphSteps + 1] = {};
     int st = GCMC_OK;
@@ -1108,9 +1130,21 @@ int build_spec_graph(gcmc_ctx* ctx, int parity) {
             const RepDev* nxt = ((parity + i) & 1) ? ctx->d_reps : ctx->d_reps_b;
             if (i > 0) e = cudaStreamWaitEvent(ctx->stream, evS[i - 1], 0);
             k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), ctx->stream>>>(cur, 1);
-            launch_energy(ctx, cur, 1, 2, ctx->gridE, ctx->stream);
+            if (pdl && !ctx->tiled) {
+                if (e == cudaSuccess)
+                    e = launch_dependent(energy_kernel(ctx->evar, -1, ctx->pme_any), ctx->gridE, kWarpsE * 32, 0,
+                                         ctx->stream, cur, 1, 2);
+            } else {
+                launch_energy(ctx, cur, 1, 2, ctx->gridE, ctx->stream);
+            }
             if (e == cudaSuccess) e = cudaEventRecord(evF[i], ctx->stream);
-            k_accept<false><<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);  // (speculating: no Ewald)
+            if (pdl) {  // (speculating: no Ewald)
+                if (e == cudaSuccess)
+                    e = launch_dependent(k_accept<false>, 1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream, cur, 1,
+                                         1);
+            } else {
+                k_accept<false><<<1, kAcceptThreads, sizeof(AcceptSmem), ctx->stream>>>(cur, 1, 1);
+            }
             if (e == cudaSuccess) e = cudaEventRecord(evA[i], ctx->stream);
             if (i > 0 && e == cudaSuccess) e = cudaStreamWaitEvent(sp, evA[i - 1], 0);
             k_prep_spec<<<1, kAcceptThreads, prep_smem(ctx), sp>>>(nxt, 0);
@@ -1150,8 +1184,18 @@ int build_graph(gcmc_ctx* ctx) {
             g = nullptr;
         }
     if (ctx->spec) {
-        int st = build_spec_graph(ctx, 0);
-        if (st == GCMC_OK) st = build_spec_graph(ctx, 1);
+        int st = build_spec_graph(ctx, 0, true);
+        if (st == GCMC_OK) st = build_spec_graph(ctx, 1, true);
+        if (st != GCMC_OK) {  // a driver that cannot capture programmatic launches: plain launches
+            for (auto& g : ctx->gexec_spec)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+            cudaGetLastError();
+            st = build_spec_graph(ctx, 0, false);
+            if (st == GCMC_OK) st = build_spec_graph(ctx, 1, false);
+        }
         return st;
     }
     const int nb = ctx->branches;
