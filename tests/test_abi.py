@@ -84,6 +84,26 @@ def test_create_rejects_inconsistent_input_without_gpu(water_small):
     assert e.value.status == 3
 
 
+def test_batched_create_validates_every_replica_without_gpu(water_small, protein_small):
+    """A batch's replicas are validated on host threads before any device call: a
+    bad replica anywhere in the batch is reported (status 2), a good batch gets
+    past validation (status 5 = no CUDA device here, or 0 on a GPU box)."""
+    from pygcmc_b200._native import GcmcError
+    from pygcmc_b200.engine import Engine
+    good = [water_small.copy() if i % 2 else protein_small.copy() for i in range(6)]
+    for bad_at in (0, 3, 5):
+        batch = [s.copy() for s in good]
+        atoms = batch[bad_at].atomInfo
+        atoms["type"][0] = 999  # a fixed (or occupied) atom's type outside the pair table
+        with pytest.raises(GcmcError) as e:
+            Engine(batch)
+        assert e.value.status == 2
+    try:
+        Engine([s.copy() for s in good]).close()
+    except GcmcError as e:
+        assert e.status == 5
+
+
 def test_reference_binding_links_to_this_library():
     """The reference's CPython binding (gcmc/cpp/gcmc.cpp, unmodified) built
     against libgcmc_b200.so loads and exposes runGCMC (calling it needs a GPU)."""
