@@ -188,6 +188,7 @@ struct gcmc_ctx {
     int ebps = 0;        // requested pose-energy CTAs per SM (0 = occupancy limit)
     int evar = 0;        // pose-energy kernel variant: 0 = 3 CTAs per SM, 1 = 4 CTAs per SM
     int fb = 0;          // force-biased moves: two pose-energy launches per step (k_energy_fb)
+    bool fb_mixed = false;  // several replicas whose move schedules differ
     bool tiled = false;  // pose energies by k_energy_tiles (every replica allows it)
     bool pme_any = false; // some replica runs Ewald electrostatics
     bool dual_any = false; // some replica evaluates translate / rotate changes in the difference form
@@ -1019,6 +1020,24 @@ int pme_init_fixed(gcmc_ctx* ctx) {
     return GCMC_OK;
 }
 
+// The force-bias pose-energy kernel: with the SM-affine split of its first launch
+// when the replicas' move schedules differ (a launch may then hold both kinds of
+// items), without it otherwise.
+using FbKernel = void (*)(const RepDev*, int, int);
+FbKernel fb_kernel(const gcmc_ctx* ctx) { return ctx->fb_mixed ? k_energy_fb<true> : k_energy_fb<false>; }
+
+// Whether the replicas' move schedules differ (over the steps all of them hold).
+void find_mixed_moves(gcmc_ctx* ctx) {
+    bool mixed = false;
+    const auto& m0 = ctx->reps[0].moves_host;
+    for (int r = 1; r < ctx->nrep && !mixed; ++r) {
+        const auto& m = ctx->reps[r].moves_host;
+        const size_t n = std::min(m.size(), m0.size());
+        mixed = m.size() != m0.size() || !std::equal(m.begin(), m.begin() + n, m0.begin());
+    }
+    ctx->fb_mixed = mixed;
+}
+
 // Pose-energy grid: SMs x min(occupancy limit, requested CTAs per SM).
 int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     int sms = 0, per_sm = 0;
@@ -1035,7 +1054,7 @@ int set_energy_grid(gcmc_ctx* ctx, int ebps) {
     ctx->per_sm_e = per_sm;
     ctx->gridE = std::max(1, sms) * per_sm;
     int per_sm_f = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_energy_fb, kWarpsG * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, fb_kernel(ctx), kWarpsG * 32, 0));
     ctx->gridF = std::max(1, sms) * std::max(1, per_sm_f);
     return GCMC_OK;
 }
@@ -1225,8 +1244,8 @@ int build_graph(gcmc_ctx* ctx) {
                 for (int r = r0; r < r0 + cnt; ++r)
                     if (pme_update(ctx, r, side[b]) != GCMC_OK) e = cudaErrorUnknown;
                 if (ctx->fb) {
-                    k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
-                    k_energy_fb<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
+                    fb_kernel(ctx)<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 1);
+                    fb_kernel(ctx)<<<gridf, kWarpsG * 32, 0, side[b]>>>(ctx->d_reps + r0, cnt, 2);
                 } else {
                     launch_energy(ctx, ctx->d_reps + r0, cnt, 0, grid, side[b]);
                 }
@@ -1334,7 +1353,10 @@ int create_impl(int nrep, const gcmc_replica_in* ins, const gcmc_options* optp, 
     for (int r = 0; r < nrep; ++r) ctx->reps[r].frag_atoms = frag_atoms[r];
     ctx->spec = spec_eligible(nrep, ins, opt);
     if (st == GCMC_OK) st = for_each_rep(nrep, ctx->device, [&](int r) { return setup_rep(ctx, r, ins[r], opt); });
-    if (st == GCMC_OK) finalize_tiling(ctx);
+    if (st == GCMC_OK) {
+        finalize_tiling(ctx);
+        find_mixed_moves(ctx);
+    }
     if (st == GCMC_OK && cudaMalloc(&ctx->d_reps, sizeof(RepDev) * nrep) != cudaSuccess) st = GCMC_ERR_CUDA;
     if (st == GCMC_OK) st = upload_reps(ctx);
     if (st == GCMC_OK) {
@@ -1394,6 +1416,8 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     if (st != GCMC_OK) return st;
     if (trace_on()) g_trace[1] = now_ms();
     finalize_tiling(ctx);
+    const bool mixed_before = ctx->fb_mixed;
+    find_mixed_moves(ctx);
     st = upload_reps(ctx);
     if (st != GCMC_OK) return st;
     build_cells(ctx);
@@ -1407,7 +1431,8 @@ int refill_impl(gcmc_ctx* ctx, int nrep, const gcmc_replica_in* ins, const gcmc_
     const bool had_graph = ctx->gexec || ctx->gexec_spec[0];
     const bool shape_changed = spec_changed || nb != ctx->branches || opt.energy_blocks_per_sm != ctx->ebps ||
                                fb != ctx->fb || evar != ctx->evar || ctx->tiled != tiled_before ||
-                               ctx->pme_any != pme_before || ctx->dual_any != dual_before;
+                               ctx->pme_any != pme_before || ctx->dual_any != dual_before ||
+                               ctx->fb_mixed != mixed_before;
     ctx->fb = fb;
     ctx->evar = evar;
     st = setup_persist(ctx, opt);
@@ -1867,8 +1892,8 @@ int gcmc_run_profiled(gcmc_ctx* ctx, int32_t nsteps, float* ms_energy, float* ms
         }
         CK(cudaEventRecord(ev[3 * i], ctx->stream));
         if (ctx->fb) {
-            k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
-            k_energy_fb<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
+            fb_kernel(ctx)<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 1);
+            fb_kernel(ctx)<<<ctx->gridF, kWarpsG * 32, 0, ctx->stream>>>(ctx->d_reps, ctx->nrep, 2);
         } else {
             launch_energy(ctx, ctx->d_reps, ctx->nrep, 0, ctx->gridE, ctx->stream);
         }

@@ -205,34 +205,71 @@ __global__ void __launch_bounds__(kWarpsG * 32)
 // ---------------------------------------------------------------------------
 // (Five CTAs per SM: at most 102 registers a thread, the budget that keeps
 // 20 warps per SM resident.)
+// Mixed: the replicas' move schedules differ, so that one launch can hold both
+// kinds of first-launch items (the SM-affine split below is compiled in only then).
+template <bool Mixed>
 __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __restrict__ reps, int nrep, int phase) {
     __shared__ WarpBuf bufs[kWarpsG];
     __shared__ GradStage stages[kWarpsG];
     __shared__ int pre[257];
+    __shared__ int pre2[257];
     __shared__ int wtot[kWarpsG];
+    __shared__ int kinds;  // bit 0: old poses of force-biased steps, bit 1: ordinary items
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // A batch's first launch can hold two kinds of items, the old poses of force-biased
+    // steps (gradient sink) and the ordinary items of the other steps: then each SM's warps
+    // take the kind their SM index selects (SMs split in proportion to the kinds' item
+    // counts, one counter per kind), then the other kind's remainder, so that an SM fetches
+    // one code path's instructions at a time.  Otherwise one kind, one counter (one
+    // replica: a fixed stride).
+    if (threadIdx.x == 0) kinds = 0;
+    __syncthreads();
     items_prefix(nrep, pre, wtot, [&](int r) {
         const StepDesc* d = reps[r].desc;
-        return phase == 1 ? (d->fb ? d->items_pre : d->items) : (d->fb ? d->items : 0);
+        const int n = phase == 1 ? (d->fb ? d->items_pre : d->items) : (d->fb ? d->items : 0);
+        if (Mixed && phase == 1 && n > 0) atomicOr(&kinds, d->fb ? 1 : 2);
+        return n;
     });
-    const int total = pre[nrep];
+    const bool affine = Mixed && phase == 1 && nrep > 1 && kinds == 3;
+    if (affine) {
+        items_prefix(nrep, pre, wtot, [&](int r) {
+            const StepDesc* d = reps[r].desc;
+            return d->fb ? d->items_pre : 0;
+        });
+        items_prefix(nrep, pre2, wtot, [&](int r) {
+            const StepDesc* d = reps[r].desc;
+            return d->fb ? 0 : d->items;
+        });
+    }
+    const int t0 = pre[nrep], t1 = affine ? pre2[nrep] : 0;
     const int nwarps = (int)(gridDim.x * kWarpsG);
-    const bool sym = total > nwarps;
+    const bool sym = t0 + t1 > nwarps;
     WarpBuf& B = bufs[warp];
     StepDesc* d0 = reps[0].desc;
     const int qi = phase == 1 ? 0 : 1;
+    int kind = 0;  // affine: 0 old poses of force-biased steps (queue[0]), 1 ordinary items (queue[1])
+    if (affine) {
+        unsigned smid, nsm;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+        kind = ((long long)smid * (t0 + t1) < (long long)t0 * nsm) ? 0 : 1;
+    }
+    for (int pass = 0; pass < (affine ? 2 : 1); ++pass, kind ^= 1) {
+    const int* P = kind ? pre2 : pre;
+    const int total = kind ? t1 : t0;
+    int* queue = &d0->queue[affine ? kind : qi];
     auto next_item = [&](int prev) {
         if (nrep == 1) return prev < 0 ? (int)blockIdx.x * kWarpsG + warp : prev + nwarps;
         int v = 0;
-        if (lane == 0) v = atomicAdd(&d0->queue[qi], 1);
+        if (lane == 0) v = atomicAdd(queue, 1);
         return __shfl_sync(kFull, v, 0);
     };
     for (int it = next_item(-1); it < total; it = next_item(it)) {
         int lo = 0, hi = nrep;
-        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (pre[mid] <= it) lo = mid; else hi = mid; }
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (P[mid] <= it) lo = mid; else hi = mid; }
         const RepDev& R = reps[lo];
         const StepDesc D = *R.desc;
-        const int local = it - pre[lo];
+        const int local = it - P[lo];
         const bool fbitem = D.fb != 0;
         const int q = local / max(1, D.k);  // pose fastest, as in k_energy_t
         const int i = local - q * D.k;
@@ -322,18 +359,23 @@ __global__ void __launch_bounds__(kWarpsG * 32, 5) k_energy_fb(const RepDev* __r
         }
         __syncwarp();
     }
+    }
     if (nrep == 1) return;
-    // the last CTA to finish resets the counter for the next launch
+    // the last CTA to finish resets the counters for the next launch
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&d0->done[qi], 1) == (int)gridDim.x - 1) {
             d0->queue[qi] = 0;
+            if (affine) d0->queue[1] = 0;
             d0->done[qi] = 0;
             __threadfence();
         }
     }
 }
+
+template __global__ void k_energy_fb<false>(const RepDev* __restrict__, int, int);
+template __global__ void k_energy_fb<true>(const RepDev* __restrict__, int, int);
 
 // gxyz[p][s][3], gq[p][s] = the slabs' partial sums in slab order (FP64).
 __global__ void k_sum_grad(const float4* __restrict__ part, int nposes, int nslab, int ns,
