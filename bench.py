@@ -941,6 +941,10 @@ def run_probe(args):
                               pair_delta=args.pair_delta)
     else:
         opt = default_options(cells_per_cutoff=args.cells if args.cells > 0 else 2, pair_delta=args.pair_delta)
+    if args.probe_fb:  # force-biased translate / rotate (h 2 A, 40 degrees)
+        opt.proposal = 2
+        opt.fb_trn = 2.0
+        opt.fb_rot = float(np.radians(40.0))
     if args.probe_pme > 0:  # Ewald electrostatics on a probe_pme^3 mesh
         opt.pme = 1
         for a in range(3):
@@ -990,6 +994,7 @@ def main():
     ap.add_argument("--probe-warm", type=int, default=64)
     ap.add_argument("--probe-steps", type=int, default=24)
     ap.add_argument("--probe-pme", type=int, default=0, help="probe: Ewald electrostatics on an N^3 mesh")
+    ap.add_argument("--probe-fb", action="store_true", help="probe: force-biased translate / rotate")
     ap.add_argument("--pair-delta", type=int, default=0,
                     help="probe: translate/rotate changes in the pairwise-difference form (0) or as two evaluations (-1)")
     ap.add_argument("--write-inputs", default="", help=argparse.SUPPRESS)  # reference arm's child process
