@@ -72,12 +72,16 @@ def test_force_biased_trajectory_matches_oracle(request, oracle_lib, which):
     assert np.array_equal(final_g.residueInfo["position"][rr], s_o.residueInfo["position"][rr])
 
 
-def test_force_biased_replicas_and_branches_match_single(protein_small, water_small):
+@pytest.mark.parametrize("branches", [1, 2])
+def test_force_biased_replicas_and_branches_match_single(protein_small, water_small, branches):
+    """Replicas with different move schedules in one context (a launch then holds
+    force-biased and plain items, split between SMs) give each replica the chain it
+    has alone."""
     from pygcmc_b200._native import default_options
     from pygcmc_b200.engine import Engine
     systems = [protein_small.copy(), water_small.copy(), protein_small.copy()]
     n = 64
-    with Engine([x.copy() for x in systems], default_options(proposal=2, branches=2)) as eng:
+    with Engine([x.copy() for x in systems], default_options(proposal=2, branches=branches)) as eng:
         eng.run(n)
         eng.sync()
         finals = [eng.download(k) for k in range(3)]
