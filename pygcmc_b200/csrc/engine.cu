@@ -519,7 +519,8 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     h.natoms = I->totalAtomNum;
     h.ngroups = I->totalResNum;
     h.ntypes = I->fragTypeNum;
-    h.G = I->totalGridNum;
+    // no grid array (accepted when the schedule holds no insertion): no base points
+    h.G = (in.grid && I->totalGridNum > 0) ? I->totalGridNum : 0;
     h.ffX = I->ffXNum;
     h.ffY = I->ffYNum;
     h.mcsteps = I->mcsteps;
@@ -592,7 +593,7 @@ int setup_rep(gcmc_ctx* ctx, int r, const gcmc_replica_in& in, const gcmc_option
     d.ntypes = I->fragTypeNum;
     d.ffX = I->ffXNum;
     d.ffY = I->ffYNum;
-    d.G = I->totalGridNum;
+    d.G = h.G;
     d.mcsteps = I->mcsteps;
     d.seed = I->seed;
     d.replica = opt.replica + (uint32_t)r;

@@ -101,6 +101,37 @@ def test_bits_past_the_last_voxel_are_ignored(water_small):
     _same(_run([water_small], 60, grid_bits=1), _run([s], 60, grid_bits=1))
 
 
+def test_no_grid_array_without_insertions(protein_small):
+    """A schedule without insertions needs no cavity grid: a NULL grid argument (either
+    grid form) runs the same chain as with the grid."""
+    import ctypes
+    from pygcmc_b200._native import ReplicaIn, check, default_options, lib, ptr
+    from pygcmc_b200.engine import Engine
+    n = 60
+    s = protein_small.copy()
+    mv = s.moveArray.copy()
+    mv[(mv % 4) == 0] += 1  # insertions become deletions
+    s.moveArray = mv
+    ref = _run([s], n)
+    for bits in (0, 1):
+        t = s.copy()
+        opts = default_options(log_steps=n, log_kmax=LOG_KMAX, grid_bits=bits)
+        arr = (ReplicaIn * 1)()
+        a = t.arrays()
+        arr[0] = ReplicaIn(*[ptr(x) for x in a[:4]], None, *[ptr(x) for x in a[5:]])
+        h = ctypes.c_void_p()
+        check(lib().gcmc_create(1, arr, ctypes.byref(opts), None, ctypes.byref(h)), "gcmc_create")
+        eng = Engine.__new__(Engine)
+        eng.systems, eng.options, eng._in, eng._h = [t], opts, arr, h
+        with eng:
+            eng.run(n)
+            eng.sync()
+            assert eng.device_error() == 0
+            logs, E = eng.logs(0)
+            out = [(logs, E, eng.download(0), eng.counters(0))]
+        _same(ref, out)
+
+
 def test_count_mismatch_is_refused(protein_small):
     from pygcmc_b200._native import GcmcError, default_options
     from pygcmc_b200.engine import Engine
